@@ -1,0 +1,106 @@
+"""ctypes binding of libsv_b200.so (declared in include/sv_b200.h).
+
+There is no fallback: if the library is missing or cannot be loaded the
+import of any calling module raises, and every entry point turns a nonzero
+status into an exception (ValueError for argument and data errors, as the
+reference raises; RuntimeError for CUDA failures).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsv_b200.so")
+
+SV_OK, SV_ERR_SHAPE, SV_ERR_PARAM, SV_ERR_DISP, SV_ERR_WORKSPACE, SV_ERR_CUDA, \
+    SV_ERR_NULL, SV_ERR_NET = range(8)
+SV_U8, SV_F32, SV_F64 = 0, 1, 2
+SV_FP32, SV_BF16 = 0, 1
+
+
+class RefineParams(ctypes.Structure):
+    """sv_refine_params (refine_fullres keyword arguments)."""
+    _fields_ = [("R", ctypes.c_int), ("P1", ctypes.c_double), ("P2", ctypes.c_double),
+                ("rx", ctypes.c_int), ("ry", ctypes.c_int), ("paths", ctypes.c_int),
+                ("uniq", ctypes.c_double), ("ad_weight", ctypes.c_double),
+                ("ad_trunc", ctypes.c_double), ("prior_w", ctypes.c_double),
+                ("prior_t", ctypes.c_double)]
+
+
+# name -> (restype, argtypes)
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+_SZ = ctypes.c_size_t
+_PRM = ctypes.POINTER(RefineParams)
+_IP = ctypes.POINTER(ctypes.c_int)
+
+SIGNATURES = {
+    "sv_status_string": (ctypes.c_char_p, [_I]),
+    "sv_last_error": (ctypes.c_char_p, []),
+    "sv_version": (_I, []),
+    "sv_refine_params_default": (None, [_PRM]),
+    "sv_workspace_status": (_I, [_VP, _VP]),
+    "sv_census": (_I, [_VP, _I, _I, _I, _I, _I, _VP, _VP]),
+    "sv_band_costs": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _VP, _VP]),
+    "sv_aggregate_path": (_I, [_VP, _VP, _I, _I, _I, _I, _I, _I, _I, _VP, _VP]),
+    "sv_left_to_right": (_I, [_VP, _I, _I, _VP, _VP]),
+    "sv_refine_workspace_size": (_SZ, [_I, _I, _PRM]),
+    "sv_refine_fullres": (_I, [_VP, _VP, _I, _VP, _I, _I, _PRM, _VP, _VP, _VP, _SZ, _VP]),
+    "sv_lr_refine_workspace_size": (_SZ, [_I, _I, _PRM]),
+    "sv_lr_refine": (_I, [_VP, _VP, _I, _VP, _I, _I, _D, _PRM, _VP, _VP, _VP, _SZ, _VP]),
+    "sv_net_create": (_I, [_VP, _I, _VP, ctypes.c_long, ctypes.POINTER(_VP)]),
+    "sv_net_destroy": (None, [_VP]),
+    "sv_resize": (_I, [_VP, _I, _I, _I, _I, _VP, _VP]),
+    "sv_forward_workspace_size": (_SZ, [_VP, _I, _I]),
+    "sv_stereonet_forward": (_I, [_VP, _VP, _VP, _I, _I, _VP, _VP, _VP, _VP, _VP, _I, _VP,
+                                  _SZ, _VP]),
+    "sv_predict_workspace_size": (_SZ, [_VP, _I, _I, _I]),
+    "sv_predict_auto": (_I, [_VP, _VP, _VP, _I, _I, _I, _D, _I, _I, _I, _I, _VP, _VP, _IP,
+                             _IP, _IP, _VP, _SZ, _VP]),
+    "sv_predict_at_scale": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _I, _VP, _VP, _IP, _IP,
+                                 _VP, _SZ, _VP]),
+}
+
+_lib = None
+
+
+def load():
+    """Load the library once; raise if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "libsv_b200.so is not built (%s); run __graft_entry__.build() or "
+            "python from-scratch-stereo-vision_b200/build.py" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols():
+    return sorted(SIGNATURES)
+
+
+def check(rc: int, what: str) -> None:
+    if rc == SV_OK:
+        return
+    lib = load()
+    detail = lib.sv_last_error().decode(errors="replace")
+    msg = "%s: %s (%s)" % (what, lib.sv_status_string(rc).decode(), detail)
+    if rc == SV_ERR_CUDA:
+        raise RuntimeError(msg)
+    raise ValueError(msg)
+
+
+def default_params() -> RefineParams:
+    p = RefineParams()
+    load().sv_refine_params_default(ctypes.byref(p))
+    return p

@@ -1,0 +1,163 @@
+/*
+ * sv_b200.h -- C ABI of the B200 (sm_100a) disparity hot path.
+ *
+ * Each entry point replaces one function of the reference's stereonet.py
+ * (Ray-5106/From-Scratch-Stereo-Vision); the comment above it names the
+ * reference lines.  Conventions:
+ *
+ *  - All image-sized buffers are row-major [H][W], device pointers owned by
+ *    the caller.  "K" is the band width 2R+1; band arrays are [H][W][K].
+ *  - Work is enqueued on `stream` (a cudaStream_t, 0 = legacy default).
+ *    Nothing synchronises unless the comment says so.
+ *  - Scratch memory comes from a caller-owned workspace whose size the
+ *    matching *_workspace_size() call returns (256-byte aligned pointer).
+ *    The library itself allocates device memory only for network weights
+ *    (sv_net_create).
+ *  - Every call returns an SV_* status.  Argument errors are detected before
+ *    anything is enqueued.  Errors that depend on data (a NaN disparity) are
+ *    recorded in the workspace by the kernels and returned by
+ *    sv_workspace_status(), which synchronises the stream.
+ *  - Reentrant: no global mutable state; sv_last_error() is thread-local.
+ */
+#ifndef SV_B200_H
+#define SV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum sv_status {
+    SV_OK = 0,
+    SV_ERR_SHAPE = 1,     /* W, H, R or census window outside the supported range   */
+    SV_ERR_PARAM = 2,     /* a parameter the exact integer path cannot honour        */
+    SV_ERR_DISP = 3,      /* a disparity is NaN, infinite or |d| >= 2^30             */
+    SV_ERR_WORKSPACE = 4, /* workspace NULL, misaligned or smaller than required     */
+    SV_ERR_CUDA = 5,      /* a CUDA runtime call failed (detail in sv_last_error)    */
+    SV_ERR_NULL = 6,      /* a required pointer is NULL                               */
+    SV_ERR_NET = 7        /* weights do not match the architecture                    */
+};
+
+enum sv_dtype { SV_U8 = 0, SV_F32 = 1, SV_F64 = 2 };
+
+/* Network arithmetic (sv_stereonet_forward and the predict_* calls). */
+enum sv_precision { SV_FP32 = 0, SV_BF16 = 1 };
+
+const char *sv_status_string(int status);
+const char *sv_last_error(void);
+int sv_version(void);
+
+/* Refinement parameters, the keyword arguments of refine_fullres
+ * (stereonet.py:5244-5246).  The exact integer path requires ad_weight == 0,
+ * prior_w == 0 and integer-valued 0 <= P1, P2 <= 4096 (every value the
+ * reference's pipeline uses: refine_disparity passes P1=12, P2=150). */
+typedef struct sv_refine_params {
+    int R;            /* band half-width, K = 2R+1, 0 <= R <= 126           */
+    double P1, P2;    /* SGM penalties                                      */
+    int rx, ry;       /* census window half-sizes, (2rx+1)(2ry+1)-1 <= 64   */
+    int paths;        /* 8 or 4                                             */
+    double uniq;      /* uniqueness threshold (0 disables)                  */
+    double ad_weight; /* must be 0                                          */
+    double ad_trunc;
+    double prior_w;   /* must be 0                                          */
+    double prior_t;
+} sv_refine_params;
+
+/* refine_fullres's own defaults (R=3, P1=1, P2=12, rx=ry=2, 8 paths). */
+void sv_refine_params_default(sv_refine_params *p);
+
+/* Returns the first data-dependent error the kernels recorded in this
+ * workspace since the last sv_* call that used it (synchronises stream). */
+int sv_workspace_status(const void *workspace, void *stream);
+
+/* census, stereonet.py:5115-5142.  img is [H][W] of `dtype` (gray values,
+ * compared exactly as stored).  out[p] has bit (nbits-1-i) set when the i-th
+ * window offset (dy-major, dx-minor, centre skipped) is darker than the
+ * centre; borders clamp to the edge.  Bit-identical to the reference. */
+int sv_census(const void *img, int dtype, int W, int H, int rx, int ry,
+              uint64_t *out, void *stream);
+
+/* band_costs, stereonet.py:5156-5189, for ad_weight = 0 and no prior term:
+ * C[p][k] = popcount(cl[p] ^ cr[p - (base[p]-R+k)]), or `invalid` (0..255;
+ * refine_fullres passes nbits+4) where that column is outside the image or
+ * the candidate is negative.  base is int32 [H][W]. */
+int sv_band_costs(const uint64_t *cl, const uint64_t *cr, const int32_t *base,
+                  int W, int H, int R, int invalid, uint8_t *C, void *stream);
+
+/* _aggregate_path, stereonet.py:5192-5241: S += L for direction (dx, dy)
+ * with integer penalties.  C is uint8 [H][W][K], S uint16 [H][W][K]. */
+int sv_aggregate_path(const uint8_t *C, const int32_t *base, int W, int H, int K,
+                      int P1, int P2, int dx, int dy, uint16_t *S, void *stream);
+
+/* left_to_right, stereonet.py:5317-5340 (FP64, bit-identical). */
+int sv_left_to_right(const double *dl, int W, int H, double *dr, void *stream);
+
+/* refine_fullres, stereonet.py:5244-5305 (one view, bit-identical output).
+ * left/right are [H][W] of `dtype`; disp0 and out are FP64 [H][W];
+ * conf (optional, may be NULL) receives the return_conf values. */
+size_t sv_refine_workspace_size(int W, int H, const sv_refine_params *p);
+int sv_refine_fullres(const void *left, const void *right, int dtype,
+                      const double *disp0, int W, int H,
+                      const sv_refine_params *p, double *out, double *conf,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+/* lr_refine, stereonet.py:5343-5391: both views, left-right check and the
+ * occlusion / mismatch fills.  status: 0 ok, 1 occluded, 2 mismatch. */
+size_t sv_lr_refine_workspace_size(int W, int H, const sv_refine_params *p);
+int sv_lr_refine(const void *left, const void *right, int dtype,
+                 const double *disp0, int W, int H, double tol,
+                 const sv_refine_params *p, double *out, uint8_t *status,
+                 void *workspace, size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------ network */
+typedef struct sv_net sv_net;
+
+/* Uploads a StereoNet checkpoint.  arch = {feat_C, cost_C, D, refine_C,
+ * ndil, dil[0..ndil-1]} (the header fields of save_weights,
+ * stereonet.py:1774-1779); params = all blocks concatenated in
+ * StereoNet.all_params() order (stereonet.py:1193-1195), FP64.
+ * Allocates device memory for the weights (freed by sv_net_destroy). */
+int sv_net_create(const int *arch, int n_arch, const double *params,
+                  long n_params, sv_net **out);
+void sv_net_destroy(sv_net *net);
+
+/* resize_gray / BilinearUpsample.forward, stereonet.py:3843-3845, 913-956:
+ * half-pixel bilinear resample computed in FP64. */
+int sv_resize(const double *img, int W, int H, int W2, int H2, double *out,
+              void *stream);
+
+/* StereoNet.forward, stereonet.py:1203-1233 (note the reference's H, W order).
+ * left/right/guide_full are FP32 [H][W], guide_half FP32 [H/2][W/2];
+ * d0 [h][w], d1 [H/2][W/2], d2 [H][W] FP32. */
+size_t sv_forward_workspace_size(const sv_net *net, int H, int W);
+int sv_stereonet_forward(const sv_net *net, const float *left, const float *right,
+                         int H, int W, const float *guide_half,
+                         const float *guide_full, float *d0, float *d1, float *d2,
+                         int precision, void *workspace, size_t workspace_bytes,
+                         void *stream);
+
+/* predict_auto, stereonet.py:3872-3929 (with predict_at_scale 3932-3960 and
+ * predict 5891-5897).  left/right are the full-resolution gray images of
+ * `dtype`.  disp_full: FP64 [H][W]; disp_work: FP64, at least W*H elements.
+ * The work-width choice needs the peak of each pass on the host, so this
+ * call synchronises the stream once per pass.  *work_trace (optional, at
+ * least passes+1 ints) receives the work widths tried, 0-terminated. */
+size_t sv_predict_workspace_size(const sv_net *net, int W, int H, int max_width);
+int sv_predict_auto(const sv_net *net, const void *left, const void *right,
+                    int dtype, int W, int H, double target_peak, int probe_width,
+                    int max_width, int passes, int precision, double *disp_full,
+                    double *disp_work, int *Ww, int *Hw, int *work_trace,
+                    void *workspace, size_t workspace_bytes, void *stream);
+
+/* predict_at_scale, stereonet.py:3932-3960. */
+int sv_predict_at_scale(const sv_net *net, const void *left, const void *right,
+                        int dtype, int W, int H, int work_width, int precision,
+                        double *disp_full, double *disp_work, int *Ww, int *Hw,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SV_B200_H */

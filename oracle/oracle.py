@@ -1,0 +1,228 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes wrapper over the FP64 C oracle.
+
+``sv_oracle.c`` restates the reference's disparity hot path (stereonet.py) in
+plain C with the reference's own operation order; the golden fixtures in
+tests/golden/ (made by running the reference itself) pin it bit-for-bit.
+Only tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+import this module.  Function names and argument meanings follow the
+reference (flat row-major FP64 arrays, ``W, H`` order except
+``stereonet_forward`` which keeps the reference's ``H, W``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "libsv_oracle.so")
+_lib = None
+
+_d = ctypes.POINTER(ctypes.c_double)
+_u64 = ctypes.POINTER(ctypes.c_uint64)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+_i32 = ctypes.POINTER(ctypes.c_int32)
+_int = ctypes.c_int
+_dbl = ctypes.c_double
+
+
+def build() -> str:
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+    return _SO
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(
+                os.path.join(_HERE, "sv_oracle.c")):
+            build()
+        L = ctypes.CDLL(_SO)
+        L.orc_fexp.restype = _dbl
+        L.orc_fexp.argtypes = [_dbl]
+        L.orc_peak.restype = _dbl
+        L.orc_peak.argtypes = [_d, ctypes.c_long, _dbl]
+        L.orc_param_count.restype = ctypes.c_long
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel())
+
+
+def _p(a, t=_d):
+    return a.ctypes.data_as(t)
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise ValueError("oracle %s failed with code %d" % (what, rc))
+
+
+# ---------------------------------------------------------------- refinement
+def census(img, W, H, rx=2, ry=2) -> np.ndarray:
+    img = _f64(img)
+    out = np.zeros(W * H, dtype=np.uint64)
+    _check(lib().orc_census(_p(img), W, H, rx, ry, _p(out, _u64)), "census")
+    return out
+
+
+def band_costs(cl, cr, gl, gr, base, W, H, R, ad_weight, ad_trunc, invalid,
+               prior=None, prior_w=0.0, prior_t=4.0) -> np.ndarray:
+    K = 2 * R + 1
+    cl = np.ascontiguousarray(cl, dtype=np.uint64)
+    cr = np.ascontiguousarray(cr, dtype=np.uint64)
+    gl, gr = _f64(gl), _f64(gr)
+    base = np.ascontiguousarray(base, dtype=np.int64)
+    pr = _f64(prior) if prior is not None else np.zeros(W * H)
+    C = np.zeros(W * H * K)
+    lib().orc_band_costs(_p(cl, _u64), _p(cr, _u64), _p(gl), _p(gr), _p(base, _i64),
+                         W, H, R, _dbl(ad_weight), _dbl(ad_trunc), _dbl(invalid),
+                         _p(pr), _dbl(prior_w), _dbl(prior_t), _p(C))
+    return C
+
+
+def aggregate_path(C, base, W, H, K, P1, P2, dx, dy, S: np.ndarray) -> None:
+    """Adds one path into ``S`` (a float64 array, modified in place)."""
+    C = _f64(C)
+    base = np.ascontiguousarray(base, dtype=np.int64)
+    assert S.dtype == np.float64 and S.flags.c_contiguous
+    lib().orc_aggregate_path(_p(C), _p(base, _i64), W, H, K, _dbl(P1), _dbl(P2),
+                             dx, dy, _p(S))
+
+
+def refine_fullres(left, right, disp0, W, H, R=3, P1=1.0, P2=12.0,
+                   ad_weight=0.0, ad_trunc=20.0, paths=8, uniq=0.0,
+                   rx=2, ry=2, prior_w=0.0, prior_t=4.0, return_conf=False):
+    left, right, disp0 = _f64(left), _f64(right), _f64(disp0)
+    out = np.zeros(W * H)
+    conf = np.zeros(W * H)
+    _check(lib().orc_refine_fullres(_p(left), _p(right), _p(disp0), W, H, R,
+                                    _dbl(P1), _dbl(P2), _dbl(ad_weight), _dbl(ad_trunc),
+                                    paths, _dbl(uniq), rx, ry, _dbl(prior_w),
+                                    _dbl(prior_t), _p(out), _p(conf)), "refine_fullres")
+    return (out, conf) if return_conf else out
+
+
+def left_to_right(dl, W, H) -> np.ndarray:
+    dl = _f64(dl)
+    dr = np.zeros(W * H)
+    _check(lib().orc_left_to_right(_p(dl), W, H, _p(dr)), "left_to_right")
+    return dr
+
+
+def lr_refine(left, right, disp0, W, H, tol=1.0, R=3, P1=1.0, P2=12.0,
+              ad_weight=0.0, ad_trunc=20.0, paths=8, uniq=0.0, rx=2, ry=2,
+              prior_w=0.0, prior_t=4.0):
+    left, right, disp0 = _f64(left), _f64(right), _f64(disp0)
+    out = np.zeros(W * H)
+    st = np.zeros(W * H, dtype=np.int32)
+    _check(lib().orc_lr_refine(_p(left), _p(right), _p(disp0), W, H, _dbl(tol), R,
+                               _dbl(P1), _dbl(P2), _dbl(ad_weight), _dbl(ad_trunc),
+                               paths, _dbl(uniq), rx, ry, _dbl(prior_w), _dbl(prior_t),
+                               _p(out), _p(st, _i32)), "lr_refine")
+    return out, st
+
+
+def refine_pipeline(left, right, disp0, W, H, R=10, P1=12.0, P2=150.0, rx=4, ry=3,
+                    tol=2.0):
+    """``lr_refine`` with ``refine_disparity``'s defaults (stereonet.py:5865-5872)."""
+    return lr_refine(left, right, disp0, W, H, tol=tol, R=R, P1=P1, P2=P2, rx=rx, ry=ry)
+
+
+# ------------------------------------------------------------------- network
+def fexp(x: float) -> float:
+    return float(lib().orc_fexp(_dbl(x)))
+
+
+def resize_gray(img, W, H, W2, H2) -> np.ndarray:
+    img = _f64(img)
+    out = np.zeros(W2 * H2)
+    lib().orc_resize(_p(img), W, H, W2, H2, _p(out))
+    return out
+
+
+def avgpool2(img, C, H, W):
+    img = _f64(img)
+    out = np.zeros(C * (H // 2) * (W // 2))
+    lib().orc_avgpool2(_p(img), C, H, W, _p(out))
+    return out, H // 2, W // 2
+
+
+def peak(disp, q=0.95) -> float:
+    d = _f64(disp)
+    return float(lib().orc_peak(_p(d), len(d), _dbl(q)))
+
+
+def _net_args(net):
+    arch = np.array(net.arch.vector(), dtype=np.int32)
+    params = net.flat
+    return arch, params
+
+
+def stereonet_forward(net, left, right, H, W, guide_half, guide_full):
+    arch, params = _net_args(net)
+    left, right = _f64(left), _f64(right)
+    gh, gf = _f64(guide_half), _f64(guide_full)
+    h = (((H - 1) // 2 + 1) - 1) // 2 + 1
+    w = (((W - 1) // 2 + 1) - 1) // 2 + 1
+    d0 = np.zeros(h * w)
+    d1 = np.zeros((H // 2) * (W // 2))
+    d2 = np.zeros(H * W)
+    oh, ow = _int(), _int()
+    _check(lib().orc_stereonet_forward(_p(arch, _i32), _p(params), _p(left), _p(right),
+                                       H, W, _p(gh), _p(gf), _p(d0), _p(d1), _p(d2),
+                                       ctypes.byref(oh), ctypes.byref(ow)), "forward")
+    return d0, d1, d2
+
+
+def predict(net, left, right, W, H) -> np.ndarray:
+    arch, params = _net_args(net)
+    left, right = _f64(left), _f64(right)
+    out = np.zeros(W * H)
+    _check(lib().orc_predict(_p(arch, _i32), _p(params), _p(left), _p(right), W, H,
+                             _p(out)), "predict")
+    return out
+
+
+def predict_at_scale(net, left, right, W, H, work_width=96):
+    arch, params = _net_args(net)
+    left, right = _f64(left), _f64(right)
+    df = np.zeros(W * H)
+    dw = np.zeros(W * H)
+    Ww, Hw = _int(), _int()
+    _check(lib().orc_predict_at_scale(_p(arch, _i32), _p(params), _p(left), _p(right),
+                                      W, H, work_width, _p(df), _p(dw), ctypes.byref(Ww),
+                                      ctypes.byref(Hw)), "predict_at_scale")
+    return df, dw[:Ww.value * Hw.value].copy(), Ww.value, Hw.value
+
+
+def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64,
+                 max_width=320, passes=3, return_trace=False):
+    arch, params = _net_args(net)
+    left, right = _f64(left), _f64(right)
+    tp = float(net.target_peak if target_peak is None else target_peak)
+    df = np.zeros(W * H)
+    dw = np.zeros(W * H)
+    Ww, Hw = _int(), _int()
+    trace = np.zeros(passes + 2, dtype=np.int32)
+    _check(lib().orc_predict_auto(_p(arch, _i32), _p(params), _p(left), _p(right), W, H,
+                                  _dbl(tp), probe_width, max_width, passes, _p(df), _p(dw),
+                                  ctypes.byref(Ww), ctypes.byref(Hw), _p(trace, _i32)),
+           "predict_auto")
+    res = (df, dw[:Ww.value * Hw.value].copy(), Ww.value, Hw.value)
+    if return_trace:
+        return res, [int(t) for t in trace if t > 0]
+    return res

@@ -1,0 +1,203 @@
+"""Generate the golden fixtures by running the reference itself.
+
+Run in a container that has the reference checkout (read-only is fine):
+
+    python tests/golden/make_golden.py /root/reference
+
+It executes ``stereonet.py`` into a namespace exactly the way the reference's
+own test suite does (test_stereonet.py:18-22: strip the ``run_demo()`` guard,
+``exec`` into a dict), feeds it seeded synthetic pairs from this package's
+generator, and stores the reference's outputs.  Small outputs are stored as
+arrays; large ones (the 450x375 workload) as SHA-256 digests of their FP64
+bytes.  The fixtures are what pins the C oracle: tests/test_oracle_golden.py
+checks the oracle against every one of them.  Nothing on the GPU box reads the
+reference; it only reads these files.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "from-scratch-stereo-vision_b200"))
+import synth  # noqa: E402
+
+
+def load_reference(ref_dir):
+    src = open(os.path.join(ref_dir, "stereonet.py")).read().replace(
+        "if __name__ == '__main__':\n    run_demo()\n", "")
+    SN = {"__name__": "stereonet_golden"}
+    exec(src, SN)
+    return SN
+
+
+def sha(a, dtype=np.float64) -> str:
+    return hashlib.sha256(np.ascontiguousarray(np.asarray(a, dtype=dtype)).tobytes()).hexdigest()
+
+
+def as_int_array(vals, dtype):
+    a = np.asarray(vals, dtype=np.float64)
+    assert np.all(a == np.round(a)), "expected integer-valued output"
+    return a.astype(dtype)
+
+
+def tricky_disp0(pair, rng, noise=3.0):
+    """Ground truth + noise, plus the values that exercise the rounding and
+    tie rules: negative zeros, exact halves, values in (-1, 0), block jumps
+    larger than a band, and ties that land on the same right-image column."""
+    W, H = pair.W, pair.H
+    d = pair.disp.ravel() + rng.uniform(-noise, noise, W * H)
+    idx = rng.choice(W * H, size=W * H // 40, replace=False)
+    d[idx[0::5]] = -0.0
+    d[idx[1::5]] = np.floor(d[idx[1::5]]) + 0.5
+    d[idx[2::5]] = -rng.uniform(0.0, 1.0, len(idx[2::5]))
+    d[idx[3::5]] = np.floor(d[idx[3::5]]) - 0.5
+    d[idx[4::5]] = 0.0
+    # a block far off the truth: band re-centring jumps larger than K
+    y0, x0 = H // 3, W // 3
+    blk = d.reshape(H, W)
+    blk[y0:y0 + H // 4, x0:x0 + W // 4] += 25.0
+    # ties on one row: equal disparities that warp to the same column
+    r = H // 2
+    for x in range(4, min(W, 12)):
+        blk[r, x] = float(x - 3)          # x - d + 0.5 = 3.5 -> column 3 for all
+    return blk.ravel().copy()
+
+
+def main(ref_dir):
+    t0 = time.time()
+    SN = load_reference(ref_dir)
+    net = SN["load_model"](os.path.join(ref_dir, "stereonet_weights.txt"))
+    flat = [v for p, _ in net.all_params() for v in p]
+    meta = {"weights_sha256": sha(flat), "n_params": len(flat),
+            "target_peak": net.target_peak}
+    print("reference loaded: %d params (%.1fs)" % (len(flat), time.time() - t0))
+
+    # ------------------------------------------------------------ primitives
+    rng = np.random.default_rng(7)
+    fx = np.array([-701.0, -50.3, -3.7, -0.5, -1e-9, 0.0, 1e-9, 0.25, 0.6931471805599453,
+                   1.0, 3.3, 20.0, 88.5, 699.9, 701.0])
+    fexp = np.array([SN["fexp"](float(v)) for v in fx])
+    img = rng.random(13 * 9)
+    rs = {}
+    for (W2, H2) in ((13, 9), (7, 5), (29, 17), (20, 9), (13, 30)):
+        rs["resize_%dx%d" % (W2, H2)] = np.array(SN["resize_gray"](list(img), 13, 9, W2, H2))
+    ap, _, _ = SN["avgpool2"](list(img), 1, 9, 13)
+    pk_in = rng.uniform(-1, 30, 1001)
+    pk_in[::7] = -0.0
+    pk = SN["_peak"](list(pk_in))
+    np.savez_compressed(os.path.join(HERE, "primitives.npz"), fexp_x=fx, fexp=fexp,
+                        img=img, avgpool=np.array(ap), peak_in=pk_in, peak=np.array([pk]),
+                        **rs)
+    print("primitives done (%.1fs)" % (time.time() - t0))
+
+    # ------------------------------------------------------ refinement, small
+    pair = synth.make_pair(11, 64, 48, 2.0, 20.0, n_planes=(2, 4))
+    W, H = pair.W, pair.H
+    L = list(pair.gray("left").ravel())
+    R = list(pair.gray("right").ravel())
+    d0 = tricky_disp0(pair, np.random.default_rng(12))
+    d0l = [float(v) for v in d0]
+    out = {"left": pair.left, "right": pair.right, "disp0": d0}
+    cl = SN["census"](L, W, H, 4, 3)
+    cr = SN["census"](R, W, H, 4, 3)
+    out["census_l_4x3"] = np.array(cl, dtype=np.uint64)
+    out["census_r_4x3"] = np.array(cr, dtype=np.uint64)
+    out["census_l_2x2"] = np.array(SN["census"](L, W, H, 2, 2), dtype=np.uint64)
+    out["census_r_1x1"] = np.array(SN["census"](R, W, H, 1, 1), dtype=np.uint64)
+    Rb = 10
+    base = [max(0, int(v + 0.5)) for v in d0l]
+    out["base"] = np.array(base, dtype=np.int64)
+    C = SN["band_costs"](cl, cr, L, R, base, W, H, Rb, 0.0, 20.0, 66.0, d0l, 0.0, 4.0)
+    out["costs_R10"] = as_int_array(C, np.uint8)
+    K = 2 * Rb + 1
+    dirs = [(1, 0), (-1, 0), (0, 1), (0, -1), (1, 1), (-1, 1), (1, -1), (-1, -1)]
+    for i, (dx, dy) in enumerate(dirs):
+        S1 = [0.0] * (W * H * K)
+        SN["_aggregate_path"](C, base, W, H, K, 12.0, 150.0, dx, dy, S1)
+        out["path%d_R10" % i] = as_int_array(S1, np.uint8)
+    S = [0.0] * (W * H * K)
+    for dx, dy in dirs:
+        SN["_aggregate_path"](C, base, W, H, K, 12.0, 150.0, dx, dy, S)
+    out["S_R10"] = as_int_array(S, np.uint16)
+    o, conf = SN["refine_fullres"](L, R, d0l, W, H, R=10, P1=12.0, P2=150.0, rx=4, ry=3,
+                                  return_conf=True)
+    out["refine_R10"] = np.array(o)
+    out["conf_R10"] = np.array(conf)
+    out["refine_default"] = np.array(SN["refine_fullres"](L, R, d0l, W, H))
+    out["refine_R4_paths4"] = np.array(SN["refine_fullres"](L, R, d0l, W, H, R=4, P1=12.0,
+                                                            P2=150.0, paths=4, rx=4, ry=3))
+    out["refine_uniq"] = np.array(SN["refine_fullres"](L, R, d0l, W, H, R=6, P1=8.0,
+                                                       P2=96.0, rx=3, ry=3, uniq=0.15))
+    out["l2r"] = np.array(SN["left_to_right"](d0l, W, H))
+    lo, st = SN["lr_refine"](L, R, d0l, W, H, tol=2.0, R=10, P1=12.0, P2=150.0, rx=4, ry=3)
+    out["lr_out"] = np.array(lo)
+    out["lr_status"] = np.array(st, dtype=np.int8)
+    lo1, st1 = SN["lr_refine"](L, R, d0l, W, H)
+    out["lr_default_out"] = np.array(lo1)
+    out["lr_default_status"] = np.array(st1, dtype=np.int8)
+    # full-range mode (eval_real.py:143-146): disp0 == R everywhere
+    Rf = int(np.max(pair.disp) + 2) // 2 + 1
+    out["fullrange_R"] = np.array([Rf])
+    out["fullrange"] = np.array(SN["refine_fullres"](L, R, [float(Rf)] * (W * H), W, H, R=Rf,
+                                                     P1=12.0, P2=150.0, rx=4, ry=3))
+    np.savez_compressed(os.path.join(HERE, "refine_small.npz"), **out)
+    print("refine_small done (%.1fs)" % (time.time() - t0))
+
+    # --------------------------------------------------------- network, small
+    npair = synth.make_pair(21, 64, 48, 2.0, 24.0, n_planes=(2, 3))
+    Wn, Hn = npair.W, npair.H
+    Ln = list(npair.gray("left").ravel())
+    Rn = list(npair.gray("right").ravel())
+    gh, _, _ = SN["avgpool2"](Ln, 1, Hn, Wn)
+    f0, f1, f2 = net.forward(Ln, Rn, Hn, Wn, gh, Ln)
+    ps = SN["predict_at_scale"](net, Ln, Rn, Wn, Hn, 48, False)
+    np.savez_compressed(os.path.join(HERE, "network_small.npz"), left=npair.left,
+                        right=npair.right, d0=np.array(f0), d1=np.array(f1), d2=np.array(f2),
+                        pas_full=np.array(ps[0]), pas_work=np.array(ps[1]),
+                        pas_dims=np.array([ps[2], ps[3]]))
+    print("network_small done (%.1fs)" % (time.time() - t0))
+
+    # ------------------------------------ the 160x120 workload, end to end
+    p1 = synth.config_small()
+    L1 = list(p1.gray("left").ravel())
+    R1 = list(p1.gray("right").ravel())
+    df, dw, Ww, Hw = SN["predict_auto"](net, L1, R1, p1.W, p1.H, verbose=False)
+    ro, rst = SN["lr_refine"](L1, R1, df, p1.W, p1.H, tol=2.0, R=10, P1=12.0, P2=150.0,
+                              rx=4, ry=3)
+    np.savez_compressed(os.path.join(HERE, "config_small.npz"), left=p1.left, right=p1.right,
+                        disp0=np.array(df), disp_work=np.array(dw), dims=np.array([Ww, Hw]),
+                        out=np.array(ro), status=np.array(rst, dtype=np.int8))
+    print("config_small done: work %dx%d (%.1fs)" % (Ww, Hw, time.time() - t0))
+
+    # ------------------------------------ the 450x375 workload, as digests
+    p2 = synth.config_full()
+    L2 = list(p2.gray("left").ravel())
+    R2 = list(p2.gray("right").ravel())
+    df2, dw2, Ww2, Hw2 = SN["predict_auto"](net, L2, R2, p2.W, p2.H, verbose=False)
+    ro2, rst2 = SN["lr_refine"](L2, R2, df2, p2.W, p2.H, tol=2.0, R=10, P1=12.0, P2=150.0,
+                                rx=4, ry=3)
+    meta["config_full"] = {
+        "W": p2.W, "H": p2.H, "images_sha256": sha(np.concatenate([p2.left.ravel(),
+                                                                   p2.right.ravel()]),
+                                                   np.uint8),
+        "work": [Ww2, Hw2], "disp0_sha256": sha(df2), "disp_work_sha256": sha(dw2),
+        "out_sha256": sha(ro2), "status_sha256": sha(rst2, np.int8),
+        "status_counts": [int(np.sum(np.array(rst2) == s)) for s in (0, 1, 2)],
+        "disp0_mean": float(np.mean(df2)), "out_mean": float(np.mean(ro2)),
+    }
+    print("config_full done: work %dx%d (%.1fs)" % (Ww2, Hw2, time.time() - t0))
+    with open(os.path.join(HERE, "golden_meta.json"), "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("all fixtures written (%.1fs)" % (time.time() - t0))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,351 @@
+"""Benchmark of the disparity hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload full|small]
+
+One step = the whole path on one rectified pair: predict_auto (probe + up to
+three StereoNet passes, FP32) followed by lr_refine with refine_disparity's
+parameters (R=10, 9x7 census, P1=12, P2=150, tol=2; both views, bit-exact).
+Default workload: the 450x375 uint8 pair (8-15 slanted planes, disparities
+0-80 px, ~10% occluded, ~20% low texture).  Metric: refined Mpix/s, i.e.
+W*H of every pair processed / device time.  Multi-GPU runs are replicas (the
+path shards by pairs, no collective): every rank refines its own pair, the
+step time is the max over ranks, value = ranks x W*H x K / that time.
+
+``value`` times the device path with the images already in HBM (L2 flushed
+by a 256 MB write before every step, outside the timed events); ``e2e`` times
+the same step through the public pipeline from pinned host buffers (H2D of
+both images and D2H of the refined disparity + status inside the events).
+``roofline`` is the SGM aggregation kernel (the dominant kernel): algorithmic
+bytes 48*K per pixel per view (uint16 C read + S read + S write per path, 8
+paths) x 2 views x W*H over its CUDA-event duration, against the measured HBM
+copy bandwidth.  ``cpu_baseline`` times the FP64 C port of the reference
+(oracle/) on the host cores over a bounded sample.
+
+``--impl reference`` times that CPU port alone (rank 0; other ranks exit).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "refined Mpix/s per B200 (bit-exact)"
+UNIT = "Mpix/s"
+PARAMS = dict(R=10, P1=12.0, P2=150.0, rx=4, ry=3)
+TOL = 2.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="full", choices=["full", "small"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="bound on the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def make_pair(pkg, workload):
+    if workload == "small":
+        return pkg.synth.config_small(), "160x120 u8 pair, 3-6 slanted planes, 2-30 px"
+    return (pkg.synth.config_full(),
+            "450x375 u8 pair, 8-15 slanted planes, 0-80 px, ~10% occluded, ~20% low texture")
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", str(rank)))
+    return rank, world, local
+
+
+# ------------------------------------------------------------------ CPU
+def cpu_port_run(pair, net, seconds, threads):
+    """Time the FP64 C port (oracle/) of predict_auto + lr_refine on the host
+    cores: whole pairs until `seconds` have passed (at least one)."""
+    import __graft_entry__
+    orc = __graft_entry__.load_oracle()
+    orc.set_threads(threads)
+    L, R = pair.gray("left").ravel(), pair.gray("right").ravel()
+    n, t0 = 0, time.perf_counter()
+    while True:
+        df, _, _, _ = orc.predict_auto(net, L, R, pair.W, pair.H)
+        orc.lr_refine(L, R, df, pair.W, pair.H, tol=TOL, **PARAMS)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return n, el
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [s.strip() for s in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def hbm_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def sgm_traffic(K, N):
+    """DRAM bytes per SGM launch from the committed ncu summary, scaled to
+    this launch's pixel count (traffic grows with the pixels swept)."""
+    p = os.path.join(REPO, "profiles", "ncu_sgm.md")
+    if not os.path.exists(p):
+        return None
+    per_px = None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_view_pixel:"):
+            per_px = float(line.split(":")[1])
+    return None if per_px is None else per_px * 2 * N
+
+
+# ------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local):
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    lib = pkg._lib.load()
+    net = pkg.weights.load_model()
+    pair, desc = make_pair(pkg, args.workload)
+    W, H, N = pair.W, pair.H, pair.W * pair.H
+    K = 2 * PARAMS["R"] + 1
+    pipe = pkg.pipeline.PairPipeline(W, H, net, **PARAMS, tol=TOL)
+    hl = torch.from_numpy(pair.left.ravel()).pin_memory()
+    hr = torch.from_numpy(pair.right.ravel()).pin_memory()
+    pipe.left.copy_(hl)
+    pipe.right.copy_(hr)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stages = pipe.refiner.STAGES
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(len(stages) + 1)]
+          for _ in range(args.steps)]
+    t0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+
+    def step(i=None):
+        pipe.predict()
+        if i is None:
+            pipe.refine()
+        else:
+            pipe.refiner.run_timed(pipe.left, pipe.right, pipe.disp0, pipe.out, pipe.status, ev[i])
+
+    for _ in range(args.warmup):
+        step()
+    pipe.refiner.data_status()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.sv_launch_count()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            t0[i].record()
+            step(i)
+            t1[i].record()
+        torch.cuda.synchronize()
+    launches = lib.sv_launch_count() - launches0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = sum(t0[i].elapsed_time(t1[i]) for i in range(args.steps))
+    stage_ms = [sum(ev[i][s].elapsed_time(ev[i][s + 1]) for i in range(args.steps)) / args.steps
+                for s in range(len(stages))]
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * N * args.steps / (ms / 1e3) / 1e6
+
+    # ---- end to end through the public pipeline from pinned host buffers
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for _ in range(2):
+        pipe.run_host(hl, hr)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.zero_()
+        e0[i].record()
+        pipe.run_host(hl, hr)
+        e1[i].record()
+    torch.cuda.synchronize()
+    ems = sum(e0[i].elapsed_time(e1[i]) for i in range(args.steps))
+    if dist:
+        t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ems = float(t.item())
+    evalue = world * N * args.steps / (ems / 1e3) / 1e6
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        sgm_ms = stage_ms[stages.index("sgm")]
+        alg = 48 * K * N * 2                      # both views in one launch
+        achieved = alg / (sgm_ms / 1e3) / 1e9
+        traffic = sgm_traffic(K, N)
+        cpu = None
+        if world == 1:
+            threads = os.cpu_count() or 1
+            n, el = cpu_port_run(pair, net, args.cpu_seconds, threads)
+            cpu = {"value": round(n * N / el / 1e6, 6), "unit": UNIT, "cores": threads,
+                   "kind": "port",
+                   "sample": "%d whole pairs (%s) through the FP64 C port of predict_auto + "
+                             "lr_refine, %.1f s, OpenMP over %d threads" % (n, desc, el, threads)}
+        result = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "u8/u64/int32 integer refinement, f64 subpixel+LR, f32 network",
+            "data": "synthetic (seeded generator; reference weights stereonet_weights.txt)",
+            "config": {"workload": "%s: predict_auto + lr_refine (R=10, 9x7 census, P1=12, "
+                                   "P2=150, tol=2)" % desc,
+                       "pairs_per_step_per_gpu": 1, "work_size": list(pipe.work_size),
+                       "work_trace": pipe.work_trace,
+                       "l2": "flushed before every step (256 MB write, untimed)",
+                       "parallelism": "replicas x%d" % world},
+            "stages_ms": {"predict_auto": round(ms / args.steps - sum(stage_ms), 4),
+                          **{s: round(v, 4) for s, v in zip(stages, stage_ms)}},
+            "roofline": {"kernel": "k_sgm (8 paths x 2 views)", "bound": "hbm",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4),
+                         "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind
+                         if peak_kind == "measured" else "fallback",
+                         "algorithmic_bytes_per_launch": alg,
+                         "traffic": traffic},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(evalue, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": pipe.h2d_bytes(),
+                    "d2h_bytes_per_step": pipe.d2h_bytes()},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+# --------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    net = pkg.weights.load_model()
+    pair, desc = make_pair(pkg, args.workload)
+    N = pair.W * pair.H
+    threads = os.cpu_count() or 1
+    budget = max(1.0, args.cpu_seconds / max(1, args.steps + args.warmup))
+    for _ in range(min(args.warmup, 1)):
+        cpu_port_run(pair, net, 0.0, threads)
+    n_tot, t_tot = 0, 0.0
+    for _ in range(args.steps):
+        n, el = cpu_port_run(pair, net, budget, threads)
+        n_tot += n
+        t_tot += el
+    value = n_tot * N / t_tot / 1e6
+    sample = ("%d whole pairs (%s) through the FP64 C port of the reference's predict_auto + "
+              "lr_refine (bit-identical to stereonet.py on the golden fixtures), OpenMP over "
+              "%d threads" % (n_tot, desc, threads))
+    return {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * t_tot / n_tot, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "%s: predict_auto + lr_refine (R=10, 9x7 census, P1=12, "
+                                   "P2=150, tol=2)" % desc, "pairs_per_step": 1},
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+    else:
+        res = run_ours(args, rank, world, local)
+    if res is not None and rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -3,6 +3,7 @@
 // Argument checks happen before anything is enqueued; data-dependent errors
 // (a NaN disparity) are flagged by the kernels in the workspace header.
 
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -14,6 +15,9 @@
 namespace sv {
 
 static thread_local char g_err[512];
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const char *fmt, ...) {
     va_list ap;
@@ -143,6 +147,8 @@ const char *sv_last_error(void) { return g_err; }
 
 int sv_version(void) { return 1; }
 
+unsigned long long sv_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
 void sv_refine_params_default(sv_refine_params *p) {
     if (!p) return;
     p->R = 3;
@@ -256,9 +262,10 @@ int sv_refine_fullres(const void *left, const void *right, int dtype, const doub
     return SV_OK;
 }
 
-int sv_lr_refine(const void *left, const void *right, int dtype, const double *disp0, int W,
-                 int H, double tol, const sv_refine_params *p, double *out, uint8_t *status,
-                 void *workspace, size_t workspace_bytes, void *stream) {
+static int lr_refine_impl(const void *left, const void *right, int dtype, const double *disp0,
+                          int W, int H, double tol, const sv_refine_params *p, double *out,
+                          uint8_t *status, void *workspace, size_t workspace_bytes,
+                          void *stream, void *const *events, int n_events) {
     if (!left || !right || !disp0 || !out || !status) {
         set_error("NULL argument");
         return SV_ERR_NULL;
@@ -266,23 +273,55 @@ int sv_lr_refine(const void *left, const void *right, int dtype, const double *d
     RefineCfg c;
     SV_TRY(check_refine(W, H, p, true, &c));
     if (!std::isfinite(tol)) { set_error("tol must be finite"); return SV_ERR_PARAM; }
+    if (events && n_events < SV_LR_STAGES + 1) {
+        set_error("stage timing needs %d events", SV_LR_STAGES + 1);
+        return SV_ERR_PARAM;
+    }
     SV_TRY(check_ws(workspace, workspace_bytes, carve_refine(nullptr, W, H, c, 2, nullptr)));
     RefineWs w;
     carve_refine(workspace, W, H, c, 2, &w);
     cudaStream_t st = (cudaStream_t)stream;
     const long N = (long)W * H;
+    int ev = 0;
+    auto mark = [&]() -> int {
+        if (events) SV_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[ev++], st));
+        return SV_OK;
+    };
+    SV_TRY(mark());
     SV_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(DevFlags), st));
     SV_TRY(launch_base(disp0, N, w.base0, &w.flags->status, st));
     SV_TRY(launch_left_to_right(disp0, W, H, w.d0r, w.base1, st));
+    SV_TRY(mark());
     SV_TRY(launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st));
+    SV_TRY(mark());
     SV_TRY(launch_band_costs(w.cen0, w.cen1, w.base0, w.base1, W, H, c.R, c.invalid, w.C0,
                              w.C1, 2, st));
+    SV_TRY(mark());
     SV_TRY(launch_sgm(w.C0, w.C1, w.base0, w.base1, W, H, c.K, c.P1, c.P2, w.L, c.l16, 2,
                       c.npaths, st));
+    SV_TRY(mark());
     SV_TRY(launch_wta(w.L, c.l16, c.npaths, 2, W, H, c.R, w.base0, w.base1, disp0, w.d0r,
                       c.uniq, w.dl, w.dr, nullptr, st));
+    SV_TRY(mark());
     SV_TRY(launch_lr_check(w.dl, w.dr, disp0, W, H, tol, out, status, st));
+    SV_TRY(mark());
     return SV_OK;
+}
+
+int sv_lr_refine(const void *left, const void *right, int dtype, const double *disp0, int W,
+                 int H, double tol, const sv_refine_params *p, double *out, uint8_t *status,
+                 void *workspace, size_t workspace_bytes, void *stream) {
+    return lr_refine_impl(left, right, dtype, disp0, W, H, tol, p, out, status, workspace,
+                          workspace_bytes, stream, nullptr, 0);
+}
+
+int sv_lr_refine_timed(const void *left, const void *right, int dtype, const double *disp0,
+                       int W, int H, double tol, const sv_refine_params *p, double *out,
+                       uint8_t *status, void *workspace, size_t workspace_bytes, void *stream,
+                       void *const *events, int n_events) {
+    if (!events) { set_error("events is NULL"); return SV_ERR_NULL; }
+    return lr_refine_impl(left, right, dtype, disp0, W, H, tol, p, out, status, workspace,
+                          workspace_bytes, stream, events, n_events);
 }
 
 }  // extern "C"

@@ -20,6 +20,10 @@ constexpr int kMaxPenalty = 4096;    // P1, P2 bound: 8 paths x (68 + P2) stays 
 // Thread-local error detail for sv_last_error().
 void set_error(const char *fmt, ...);
 
+// Process-wide count of kernels this library has launched (sv_launch_count);
+// a relaxed atomic increment per launch, read only for reporting.
+void count_launch();
+
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Bump allocator over a caller workspace.  With base == nullptr it only

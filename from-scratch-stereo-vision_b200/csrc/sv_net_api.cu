@@ -1,0 +1,382 @@
+// sv_net_api.cu -- extern "C" network entry points of include/sv_b200.h:
+// checkpoint upload, StereoNet.forward, resize, predict_at_scale and the
+// host-side control flow of predict_auto (stereonet.py:3872-3960).
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "sv_common.cuh"
+#include "sv_network.cuh"
+
+struct sv_net {
+    sv::NetView view;
+    float *dev = nullptr;     // all FP32 parameters, one allocation
+    int arch[16];
+    int n_arch;
+};
+
+namespace sv {
+
+static long param_count(const int *a) {
+    long C = a[0], Cm = a[1], Rc = a[3], nd = a[4];
+    long n = C * 9 + C + 3 * (C * C * 9 + C);
+    n += Cm * C * 27 + Cm + Cm * Cm * 27 + Cm + Cm * 27 + 1;
+    long lv = 0, prev = 2;
+    for (int i = 0; i < nd; ++i) { lv += Rc * prev * 9 + Rc; prev = Rc; }
+    lv += prev * 9 + 1;
+    return n + 2 * lv;
+}
+
+static void bind_view(sv_net *net) {
+    NetView &v = net->view;
+    const int *a = net->arch;
+    v.C = a[0]; v.Cm = a[1]; v.D = a[2]; v.Rc = a[3]; v.ndil = a[4];
+    for (int i = 0; i < v.ndil; ++i) v.dil[i] = a[5 + i];
+    const float *p = net->dev;
+    const int C = v.C, Cm = v.Cm, Rc = v.Rc;
+    const int fic[4] = {1, C, C, C};
+    for (int i = 0; i < 4; ++i) {
+        v.fw[i] = p; p += C * fic[i] * 9;
+        v.fb[i] = p; p += C;
+    }
+    const int cic[3] = {C, Cm, Cm}, coc[3] = {Cm, Cm, 1};
+    for (int i = 0; i < 3; ++i) {
+        v.cw[i] = p; p += coc[i] * cic[i] * 27;
+        v.cb[i] = p; p += coc[i];
+    }
+    for (int lv = 0; lv < 2; ++lv) {
+        int prev = 2;
+        for (int i = 0; i < v.ndil; ++i) {
+            v.rw[lv][i] = p; p += Rc * prev * 9;
+            v.rb[lv][i] = p; p += Rc;
+            prev = Rc;
+        }
+        v.rw[lv][v.ndil] = p; p += prev * 9;
+        v.rb[lv][v.ndil] = p; p += 1;
+    }
+}
+
+static void conv_out(int H, int W, int *h1, int *w1, int *h, int *w) {
+    *h1 = (H - 1) / 2 + 1;
+    *w1 = (W - 1) / 2 + 1;
+    *h = (*h1 - 1) / 2 + 1;
+    *w = (*w1 - 1) / 2 + 1;
+}
+
+// Forward scratch for an (H, W) input (sizes are monotone in H and W).
+static size_t carve_fwd(Carver &cv, const NetView &n, int H, int W, FwdBufs *b) {
+    int h1, w1, h, w;
+    conv_out(H, W, &h1, &w1, &h, &w);
+    const size_t f1 = (size_t)n.C * h1 * w1, f2 = (size_t)n.C * h * w;
+    const size_t vol = (size_t)n.Cm * n.D * h * w, HW = (size_t)H * W;
+    size_t start = cv.off;
+    FwdBufs t{};
+    t.fa[0] = cv.take<float>(f1);
+    t.fa[1] = cv.take<float>(f1);
+    t.fb[0] = cv.take<float>(f2);
+    t.fb[1] = cv.take<float>(f2);
+    t.v0 = cv.take<float>(vol);
+    t.v1 = cv.take<float>(vol);
+    t.rin = cv.take<float>(2 * HW);
+    t.ra = cv.take<float>((size_t)n.Rc * HW);
+    t.rb = cv.take<float>((size_t)n.Rc * HW);
+    if (b) *b = t;
+    return cv.off - start;
+}
+
+static int check_net_shape(const NetView &n, int H, int W) {
+    if (H < 2 || W < 2) {
+        set_error("network input %dx%d too small", W, H);
+        return SV_ERR_SHAPE;
+    }
+    int h1, w1, h, w;
+    conv_out(H, W, &h1, &w1, &h, &w);
+    // CostVolume.invalid_mask (stereonet.py:837-839) indexes past its list,
+    // and the reference raises IndexError, when the quarter width <= D-2.
+    if (w <= n.D - 2) {
+        set_error("quarter-resolution width %d <= D-2 = %d (the reference raises IndexError)",
+                  w, n.D - 2);
+        return SV_ERR_SHAPE;
+    }
+    return SV_OK;
+}
+
+static int width_for(int W, double target_peak, int max_width, double pk) {
+    double m = pk > 1.0e-6 ? pk : 1.0e-6;
+    int w = (int)(W * target_peak / m + 0.5);
+    if (w > W) w = W;
+    if (w > max_width) w = max_width;
+    if (w < 48) w = 48;
+    return w;
+}
+
+// Workspace of predict_auto / predict_at_scale for a W x H pair.
+struct PredictWs {
+    float *lw, *rw, *gh, *d0, *d1, *d2;
+    double *probe64;
+    SelState *sel;
+    unsigned *hist;
+    FwdBufs fwd;
+};
+
+static void predict_dims(int W, int H, int max_width, int probe_width, int *Wm, int *Hm) {
+    const int cap = max_width > 48 ? max_width : 48;   // width_for's range
+    int ww = W <= cap ? W : cap;
+    int pw = probe_width < W ? probe_width : W;
+    int ph = (int)(H * pw / (double)W + 0.5);
+    if (ph < 8) ph = 8;
+    *Wm = ww > pw ? ww : pw;
+    int hm = H > 8 ? H : 8;
+    *Hm = hm > ph ? hm : ph;
+}
+
+static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictWs *o) {
+    Carver cv(ws);
+    PredictWs p{};
+    cv.take<DevFlags>(1);
+    const size_t HW = (size_t)Wm * Hm;
+    int h1, w1, h, w;
+    conv_out(Hm, Wm, &h1, &w1, &h, &w);
+    p.lw = cv.take<float>(HW);
+    p.rw = cv.take<float>(HW);
+    p.gh = cv.take<float>(HW / 4 + 1);
+    p.d0 = cv.take<float>((size_t)h * w);
+    p.d1 = cv.take<float>(HW / 4 + 1);
+    p.d2 = cv.take<float>(HW);
+    p.probe64 = cv.take<double>(HW);
+    p.sel = reinterpret_cast<SelState *>(cv.take<unsigned char>(select_state_bytes()));
+    p.hist = cv.take<unsigned>(2048);
+    carve_fwd(cv, n, Hm, Wm, &p.fwd);
+    if (o) *o = p;
+    return cv.off;
+}
+
+static int read_peak(const PredictWs &w, const double *x, long n, cudaStream_t st,
+                     double *peak) {
+    long long rank = (long long)(n * 0.95);      // int(len(s) * q)
+    int rc = launch_select(x, n, rank, w.sel, w.hist, st);
+    if (rc) return rc;
+    double v = 0.0;
+    SV_CUDA_TRY(cudaMemcpyAsync(&v, reinterpret_cast<const char *>(w.sel) + select_value_offset(),
+                                sizeof(double), cudaMemcpyDeviceToHost, st));
+    SV_CUDA_TRY(cudaStreamSynchronize(st));
+    *peak = v > 0.5 ? v : 0.5;
+    return SV_OK;
+}
+
+// predict (stereonet.py:5891-5897) on FP32 images already in lw/rw.
+static int predict_f32(const sv_net *net, const PredictWs &w, int W, int H, cudaStream_t st) {
+    int rc = check_net_shape(net->view, H, W);
+    if (rc) return rc;
+    rc = launch_avgpool2(w.lw, H, W, w.gh, st);
+    if (rc) return rc;
+    return launch_forward(net->view, w.lw, w.rw, H, W, w.gh, w.lw, w.d0, w.d1, w.d2, w.fwd, st);
+}
+
+static int predict_at_scale_impl(const sv_net *net, const PredictWs &w, const void *left,
+                                 const void *right, int dtype, int W, int H, int work,
+                                 double *disp_full, double *disp_work, int *pWw, int *pHw,
+                                 cudaStream_t st) {
+    int rc;
+    if (work >= W) {
+        rc = launch_to_f32_pair(left, right, dtype, (long)W * H, w.lw, w.rw, st);
+        if (!rc) rc = predict_f32(net, w, W, H, st);
+        if (!rc) rc = launch_promote(w.d2, (long)W * H, disp_full, st);
+        if (rc) return rc;
+        SV_CUDA_TRY(cudaMemcpyAsync(disp_work, disp_full, sizeof(double) * W * H,
+                                    cudaMemcpyDeviceToDevice, st));
+        *pWw = W;
+        *pHw = H;
+        return SV_OK;
+    }
+    const double scale = work / (double)W;
+    const int Ww = work;
+    int Hw = (int)(H * scale + 0.5);
+    if (Hw < 8) Hw = 8;
+    rc = launch_resize_pair(left, right, dtype, W, H, Ww, Hw, w.lw, w.rw, st);
+    if (!rc) rc = predict_f32(net, w, Ww, Hw, st);
+    if (!rc) rc = launch_promote(w.d2, (long)Ww * Hw, disp_work, st);
+    if (!rc) rc = launch_upscale_disp(w.d2, Ww, Hw, W, H, 1.0 / scale, disp_full, st);
+    *pWw = Ww;
+    *pHw = Hw;
+    return rc;
+}
+
+#define SV_TRY(expr)                  \
+    do {                              \
+        int rc_ = (expr);             \
+        if (rc_ != SV_OK) return rc_; \
+    } while (0)
+
+}  // namespace sv
+
+using namespace sv;
+
+extern "C" {
+
+int sv_net_create(const int *arch, int n_arch, const double *params, long n_params,
+                  sv_net **out) {
+    if (!arch || !params || !out) { set_error("NULL argument"); return SV_ERR_NULL; }
+    if (n_arch < 6 || n_arch > 13 || arch[4] < 1 || arch[4] > 8 || n_arch != 5 + arch[4]) {
+        set_error("arch vector must be {feat_C, cost_C, D, refine_C, ndil, dil...}");
+        return SV_ERR_NET;
+    }
+    long need = param_count(arch);
+    if (need != n_params) {
+        set_error("checkpoint has %ld parameters, the architecture needs %ld", n_params, need);
+        return SV_ERR_NET;
+    }
+    sv_net *net = new sv_net();
+    memcpy(net->arch, arch, sizeof(int) * n_arch);
+    net->n_arch = n_arch;
+    std::vector<float> f(n_params);
+    for (long i = 0; i < n_params; ++i) f[i] = (float)params[i];
+    cudaError_t e = cudaMalloc(&net->dev, sizeof(float) * n_params);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(net->dev, f.data(), sizeof(float) * n_params, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        set_error("weight upload failed: %s", cudaGetErrorString(e));
+        if (net->dev) cudaFree(net->dev);
+        delete net;
+        return SV_ERR_CUDA;
+    }
+    bind_view(net);
+    *out = net;
+    return SV_OK;
+}
+
+void sv_net_destroy(sv_net *net) {
+    if (!net) return;
+    if (net->dev) cudaFree(net->dev);
+    delete net;
+}
+
+int sv_resize(const double *img, int W, int H, int W2, int H2, double *out, void *stream) {
+    if (!img || !out) { set_error("NULL argument"); return SV_ERR_NULL; }
+    if (W < 1 || H < 1 || W2 < 1 || H2 < 1) { set_error("bad shape"); return SV_ERR_SHAPE; }
+    return launch_resize_f64(img, W, H, W2, H2, out, (cudaStream_t)stream);
+}
+
+int sv_avgpool2(const double *img, int C, int H, int W, double *out, void *stream) {
+    if (!img || !out) { set_error("NULL argument"); return SV_ERR_NULL; }
+    if (C < 1 || H < 1 || W < 1) { set_error("bad shape"); return SV_ERR_SHAPE; }
+    return launch_avgpool2_f64(img, C, H, W, out, (cudaStream_t)stream);
+}
+
+size_t sv_forward_workspace_size(const sv_net *net, int H, int W) {
+    if (!net || H < 1 || W < 1) return 0;
+    Carver cv(nullptr);
+    cv.take<DevFlags>(1);
+    carve_fwd(cv, net->view, H, W, nullptr);
+    return cv.off;
+}
+
+int sv_stereonet_forward(const sv_net *net, const float *left, const float *right, int H,
+                         int W, const float *guide_half, const float *guide_full, float *d0,
+                         float *d1, float *d2, int precision, void *workspace,
+                         size_t workspace_bytes, void *stream) {
+    if (!net || !left || !right || !guide_half || !guide_full || !d0 || !d1 || !d2) {
+        set_error("NULL argument");
+        return SV_ERR_NULL;
+    }
+    if (precision != SV_FP32) { set_error("precision %d not available", precision); return SV_ERR_PARAM; }
+    SV_TRY(check_net_shape(net->view, H, W));
+    size_t need = sv_forward_workspace_size(net, H, W);
+    if (!workspace || ((uintptr_t)workspace & 255) || workspace_bytes < need) {
+        set_error("workspace needs %zu bytes, 256-aligned", need);
+        return SV_ERR_WORKSPACE;
+    }
+    Carver cv(workspace);
+    cv.take<DevFlags>(1);
+    FwdBufs b;
+    carve_fwd(cv, net->view, H, W, &b);
+    return launch_forward(net->view, left, right, H, W, guide_half, guide_full, d0, d1, d2, b,
+                          (cudaStream_t)stream);
+}
+
+size_t sv_predict_workspace_size(const sv_net *net, int W, int H, int max_width) {
+    if (!net || W < 1 || H < 1) return 0;
+    int Wm, Hm;
+    predict_dims(W, H, max_width, 64, &Wm, &Hm);
+    return carve_predict(nullptr, net->view, Wm, Hm, nullptr);
+}
+
+static int predict_ws(const sv_net *net, int W, int H, int max_width, int probe_width,
+                      void *ws, size_t bytes, PredictWs *w) {
+    int Wm, Hm;
+    predict_dims(W, H, max_width, probe_width, &Wm, &Hm);
+    size_t need = carve_predict(nullptr, net->view, Wm, Hm, nullptr);
+    if (!ws || ((uintptr_t)ws & 255) || bytes < need) {
+        set_error("workspace needs %zu bytes, 256-aligned (have %zu)", need, bytes);
+        return SV_ERR_WORKSPACE;
+    }
+    carve_predict(ws, net->view, Wm, Hm, w);
+    return SV_OK;
+}
+
+int sv_predict_at_scale(const sv_net *net, const void *left, const void *right, int dtype,
+                        int W, int H, int work_width, int precision, double *disp_full,
+                        double *disp_work, int *Ww, int *Hw, void *workspace,
+                        size_t workspace_bytes, void *stream) {
+    if (!net || !left || !right || !disp_full || !disp_work || !Ww || !Hw) {
+        set_error("NULL argument");
+        return SV_ERR_NULL;
+    }
+    if (precision != SV_FP32) { set_error("precision %d not available", precision); return SV_ERR_PARAM; }
+    if (W < 1 || H < 1 || work_width < 1) { set_error("bad shape"); return SV_ERR_SHAPE; }
+    PredictWs w;
+    int mw = work_width > 48 ? work_width : 48;
+    SV_TRY(predict_ws(net, W, H, mw, 64, workspace, workspace_bytes, &w));
+    return predict_at_scale_impl(net, w, left, right, dtype, W, H, work_width, disp_full,
+                                 disp_work, Ww, Hw, (cudaStream_t)stream);
+}
+
+int sv_predict_auto(const sv_net *net, const void *left, const void *right, int dtype, int W,
+                    int H, double target_peak, int probe_width, int max_width, int passes,
+                    int precision, double *disp_full, double *disp_work, int *pWw, int *pHw,
+                    int *work_trace, void *workspace, size_t workspace_bytes, void *stream) {
+    if (!net || !left || !right || !disp_full || !disp_work || !pWw || !pHw) {
+        set_error("NULL argument");
+        return SV_ERR_NULL;
+    }
+    if (precision != SV_FP32) { set_error("precision %d not available", precision); return SV_ERR_PARAM; }
+    if (W < 1 || H < 1 || probe_width < 1 || max_width < 1 || passes < 1 ||
+        !std::isfinite(target_peak)) {
+        set_error("bad arguments");
+        return SV_ERR_PARAM;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    PredictWs w;
+    SV_TRY(predict_ws(net, W, H, max_width, probe_width, workspace, workspace_bytes, &w));
+    // probe (stereonet.py:3900-3907)
+    const int pw = probe_width < W ? probe_width : W;
+    int ph = (int)(H * pw / (double)W + 0.5);
+    if (ph < 8) ph = 8;
+    SV_TRY(launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st));
+    SV_TRY(predict_f32(net, w, pw, ph, st));
+    SV_TRY(launch_promote(w.d2, (long)pw * ph, w.probe64, st));
+    double pk;
+    SV_TRY(read_peak(w, w.probe64, (long)pw * ph, st, &pk));
+    const double peak = pk * (W / (double)pw);
+    int work = width_for(W, target_peak, max_width, peak);
+    int nt = 0;
+    if (work_trace) work_trace[nt++] = work;
+    SV_TRY(predict_at_scale_impl(net, w, left, right, dtype, W, H, work, disp_full, disp_work,
+                                 pWw, pHw, st));
+    for (int it = 0; it < passes - 1; ++it) {
+        double np_;
+        SV_TRY(read_peak(w, disp_full, (long)W * H, st, &np_));
+        int nw = width_for(W, target_peak, max_width, np_);
+        if (std::abs(nw - work) <= 0.08 * work) break;
+        work = nw;
+        if (work_trace) work_trace[nt++] = work;
+        SV_TRY(predict_at_scale_impl(net, w, left, right, dtype, W, H, work, disp_full,
+                                     disp_work, pWw, pHw, st));
+    }
+    if (work_trace) work_trace[nt] = 0;
+    return SV_OK;
+}
+
+}  // extern "C"

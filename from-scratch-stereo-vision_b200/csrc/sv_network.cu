@@ -1,0 +1,657 @@
+// sv_network.cu -- StereoNet forward (stereonet.py:998-1233) and the
+// resolution-selection helpers of predict_auto (3832-3961), FP32 path.
+//
+// Layouts are the reference's planar ones: feature maps [C][h][w], the cost
+// volume and its filtered versions [C][D][h][w].  Convolutions are direct
+// (one thread per output pixel computing every output channel, weights in
+// shared memory, read by broadcast) with bias and activation fused:
+//   * both siamese towers run in one launch (blockIdx.z picks the image);
+//   * the cost volume is never stored: the first 3-D convolution computes
+//     |fl - fr(x-d)| (or INVALID_COST 2.0) for each tap it reads;
+//   * the last 3-D convolution, the invalid-disparity penalty and the
+//     soft-argmin are one kernel, one thread per (y, x) over all D;
+//   * each refinement level's bilinear x2 upsample writes the 2-channel
+//     [disp*2, guide] input of its first convolution; the last convolution
+//     adds the residual and applies relu (v > 0 ? v : v*0).
+// Resampling positions follow BilinearUpsample (half-pixel centres, int()
+// truncation) computed in FP64; image and disparity resizes blend in FP64.
+
+#include <cmath>
+
+#include "sv_common.cuh"
+#include "sv_network.cuh"
+
+namespace sv {
+
+// ---------------------------------------------------------------- resample
+struct Taps {
+    int i00, i01, i10, i11;
+    double w00, w01, w10, w11;
+};
+
+// BilinearUpsample.forward tap computation, stereonet.py:921-949.
+__device__ __forceinline__ Taps bilinear_taps(int oy, int ox, int H, int W, int H2,
+                                              int W2) {
+    double sy = __ddiv_rn((double)H, (double)H2);
+    double sx = __ddiv_rn((double)W, (double)W2);
+    double fy = __dsub_rn(__dmul_rn(__dadd_rn((double)oy, 0.5), sy), 0.5);
+    if (fy < 0.0) fy = 0.0;
+    int y0 = (int)fy;
+    if (y0 > H - 1) y0 = H - 1;
+    int y1 = y0 + 1 < H ? y0 + 1 : y0;
+    double wy = __dsub_rn(fy, (double)y0);
+    double fx = __dsub_rn(__dmul_rn(__dadd_rn((double)ox, 0.5), sx), 0.5);
+    if (fx < 0.0) fx = 0.0;
+    int x0 = (int)fx;
+    if (x0 > W - 1) x0 = W - 1;
+    int x1 = x0 + 1 < W ? x0 + 1 : x0;
+    double wx = __dsub_rn(fx, (double)x0);
+    Taps t;
+    t.w00 = __dmul_rn(__dsub_rn(1.0, wy), __dsub_rn(1.0, wx));
+    t.w01 = __dmul_rn(__dsub_rn(1.0, wy), wx);
+    t.w10 = __dmul_rn(wy, __dsub_rn(1.0, wx));
+    t.w11 = __dmul_rn(wy, wx);
+    t.i00 = y0 * W + x0;
+    t.i01 = y0 * W + x1;
+    t.i10 = y1 * W + x0;
+    t.i11 = y1 * W + x1;
+    return t;
+}
+
+template <typename T>
+__device__ __forceinline__ double gray_at(const T *img, int i);
+template <>
+__device__ __forceinline__ double gray_at<uint8_t>(const uint8_t *img, int i) {
+    return __ddiv_rn((double)img[i], 255.0);
+}
+template <>
+__device__ __forceinline__ double gray_at<float>(const float *img, int i) {
+    return (double)img[i];
+}
+template <>
+__device__ __forceinline__ double gray_at<double>(const double *img, int i) {
+    return img[i];
+}
+
+// FP64 blend in the reference's order: ((a*w00 + b*w01) + c*w10) + d*w11.
+template <typename T>
+__device__ __forceinline__ double blend64(const T *x, const Taps &t) {
+    double a = __dmul_rn(gray_at<T>(x, t.i00), t.w00);
+    a = __dadd_rn(a, __dmul_rn(gray_at<T>(x, t.i01), t.w01));
+    a = __dadd_rn(a, __dmul_rn(gray_at<T>(x, t.i10), t.w10));
+    return __dadd_rn(a, __dmul_rn(gray_at<T>(x, t.i11), t.w11));
+}
+
+// resize_gray of a left/right pair (blockIdx.z) from full resolution to the
+// work resolution, FP64 blend, FP32 output for the network.  Also writes
+// avgpool2 of the left result when guide_half != nullptr is requested by a
+// second launch (k_avgpool2).
+template <typename T>
+__global__ void k_resize_pair(const T *__restrict__ l, const T *__restrict__ r, int W, int H,
+                              int W2, int H2, float *__restrict__ lo, float *__restrict__ ro) {
+    const T *src = blockIdx.z ? r : l;
+    float *dst = blockIdx.z ? ro : lo;
+    int ox = blockIdx.x * blockDim.x + threadIdx.x;
+    int oy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ox >= W2 || oy >= H2) return;
+    Taps t = bilinear_taps(oy, ox, H, W, H2, W2);
+    dst[oy * W2 + ox] = (float)blend64<T>(src, t);
+}
+
+// Copy (no resample) of a pair into FP32, for predict at native resolution.
+template <typename T>
+__global__ void k_to_f32_pair(const T *__restrict__ l, const T *__restrict__ r, long n,
+                              float *__restrict__ lo, float *__restrict__ ro) {
+    const T *src = blockIdx.y ? r : l;
+    float *dst = blockIdx.y ? ro : lo;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+        dst[i] = (float)gray_at<T>(src, (int)i);
+}
+
+// resize of an FP64 map (sv_resize) and of the FP32 network disparity back
+// to full resolution, scaled by inv (predict_at_scale, stereonet.py:3957-3959).
+template <typename T>
+__global__ void k_resize_scale(const T *__restrict__ x, int W, int H, int W2, int H2,
+                               double inv, int scale, double *__restrict__ out) {
+    int ox = blockIdx.x * blockDim.x + threadIdx.x;
+    int oy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ox >= W2 || oy >= H2) return;
+    Taps t = bilinear_taps(oy, ox, H, W, H2, W2);
+    double v = blend64<T>(x, t);
+    out[(long)oy * W2 + ox] = scale ? __dmul_rn(v, inv) : v;
+}
+
+template <typename T>
+__global__ void k_promote(const T *__restrict__ x, long n, double *__restrict__ out) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+        out[i] = (double)x[i];
+}
+
+// avgpool2, stereonet.py:979-995: 0.25 * (((a + b) + c) + d).
+__global__ void k_avgpool2(const float *__restrict__ img, int H, int W,
+                           float *__restrict__ out) {
+    int H2 = H / 2, W2 = W / 2;
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W2 || y >= H2) return;
+    const float *r0 = img + (2 * y) * W + 2 * x;
+    const float *r1 = r0 + W;
+    out[y * W2 + x] = 0.25f * (((r0[0] + r0[1]) + r1[0]) + r1[1]);
+}
+
+// avgpool2 in FP64 over C planes (the drop-in for the reference function).
+__global__ void k_avgpool2_f64(const double *__restrict__ img, int C, int H, int W,
+                               double *__restrict__ out) {
+    const int H2 = H / 2, W2 = W / 2;
+    const long n = (long)C * H2 * W2;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i / ((long)H2 * W2));
+        const int rem = (int)(i - (long)c * H2 * W2);
+        const int y = rem / W2, x = rem - (rem / W2) * W2;
+        const double *r0 = img + (long)c * H * W + (long)(2 * y) * W + 2 * x;
+        const double *r1 = r0 + W;
+        out[i] = __dmul_rn(0.25, __dadd_rn(__dadd_rn(__dadd_rn(r0[0], r0[1]), r1[0]), r1[1]));
+    }
+}
+
+// ------------------------------------------------------------- conv 2d
+// act: 0 none, 1 leaky 0.2, 2 residual + relu0 (Refinement output).
+template <int IC, int OC, int ACT>
+__global__ void __launch_bounds__(256)
+    k_conv2d(const float *__restrict__ x0, const float *__restrict__ x1, int H, int W, int OH,
+             int OW, int stride, int pad, int dil, const float *__restrict__ w,
+             const float *__restrict__ b, float *__restrict__ y0, float *__restrict__ y1,
+             const float *__restrict__ resid) {
+    __shared__ float sw[OC * IC * 9];
+    __shared__ float sb[OC];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int i = tid; i < OC * IC * 9; i += blockDim.x * blockDim.y) sw[i] = w[i];
+    if (tid < OC) sb[tid] = b[tid];
+    __syncthreads();
+    const float *x = blockIdx.z ? x1 : x0;
+    float *y = blockIdx.z ? y1 : y0;
+    const int ox = blockIdx.x * blockDim.x + threadIdx.x;
+    const int oy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ox >= OW || oy >= OH) return;
+    float acc[OC];
+#pragma unroll
+    for (int o = 0; o < OC; ++o) acc[o] = sb[o];
+    const int iy0 = oy * stride - pad, ix0 = ox * stride - pad;
+    const long HW = (long)H * W;
+#pragma unroll
+    for (int c = 0; c < IC; ++c) {
+        const float *xc = x + c * HW;
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            const int iy = iy0 + ky * dil;
+            if (iy < 0 || iy >= H) continue;
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+                const int ix = ix0 + kx * dil;
+                if (ix < 0 || ix >= W) continue;
+                const float v = __ldg(xc + (long)iy * W + ix);
+#pragma unroll
+                for (int o = 0; o < OC; ++o)
+                    acc[o] = fmaf(v, sw[(o * IC + c) * 9 + ky * 3 + kx], acc[o]);
+            }
+        }
+    }
+    const long OHW = (long)OH * OW, oi = (long)oy * OW + ox;
+#pragma unroll
+    for (int o = 0; o < OC; ++o) {
+        float v = acc[o];
+        if (ACT == 1) v = v > 0.f ? v : v * 0.2f;
+        if (ACT == 2) {
+            v = resid[oi] + v;
+            v = v > 0.f ? v : v * 0.f;
+        }
+        y[o * OHW + oi] = v;
+    }
+}
+
+// -------------------------------------------------- cost volume + conv3d #1
+// CostVolume.forward (stereonet.py:771-799) fused into Conv3d #1 (596-641)
+// and its leaky ReLU: each tap of the 3x3x3 window reads |fl - fr(x-d)|
+// (2.0 where x-d < 0), zero outside the volume (same padding).
+template <int C, int OC>
+__global__ void __launch_bounds__(128)
+    k_costvol_conv3d(const float *__restrict__ fl, const float *__restrict__ fr, int D, int h,
+                     int w, const float *__restrict__ wt, const float *__restrict__ b,
+                     float *__restrict__ y) {
+    __shared__ float sw[OC * C * 27];
+    __shared__ float sb[OC];
+    for (int i = threadIdx.x; i < OC * C * 27; i += blockDim.x) sw[i] = wt[i];
+    if (threadIdx.x < OC) sb[threadIdx.x] = b[threadIdx.x];
+    __syncthreads();
+    const long hw = (long)h * w;
+    const long total = (long)D * hw;
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int od = (int)(idx / hw);
+    const int rem = (int)(idx - od * hw);
+    const int oy = rem / w, ox = rem - (rem / w) * w;
+    float acc[OC];
+#pragma unroll
+    for (int o = 0; o < OC; ++o) acc[o] = sb[o];
+    for (int c = 0; c < C; ++c) {
+        const float *flc = fl + c * hw, *frc = fr + c * hw;
+#pragma unroll
+        for (int kd = 0; kd < 3; ++kd) {
+            const int dd = od + kd - 1;
+            if (dd < 0 || dd >= D) continue;
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                const int yy = oy + ky - 1;
+                if (yy < 0 || yy >= h) continue;
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) {
+                    const int xx = ox + kx - 1;
+                    if (xx < 0 || xx >= w) continue;
+                    float v;
+                    if (xx - dd < 0) {
+                        v = 2.0f;
+                    } else {
+                        v = fabsf(__ldg(flc + yy * w + xx) - __ldg(frc + yy * w + xx - dd));
+                    }
+#pragma unroll
+                    for (int o = 0; o < OC; ++o)
+                        acc[o] = fmaf(v, sw[(o * C + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 0; o < OC; ++o) {
+        float v = acc[o];
+        y[o * total + idx] = v > 0.f ? v : v * 0.2f;
+    }
+}
+
+// ---------------------------------------------------------- conv3d #2
+template <int IC, int OC>
+__global__ void __launch_bounds__(128)
+    k_conv3d(const float *__restrict__ x, int D, int h, int w, const float *__restrict__ wt,
+             const float *__restrict__ b, float *__restrict__ y) {
+    __shared__ float sw[OC * IC * 27];
+    __shared__ float sb[OC];
+    for (int i = threadIdx.x; i < OC * IC * 27; i += blockDim.x) sw[i] = wt[i];
+    if (threadIdx.x < OC) sb[threadIdx.x] = b[threadIdx.x];
+    __syncthreads();
+    const long hw = (long)h * w;
+    const long total = (long)D * hw;
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int od = (int)(idx / hw);
+    const int rem = (int)(idx - od * hw);
+    const int oy = rem / w, ox = rem - (rem / w) * w;
+    float acc[OC];
+#pragma unroll
+    for (int o = 0; o < OC; ++o) acc[o] = sb[o];
+    for (int c = 0; c < IC; ++c) {
+        const float *xc = x + c * total;
+#pragma unroll
+        for (int kd = 0; kd < 3; ++kd) {
+            const int dd = od + kd - 1;
+            if (dd < 0 || dd >= D) continue;
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                const int yy = oy + ky - 1;
+                if (yy < 0 || yy >= h) continue;
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) {
+                    const int xx = ox + kx - 1;
+                    if (xx < 0 || xx >= w) continue;
+                    const float v = __ldg(xc + dd * hw + yy * w + xx);
+#pragma unroll
+                    for (int o = 0; o < OC; ++o)
+                        acc[o] = fmaf(v, sw[(o * IC + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 0; o < OC; ++o) {
+        float v = acc[o];
+        y[o * total + idx] = v > 0.f ? v : v * 0.2f;
+    }
+}
+
+// ----------------------------------- conv3d #3 + invalid mask + soft-argmin
+// Conv3d #3 (Cm -> 1), CostVolume.invalid_mask (+8 where x < d, d >= 1,
+// stereonet.py:827-840) and SoftArgmin.forward (858-885) in FP32 with
+// max-subtraction: disp = sum_d d * exp(-c_d - max(-c)) / sum_d exp(...).
+template <int IC, int DMAX>
+__global__ void __launch_bounds__(128)
+    k_conv3d_softargmin(const float *__restrict__ x, int D, int h, int w,
+                        const float *__restrict__ wt, const float *__restrict__ b,
+                        float *__restrict__ disp) {
+    __shared__ float sw[IC * 27];
+    for (int i = threadIdx.x; i < IC * 27; i += blockDim.x) sw[i] = wt[i];
+    __syncthreads();
+    const long hw = (long)h * w;
+    const long total = (long)D * hw;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= hw) return;
+    const int oy = idx / w, ox = idx - (idx / w) * w;
+    float cost[DMAX];
+    const float bias = __ldg(b);
+#pragma unroll
+    for (int od = 0; od < DMAX; ++od) {
+        if (od >= D) break;
+        float acc = bias;
+        for (int c = 0; c < IC; ++c) {
+            const float *xc = x + c * total;
+#pragma unroll
+            for (int kd = 0; kd < 3; ++kd) {
+                const int dd = od + kd - 1;
+                if (dd < 0 || dd >= D) continue;
+#pragma unroll
+                for (int ky = 0; ky < 3; ++ky) {
+                    const int yy = oy + ky - 1;
+                    if (yy < 0 || yy >= h) continue;
+#pragma unroll
+                    for (int kx = 0; kx < 3; ++kx) {
+                        const int xx = ox + kx - 1;
+                        if (xx < 0 || xx >= w) continue;
+                        acc = fmaf(__ldg(xc + dd * hw + yy * w + xx),
+                                   sw[c * 27 + kd * 9 + ky * 3 + kx], acc);
+                    }
+                }
+            }
+        }
+        if (od >= 1 && ox < od) acc += 8.0f;
+        cost[od] = acc;
+    }
+    float best = -cost[0];
+#pragma unroll
+    for (int d = 1; d < DMAX; ++d)
+        if (d < D) best = fmaxf(best, -cost[d]);
+    float total_e = 0.f, acc = 0.f;
+#pragma unroll
+    for (int d = 0; d < DMAX; ++d) {
+        if (d < D) {
+            float e = expf(-cost[d] - best);
+            total_e += e;
+            acc = fmaf((float)d, e, acc);
+        }
+    }
+    disp[idx] = acc / total_e;
+}
+
+// ---------------------------------------------- refinement input: up x2
+// d_up = 2 * bilinear(d) at (H2, W2) into channel 0, guide into channel 1.
+__global__ void k_upsample_concat(const float *__restrict__ d, int h, int w, int H2, int W2,
+                                  const float *__restrict__ guide, float *__restrict__ out) {
+    int ox = blockIdx.x * blockDim.x + threadIdx.x;
+    int oy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ox >= W2 || oy >= H2) return;
+    Taps t = bilinear_taps(oy, ox, h, w, H2, W2);
+    float v = __ldg(d + t.i00) * (float)t.w00 + __ldg(d + t.i01) * (float)t.w01 +
+              __ldg(d + t.i10) * (float)t.w10 + __ldg(d + t.i11) * (float)t.w11;
+    long i = (long)oy * W2 + ox;
+    out[i] = v * 2.0f;
+    out[(long)H2 * W2 + i] = guide[i];
+}
+
+// ====================================================================
+// Host side
+// ====================================================================
+
+static dim3 grid2d(int W, int H, dim3 blk, int z = 1) {
+    return dim3((W + blk.x - 1) / blk.x, (H + blk.y - 1) / blk.y, z);
+}
+
+int launch_resize_pair(const void *l, const void *r, int dtype, int W, int H, int W2, int H2,
+                       float *lo, float *ro, cudaStream_t st) {
+    dim3 blk(32, 8);
+    dim3 g = grid2d(W2, H2, blk, 2);
+    if (W2 == W && H2 == H) {
+        // a resample to the same size still runs the reference's arithmetic
+    }
+    switch (dtype) {
+    case SV_U8: count_launch(); k_resize_pair<uint8_t><<<g, blk, 0, st>>>((const uint8_t *)l, (const uint8_t *)r, W, H, W2, H2, lo, ro); break;
+    case SV_F32: count_launch(); k_resize_pair<float><<<g, blk, 0, st>>>((const float *)l, (const float *)r, W, H, W2, H2, lo, ro); break;
+    case SV_F64: count_launch(); k_resize_pair<double><<<g, blk, 0, st>>>((const double *)l, (const double *)r, W, H, W2, H2, lo, ro); break;
+    default: set_error("unknown dtype %d", dtype); return SV_ERR_PARAM;
+    }
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_to_f32_pair(const void *l, const void *r, int dtype, long n, float *lo, float *ro,
+                       cudaStream_t st) {
+    dim3 g(grid_for(n, 256), 2);
+    switch (dtype) {
+    case SV_U8: count_launch(); k_to_f32_pair<uint8_t><<<g, 256, 0, st>>>((const uint8_t *)l, (const uint8_t *)r, n, lo, ro); break;
+    case SV_F32: count_launch(); k_to_f32_pair<float><<<g, 256, 0, st>>>((const float *)l, (const float *)r, n, lo, ro); break;
+    case SV_F64: count_launch(); k_to_f32_pair<double><<<g, 256, 0, st>>>((const double *)l, (const double *)r, n, lo, ro); break;
+    default: set_error("unknown dtype %d", dtype); return SV_ERR_PARAM;
+    }
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_resize_f64(const double *x, int W, int H, int W2, int H2, double *out,
+                      cudaStream_t st) {
+    dim3 blk(32, 8);
+    count_launch(); k_resize_scale<double><<<grid2d(W2, H2, blk), blk, 0, st>>>(x, W, H, W2, H2, 1.0, 0, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_upscale_disp(const float *dw, int Ww, int Hw, int W, int H, double inv,
+                        double *out, cudaStream_t st) {
+    dim3 blk(32, 8);
+    count_launch(); k_resize_scale<float><<<grid2d(W, H, blk), blk, 0, st>>>(dw, Ww, Hw, W, H, inv, 1, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_promote(const float *x, long n, double *out, cudaStream_t st) {
+    count_launch(); k_promote<float><<<grid_for(n, 256), 256, 0, st>>>(x, n, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_avgpool2_f64(const double *img, int C, int H, int W, double *out, cudaStream_t st) {
+    long n = (long)C * (H / 2) * (W / 2);
+    if (n > 0) {
+        count_launch();
+        k_avgpool2_f64<<<grid_for(n, 256), 256, 0, st>>>(img, C, H, W, out);
+    }
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_avgpool2(const float *img, int H, int W, float *out, cudaStream_t st) {
+    dim3 blk(32, 8);
+    count_launch(); k_avgpool2<<<grid2d(W / 2, H / 2, blk), blk, 0, st>>>(img, H, W, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+// The network shapes this build instantiates: the reference's shipped
+// architectures (feat_C, cost_C, refine_C) = (12, 6, 8), (8, 4, 8), (8, 4, 4),
+// (16, 8, 8) with D <= 16.
+template <int C, int CM, int RC>
+static int forward_impl(const NetView &n, const float *left, const float *right, int H, int W,
+                        const float *gh, const float *gf, float *d0, float *d1, float *d2,
+                        const FwdBufs &b, cudaStream_t st) {
+    const int h1 = (H - 1) / 2 + 1, w1 = (W - 1) / 2 + 1;
+    const int h = (h1 - 1) / 2 + 1, w = (w1 - 1) / 2 + 1;
+    const int D = n.D;
+    dim3 blk(32, 8);
+    // FeatureNet, both images: c1 s2, c2 s2, c3, c4
+    count_launch(); k_conv2d<1, C, 1><<<grid2d(w1, h1, blk, 2), blk, 0, st>>>(
+        left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
+    count_launch(); k_conv2d<C, C, 1><<<grid2d(w, h, blk, 2), blk, 0, st>>>(
+        b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
+    count_launch(); k_conv2d<C, C, 1><<<grid2d(w, h, blk, 2), blk, 0, st>>>(
+        b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1], nullptr);
+    count_launch(); k_conv2d<C, C, 0><<<grid2d(w, h, blk, 2), blk, 0, st>>>(
+        b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
+    SV_LAUNCH_CHECK();
+    // cost volume + CostFilter + soft-argmin
+    const long vox = (long)D * h * w;
+    count_launch(); k_costvol_conv3d<C, CM><<<grid_for(vox, 128, 1 << 30), 128, 0, st>>>(
+        b.fb[0], b.fb[1], D, h, w, n.cw[0], n.cb[0], b.v0);
+    count_launch(); k_conv3d<CM, CM><<<grid_for(vox, 128, 1 << 30), 128, 0, st>>>(b.v0, D, h, w, n.cw[1],
+                                                                  n.cb[1], b.v1);
+    count_launch(); k_conv3d_softargmin<CM, 16><<<grid_for((long)h * w, 128, 1 << 30), 128, 0, st>>>(
+        b.v1, D, h, w, n.cw[2], n.cb[2], d0);
+    SV_LAUNCH_CHECK();
+    // Refinement levels
+    const int Hs[2] = {H / 2, H}, Ws[2] = {W / 2, W};
+    const float *guides[2] = {gh, gf};
+    float *outs[2] = {d1, d2};
+    const float *prev = d0;
+    int ph = h, pw = w;
+    for (int lv = 0; lv < 2; ++lv) {
+        const int Hl = Hs[lv], Wl = Ws[lv];
+        count_launch(); k_upsample_concat<<<grid2d(Wl, Hl, blk), blk, 0, st>>>(prev, ph, pw, Hl, Wl, guides[lv],
+                                                              b.rin);
+        const float *cur = b.rin;
+        float *bufs[2] = {b.ra, b.rb};
+        for (int i = 0; i < n.ndil; ++i) {
+            float *dst = bufs[i & 1];
+            const int dl = n.dil[i];
+            count_launch();
+            if (i == 0)
+                k_conv2d<2, RC, 1><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
+                    cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
+                    nullptr);
+            else
+                k_conv2d<RC, RC, 1><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
+                    cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
+                    nullptr);
+            cur = dst;
+        }
+        count_launch(); k_conv2d<RC, 1, 2><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
+            cur, cur, Hl, Wl, Hl, Wl, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
+            outs[lv], b.rin);
+        SV_LAUNCH_CHECK();
+        prev = outs[lv];
+        ph = Hl;
+        pw = Wl;
+    }
+    return SV_OK;
+}
+
+int launch_forward(const NetView &n, const float *left, const float *right, int H, int W,
+                   const float *gh, const float *gf, float *d0, float *d1, float *d2,
+                   const FwdBufs &b, cudaStream_t st) {
+    if (n.D < 1 || n.D > 16) {
+        set_error("D=%d outside 1..16", n.D);
+        return SV_ERR_NET;
+    }
+    if (n.C == 12 && n.Cm == 6 && n.Rc == 8)
+        return forward_impl<12, 6, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+    if (n.C == 8 && n.Cm == 4 && n.Rc == 8)
+        return forward_impl<8, 4, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+    if (n.C == 8 && n.Cm == 4 && n.Rc == 4)
+        return forward_impl<8, 4, 4>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+    if (n.C == 16 && n.Cm == 8 && n.Rc == 8)
+        return forward_impl<16, 8, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+    set_error("architecture feat_C=%d cost_C=%d refine_C=%d is not instantiated", n.C, n.Cm,
+              n.Rc);
+    return SV_ERR_NET;
+}
+
+// ------------------------------------------------------------- _peak
+// sorted(disp)[int(n*q)] by radix selection on order-preserving 64-bit keys
+// (stereonet.py:3866-3869), 11/11/11/11/11/9-bit digits.  State in device
+// memory: {prefix, rank}.  Signed zeros share one key (they compare equal,
+// and a zero peak is replaced by 0.5 anyway).
+constexpr int SEL_BINS = 2048;
+
+struct SelState {
+    unsigned long long prefix;
+    long long rank;
+    double value;
+};
+
+__device__ __forceinline__ unsigned long long sel_key(double d) {
+    return ordkey(d == 0.0 ? 0.0 : d);
+}
+
+// Histogram of digit `shift` among keys whose bits above (shift+bits) equal
+// the current prefix.  pass 0 has no prefix.
+__global__ void k_sel_hist(const double *__restrict__ x, long n, int shift, int bits,
+                           const SelState *__restrict__ s, unsigned *__restrict__ hist) {
+    __shared__ unsigned sh[SEL_BINS];
+    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const int top = shift + bits;
+    const unsigned long long pre = top >= 64 ? 0ull : (s->prefix >> top);
+    const unsigned mask = (1u << bits) - 1u;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        unsigned long long k = sel_key(x[i]);
+        if (top < 64 && (k >> top) != pre) continue;
+        atomicAdd(&sh[(unsigned)(k >> shift) & mask], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// One CTA: find the bin holding `rank`, extend the prefix, clear hist.
+__global__ void k_sel_pick(unsigned *__restrict__ hist, int shift, int bits, SelState *s,
+                           const double *__restrict__ x, long n, int last) {
+    __shared__ unsigned cnt[SEL_BINS];
+    const int nb = 1 << bits;
+    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) {
+        cnt[i] = i < nb ? hist[i] : 0u;
+        hist[i] = 0u;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long r = s->rank;
+        int bin = 0;
+        for (; bin < nb; ++bin) {
+            if (r < (long long)cnt[bin]) break;
+            r -= cnt[bin];
+        }
+        if (bin >= nb) bin = nb - 1;     // unreachable for a valid rank
+        s->prefix |= ((unsigned long long)bin) << shift;
+        s->rank = r;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        unsigned long long k = s->prefix;
+        // invert ordkey
+        unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+        s->value = __longlong_as_double((long long)b);
+    }
+    (void)x;
+    (void)n;
+}
+
+__global__ void k_sel_init(SelState *s, long long rank) {
+    s->prefix = 0ull;
+    s->rank = rank;
+    s->value = 0.0;
+}
+
+int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
+                  cudaStream_t st) {
+    count_launch(); k_sel_init<<<1, 1, 0, st>>>(state, rank);
+    SV_CUDA_TRY(cudaMemsetAsync(hist, 0, SEL_BINS * sizeof(unsigned), st));
+    const int shifts[6] = {53, 42, 31, 20, 9, 0};
+    const int bits[6] = {11, 11, 11, 11, 11, 9};
+    const int blocks = grid_for(n, 256, 148 * 4);
+    for (int p = 0; p < 6; ++p) {
+        count_launch(); k_sel_hist<<<blocks, 256, 0, st>>>(x, n, shifts[p], bits[p], state, hist);
+        count_launch(); k_sel_pick<<<1, 256, 0, st>>>(hist, shifts[p], bits[p], state, x, n, p == 5);
+    }
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+size_t select_state_bytes() { return sizeof(SelState); }
+size_t select_value_offset() { return offsetof(SelState, value); }
+
+}  // namespace sv

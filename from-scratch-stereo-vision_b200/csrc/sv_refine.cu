@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(256)
 
 int launch_base(const double *disp0, long N, int32_t *base, int *flag,
                 cudaStream_t st) {
-    k_base<<<grid_for(N, 256), 256, 0, st>>>(disp0, N, base, flag);
+    count_launch(); k_base<<<grid_for(N, 256), 256, 0, st>>>(disp0, N, base, flag);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -527,15 +527,15 @@ int launch_census(const void *img0, const void *img1, int dtype, int W, int H,
     size_t cells = (size_t)(CT_W + 2 * rx) * (CT_H + 2 * ry);
     switch (dtype) {
     case SV_U8:
-        k_census<uint8_t><<<grd, blk, cells * 1, st>>>(
+        count_launch(); k_census<uint8_t><<<grd, blk, cells * 1, st>>>(
             (const uint8_t *)img0, (const uint8_t *)img1, W, H, rx, ry, out0, out1);
         break;
     case SV_F32:
-        k_census<float><<<grd, blk, cells * 4, st>>>(
+        count_launch(); k_census<float><<<grd, blk, cells * 4, st>>>(
             (const float *)img0, (const float *)img1, W, H, rx, ry, out0, out1);
         break;
     case SV_F64:
-        k_census<double><<<grd, blk, cells * 8, st>>>(
+        count_launch(); k_census<double><<<grd, blk, cells * 8, st>>>(
             (const double *)img0, (const double *)img1, W, H, rx, ry, out0, out1);
         break;
     default:
@@ -552,7 +552,7 @@ int launch_band_costs(const uint64_t *cl, const uint64_t *cr, const int32_t *bas
     const long N = (long)W * H;
     const int K = 2 * R + 1;
     dim3 grd(grid_for(N * K, 256, 148 * 8), nviews);
-    k_band_costs<<<grd, 256, 0, st>>>(cl, cr, base0, base1, W, N, R, K, invalid, C0, C1);
+    count_launch(); k_band_costs<<<grd, 256, 0, st>>>(cl, cr, base0, base1, W, N, R, K, invalid, C0, C1);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -566,7 +566,7 @@ static int sgm_dispatch_lt(const uint8_t *C0, const uint8_t *C1, const int32_t *
                            cudaStream_t st) {
     long warps = tasks.start[tasks.nseg];
     int blocks = (int)((warps * 32 + 255) / 256);
-    k_sgm<V, LT, ADD><<<blocks, 256, 0, st>>>(C0, C1, b0, b1, W, H, K, P1, P2,
+    count_launch(); k_sgm<V, LT, ADD><<<blocks, 256, 0, st>>>(C0, C1, b0, b1, W, H, K, P1, P2,
                                               (LT *)Lout, npaths, tasks);
     SV_LAUNCH_CHECK();
     return SV_OK;
@@ -632,6 +632,7 @@ static int wta_v(const void *L, bool l16, int npaths, int nviews, long N, int K,
                  const double *d01, double uniq, double *out0, double *out1,
                  double *conf0, cudaStream_t st) {
     int blocks = grid_for(nviews * N * 32, 256, 148 * 16);
+    count_launch();
     if (l16)
         k_wta<V, uint16_t><<<blocks, 256, 0, st>>>((const uint16_t *)L, npaths, nviews, N, K, R,
                                                    b0, b1, d00, d01, uniq, conf0 != nullptr,
@@ -664,7 +665,7 @@ int launch_left_to_right(const double *dl, int W, int H, double *dr, int32_t *ba
         SV_CUDA_TRY(cudaFuncSetAttribute(k_left_to_right,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
-    k_left_to_right<<<H, 256, smem, st>>>(dl, W, dr, base_r);
+    count_launch(); k_left_to_right<<<H, 256, smem, st>>>(dl, W, dr, base_r);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -676,7 +677,7 @@ int launch_lr_check(const double *dl, const double *dr, const double *disp0, int
         SV_CUDA_TRY(cudaFuncSetAttribute(k_lr_check,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
-    k_lr_check<<<H, 256, smem, st>>>(dl, dr, disp0, W, tol, out, status);
+    count_launch(); k_lr_check<<<H, 256, smem, st>>>(dl, dr, disp0, W, tol, out, status);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

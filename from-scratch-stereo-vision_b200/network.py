@@ -1,0 +1,200 @@
+"""Drop-ins for the StereoNet forward and resolution selection of stereonet.py.
+
+    resize_gray(img, W, H, W2, H2)                                 (3843-3845)
+    avgpool2(img, C, H, W)                                         (979-995)
+    forward(net, left, right, H, W, guide_half, guide_full)        (1203-1233)
+    predict(net, left, right, W, H)                                (5891-5897)
+    predict_at_scale(net, left, right, W, H, work_width=96, verbose=True)
+    predict_auto(net, left, right, W, H, target_peak=None, probe_width=64,
+                 max_width=320, passes=3, verbose=True)             (3872-3929)
+
+``net`` is either a checkpoint from ``weights.load_model`` or the
+reference's own ``StereoNet`` object (its parameters are read through
+``all_params()``).  The weights are uploaded once per object and reused.
+The network runs in FP32 on the GPU (convolutions accumulate in FP32,
+soft-argmin in FP32 with max subtraction); resampling runs in FP64 like the
+reference.  Outputs follow the reference's return types: lists for list
+inputs, numpy for numpy, CUDA tensors for tensors.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import weakref
+
+import numpy as np
+import torch
+
+from . import _lib
+from .refine import _device, _image, _kind, _ptr, _ret, _stream, _to_dev
+from .weights import NetArch, StereoNetWeights
+
+
+class GpuNet:
+    """One checkpoint uploaded to the current device (sv_net)."""
+
+    def __init__(self, w: StereoNetWeights):
+        self.lib = _lib.load()
+        self.weights = w
+        arch = (ctypes.c_int * len(w.arch.vector()))(*w.arch.vector())
+        flat = np.ascontiguousarray(w.flat, dtype=np.float64)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.sv_net_create(arch, len(w.arch.vector()),
+                                          flat.ctypes.data_as(ctypes.c_void_p), flat.size,
+                                          ctypes.byref(h)), "sv_net_create")
+        self.handle = h
+        self.target_peak = w.target_peak
+        self.D = w.arch.D
+
+    def __del__(self):
+        try:
+            if self.handle:
+                self.lib.sv_net_destroy(self.handle)
+        except Exception:
+            pass
+
+
+_cache: "weakref.WeakKeyDictionary" = weakref.WeakKeyDictionary()
+_cache_by_id: dict = {}
+
+
+def _weights_of(net) -> StereoNetWeights:
+    if isinstance(net, StereoNetWeights):
+        return net
+    if hasattr(net, "all_params"):          # the reference's StereoNet
+        arch = NetArch(feat_C=int(net.feat_C), cost_C=int(net.filt.c1.oc), D=int(net.D),
+                       max_disp=int(getattr(net, "max_disp", 32)),
+                       refine_C=int(net.ref1.convs[0].oc),
+                       refine_dil=tuple(int(d) for d in net.ref1.dilations),
+                       target_peak=int(getattr(net, "target_peak", 20)))
+        blocks = [np.asarray(p, dtype=np.float64) for p, _ in net.all_params()]
+        return StereoNetWeights(arch, blocks)
+    raise TypeError("net must be a StereoNetWeights or a reference StereoNet")
+
+
+def gpu_net(net) -> GpuNet:
+    """The uploaded copy of ``net`` (re-uploaded if its parameters changed)."""
+    if isinstance(net, GpuNet):
+        return net
+    w = _weights_of(net)
+    key = (id(net), torch.cuda.current_device())
+    fp = hash(w.flat.tobytes())
+    hit = _cache_by_id.get(key)
+    if hit is not None and hit[0] == fp:
+        return hit[1]
+    g = GpuNet(w)
+    _cache_by_id[key] = (fp, g)
+    return g
+
+
+# ------------------------------------------------------------ resampling
+def resize_gray(img, W, H, W2, H2):
+    """stereonet.py:3843-3845 (FP64 on the GPU, bit-identical)."""
+    lib = _lib.load()
+    t = _to_dev(img, W * H, torch.float64, name="img")
+    out = torch.empty(W2 * H2, dtype=torch.float64, device=t.device)
+    _lib.check(lib.sv_resize(_ptr(t), W, H, W2, H2, _ptr(out), _stream()), "resize_gray")
+    return _ret(out, img)
+
+
+def avgpool2(img, C, H, W):
+    """stereonet.py:979-995 -> (pooled, H//2, W//2), FP64, bit-identical."""
+    lib = _lib.load()
+    t = _to_dev(img, C * H * W, torch.float64, name="img")
+    out = torch.empty(C * (H // 2) * (W // 2), dtype=torch.float64, device=t.device)
+    _lib.check(lib.sv_avgpool2(_ptr(t), C, H, W, _ptr(out), _stream()), "avgpool2")
+    return _ret(out, img), H // 2, W // 2
+
+
+# --------------------------------------------------------------- forward
+def _f32(x, n, name):
+    return _to_dev(x, n, torch.float32, name=name)
+
+
+def forward(net, left, right, H, W, guide_half, guide_full):
+    """StereoNet.forward (stereonet.py:1203-1233): (d_quarter, d_half, d_full)."""
+    g = gpu_net(net)
+    lib = g.lib
+    h1, w1 = (H - 1) // 2 + 1, (W - 1) // 2 + 1
+    h, w = (h1 - 1) // 2 + 1, (w1 - 1) // 2 + 1
+    tl, tr = _f32(left, H * W, "left"), _f32(right, H * W, "right")
+    gh = _f32(guide_half, (H // 2) * (W // 2), "guide_half")
+    gf = _f32(guide_full, H * W, "guide_full")
+    dev = tl.device
+    d0 = torch.empty(h * w, dtype=torch.float32, device=dev)
+    d1 = torch.empty((H // 2) * (W // 2), dtype=torch.float32, device=dev)
+    d2 = torch.empty(H * W, dtype=torch.float32, device=dev)
+    need = lib.sv_forward_workspace_size(g.handle, H, W)
+    ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+    _lib.check(lib.sv_stereonet_forward(g.handle, _ptr(tl), _ptr(tr), H, W, _ptr(gh), _ptr(gf),
+                                        _ptr(d0), _ptr(d1), _ptr(d2), _lib.SV_FP32, _ptr(ws),
+                                        need, _stream()), "forward")
+    return tuple(_ret(d.to(torch.float64), left) for d in (d0, d1, d2))
+
+
+def predict(net, left, right, W, H):
+    """stereonet.py:5891-5897: full-resolution disparity of the network
+    (guide_half = avgpool2(left), guide_full = left)."""
+    return predict_at_scale(net, left, right, W, H, work_width=W, verbose=False)[0]
+
+
+# ------------------------------------------------- resolution selection
+def _pair_inputs(left, right, W, H):
+    tl, code = _image(left, W * H, "left")
+    tr, code_r = _image(right, W * H, "right")
+    if code_r != code:
+        tr = tr.to(tl.dtype)
+    return tl, tr, code
+
+
+def predict_at_scale(net, left, right, W, H, work_width=96, verbose=True):
+    """stereonet.py:3932-3960 -> (disp_full, disp_work, W_work, H_work)."""
+    g = gpu_net(net)
+    lib = g.lib
+    tl, tr, code = _pair_inputs(left, right, W, H)
+    dev = tl.device
+    df = torch.empty(W * H, dtype=torch.float64, device=dev)
+    dw = torch.empty(max(W * H, 64 * 64), dtype=torch.float64, device=dev)
+    need = lib.sv_predict_workspace_size(g.handle, W, H, max(int(work_width), 48))
+    ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+    Ww, Hw = ctypes.c_int(), ctypes.c_int()
+    _lib.check(lib.sv_predict_at_scale(g.handle, _ptr(tl), _ptr(tr), code, W, H, int(work_width),
+                                       _lib.SV_FP32, _ptr(df), _ptr(dw), ctypes.byref(Ww),
+                                       ctypes.byref(Hw), _ptr(ws), need, _stream()),
+               "predict_at_scale")
+    if verbose and work_width < W:
+        print("  running at %dx%d (input %dx%d, scale %.3f)"
+              % (Ww.value, Hw.value, W, H, work_width / float(W)))
+    dwv = dw[:Ww.value * Hw.value]
+    return _ret(df, left), _ret(dwv, left), Ww.value, Hw.value
+
+
+def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64, max_width=320,
+                 passes=3, verbose=True, return_trace=False):
+    """stereonet.py:3872-3929 -> (disp_full, disp_work, W_work, H_work).
+
+    The work width depends on each pass's 95% disparity quantile, so the
+    call reads one number back from the GPU per pass."""
+    g = gpu_net(net)
+    lib = g.lib
+    tp = float(g.target_peak if target_peak is None else target_peak)
+    tl, tr, code = _pair_inputs(left, right, W, H)
+    dev = tl.device
+    df = torch.empty(W * H, dtype=torch.float64, device=dev)
+    dw = torch.empty(max(W * H, 64 * 64), dtype=torch.float64, device=dev)
+    need = lib.sv_predict_workspace_size(g.handle, W, H, int(max_width))
+    ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
+    Ww, Hw = ctypes.c_int(), ctypes.c_int()
+    trace = (ctypes.c_int * (passes + 2))()
+    _lib.check(lib.sv_predict_auto(g.handle, _ptr(tl), _ptr(tr), code, W, H, tp,
+                                   int(probe_width), int(max_width), int(passes), _lib.SV_FP32,
+                                   _ptr(df), _ptr(dw), ctypes.byref(Ww), ctypes.byref(Hw), trace,
+                                   _ptr(ws), need, _stream()), "predict_auto")
+    widths = [int(t) for t in trace if t > 0]
+    if verbose:
+        for i, wd in enumerate(widths):
+            print("  %s work width %d" % ("probe chose" if i == 0 else "rescaled to", wd))
+    res = (_ret(df, left), _ret(dw[:Ww.value * Hw.value], left), Ww.value, Hw.value)
+    if return_trace:
+        return res, widths
+    return res

@@ -66,7 +66,9 @@ def _to_dev(x, n, dtype=None, name="array"):
         a = np.asarray(x)
         if dtype is not None:
             a = a.astype(torch.empty(0, dtype=dtype).numpy().dtype, copy=False)
-        elif a.dtype not in _NP_CODE:
+        elif a.dtype == np.uint64:
+            a = a.view(np.int64)                   # census words: keep the bits
+        elif a.dtype.kind not in "uif":
             a = a.astype(np.float64)
         t = torch.from_numpy(np.ascontiguousarray(a).reshape(-1)).to(dev)
     if t.numel() != n:
@@ -136,6 +138,19 @@ def census(img, W, H, rx=2, ry=2):
     return a if _kind(img) == "numpy" else [int(v) for v in a]
 
 
+def _census_words(c, n, name):
+    """Census descriptors (Python ints, uint64 or int64) as a device int64
+    tensor holding the same 64 bits."""
+    if isinstance(c, torch.Tensor):
+        t = c.reshape(-1).to(_device())
+        if t.dtype != torch.int64:
+            raise ValueError("%s must be an int64 tensor of census words" % name)
+        if t.numel() != n:
+            raise ValueError("%s has %d elements, expected %d" % (name, t.numel(), n))
+        return t.contiguous()
+    return _to_dev(np.asarray(c, dtype=np.uint64).view(np.int64), n, name=name)
+
+
 # -------------------------------------------------------------- band_costs
 def band_costs(cl, cr, gl, gr, base, W, H, R, ad_weight, ad_trunc, invalid,
                prior=None, prior_w=0.0, prior_t=4.0):
@@ -147,8 +162,8 @@ def band_costs(cl, cr, gl, gr, base, W, H, R, ad_weight, ad_trunc, invalid,
         raise ValueError("invalid cost %r must be an integer in 0..255" % invalid)
     lib = _lib.load()
     N, K = W * H, 2 * R + 1
-    tl = _to_dev(np.asarray(cl, dtype=np.uint64).view(np.int64) if not isinstance(cl, torch.Tensor) else cl, N, name="cl")
-    tr = _to_dev(np.asarray(cr, dtype=np.uint64).view(np.int64) if not isinstance(cr, torch.Tensor) else cr, N, name="cr")
+    tl = _census_words(cl, N, "cl")
+    tr = _census_words(cr, N, "cr")
     tb = _to_dev(base, N, torch.int32, name="base")
     C = torch.empty(N * K, dtype=torch.uint8, device=tl.device)
     _lib.check(lib.sv_band_costs(_ptr(tl), _ptr(tr), _ptr(tb), W, H, R, int(inv), _ptr(C),
@@ -206,9 +221,7 @@ def refine_fullres(left, right, disp0, W, H, R=3, P1=1.0, P2=12.0, ad_weight=0.0
     td = _to_dev(disp0, N, torch.float64, name="disp0")
     need = lib.sv_refine_workspace_size(W, H, ctypes.byref(p))
     if need == 0:
-        _lib.check(lib.sv_refine_fullres(None, None, code, None, W, H, ctypes.byref(p), None,
-                                         None, None, 0, _stream()) or _lib.SV_ERR_PARAM,
-                   "refine_fullres")
+        _lib.raise_last("refine_fullres")
     ws = _workspace(need)
     out = torch.empty(N, dtype=torch.float64, device=td.device)
     conf = torch.empty(N, dtype=torch.float64, device=td.device) if return_conf else None
@@ -246,9 +259,7 @@ def lr_refine(left, right, disp0, W, H, tol=1.0, **kw):
     td = _to_dev(disp0, N, torch.float64, name="disp0")
     need = lib.sv_lr_refine_workspace_size(W, H, ctypes.byref(p))
     if need == 0:
-        _lib.check(lib.sv_lr_refine(None, None, code, None, W, H, float(tol), ctypes.byref(p),
-                                    None, None, None, 0, _stream()) or _lib.SV_ERR_PARAM,
-                   "lr_refine")
+        _lib.raise_last("lr_refine")
     ws = _workspace(need)
     out = torch.empty(N, dtype=torch.float64, device=td.device)
     st = torch.empty(N, dtype=torch.uint8, device=td.device)
@@ -282,6 +293,22 @@ class LRRefiner:
                                          _ptr(status), _ptr(self.ws), self.need,
                                          _stream() if stream is None else stream),
                    "lr_refine")
+
+    def run_timed(self, left, right, disp0, out, status, events, stream=None) -> None:
+        """``run`` that also records ``events`` (STAGES + 1 torch.cuda.Event
+        with timing enabled) around its stages: base + left_to_right, census,
+        band costs, SGM, WTA, left-right check."""
+        code = _TORCH_CODE[left.dtype]
+        for e in events:
+            if e.cuda_event == 0:          # torch creates events lazily
+                e.record()
+        arr = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
+        _lib.check(self.lib.sv_lr_refine_timed(
+            _ptr(left), _ptr(right), code, _ptr(disp0), self.W, self.H, self.tol,
+            ctypes.byref(self.p), _ptr(out), _ptr(status), _ptr(self.ws), self.need,
+            _stream() if stream is None else stream, arr, len(events)), "lr_refine")
+
+    STAGES = ("base+left_to_right", "census", "band_costs", "sgm", "wta", "lr_check")
 
     def data_status(self) -> None:
         _data_status(self.ws, "lr_refine")

@@ -49,6 +49,11 @@ const char *sv_status_string(int status);
 const char *sv_last_error(void);
 int sv_version(void);
 
+/* Number of kernels this library has launched in this process, on any
+ * device (a reporting counter; the difference across a region is that
+ * region's launch count).  No reference counterpart. */
+unsigned long long sv_launch_count(void);
+
 /* Refinement parameters, the keyword arguments of refine_fullres
  * (stereonet.py:5244-5246).  The exact integer path requires ad_weight == 0,
  * prior_w == 0 and integer-valued 0 <= P1, P2 <= 4096 (every value the
@@ -111,6 +116,18 @@ int sv_lr_refine(const void *left, const void *right, int dtype,
                  const sv_refine_params *p, double *out, uint8_t *status,
                  void *workspace, size_t workspace_bytes, void *stream);
 
+/* sv_lr_refine with stage timing for profiling: events[0..SV_LR_STAGES] are
+ * caller-created cudaEvent_t recorded on `stream` before the first kernel
+ * and after each stage (base + left_to_right, census, band costs, SGM, WTA,
+ * left-right check), so cudaEventElapsedTime(events[i], events[i+1]) is the
+ * device time of stage i.  Same results as sv_lr_refine. */
+#define SV_LR_STAGES 6
+int sv_lr_refine_timed(const void *left, const void *right, int dtype,
+                       const double *disp0, int W, int H, double tol,
+                       const sv_refine_params *p, double *out, uint8_t *status,
+                       void *workspace, size_t workspace_bytes, void *stream,
+                       void *const *events, int n_events);
+
 /* ------------------------------------------------------------ network */
 typedef struct sv_net sv_net;
 
@@ -127,6 +144,10 @@ void sv_net_destroy(sv_net *net);
  * half-pixel bilinear resample computed in FP64. */
 int sv_resize(const double *img, int W, int H, int W2, int H2, double *out,
               void *stream);
+
+/* avgpool2, stereonet.py:979-995: 2x2 mean of C planes [C][H][W] into
+ * [C][H/2][W/2], FP64 in the reference's order (bit-identical). */
+int sv_avgpool2(const double *img, int C, int H, int W, double *out, void *stream);
 
 /* StereoNet.forward, stereonet.py:1203-1233 (note the reference's H, W order).
  * left/right/guide_full are FP32 [H][W], guide_half FP32 [H/2][W/2];

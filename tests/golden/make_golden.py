@@ -199,5 +199,26 @@ def main(ref_dir):
     print("all fixtures written (%.1fs)" % (time.time() - t0))
 
 
+HOT_PATH = ["census", "band_costs", "_aggregate_path", "refine_fullres", "left_to_right",
+            "lr_refine", "resize_gray", "avgpool2", "predict", "predict_at_scale",
+            "predict_auto", "refine_disparity"]
+
+
+def signatures(ref_dir):
+    """The reference's signatures of the hot-path functions (and
+    StereoNet.forward), which the drop-ins must keep."""
+    import inspect
+    SN = load_reference(ref_dir)
+    sig = {n: str(inspect.signature(SN[n])) for n in HOT_PATH}
+    sig["StereoNet.forward"] = str(inspect.signature(SN["StereoNet"].forward))
+    with open(os.path.join(HERE, "signatures.json"), "w") as f:
+        json.dump(sig, f, indent=1, sort_keys=True)
+    print("signatures written")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    ref = args[0] if args else "/root/reference"
+    if "--signatures-only" not in sys.argv:
+        main(ref)
+    signatures(ref)

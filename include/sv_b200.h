@@ -128,6 +128,29 @@ int sv_lr_refine_timed(const void *left, const void *right, int dtype,
                        void *workspace, size_t workspace_bytes, void *stream,
                        void *const *events, int n_events);
 
+/* refine_fullres for callers that cannot allocate device memory (an engine
+ * that reserves all GPU memory up front, a plugin host without an
+ * allocator): same kernels and bit-identical output as sv_refine_fullres,
+ * but the scratch is one static device array of SV_NOALLOC_SCRATCH_BYTES
+ * inside this library, held on every GPU that loads it until exit.  No
+ * counterpart in the reference (it is an allocation-free variant of this
+ * library's own sv_refine_fullres).
+ *  - Images up to the scratch size: W*H*(20 + 9K) bytes plus alignment
+ *    (uint8 path costs; 20 + 17K when 4 + nbits + P2 > 255), e.g. 320x240 at
+ *    K=21.  Larger sizes return SV_ERR_SHAPE and allocate nothing.
+ *  - The first call on a device resolves the array's address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - All calls share the array, which keeps the last call's contents; each
+ *    call clears what must start at zero.  Calls that overlap on the GPU
+ *    race on it: serialise them.
+ *  - data_status (optional): a device int that receives SV_ERR_DISP if a
+ *    disparity is NaN, infinite or out of range (cleared by the call). */
+#define SV_NOALLOC_SCRATCH_BYTES (16u << 20)
+int sv_refine_fullres_noalloc(const void *left, const void *right, int dtype,
+                              const double *disp0, int W, int H,
+                              const sv_refine_params *p, double *out,
+                              int *data_status, void *stream);
+
 /* ------------------------------------------------------------ network */
 typedef struct sv_net sv_net;
 

@@ -225,10 +225,7 @@ def run_ours(args, rank, world, local):
     ms = sum(t0[i].elapsed_time(t1[i]) for i in range(args.steps))
     stage_ms = [sum(ev[i][s].elapsed_time(ev[i][s + 1]) for i in range(args.steps)) / args.steps
                 for s in range(len(stages))]
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = pkg.shard.max_over_ranks(ms, device="cuda")
     value = world * N * args.steps / (ms / 1e3) / 1e6
 
     # ---- end to end through the public pipeline from pinned host buffers
@@ -246,10 +243,7 @@ def run_ours(args, rank, world, local):
         e1[i].record()
     torch.cuda.synchronize()
     ems = sum(e0[i].elapsed_time(e1[i]) for i in range(args.steps))
-    if dist:
-        t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
+    ems = pkg.shard.max_over_ranks(ems, device="cuda")
     evalue = world * N * args.steps / (ems / 1e3) / 1e6
 
     result = None

@@ -86,7 +86,7 @@ struct RefineWs {
 
 static size_t carve_refine(void *ws, int W, int H, const RefineCfg &c, int nviews,
                            RefineWs *o) {
-    const size_t N = (size_t)W * H, NK = N * c.K;
+    const size_t N = (size_t)W * H, NK = N * slot_width(c.K);
     Carver cv(ws);
     RefineWs r{};
     r.flags = cv.take<DevFlags>(1);
@@ -253,11 +253,11 @@ int sv_refine_fullres(const void *left, const void *right, int dtype, const doub
     SV_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(DevFlags), st));
     SV_TRY(launch_base(disp0, N, w.base0, &w.flags->status, st));
     SV_TRY(launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st));
-    SV_TRY(launch_band_costs(w.cen0, w.cen1, w.base0, nullptr, W, H, c.R, c.invalid, w.C0,
+    SV_TRY(launch_band_costs_slot(w.cen0, w.cen1, w.base0, nullptr, W, H, c.R, c.invalid, w.C0,
                              nullptr, 1, st));
-    SV_TRY(launch_sgm(w.C0, nullptr, w.base0, nullptr, W, H, c.K, c.P1, c.P2, w.L, c.l16, 1,
+    SV_TRY(launch_sgm_packed(w.C0, nullptr, w.base0, nullptr, W, H, c.K, c.P1, c.P2, w.L, c.l16, 1,
                       c.npaths, st));
-    SV_TRY(launch_wta(w.L, c.l16, c.npaths, 1, W, H, c.R, w.base0, nullptr, disp0, nullptr,
+    SV_TRY(launch_wta_slot(w.L, c.l16, c.npaths, 1, W, H, c.R, w.base0, nullptr, disp0, nullptr,
                       c.uniq, out, nullptr, conf, st));
     return SV_OK;
 }
@@ -294,13 +294,13 @@ static int lr_refine_impl(const void *left, const void *right, int dtype, const 
     SV_TRY(mark());
     SV_TRY(launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st));
     SV_TRY(mark());
-    SV_TRY(launch_band_costs(w.cen0, w.cen1, w.base0, w.base1, W, H, c.R, c.invalid, w.C0,
+    SV_TRY(launch_band_costs_slot(w.cen0, w.cen1, w.base0, w.base1, W, H, c.R, c.invalid, w.C0,
                              w.C1, 2, st));
     SV_TRY(mark());
-    SV_TRY(launch_sgm(w.C0, w.C1, w.base0, w.base1, W, H, c.K, c.P1, c.P2, w.L, c.l16, 2,
+    SV_TRY(launch_sgm_packed(w.C0, w.C1, w.base0, w.base1, W, H, c.K, c.P1, c.P2, w.L, c.l16, 2,
                       c.npaths, st));
     SV_TRY(mark());
-    SV_TRY(launch_wta(w.L, c.l16, c.npaths, 2, W, H, c.R, w.base0, w.base1, disp0, w.d0r,
+    SV_TRY(launch_wta_slot(w.L, c.l16, c.npaths, 2, W, H, c.R, w.base0, w.base1, disp0, w.d0r,
                       c.uniq, w.dl, w.dr, nullptr, st));
     SV_TRY(mark());
     SV_TRY(launch_lr_check(w.dl, w.dr, disp0, W, H, tol, out, status, st));

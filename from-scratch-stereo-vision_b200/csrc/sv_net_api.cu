@@ -147,7 +147,7 @@ static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictW
     p.d2 = cv.take<float>(HW);
     p.probe64 = cv.take<double>(HW);
     p.sel = reinterpret_cast<SelState *>(cv.take<unsigned char>(select_state_bytes()));
-    p.hist = cv.take<unsigned>(2048);
+    p.hist = cv.take<unsigned>(select_hist_words());
     carve_fwd(cv, n, Hm, Wm, &p.fwd);
     if (o) *o = p;
     return cv.off;

@@ -158,27 +158,32 @@ __global__ void k_avgpool2_f64(const double *__restrict__ img, int C, int H, int
 }
 
 // ------------------------------------------------------------- conv 2d
-// act: 0 none, 1 leaky 0.2, 2 residual + relu0 (Refinement output).
-template <int IC, int OC, int ACT>
+// One thread per (output pixel, group of OCG output channels); blockIdx.z =
+// image * (OC / OCG) + channel group, so the small maps of this network still
+// fill the GPU.  act: 0 none, 1 leaky 0.2, 2 residual + relu0 (the
+// Refinement output, v > 0 ? v : v * 0).
+template <int IC, int OC, int OCG, int ACT>
 __global__ void __launch_bounds__(256)
     k_conv2d(const float *__restrict__ x0, const float *__restrict__ x1, int H, int W, int OH,
              int OW, int stride, int pad, int dil, const float *__restrict__ w,
-             const float *__restrict__ b, float *__restrict__ y0, float *__restrict__ y1,
-             const float *__restrict__ resid) {
-    __shared__ float sw[OC * IC * 9];
-    __shared__ float sb[OC];
+             const float *__restrict__ b, float *y0, float *y1, const float *__restrict__ resid) {
+    constexpr int NG = OC / OCG;
+    const int img = blockIdx.z / NG, og = blockIdx.z - img * NG;
+    __shared__ float sw[OCG * IC * 9];
+    __shared__ float sb[OCG];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    for (int i = tid; i < OC * IC * 9; i += blockDim.x * blockDim.y) sw[i] = w[i];
-    if (tid < OC) sb[tid] = b[tid];
+    for (int i = tid; i < OCG * IC * 9; i += blockDim.x * blockDim.y)
+        sw[i] = w[og * OCG * IC * 9 + i];
+    if (tid < OCG) sb[tid] = b[og * OCG + tid];
     __syncthreads();
-    const float *x = blockIdx.z ? x1 : x0;
-    float *y = blockIdx.z ? y1 : y0;
+    const float *x = img ? x1 : x0;
+    float *y = img ? y1 : y0;
     const int ox = blockIdx.x * blockDim.x + threadIdx.x;
     const int oy = blockIdx.y * blockDim.y + threadIdx.y;
     if (ox >= OW || oy >= OH) return;
-    float acc[OC];
+    float acc[OCG];
 #pragma unroll
-    for (int o = 0; o < OC; ++o) acc[o] = sb[o];
+    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
     const int iy0 = oy * stride - pad, ix0 = ox * stride - pad;
     const long HW = (long)H * W;
 #pragma unroll
@@ -194,37 +199,39 @@ __global__ void __launch_bounds__(256)
                 if (ix < 0 || ix >= W) continue;
                 const float v = __ldg(xc + (long)iy * W + ix);
 #pragma unroll
-                for (int o = 0; o < OC; ++o)
+                for (int o = 0; o < OCG; ++o)
                     acc[o] = fmaf(v, sw[(o * IC + c) * 9 + ky * 3 + kx], acc[o]);
             }
         }
     }
     const long OHW = (long)OH * OW, oi = (long)oy * OW + ox;
 #pragma unroll
-    for (int o = 0; o < OC; ++o) {
+    for (int o = 0; o < OCG; ++o) {
         float v = acc[o];
         if (ACT == 1) v = v > 0.f ? v : v * 0.2f;
         if (ACT == 2) {
             v = resid[oi] + v;
             v = v > 0.f ? v : v * 0.f;
         }
-        y[o * OHW + oi] = v;
+        y[(og * OCG + o) * OHW + oi] = v;
     }
 }
 
 // -------------------------------------------------- cost volume + conv3d #1
 // CostVolume.forward (stereonet.py:771-799) fused into Conv3d #1 (596-641)
 // and its leaky ReLU: each tap of the 3x3x3 window reads |fl - fr(x-d)|
-// (2.0 where x-d < 0), zero outside the volume (same padding).
-template <int C, int OC>
+// (2.0 where x-d < 0), zero outside the volume (same padding).  One thread
+// per (voxel, OCG output channels); blockIdx.y is the channel group.
+template <int C, int OC, int OCG>
 __global__ void __launch_bounds__(128)
     k_costvol_conv3d(const float *__restrict__ fl, const float *__restrict__ fr, int D, int h,
                      int w, const float *__restrict__ wt, const float *__restrict__ b,
                      float *__restrict__ y) {
-    __shared__ float sw[OC * C * 27];
-    __shared__ float sb[OC];
-    for (int i = threadIdx.x; i < OC * C * 27; i += blockDim.x) sw[i] = wt[i];
-    if (threadIdx.x < OC) sb[threadIdx.x] = b[threadIdx.x];
+    const int og = blockIdx.y;
+    __shared__ float sw[OCG * C * 27];
+    __shared__ float sb[OCG];
+    for (int i = threadIdx.x; i < OCG * C * 27; i += blockDim.x) sw[i] = wt[og * OCG * C * 27 + i];
+    if (threadIdx.x < OCG) sb[threadIdx.x] = b[og * OCG + threadIdx.x];
     __syncthreads();
     const long hw = (long)h * w;
     const long total = (long)D * hw;
@@ -233,9 +240,9 @@ __global__ void __launch_bounds__(128)
     const int od = (int)(idx / hw);
     const int rem = (int)(idx - od * hw);
     const int oy = rem / w, ox = rem - (rem / w) * w;
-    float acc[OC];
+    float acc[OCG];
 #pragma unroll
-    for (int o = 0; o < OC; ++o) acc[o] = sb[o];
+    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
     for (int c = 0; c < C; ++c) {
         const float *flc = fl + c * hw, *frc = fr + c * hw;
 #pragma unroll
@@ -257,28 +264,29 @@ __global__ void __launch_bounds__(128)
                         v = fabsf(__ldg(flc + yy * w + xx) - __ldg(frc + yy * w + xx - dd));
                     }
 #pragma unroll
-                    for (int o = 0; o < OC; ++o)
+                    for (int o = 0; o < OCG; ++o)
                         acc[o] = fmaf(v, sw[(o * C + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
                 }
             }
         }
     }
 #pragma unroll
-    for (int o = 0; o < OC; ++o) {
-        float v = acc[o];
-        y[o * total + idx] = v > 0.f ? v : v * 0.2f;
+    for (int o = 0; o < OCG; ++o) {
+        const float v = acc[o];
+        y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
     }
 }
 
 // ---------------------------------------------------------- conv3d #2
-template <int IC, int OC>
+template <int IC, int OC, int OCG>
 __global__ void __launch_bounds__(128)
     k_conv3d(const float *__restrict__ x, int D, int h, int w, const float *__restrict__ wt,
              const float *__restrict__ b, float *__restrict__ y) {
-    __shared__ float sw[OC * IC * 27];
-    __shared__ float sb[OC];
-    for (int i = threadIdx.x; i < OC * IC * 27; i += blockDim.x) sw[i] = wt[i];
-    if (threadIdx.x < OC) sb[threadIdx.x] = b[threadIdx.x];
+    const int og = blockIdx.y;
+    __shared__ float sw[OCG * IC * 27];
+    __shared__ float sb[OCG];
+    for (int i = threadIdx.x; i < OCG * IC * 27; i += blockDim.x) sw[i] = wt[og * OCG * IC * 27 + i];
+    if (threadIdx.x < OCG) sb[threadIdx.x] = b[og * OCG + threadIdx.x];
     __syncthreads();
     const long hw = (long)h * w;
     const long total = (long)D * hw;
@@ -287,9 +295,9 @@ __global__ void __launch_bounds__(128)
     const int od = (int)(idx / hw);
     const int rem = (int)(idx - od * hw);
     const int oy = rem / w, ox = rem - (rem / w) * w;
-    float acc[OC];
+    float acc[OCG];
 #pragma unroll
-    for (int o = 0; o < OC; ++o) acc[o] = sb[o];
+    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
     for (int c = 0; c < IC; ++c) {
         const float *xc = x + c * total;
 #pragma unroll
@@ -306,16 +314,16 @@ __global__ void __launch_bounds__(128)
                     if (xx < 0 || xx >= w) continue;
                     const float v = __ldg(xc + dd * hw + yy * w + xx);
 #pragma unroll
-                    for (int o = 0; o < OC; ++o)
+                    for (int o = 0; o < OCG; ++o)
                         acc[o] = fmaf(v, sw[(o * IC + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
                 }
             }
         }
     }
 #pragma unroll
-    for (int o = 0; o < OC; ++o) {
-        float v = acc[o];
-        y[o * total + idx] = v > 0.f ? v : v * 0.2f;
+    for (int o = 0; o < OCG; ++o) {
+        const float v = acc[o];
+        y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
     }
 }
 
@@ -323,25 +331,25 @@ __global__ void __launch_bounds__(128)
 // Conv3d #3 (Cm -> 1), CostVolume.invalid_mask (+8 where x < d, d >= 1,
 // stereonet.py:827-840) and SoftArgmin.forward (858-885) in FP32 with
 // max-subtraction: disp = sum_d d * exp(-c_d - max(-c)) / sum_d exp(...).
-template <int IC, int DMAX>
-__global__ void __launch_bounds__(128)
+// A CTA is 32 columns x 16 disparities of one row: thread (x, d) computes
+// cost d, the first warp reduces over d.
+constexpr int SA_DMAX = 16;
+
+template <int IC>
+__global__ void __launch_bounds__(32 * SA_DMAX)
     k_conv3d_softargmin(const float *__restrict__ x, int D, int h, int w,
                         const float *__restrict__ wt, const float *__restrict__ b,
                         float *__restrict__ disp) {
     __shared__ float sw[IC * 27];
-    for (int i = threadIdx.x; i < IC * 27; i += blockDim.x) sw[i] = wt[i];
+    __shared__ float cost[SA_DMAX][33];
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < IC * 27; i += blockDim.x * blockDim.y) sw[i] = wt[i];
     __syncthreads();
     const long hw = (long)h * w;
     const long total = (long)D * hw;
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= hw) return;
-    const int oy = idx / w, ox = idx - (idx / w) * w;
-    float cost[DMAX];
-    const float bias = __ldg(b);
-#pragma unroll
-    for (int od = 0; od < DMAX; ++od) {
-        if (od >= D) break;
-        float acc = bias;
+    const int ox = blockIdx.x * 32 + threadIdx.x, oy = blockIdx.y, od = threadIdx.y;
+    if (ox < w && od < D) {
+        float acc = __ldg(b);
         for (int c = 0; c < IC; ++c) {
             const float *xc = x + c * total;
 #pragma unroll
@@ -363,22 +371,19 @@ __global__ void __launch_bounds__(128)
             }
         }
         if (od >= 1 && ox < od) acc += 8.0f;
-        cost[od] = acc;
+        cost[od][threadIdx.x] = acc;
     }
-    float best = -cost[0];
-#pragma unroll
-    for (int d = 1; d < DMAX; ++d)
-        if (d < D) best = fmaxf(best, -cost[d]);
+    __syncthreads();
+    if (threadIdx.y != 0 || ox >= w) return;
+    float best = -cost[0][threadIdx.x];
+    for (int d = 1; d < D; ++d) best = fmaxf(best, -cost[d][threadIdx.x]);
     float total_e = 0.f, acc = 0.f;
-#pragma unroll
-    for (int d = 0; d < DMAX; ++d) {
-        if (d < D) {
-            float e = expf(-cost[d] - best);
-            total_e += e;
-            acc = fmaf((float)d, e, acc);
-        }
+    for (int d = 0; d < D; ++d) {
+        const float e = expf(-cost[d][threadIdx.x] - best);
+        total_e += e;
+        acc = fmaf((float)d, e, acc);
     }
-    disp[idx] = acc / total_e;
+    disp[(long)oy * w + ox] = acc / total_e;
 }
 
 // ---------------------------------------------- refinement input: up x2
@@ -484,23 +489,32 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
     const int h = (h1 - 1) / 2 + 1, w = (w1 - 1) / 2 + 1;
     const int D = n.D;
     dim3 blk(32, 8);
-    // FeatureNet, both images: c1 s2, c2 s2, c3, c4
-    count_launch(); k_conv2d<1, C, 1><<<grid2d(w1, h1, blk, 2), blk, 0, st>>>(
+    // FeatureNet, both images: c1 s2, c2 s2, c3, c4 (4 output channels per thread)
+    constexpr int FG = C % 4 == 0 ? 4 : C;
+    count_launch();
+    k_conv2d<1, C, FG, 1><<<grid2d(w1, h1, blk, 2 * (C / FG)), blk, 0, st>>>(
         left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
-    count_launch(); k_conv2d<C, C, 1><<<grid2d(w, h, blk, 2), blk, 0, st>>>(
+    count_launch();
+    k_conv2d<C, C, FG, 1><<<grid2d(w, h, blk, 2 * (C / FG)), blk, 0, st>>>(
         b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
-    count_launch(); k_conv2d<C, C, 1><<<grid2d(w, h, blk, 2), blk, 0, st>>>(
+    count_launch();
+    k_conv2d<C, C, FG, 1><<<grid2d(w, h, blk, 2 * (C / FG)), blk, 0, st>>>(
         b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1], nullptr);
-    count_launch(); k_conv2d<C, C, 0><<<grid2d(w, h, blk, 2), blk, 0, st>>>(
+    count_launch();
+    k_conv2d<C, C, FG, 0><<<grid2d(w, h, blk, 2 * (C / FG)), blk, 0, st>>>(
         b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
     SV_LAUNCH_CHECK();
-    // cost volume + CostFilter + soft-argmin
+    // cost volume + CostFilter + soft-argmin (2 output channels per thread)
+    constexpr int CG = CM % 2 == 0 ? 2 : CM;
     const long vox = (long)D * h * w;
-    count_launch(); k_costvol_conv3d<C, CM><<<grid_for(vox, 128, 1 << 30), 128, 0, st>>>(
+    count_launch();
+    k_costvol_conv3d<C, CM, CG><<<dim3(grid_for(vox, 128, 1 << 30), CM / CG), 128, 0, st>>>(
         b.fb[0], b.fb[1], D, h, w, n.cw[0], n.cb[0], b.v0);
-    count_launch(); k_conv3d<CM, CM><<<grid_for(vox, 128, 1 << 30), 128, 0, st>>>(b.v0, D, h, w, n.cw[1],
-                                                                  n.cb[1], b.v1);
-    count_launch(); k_conv3d_softargmin<CM, 16><<<grid_for((long)h * w, 128, 1 << 30), 128, 0, st>>>(
+    count_launch();
+    k_conv3d<CM, CM, CG><<<dim3(grid_for(vox, 128, 1 << 30), CM / CG), 128, 0, st>>>(
+        b.v0, D, h, w, n.cw[1], n.cb[1], b.v1);
+    count_launch();
+    k_conv3d_softargmin<CM><<<dim3((w + 31) / 32, h), dim3(32, SA_DMAX), 0, st>>>(
         b.v1, D, h, w, n.cw[2], n.cb[2], d0);
     SV_LAUNCH_CHECK();
     // Refinement levels
@@ -515,21 +529,23 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
                                                               b.rin);
         const float *cur = b.rin;
         float *bufs[2] = {b.ra, b.rb};
+        constexpr int RG = RC % 4 == 0 ? 4 : RC;
         for (int i = 0; i < n.ndil; ++i) {
             float *dst = bufs[i & 1];
             const int dl = n.dil[i];
             count_launch();
             if (i == 0)
-                k_conv2d<2, RC, 1><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
+                k_conv2d<2, RC, RG, 1><<<grid2d(Wl, Hl, blk, RC / RG), blk, 0, st>>>(
                     cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
                     nullptr);
             else
-                k_conv2d<RC, RC, 1><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
+                k_conv2d<RC, RC, RG, 1><<<grid2d(Wl, Hl, blk, RC / RG), blk, 0, st>>>(
                     cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
                     nullptr);
             cur = dst;
         }
-        count_launch(); k_conv2d<RC, 1, 2><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
+        count_launch();
+        k_conv2d<RC, 1, 1, 2><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
             cur, cur, Hl, Wl, Hl, Wl, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
             outs[lv], b.rin);
         SV_LAUNCH_CHECK();
@@ -561,11 +577,21 @@ int launch_forward(const NetView &n, const float *left, const float *right, int 
 }
 
 // ------------------------------------------------------------- _peak
-// sorted(disp)[int(n*q)] by radix selection on order-preserving 64-bit keys
-// (stereonet.py:3866-3869), 11/11/11/11/11/9-bit digits.  State in device
-// memory: {prefix, rank}.  Signed zeros share one key (they compare equal,
-// and a zero peak is replaced by 0.5 anyway).
+// sorted(disp)[int(n*q)] (stereonet.py:3866-3869) by exact radix selection
+// on order-preserving 64-bit keys, digits of 11/11/11/11/11/9 bits from the
+// top.  Signed zeros share one key (they compare equal in the sort, and a
+// zero peak becomes 0.5 anyway).
+//
+// Multi-CTA form: pass p histograms the p-th digit of the keys that match
+// the prefix chosen by passes 0..p-1; every CTA rebuilds that prefix itself
+// from the earlier histograms (a parallel scan over 2048 bins each), so a
+// pass is one launch and no CTA waits on another.  A last one-CTA launch
+// turns the full prefix back into the double.  Small inputs use one CTA for
+// everything.
 constexpr int SEL_BINS = 2048;
+constexpr int SEL_PASSES = 6;
+__constant__ int c_sel_shift[SEL_PASSES] = {53, 42, 31, 20, 9, 0};
+__constant__ int c_sel_bits[SEL_PASSES] = {11, 11, 11, 11, 11, 9};
 
 struct SelState {
     unsigned long long prefix;
@@ -577,81 +603,167 @@ __device__ __forceinline__ unsigned long long sel_key(double d) {
     return ordkey(d == 0.0 ? 0.0 : d);
 }
 
-// Histogram of digit `shift` among keys whose bits above (shift+bits) equal
-// the current prefix.  pass 0 has no prefix.
-__global__ void k_sel_hist(const double *__restrict__ x, long n, int shift, int bits,
-                           const SelState *__restrict__ s, unsigned *__restrict__ hist) {
-    __shared__ unsigned sh[SEL_BINS];
-    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) sh[i] = 0;
-    __syncthreads();
-    const int top = shift + bits;
-    const unsigned long long pre = top >= 64 ? 0ull : (s->prefix >> top);
-    const unsigned mask = (1u << bits) - 1u;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
-         i += (long)gridDim.x * blockDim.x) {
-        unsigned long long k = sel_key(x[i]);
-        if (top < 64 && (k >> top) != pre) continue;
-        atomicAdd(&sh[(unsigned)(k >> shift) & mask], 1u);
+__device__ __forceinline__ double sel_unkey(unsigned long long k) {
+    unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+// Count element i (if < n and on the current prefix) into cnt[digit].  The
+// first digits are mostly exponent bits, so most lanes of a warp hit the same
+// bin: lanes with equal digits are merged (__match_any_sync) and one atomic
+// per distinct digit is issued.  Called by every lane of the warp.
+__device__ __forceinline__ void sel_count(const double *__restrict__ x, long n, long i,
+                                          unsigned long long pre, int top, int shift,
+                                          unsigned mask, unsigned *cnt) {
+    unsigned digit = 0xffffffffu;
+    if (i < n) {
+        const unsigned long long k = sel_key(x[i]);
+        if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
     }
+    const unsigned same = __match_any_sync(kFull, digit);
+    if (digit != 0xffffffffu && (threadIdx.x & 31) == __ffs(same) - 1)
+        atomicAdd(&cnt[digit], (unsigned)__popc(same));
+}
+
+// With cnt[] (nb bins) in shared memory and a rank below their total, find
+// the bin holding that rank; every thread returns (bin, rank within bin).
+// Needs blockDim.x == 256 (8 bins per thread).
+__device__ __forceinline__ void sel_find(const unsigned *cnt, long long rank, int *bin,
+                                         long long *rem, long long *sbuf /*33*/) {
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    long long loc = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) loc += cnt[t * 8 + i];
+    long long x = loc;                                       // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        long long y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sbuf[wid] = x;
+    __syncthreads();
+    if (t == 0) {
+        long long run = 0;
+        for (int w = 0; w < 8; ++w) { long long v = sbuf[w]; sbuf[w] = run; run += v; }
+    }
+    __syncthreads();
+    const long long excl = sbuf[wid] + x - loc;
+    if (rank >= excl && rank < excl + loc) {
+        long long r = rank - excl;
+        int b = t * 8;
+        for (int i = 0; i < 8; ++i, ++b) {
+            if (r < (long long)cnt[b]) break;
+            r -= cnt[b];
+        }
+        sbuf[32] = ((long long)b << 40) | r;                 // r < 2^40
+    }
+    __syncthreads();
+    const long long packed = sbuf[32];
+    *bin = (int)(packed >> 40);
+    *rem = packed & ((1ll << 40) - 1);
+    __syncthreads();
+}
+
+// Rebuild prefix/rank after passes 0..upto-1 from their histograms.
+__device__ __forceinline__ void sel_replay(const unsigned *__restrict__ hist, int upto,
+                                           long long rank0, unsigned *cnt, long long *sbuf,
+                                           unsigned long long *prefix, long long *rank) {
+    unsigned long long pre = 0;
+    long long r = rank0;
+    for (int q = 0; q < upto; ++q) {
+        const int nb = 1 << c_sel_bits[q];
+        for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x)
+            cnt[i] = i < nb ? hist[q * SEL_BINS + i] : 0u;
+        __syncthreads();
+        int b;
+        long long rem;
+        sel_find(cnt, r, &b, &rem, sbuf);
+        pre |= (unsigned long long)b << c_sel_shift[q];
+        r = rem;
+    }
+    *prefix = pre;
+    *rank = r;
+}
+
+__global__ void __launch_bounds__(256)
+    k_sel_pass(const double *__restrict__ x, long n, int pass, long long rank0,
+               unsigned *__restrict__ hist, SelState *__restrict__ out) {
+    __shared__ unsigned cnt[SEL_BINS];
+    __shared__ long long sbuf[33];
+    unsigned long long pre;
+    long long r;
+    sel_replay(hist, pass, rank0, cnt, sbuf, &pre, &r);
+    if (pass == SEL_PASSES) {                                // final: the value
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            out->prefix = pre;
+            out->rank = r;
+            out->value = sel_unkey(pre);
+        }
+        return;
+    }
+    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) cnt[i] = 0u;
+    __syncthreads();
+    const int shift = c_sel_shift[pass], bits = c_sel_bits[pass];
+    const int top = shift + bits;
+    const unsigned mask = (1u << bits) - 1u;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i0 = blockIdx.x * (long)blockDim.x; i0 < n; i0 += stride)
+        sel_count(x, n, i0 + threadIdx.x, pre, top, shift, mask, cnt);
     __syncthreads();
     for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x)
-        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+        if (cnt[i]) atomicAdd(&hist[pass * SEL_BINS + i], cnt[i]);
 }
 
-// One CTA: find the bin holding `rank`, extend the prefix, clear hist.
-__global__ void k_sel_pick(unsigned *__restrict__ hist, int shift, int bits, SelState *s,
-                           const double *__restrict__ x, long n, int last) {
+// One CTA, all passes (inputs up to a few tens of thousands of values).
+__global__ void __launch_bounds__(256)
+    k_sel_small(const double *__restrict__ x, long n, long long rank, SelState *__restrict__ out) {
     __shared__ unsigned cnt[SEL_BINS];
-    const int nb = 1 << bits;
-    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) {
-        cnt[i] = i < nb ? hist[i] : 0u;
-        hist[i] = 0u;
+    __shared__ long long sbuf[33];
+    unsigned long long pre = 0;
+    long long r = rank;
+    for (int p = 0; p < SEL_PASSES; ++p) {
+        for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) cnt[i] = 0u;
+        __syncthreads();
+        const int shift = c_sel_shift[p], bits = c_sel_bits[p], top = shift + bits;
+        const unsigned mask = (1u << bits) - 1u;
+        for (long i0 = 0; i0 < n; i0 += blockDim.x)
+            sel_count(x, n, i0 + threadIdx.x, pre, top, shift, mask, cnt);
+        __syncthreads();
+        int b;
+        long long rem;
+        sel_find(cnt, r, &b, &rem, sbuf);
+        pre |= (unsigned long long)b << shift;
+        r = rem;
     }
-    __syncthreads();
     if (threadIdx.x == 0) {
-        long long r = s->rank;
-        int bin = 0;
-        for (; bin < nb; ++bin) {
-            if (r < (long long)cnt[bin]) break;
-            r -= cnt[bin];
-        }
-        if (bin >= nb) bin = nb - 1;     // unreachable for a valid rank
-        s->prefix |= ((unsigned long long)bin) << shift;
-        s->rank = r;
+        out->prefix = pre;
+        out->rank = r;
+        out->value = sel_unkey(pre);
     }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        unsigned long long k = s->prefix;
-        // invert ordkey
-        unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
-        s->value = __longlong_as_double((long long)b);
-    }
-    (void)x;
-    (void)n;
-}
-
-__global__ void k_sel_init(SelState *s, long long rank) {
-    s->prefix = 0ull;
-    s->rank = rank;
-    s->value = 0.0;
 }
 
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st) {
-    count_launch(); k_sel_init<<<1, 1, 0, st>>>(state, rank);
-    SV_CUDA_TRY(cudaMemsetAsync(hist, 0, SEL_BINS * sizeof(unsigned), st));
-    const int shifts[6] = {53, 42, 31, 20, 9, 0};
-    const int bits[6] = {11, 11, 11, 11, 11, 9};
-    const int blocks = grid_for(n, 256, 148 * 4);
-    for (int p = 0; p < 6; ++p) {
-        count_launch(); k_sel_hist<<<blocks, 256, 0, st>>>(x, n, shifts[p], bits[p], state, hist);
-        count_launch(); k_sel_pick<<<1, 256, 0, st>>>(hist, shifts[p], bits[p], state, x, n, p == 5);
+    if (n <= 8192) {
+        count_launch();
+        k_sel_small<<<1, 256, 0, st>>>(x, n, rank, state);
+        SV_LAUNCH_CHECK();
+        return SV_OK;
     }
+    SV_CUDA_TRY(cudaMemsetAsync(hist, 0, SEL_PASSES * SEL_BINS * sizeof(unsigned), st));
+    const int blocks = grid_for(n, 256 * 8, 148);
+    for (int p = 0; p < SEL_PASSES; ++p) {
+        count_launch();
+        k_sel_pass<<<blocks, 256, 0, st>>>(x, n, p, rank, hist, state);
+    }
+    count_launch();
+    k_sel_pass<<<1, 256, 0, st>>>(x, n, SEL_PASSES, rank, hist, state);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
 
 size_t select_state_bytes() { return sizeof(SelState); }
 size_t select_value_offset() { return offsetof(SelState, value); }
+size_t select_hist_words() { return (size_t)SEL_PASSES * SEL_BINS; }
 
 }  // namespace sv

@@ -44,5 +44,6 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
                   cudaStream_t st);
 size_t select_state_bytes();
 size_t select_value_offset();
+size_t select_hist_words();
 
 }  // namespace sv

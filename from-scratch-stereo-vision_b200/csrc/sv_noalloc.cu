@@ -106,7 +106,7 @@ extern "C" int sv_refine_fullres_noalloc(const void *left, const void *right, in
     const int P1 = (int)p->P1, P2 = (int)p->P2;
     const int npaths = p->paths == 8 ? 8 : 4;
     const bool l16 = invalid + P2 > 255;
-    const size_t N = (size_t)W * H, NK = N * K;
+    const size_t N = (size_t)W * H, NK = N * slot_width(K);
     // layout: flag | base | census left | census right | costs | path costs
     const size_t o_base = 256;
     const size_t o_cl = o_base + up256(N * 4);
@@ -133,10 +133,12 @@ extern "C" int sv_refine_fullres_noalloc(const void *left, const void *right, in
     SV_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), st));
     if ((rc = launch_base(disp0, (long)N, base, flag, st))) return rc;
     if ((rc = launch_census(left, right, dtype, W, H, p->rx, p->ry, cl, cr, st))) return rc;
-    if ((rc = launch_band_costs(cl, cr, base, nullptr, W, H, p->R, invalid, C, nullptr, 1, st)))
+    if ((rc = launch_band_costs_slot(cl, cr, base, nullptr, W, H, p->R, invalid, C, nullptr, 1,
+                                    st)))
         return rc;
-    if ((rc = launch_sgm(C, nullptr, base, nullptr, W, H, K, P1, P2, L, l16, 1, npaths, st)))
+    if ((rc = launch_sgm_packed(C, nullptr, base, nullptr, W, H, K, P1, P2, L, l16, 1, npaths,
+                               st)))
         return rc;
-    return launch_wta(L, l16, npaths, 1, W, H, p->R, base, nullptr, disp0, nullptr, p->uniq,
+    return launch_wta_slot(L, l16, npaths, 1, W, H, p->R, base, nullptr, disp0, nullptr, p->uniq,
                       out, nullptr, nullptr, st);
 }

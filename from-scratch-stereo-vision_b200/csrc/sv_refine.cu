@@ -155,13 +155,6 @@ __device__ __forceinline__ void shift_band(const int (&t)[V], int (&o)[V], int s
     }
 }
 
-struct SgmTasks {
-    int nseg;
-    int start[17];    // cumulative warp counts per segment
-    int view[16];
-    int dir[16];
-};
-
 template <int V, typename LT, bool ADD_S>
 __global__ void __launch_bounds__(256)
     k_sgm(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
@@ -290,86 +283,6 @@ __global__ void __launch_bounds__(256)
         if (g + 1 >= ng) break;
         if (g + 2 < ng) load(g + 2, ca, ba);
         process(g + 1, cb2, bb);
-    }
-}
-
-// ------------------------------------------------------------------- WTA
-// stereonet.py:5271-5303.  One warp per pixel, k = lane*V + j.  The first
-// minimum (strict <, ascending k) is the smallest (S << 8 | k) key.
-template <int V, typename LT>
-__global__ void __launch_bounds__(256)
-    k_wta(const LT *__restrict__ Lall, int npaths, int nviews, long N, int K, int R,
-          const int32_t *__restrict__ base0, const int32_t *__restrict__ base1,
-          const double *__restrict__ d00, const double *__restrict__ d01, double uniq,
-          int want_conf, double *__restrict__ out0, double *__restrict__ out1,
-          double *__restrict__ conf0) {
-    const int lane = threadIdx.x & 31;
-    const long nw = ((long)gridDim.x * blockDim.x) >> 5;
-    for (long w = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; w < nviews * N;
-         w += nw) {
-        const int view = (int)(w / N);
-        const long p = w - view * N;
-        int S[V];
-        unsigned key = 0xffffffffu;
-#pragma unroll
-        for (int j = 0; j < V; ++j) {
-            int k = lane * V + j;
-            S[j] = 0;
-            if (k < K) {
-                int acc = 0;
-                for (int d = 0; d < npaths; ++d)
-                    acc += (int)__ldg(Lall + ((long)(view * npaths + d) * N + p) * K + k);
-                S[j] = acc;
-                key = min(key, ((unsigned)acc << 8) | (unsigned)k);
-            }
-        }
-        key = __reduce_min_sync(kFull, key);
-        const int bk = (int)(key & 255u);
-        const int bv = (int)(key >> 8);
-        const double *d0 = view ? d01 : d00;
-        double *out = view ? out1 : out0;
-        if (bk == 0 || bk == K - 1) {
-            if (lane == 0) {
-                out[p] = d0[p];
-                if (want_conf && view == 0) conf0[p] = 0.0;
-            }
-            continue;
-        }
-        // neighbours of the winner
-        const int ka = bk - 1, kb = bk + 1;
-        int va = __shfl_sync(kFull, pick<V>(S, ka % V), ka / V);
-        int vb = __shfl_sync(kFull, pick<V>(S, kb % V), kb / V);
-        bool use_d0 = false;
-        double conf = 0.0;
-        if (uniq > 0.0 || want_conf) {
-            unsigned sv = 0xffffffffu;
-#pragma unroll
-            for (int j = 0; j < V; ++j) {
-                int k = lane * V + j;
-                if (k < K && (k < bk - 1 || k > bk + 1)) sv = min(sv, (unsigned)S[j]);
-            }
-            sv = __reduce_min_sync(kFull, sv);
-            if (sv != 0xffffffffu) {
-                double dsv = (double)sv, dbv = (double)bv;
-                conf = __ddiv_rn(__dsub_rn(dsv, dbv), __dadd_rn(dbv, 1.0e-6));
-            } else {
-                conf = 1.0;
-            }
-            use_d0 = conf < uniq;
-        }
-        if (lane == 0) {
-            if (want_conf && view == 0) conf0[p] = conf;
-            if (use_d0) {
-                out[p] = d0[p];
-            } else {
-                double a = (double)va, b = (double)vb, dbv = (double)bv;
-                double den = __dadd_rn(__dsub_rn(a, __dmul_rn(2.0, dbv)), b);
-                double off = 0.0;
-                if (den > 1.0e-9) off = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(a, b)), den);
-                const int32_t *base = view ? base1 : base0;
-                out[p] = __dadd_rn((double)(base[p] - R + bk), off);
-            }
-        }
     }
 }
 
@@ -585,77 +498,10 @@ static int sgm_dispatch(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
     }
 }
 
-// Segment table: longest scanlines first (horizontal, vertical, diagonal).
-static SgmTasks make_tasks(int W, int H, int nviews, int npaths, const int *dirs_only,
-                           int ndirs_only) {
-    SgmTasks t{};
-    int order[8] = {0, 1, 2, 3, 4, 5, 6, 7};
-    if (H > W) { order[0] = 2; order[1] = 3; order[2] = 0; order[3] = 1; }
-    t.start[0] = 0;
-    for (int oi = 0; oi < 8; ++oi) {
-        int d = order[oi];
-        if (dirs_only) {
-            bool keep = false;
-            for (int i = 0; i < ndirs_only; ++i) keep |= dirs_only[i] == d;
-            if (!keep) continue;
-        } else if (d >= npaths) {
-            continue;
-        }
-        int cnt = d < 2 ? H : d < 4 ? W : W + H - 1;
-        for (int v = 0; v < nviews; ++v) {
-            t.view[t.nseg] = v;
-            t.dir[t.nseg] = d;
-            t.start[t.nseg + 1] = t.start[t.nseg] + cnt;
-            t.nseg++;
-        }
-    }
-    return t;
-}
-
-int launch_sgm(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
-               const int32_t *b1, int W, int H, int K, int P1, int P2, void *Lout,
-               bool l16, int nviews, int npaths, cudaStream_t st) {
-    SgmTasks t = make_tasks(W, H, nviews, npaths, nullptr, 0);
-    if (l16) return sgm_dispatch<uint16_t, false>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
-    return sgm_dispatch<uint8_t, false>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
-}
-
 int launch_sgm_add_path(const uint8_t *C, const int32_t *base, int W, int H, int K,
                         int P1, int P2, int dir, uint16_t *S, cudaStream_t st) {
-    SgmTasks t = make_tasks(W, H, 1, 8, &dir, 1);
+    SgmTasks t = make_sgm_tasks(W, H, 1, 8, &dir, 1);
     return sgm_dispatch<uint16_t, true>(C, C, base, base, W, H, K, P1, P2, S, 1, t, st);
-}
-
-template <int V>
-static int wta_v(const void *L, bool l16, int npaths, int nviews, long N, int K, int R,
-                 const int32_t *b0, const int32_t *b1, const double *d00,
-                 const double *d01, double uniq, double *out0, double *out1,
-                 double *conf0, cudaStream_t st) {
-    int blocks = grid_for(nviews * N * 32, 256, 148 * 16);
-    count_launch();
-    if (l16)
-        k_wta<V, uint16_t><<<blocks, 256, 0, st>>>((const uint16_t *)L, npaths, nviews, N, K, R,
-                                                   b0, b1, d00, d01, uniq, conf0 != nullptr,
-                                                   out0, out1, conf0);
-    else
-        k_wta<V, uint8_t><<<blocks, 256, 0, st>>>((const uint8_t *)L, npaths, nviews, N, K, R,
-                                                  b0, b1, d00, d01, uniq, conf0 != nullptr,
-                                                  out0, out1, conf0);
-    SV_LAUNCH_CHECK();
-    return SV_OK;
-}
-
-int launch_wta(const void *L, bool l16, int npaths, int nviews, int W, int H, int R,
-               const int32_t *b0, const int32_t *b1, const double *d00,
-               const double *d01, double uniq, double *out0, double *out1,
-               double *conf0, cudaStream_t st) {
-    const long N = (long)W * H;
-    const int K = 2 * R + 1;
-    int v = (K + 31) / 32;
-    if (v <= 1) return wta_v<1>(L, l16, npaths, nviews, N, K, R, b0, b1, d00, d01, uniq, out0, out1, conf0, st);
-    if (v <= 2) return wta_v<2>(L, l16, npaths, nviews, N, K, R, b0, b1, d00, d01, uniq, out0, out1, conf0, st);
-    if (v <= 4) return wta_v<4>(L, l16, npaths, nviews, N, K, R, b0, b1, d00, d01, uniq, out0, out1, conf0, st);
-    return wta_v<8>(L, l16, npaths, nviews, N, K, R, b0, b1, d00, d01, uniq, out0, out1, conf0, st);
 }
 
 int launch_left_to_right(const double *dl, int W, int H, double *dr, int32_t *base_r,

@@ -6,20 +6,65 @@
 
 namespace sv {
 
+// Scanline work table of the SGM kernels: segment i covers the scanlines of
+// (view[i], dir[i]); start[] are cumulative scanline counts.
+struct SgmTasks {
+    int nseg;
+    int start[17];
+    int view[16];
+    int dir[16];
+};
+
+// Longest scanlines first (horizontal, vertical, diagonal) so that the
+// longest-running warps start in the first wave.  dirs_only restricts the
+// table to the listed directions (one view).
+inline SgmTasks make_sgm_tasks(int W, int H, int nviews, int npaths, const int *dirs_only,
+                               int ndirs_only) {
+    SgmTasks t{};
+    int order[8] = {0, 1, 2, 3, 4, 5, 6, 7};
+    if (H > W) { order[0] = 2; order[1] = 3; order[2] = 0; order[3] = 1; }
+    t.start[0] = 0;
+    for (int oi = 0; oi < 8; ++oi) {
+        const int d = order[oi];
+        if (dirs_only) {
+            bool keep = false;
+            for (int i = 0; i < ndirs_only; ++i) keep |= dirs_only[i] == d;
+            if (!keep) continue;
+        } else if (d >= npaths) {
+            continue;
+        }
+        const int cnt = d < 2 ? H : d < 4 ? W : W + H - 1;
+        for (int v = 0; v < nviews; ++v) {
+            t.view[t.nseg] = v;
+            t.dir[t.nseg] = d;
+            t.start[t.nseg + 1] = t.start[t.nseg] + cnt;
+            t.nseg++;
+        }
+    }
+    return t;
+}
+
+// Bytes per pixel of the slot layout used by the fused refinement (K + 2
+// slots rounded up to a multiple of 8).
+int slot_width(int K);
+
 int launch_base(const double *disp0, long N, int32_t *base, int *flag, cudaStream_t st);
 int launch_census(const void *img0, const void *img1, int dtype, int W, int H, int rx,
                   int ry, uint64_t *out0, uint64_t *out1, cudaStream_t st);
 int launch_band_costs(const uint64_t *cl, const uint64_t *cr, const int32_t *base0,
                       const int32_t *base1, int W, int H, int R, int invalid, uint8_t *C0,
                       uint8_t *C1, int nviews, cudaStream_t st);
-int launch_sgm(const uint8_t *C0, const uint8_t *C1, const int32_t *b0, const int32_t *b1,
-               int W, int H, int K, int P1, int P2, void *Lout, bool l16, int nviews,
-               int npaths, cudaStream_t st);
 int launch_sgm_add_path(const uint8_t *C, const int32_t *base, int W, int H, int K, int P1,
                         int P2, int dir, uint16_t *S, cudaStream_t st);
-int launch_wta(const void *L, bool l16, int npaths, int nviews, int W, int H, int R,
-               const int32_t *b0, const int32_t *b1, const double *d00, const double *d01,
-               double uniq, double *out0, double *out1, double *conf0, cudaStream_t st);
+int launch_band_costs_slot(const uint64_t *cl, const uint64_t *cr, const int32_t *base0,
+                           const int32_t *base1, int W, int H, int R, int invalid, uint8_t *C0,
+                           uint8_t *C1, int nviews, cudaStream_t st);
+int launch_sgm_packed(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
+                      const int32_t *b1, int W, int H, int K, int P1, int P2, void *Lout,
+                      bool l16, int nviews, int npaths, cudaStream_t st);
+int launch_wta_slot(const void *L, bool l16, int npaths, int nviews, int W, int H, int R,
+                    const int32_t *b0, const int32_t *b1, const double *d00, const double *d01,
+                    double uniq, double *out0, double *out1, double *conf0, cudaStream_t st);
 int launch_left_to_right(const double *dl, int W, int H, double *dr, int32_t *base_r,
                          cudaStream_t st);
 int launch_lr_check(const double *dl, const double *dr, const double *disp0, int W, int H,

@@ -1,0 +1,441 @@
+// sv_sgm.cu -- the band costs, 8-path SGM and winner-take-all of the fused
+// refinement (refine_fullres / lr_refine), on a slot layout built for packed
+// 16-bit SIMD.
+//
+// Slot layout.  Each pixel owns Kp bytes (Kp = K+2 rounded up to a table
+// size, a multiple of 8); slot i holds band index k = i-1, so slot 0 is
+// k = -1, slots 1..K the band and the rest padding.  The padding makes every
+// pixel's row 8-byte aligned and gives the SGM recurrence room for the
+// candidates just outside the band.
+//
+// SGM (stereonet.py:5192-5241).  A group of LP lanes (4..32) sweeps one
+// scanline of one direction of one view; each lane holds S = Kp/LP slots as
+// NR = S/2 registers of two uint16 values (u16x2).  Per pixel:
+//   t(k)    = min(Lq(k), Lq(k-1) + P1, Lq(k+1) + P1)   -- byte_perm + vimin3
+//   best(k) = min(t(k + shift), mq + P2)                 -- vminu2
+//   L(k)    = C(k) + best(k) - mq                         -- 32-bit adds
+// with INF (0x7FFF) outside 0..K-1, which is exactly the reference's set of
+// candidates (mq + P2 always; the other three only inside the band).  No
+// lane ever carries across the 16-bit boundary: L <= nbits + 4 + P2 <= 4164
+// and INF + P1 < 0x10000.  mq, the path minimum of the predecessor, is a
+// min over the group (log2 LP xor-shuffles).  A nonzero shift (band
+// re-centring between neighbours, stereonet.py:5218) goes through a per-group
+// shared-memory copy of t; shift 0 (most pixels) costs nothing.
+//
+// WTA (stereonet.py:5271-5303).  One thread per pixel sums the 8 path arrays
+// 8 slots at a time (64-bit loads, byte -> u16x2 expansion), keeps the first
+// minimum (strict <, ascending k) and re-reads the two neighbours of the
+// winner for the FP64 parabola.
+
+#include "sv_common.cuh"
+#include "sv_refine.cuh"
+
+namespace sv {
+
+constexpr unsigned kInf2 = 0x7FFF7FFFu;
+
+__device__ __forceinline__ void dir_of(int d, int &dx, int &dy) {
+    // order of refine_fullres's dirs list (stereonet.py:5266-5268)
+    dx = (d == 0 || d == 4 || d == 6) ? 1 : (d == 2 || d == 3) ? 0 : -1;
+    dy = (d == 0 || d == 1) ? 0 : (d == 2 || d == 4 || d == 5) ? 1 : -1;
+}
+
+// ----------------------------------------------------------- band costs
+// One thread per pixel writes its Kp slots (slot 0 and padding are 0).
+__global__ void __launch_bounds__(256)
+    k_band_costs_slot(const uint64_t *__restrict__ cl, const uint64_t *__restrict__ cr,
+                      const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
+                      long N, int R, int K, int Kp, int invalid, uint8_t *__restrict__ C0,
+                      uint8_t *__restrict__ C1) {
+    const int view = blockIdx.y;
+    const uint64_t *ref = view ? cr : cl;
+    const uint64_t *oth = view ? cl : cr;
+    const int32_t *base = view ? base1 : base0;
+    uint8_t *C = view ? C1 : C0;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < N;
+         p += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(p % W);
+        const uint64_t a = ref[p];
+        const int b = base[p] - R;
+        uint64_t *dst = reinterpret_cast<uint64_t *>(C + p * Kp);
+        for (int c = 0; c < Kp; c += 8) {
+            uint64_t word = 0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = c + u - 1;
+                uint64_t v = 0;
+                if (k >= 0 && k < K) {
+                    const int d = b + k;
+                    int cost = invalid;
+                    if (view == 0) {
+                        if (d >= 0 && x - d >= 0) cost = __popcll(a ^ oth[p - d]);
+                    } else {
+                        if (d >= 0 && x + d <= W - 1) cost = __popcll(a ^ oth[p + d]);
+                    }
+                    v = (uint64_t)cost;
+                }
+                word |= v << (8 * u);
+            }
+            dst[c >> 3] = word;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ SGM
+constexpr int SGM_PF = 8;   // prefetch distance in pixels
+
+template <int NR, int LP, typename LT>
+__global__ void __launch_bounds__(256)
+    k_sgm_packed(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
+                 const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
+                 int H, int K, int Kp, int P1, int P2, LT *__restrict__ Lout, int npaths,
+                 SgmTasks tasks) {
+    constexpr int S = 2 * NR;
+    extern __shared__ __align__(16) unsigned char sgm_smem[];
+    const int lane = threadIdx.x & 31;
+    const int g = lane & (LP - 1);
+    const unsigned gmask = LP == 32 ? 0xffffffffu : (((1u << LP) - 1u) << (lane & ~(LP - 1)));
+    const long gid = (blockIdx.x * (long)blockDim.x + threadIdx.x) / LP;
+    if (gid >= tasks.start[tasks.nseg]) return;            // whole groups leave together
+    unsigned short *buf = reinterpret_cast<unsigned short *>(sgm_smem) + (threadIdx.x / LP) * Kp;
+
+    int sg = 0;
+    while (gid >= tasks.start[sg + 1]) ++sg;
+    const int j0 = (int)(gid - tasks.start[sg]);
+    const int view = tasks.view[sg], dir = tasks.dir[sg];
+    int dx, dy;
+    dir_of(dir, dx, dy);
+    int x0, y0, n;
+    if (dy == 0) {
+        y0 = j0; x0 = dx > 0 ? 0 : W - 1; n = W;
+    } else if (dx == 0) {
+        x0 = j0; y0 = dy > 0 ? 0 : H - 1; n = H;
+    } else {
+        if (j0 < W) {
+            x0 = j0; y0 = dy > 0 ? 0 : H - 1;
+        } else {
+            const int i = j0 - W + 1;
+            x0 = dx > 0 ? 0 : W - 1;
+            y0 = dy > 0 ? i : H - 1 - i;
+        }
+        n = min(dx > 0 ? W - x0 : x0 + 1, dy > 0 ? H - y0 : y0 + 1);
+    }
+    const uint8_t *__restrict__ C = view ? C1 : C0;
+    const int32_t *__restrict__ base = view ? base1 : base0;
+    const long N = (long)W * H;
+    LT *__restrict__ Lo = Lout + (long)(view * npaths + dir) * N * Kp;
+    const long step = (long)dy * W + dx;
+    const long p0 = (long)y0 * W + x0;
+    const int s0 = g * S;                                  // first slot of this lane
+
+    unsigned vm[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int sa = s0 + 2 * r, sb = sa + 1;
+        vm[r] = ((sa >= 1 && sa <= K) ? 0x0000FFFFu : 0u) | ((sb >= 1 && sb <= K) ? 0xFFFF0000u : 0u);
+    }
+    const unsigned P1P1 = (unsigned)P1 * 0x10001u;
+
+    // Prefetch ring: the costs and band centre of step t + SGM_PF are loaded
+    // as soon as step t has read its slot, so every load has SGM_PF steps of
+    // recurrence latency to arrive from L2.
+    unsigned cring[SGM_PF][NR];
+    int bring[SGM_PF];
+    auto load = [&](int t, int slot) {
+        const long pp = p0 + t * step;
+        bring[slot] = __ldg(base + pp);
+        const unsigned short *cp = reinterpret_cast<const unsigned short *>(C + pp * Kp + s0);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) cring[slot][r] = (unsigned)__ldg(cp + r);
+    };
+#pragma unroll
+    for (int u = 0; u < SGM_PF; ++u)
+        if (u < n) load(u, u);
+
+    unsigned t_[NR];
+    int mq = 0, bprev = 0;
+    for (int t0 = 0; t0 < n; t0 += SGM_PF) {
+#pragma unroll
+        for (int u = 0; u < SGM_PF; ++u) {
+            const int t = t0 + u;
+            if (t >= n) break;                                  // group-uniform
+            unsigned c[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) c[r] = __byte_perm(cring[u][r], 0, 0x4140);
+            const int bcur = bring[u];
+            if (t + SGM_PF < n) load(t + SGM_PF, u);
+            const long pp = p0 + t * step;
+            unsigned L[NR];
+            if (t == 0) {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) L[r] = (c[r] & vm[r]) | (kInf2 & ~vm[r]);
+            } else {
+                const int s = bcur - bprev;                     // group-uniform
+                unsigned ts[NR];
+                if (s == 0) {
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) ts[r] = t_[r];
+                } else if (s == 1 || s == -1) {
+                    // one-slot re-centring with two lanes' edge registers
+                    unsigned tup = __shfl_up_sync(gmask, t_[NR - 1], 1, LP);
+                    unsigned tdn = __shfl_down_sync(gmask, t_[0], 1, LP);
+                    if (g == 0) tup = kInf2;
+                    if (g == LP - 1) tdn = kInf2;
+                    if (s == 1) {
+#pragma unroll
+                        for (int r = 0; r < NR; ++r)
+                            ts[r] = __byte_perm(t_[r], r < NR - 1 ? t_[r + 1] : tdn, 0x5432);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < NR; ++r)
+                            ts[r] = __byte_perm(r > 0 ? t_[r - 1] : tup, t_[r], 0x5432);
+                    }
+                } else {
+                    // larger jumps (depth edges): through this group's shared copy
+                    const int sc = max(-Kp - 2, min(Kp + 2, s));
+                    unsigned *b32 = reinterpret_cast<unsigned *>(buf);
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) b32[(s0 >> 1) + r] = t_[r];
+                    __syncwarp(gmask);
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) {
+                        const int ia = s0 + 2 * r + sc, ib = ia + 1;
+                        const unsigned lo = (ia >= 0 && ia < Kp) ? buf[ia] : 0x7FFFu;
+                        const unsigned hi = (ib >= 0 && ib < Kp) ? buf[ib] : 0x7FFFu;
+                        ts[r] = lo | (hi << 16);
+                    }
+                    __syncwarp(gmask);
+                }
+                const unsigned cap = (unsigned)(mq + P2) * 0x10001u;
+                const unsigned mm = (unsigned)mq * 0x10001u;
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    const unsigned v = c[r] + __vminu2(ts[r], cap) - mm;
+                    L[r] = (v & vm[r]) | (kInf2 & ~vm[r]);
+                }
+            }
+            bprev = bcur;
+            // path minimum over the group
+            unsigned m2 = L[0];
+#pragma unroll
+            for (int r = 1; r < NR; ++r) m2 = __vminu2(m2, L[r]);
+            int m = (int)min(m2 & 0xFFFFu, m2 >> 16);
+#pragma unroll
+            for (int o = 1; o < LP; o <<= 1) m = min(m, __shfl_xor_sync(gmask, m, o, LP));
+            mq = m;
+            // store this pixel's path costs (padding slots as 0, so the WTA sums never carry)
+            if (sizeof(LT) == 1) {
+                unsigned short *dst = reinterpret_cast<unsigned short *>(Lo + pp * Kp + s0);
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    dst[r] = (unsigned short)__byte_perm(L[r] & vm[r], 0, 0x0020);
+            } else {
+                unsigned *dst = reinterpret_cast<unsigned *>(Lo + pp * Kp + s0);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) dst[r] = L[r] & vm[r];
+            }
+            // t for the next pixel
+            unsigned up = __shfl_up_sync(gmask, L[NR - 1], 1, LP);
+            unsigned dn = __shfl_down_sync(gmask, L[0], 1, LP);
+            if (g == 0) up = kInf2;
+            if (g == LP - 1) dn = kInf2;
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const unsigned lm = __byte_perm(r > 0 ? L[r - 1] : up, L[r], 0x5432);
+                const unsigned lp = __byte_perm(L[r], r < NR - 1 ? L[r + 1] : dn, 0x5432);
+                t_[r] = __vimin3_u16x2(L[r], lm + P1P1, lp + P1P1);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ WTA
+template <typename LT>
+__device__ __forceinline__ int path_sum_slot(const LT *__restrict__ L, long stride, int npaths,
+                                             int slot) {
+    int acc = 0;
+    for (int d = 0; d < npaths; ++d) acc += (int)L[d * stride + slot];
+    return acc;
+}
+
+template <typename LT>
+__global__ void __launch_bounds__(256)
+    k_wta_slot(const LT *__restrict__ Lall, int npaths, int nviews, long N, int K, int Kp, int R,
+               const int32_t *__restrict__ base0, const int32_t *__restrict__ base1,
+               const double *__restrict__ d00, const double *__restrict__ d01, double uniq,
+               int want_conf, double *__restrict__ out0, double *__restrict__ out1,
+               double *__restrict__ conf0) {
+    constexpr int PER64 = 8 / sizeof(LT);                  // slots per 64-bit load
+    const long stride = N * Kp;                            // between path arrays
+    for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < nviews * N;
+         w += (long)gridDim.x * blockDim.x) {
+        const int view = (int)(w / N);
+        const long p = w - view * N;
+        const LT *Lp = Lall + (long)view * npaths * stride + p * Kp;
+        int bv = 0x7FFFFFFF, bs = -1;                      // best value, its slot
+        for (int c = 0; c < Kp; c += 8) {
+            unsigned acc[4] = {0u, 0u, 0u, 0u};            // 8 slots as u16x2
+            for (int d = 0; d < npaths; ++d) {
+                if (PER64 == 8) {
+                    const uint2 v = __ldg(reinterpret_cast<const uint2 *>(Lp + d * stride + c));
+                    acc[0] += __byte_perm(v.x, 0, 0x4140);
+                    acc[1] += __byte_perm(v.x, 0, 0x4342);
+                    acc[2] += __byte_perm(v.y, 0, 0x4140);
+                    acc[3] += __byte_perm(v.y, 0, 0x4342);
+                } else {
+                    const uint4 v = __ldg(reinterpret_cast<const uint4 *>(Lp + d * stride + c));
+                    acc[0] += v.x;
+                    acc[1] += v.y;
+                    acc[2] += v.z;
+                    acc[3] += v.w;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int slot = c + u;
+                const int v = (int)((acc[u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+                if (slot >= 1 && slot <= K && v < bv) {
+                    bv = v;
+                    bs = slot;
+                }
+            }
+        }
+        const int bk = bs - 1;
+        const double *d0 = view ? d01 : d00;
+        double *out = view ? out1 : out0;
+        if (bk == 0 || bk == K - 1) {
+            out[p] = d0[p];
+            if (want_conf && view == 0) conf0[p] = 0.0;
+            continue;
+        }
+        const int va = path_sum_slot(Lp, stride, npaths, bs - 1);
+        const int vb = path_sum_slot(Lp, stride, npaths, bs + 1);
+        bool use_d0 = false;
+        if (uniq > 0.0 || want_conf) {
+            // second best away from the winner's neighbours (stereonet.py:5286-5290)
+            int sv = 0x7FFFFFFF;
+            for (int k = 0; k < K; ++k)
+                if (k < bk - 1 || k > bk + 1) sv = min(sv, path_sum_slot(Lp, stride, npaths, k + 1));
+            double conf = 1.0;
+            if (sv != 0x7FFFFFFF) {
+                const double dsv = (double)sv, dbv = (double)bv;
+                conf = __ddiv_rn(__dsub_rn(dsv, dbv), __dadd_rn(dbv, 1.0e-6));
+            }
+            if (want_conf && view == 0) conf0[p] = conf;
+            use_d0 = conf < uniq;
+        }
+        if (use_d0) {
+            out[p] = d0[p];
+            continue;
+        }
+        const double a = (double)va, b = (double)vb, dbv = (double)bv;
+        const double den = __dadd_rn(__dsub_rn(a, __dmul_rn(2.0, dbv)), b);
+        double off = 0.0;
+        if (den > 1.0e-9) off = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(a, b)), den);
+        const int32_t *base = view ? base1 : base0;
+        out[p] = __dadd_rn((double)(base[p] - R + bk), off);
+    }
+}
+
+// ====================================================================
+// Host
+// ====================================================================
+
+// (Kp, lanes per scanline, registers per lane) for K + 2 slots
+struct SgmGeom {
+    int Kp, LP, NR;
+};
+static const SgmGeom kGeom[] = {{8, 4, 1},    {16, 4, 2},   {24, 4, 3},  {32, 4, 4},
+                                {48, 8, 3},   {64, 8, 4},   {96, 16, 3}, {128, 16, 4},
+                                {192, 32, 3}, {256, 32, 4}};
+
+static SgmGeom geom_for(int K) {
+    for (const SgmGeom &g : kGeom)
+        if (g.Kp >= K + 2) return g;
+    return kGeom[sizeof(kGeom) / sizeof(kGeom[0]) - 1];
+}
+
+int slot_width(int K) { return geom_for(K).Kp; }
+
+int launch_band_costs_slot(const uint64_t *cl, const uint64_t *cr, const int32_t *base0,
+                           const int32_t *base1, int W, int H, int R, int invalid, uint8_t *C0,
+                           uint8_t *C1, int nviews, cudaStream_t st) {
+    const long N = (long)W * H;
+    const int K = 2 * R + 1;
+    dim3 grd(grid_for(N, 256, 148 * 8), nviews);
+    count_launch();
+    k_band_costs_slot<<<grd, 256, 0, st>>>(cl, cr, base0, base1, W, N, R, K, slot_width(K),
+                                           invalid, C0, C1);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+template <int NR, int LP, typename LT>
+static int sgm_packed_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
+                         const int32_t *b1, int W, int H, int K, int Kp, int P1, int P2,
+                         void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
+    const long groups = t.start[t.nseg];
+    const long threads = groups * LP;
+    const int blocks = (int)((threads + 255) / 256);
+    const size_t smem = (size_t)(256 / LP) * Kp * sizeof(unsigned short);
+    count_launch();
+    k_sgm_packed<NR, LP, LT><<<blocks, 256, smem, st>>>(C0, C1, b0, b1, W, H, K, Kp, P1, P2,
+                                                         (LT *)Lout, npaths, t);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+template <typename LT>
+static int sgm_packed_dispatch(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
+                               const int32_t *b1, int W, int H, int K, int P1, int P2,
+                               void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
+    const SgmGeom g = geom_for(K);
+#define SV_GEOM(KP, LPV, NRV)                                                                \
+    if (g.Kp == KP)                                                                          \
+        return sgm_packed_go<NRV, LPV, LT>(C0, C1, b0, b1, W, H, K, KP, P1, P2, Lout, npaths, \
+                                           t, st);
+    SV_GEOM(8, 4, 1)
+    SV_GEOM(16, 4, 2)
+    SV_GEOM(24, 4, 3)
+    SV_GEOM(32, 4, 4)
+    SV_GEOM(48, 8, 3)
+    SV_GEOM(64, 8, 4)
+    SV_GEOM(96, 16, 3)
+    SV_GEOM(128, 16, 4)
+    SV_GEOM(192, 32, 3)
+    SV_GEOM(256, 32, 4)
+#undef SV_GEOM
+    set_error("no SGM geometry for K=%d", K);
+    return SV_ERR_SHAPE;
+}
+
+int launch_sgm_packed(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
+                      const int32_t *b1, int W, int H, int K, int P1, int P2, void *Lout,
+                      bool l16, int nviews, int npaths, cudaStream_t st) {
+    SgmTasks t = make_sgm_tasks(W, H, nviews, npaths, nullptr, 0);
+    if (l16)
+        return sgm_packed_dispatch<uint16_t>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+    return sgm_packed_dispatch<uint8_t>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+}
+
+int launch_wta_slot(const void *L, bool l16, int npaths, int nviews, int W, int H, int R,
+                    const int32_t *b0, const int32_t *b1, const double *d00, const double *d01,
+                    double uniq, double *out0, double *out1, double *conf0, cudaStream_t st) {
+    const long N = (long)W * H;
+    const int K = 2 * R + 1;
+    const int Kp = slot_width(K);
+    const int blocks = grid_for(nviews * N, 256, 148 * 16);
+    count_launch();
+    if (l16)
+        k_wta_slot<uint16_t><<<blocks, 256, 0, st>>>((const uint16_t *)L, npaths, nviews, N, K, Kp,
+                                                     R, b0, b1, d00, d01, uniq, conf0 != nullptr,
+                                                     out0, out1, conf0);
+    else
+        k_wta_slot<uint8_t><<<blocks, 256, 0, st>>>((const uint8_t *)L, npaths, nviews, N, K, Kp,
+                                                    R, b0, b1, d00, d01, uniq, conf0 != nullptr,
+                                                    out0, out1, conf0);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+}  // namespace sv

@@ -201,9 +201,13 @@ def run_ours(args, rank, world, local):
         else:
             pipe.refiner.run_timed(pipe.left, pipe.right, pipe.disp0, pipe.out, pipe.status, ev[i])
 
-    for _ in range(args.warmup):
-        step()
-    pipe.refiner.data_status()
+    # everything runs on the pipeline's own stream (captured passes replay as
+    # graphs there); events are recorded on that stream
+    sm = torch.cuda.stream(pipe.stream)
+    with sm:
+        for _ in range(args.warmup):
+            step()
+        pipe.refiner.data_status()
     torch.cuda.synchronize()
 
     # ---- device-resident timed region
@@ -211,7 +215,7 @@ def run_ours(args, rank, world, local):
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = lib.sv_launch_count()
-    with ClockSampler(local) as clk:
+    with ClockSampler(local) as clk, torch.cuda.stream(pipe.stream):
         for i in range(args.steps):
             flush.zero_()
             t0[i].record()
@@ -237,10 +241,11 @@ def run_ours(args, rank, world, local):
         dist.barrier()
     torch.cuda.synchronize()
     for i in range(args.steps):
-        flush.zero_()
-        e0[i].record()
+        with torch.cuda.stream(pipe.stream):
+            flush.zero_()
+            e0[i].record()
         pipe.run_host(hl, hr)
-        e1[i].record()
+        e1[i].record(pipe.stream)
     torch.cuda.synchronize()
     ems = sum(e0[i].elapsed_time(e1[i]) for i in range(args.steps))
     ems = pkg.shard.max_over_ranks(ems, device="cuda")

@@ -23,6 +23,9 @@ void set_error(const char *fmt, ...);
 // Process-wide count of kernels this library has launched (sv_launch_count);
 // a relaxed atomic increment per launch, read only for reporting.
 void count_launch();
+void count_launches(unsigned long long n);     // a graph replay's kernels
+void uncount_launches(unsigned long long n);   // kernels recorded, not yet run
+unsigned long long launch_count_now();
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 

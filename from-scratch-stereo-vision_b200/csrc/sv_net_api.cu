@@ -5,16 +5,40 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
+
+// One captured predict_auto stage (a network pass, optionally with the peak
+// selection that follows it), keyed by everything its kernels' arguments
+// depend on.
+struct sv_graph_key {
+    int kind, W, H, dtype, work, with_sel;
+    const void *left, *right;
+    void *disp_full, *disp_work, *ws;
+    bool operator==(const sv_graph_key &o) const {
+        return kind == o.kind && W == o.W && H == o.H && dtype == o.dtype && work == o.work &&
+               with_sel == o.with_sel && left == o.left && right == o.right &&
+               disp_full == o.disp_full && disp_work == o.disp_work && ws == o.ws;
+    }
+};
+
+struct sv_graph_entry {
+    sv_graph_key key;
+    cudaGraphExec_t exec;
+    unsigned long long kernels;
+    int device;
+};
 
 struct sv_net {
     sv::NetView view;
     float *dev = nullptr;     // all FP32 parameters, one allocation
     int arch[16];
     int n_arch;
+    std::mutex graph_mu;      // guards graphs (the weights themselves are immutable)
+    std::vector<sv_graph_entry> graphs;
 };
 
 namespace sv {
@@ -153,19 +177,6 @@ static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictW
     return cv.off;
 }
 
-static int read_peak(const PredictWs &w, const double *x, long n, cudaStream_t st,
-                     double *peak) {
-    long long rank = (long long)(n * 0.95);      // int(len(s) * q)
-    int rc = launch_select(x, n, rank, w.sel, w.hist, st);
-    if (rc) return rc;
-    double v = 0.0;
-    SV_CUDA_TRY(cudaMemcpyAsync(&v, reinterpret_cast<const char *>(w.sel) + select_value_offset(),
-                                sizeof(double), cudaMemcpyDeviceToHost, st));
-    SV_CUDA_TRY(cudaStreamSynchronize(st));
-    *peak = v > 0.5 ? v : 0.5;
-    return SV_OK;
-}
-
 // predict (stereonet.py:5891-5897) on FP32 images already in lw/rw.
 static int predict_f32(const sv_net *net, const PredictWs &w, int W, int H, cudaStream_t st) {
     int rc = check_net_shape(net->view, H, W);
@@ -210,6 +221,84 @@ static int predict_at_scale_impl(const sv_net *net, const PredictWs &w, const vo
         if (rc_ != SV_OK) return rc_; \
     } while (0)
 
+static void work_dims(int W, int H, int work, int *Ww, int *Hw) {
+    if (work >= W) {
+        *Ww = W;
+        *Hw = H;
+        return;
+    }
+    const double scale = work / (double)W;
+    int hw = (int)(H * scale + 0.5);
+    *Ww = work;
+    *Hw = hw < 8 ? 8 : hw;
+}
+
+// Read back the selected peak (the one host synchronisation of a stage).
+static int fetch_peak(const PredictWs &w, cudaStream_t st, double *peak) {
+    double v = 0.0;
+    SV_CUDA_TRY(cudaMemcpyAsync(&v, reinterpret_cast<const char *>(w.sel) + select_value_offset(),
+                                sizeof(double), cudaMemcpyDeviceToHost, st));
+    SV_CUDA_TRY(cudaStreamSynchronize(st));
+    *peak = v > 0.5 ? v : 0.5;                      // _peak's floor
+    return SV_OK;
+}
+
+// Run one predict_auto stage.  On a capturable stream the stage is recorded
+// into a CUDA graph the first time (per shape, buffers and device) and
+// replayed afterwards, so a network pass costs one launch on the host.  On
+// the legacy default stream, or inside the caller's own capture, the
+// kernels are enqueued directly.
+constexpr size_t kMaxGraphs = 48;
+
+template <typename F>
+static int run_stage(sv_net *net, const sv_graph_key &key, cudaStream_t st, F &&enqueue) {
+    if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) return enqueue();
+    cudaStreamCaptureStatus cs;
+    SV_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return enqueue();
+    int dev = 0;
+    SV_CUDA_TRY(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lock(net->graph_mu);
+        for (auto &g : net->graphs) {
+            if (g.device == dev && g.key == key) {
+                SV_CUDA_TRY(cudaGraphLaunch(g.exec, st));
+                count_launches(g.kernels);
+                return SV_OK;
+            }
+        }
+    }
+    const unsigned long long before = launch_count_now();
+    SV_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    const unsigned long long kernels = launch_count_now() - before;
+    uncount_launches(kernels);                       // they run at the launch below
+    if (rc || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc) return rc;
+        set_error("stream capture failed: %s", cudaGetErrorString(e));
+        return SV_ERR_CUDA;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        set_error("graph instantiation failed: %s", cudaGetErrorString(ei));
+        return SV_ERR_CUDA;
+    }
+    SV_CUDA_TRY(cudaGraphLaunch(exec, st));
+    count_launches(kernels);
+    std::lock_guard<std::mutex> lock(net->graph_mu);
+    if (net->graphs.size() >= kMaxGraphs) {
+        cudaGraphExecDestroy(net->graphs.front().exec);
+        net->graphs.erase(net->graphs.begin());
+    }
+    net->graphs.push_back({key, exec, kernels, dev});
+    return SV_OK;
+}
+
 }  // namespace sv
 
 using namespace sv;
@@ -249,6 +338,7 @@ int sv_net_create(const int *arch, int n_arch, const double *params, long n_para
 
 void sv_net_destroy(sv_net *net) {
     if (!net) return;
+    for (auto &g : net->graphs) cudaGraphExecDestroy(g.exec);
     if (net->dev) cudaFree(net->dev);
     delete net;
 }
@@ -348,32 +438,54 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
         return SV_ERR_PARAM;
     }
     cudaStream_t st = (cudaStream_t)stream;
+    sv_net *mnet = const_cast<sv_net *>(net);       // only its graph cache changes
     PredictWs w;
     SV_TRY(predict_ws(net, W, H, max_width, probe_width, workspace, workspace_bytes, &w));
     // probe (stereonet.py:3900-3907)
     const int pw = probe_width < W ? probe_width : W;
     int ph = (int)(H * pw / (double)W + 0.5);
     if (ph < 8) ph = 8;
-    SV_TRY(launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st));
-    SV_TRY(predict_f32(net, w, pw, ph, st));
-    SV_TRY(launch_promote(w.d2, (long)pw * ph, w.probe64, st));
+    sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, left, right, disp_full, disp_work,
+                     workspace};
+    SV_TRY(run_stage(mnet, key, st, [&]() -> int {
+        int rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st);
+        if (!rc) rc = predict_f32(net, w, pw, ph, st);
+        if (!rc) rc = launch_promote(w.d2, (long)pw * ph, w.probe64, st);
+        if (!rc) rc = launch_select(w.probe64, (long)pw * ph, (long long)((long)pw * ph * 0.95),
+                                    w.sel, w.hist, st);
+        return rc;
+    }));
     double pk;
-    SV_TRY(read_peak(w, w.probe64, (long)pw * ph, st, &pk));
+    SV_TRY(fetch_peak(w, st, &pk));
     const double peak = pk * (W / (double)pw);
     int work = width_for(W, target_peak, max_width, peak);
     int nt = 0;
     if (work_trace) work_trace[nt++] = work;
-    SV_TRY(predict_at_scale_impl(net, w, left, right, dtype, W, H, work, disp_full, disp_work,
-                                 pWw, pHw, st));
-    for (int it = 0; it < passes - 1; ++it) {
+    // passes (stereonet.py:3908-3929): the peak after pass i is needed only
+    // when another pass may follow
+    for (int pass = 1;; ++pass) {
+        const bool with_sel = pass < passes;
+        sv_graph_key k{1, W, H, dtype, work, with_sel ? 1 : 0, left, right, disp_full, disp_work,
+                       workspace};
+        int Ww, Hw;
+        SV_TRY(run_stage(mnet, k, st, [&]() -> int {
+            int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, disp_full,
+                                           disp_work, &Ww, &Hw, st);
+            if (!rc && with_sel)
+                rc = launch_select(disp_full, (long)W * H, (long long)((long)W * H * 0.95), w.sel,
+                                   w.hist, st);
+            return rc;
+        }));
+        work_dims(W, H, work, &Ww, &Hw);
+        *pWw = Ww;
+        *pHw = Hw;
+        if (!with_sel) break;
         double np_;
-        SV_TRY(read_peak(w, disp_full, (long)W * H, st, &np_));
-        int nw = width_for(W, target_peak, max_width, np_);
+        SV_TRY(fetch_peak(w, st, &np_));
+        const int nw = width_for(W, target_peak, max_width, np_);
         if (std::abs(nw - work) <= 0.08 * work) break;
         work = nw;
         if (work_trace) work_trace[nt++] = work;
-        SV_TRY(predict_at_scale_impl(net, w, left, right, dtype, W, H, work, disp_full,
-                                     disp_work, pWw, pHw, st));
     }
     if (work_trace) work_trace[nt] = 0;
     return SV_OK;

@@ -217,6 +217,217 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Shared-memory tiled 3x3 conv2d: a CTA of CT_TW x CT_TH threads computes a
+// CT_TW x CT_TH output tile for OCG output channels (blockIdx.z = image *
+// OC/OCG + group).  The input tile with its halo, for every input channel,
+// is staged once in shared memory (zeros outside the image, which adds
+// exactly what the reference's skipped taps add: nothing); weights are read
+// by broadcast.  Same arithmetic as k_conv2d, ~8x fewer global loads.
+constexpr int CT2_TW = 32, CT2_TH = 4;
+
+template <int IC, int OC, int OCG, int ACT>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH)
+    k_conv2d_tiled(const float *__restrict__ x0, const float *__restrict__ x1, int H, int W,
+                   int OH, int OW, int stride, int pad, int dil, const float *__restrict__ w,
+                   const float *__restrict__ b, float *y0, float *y1,
+                   const float *__restrict__ resid) {
+    constexpr int NG = OC / OCG;
+    extern __shared__ __align__(16) float tile[];
+    __shared__ float sw[OCG * IC * 9];
+    __shared__ float sb[OCG];
+    const int img = blockIdx.z / NG, og = blockIdx.z - img * NG;
+    const int tid = threadIdx.y * CT2_TW + threadIdx.x;
+    for (int i = tid; i < OCG * IC * 9; i += CT2_TW * CT2_TH) sw[i] = w[og * OCG * IC * 9 + i];
+    if (tid < OCG) sb[tid] = b[og * OCG + tid];
+    const float *x = img ? x1 : x0;
+    float *y = img ? y1 : y0;
+    const int ox0 = blockIdx.x * CT2_TW, oy0 = blockIdx.y * CT2_TH;
+    const int ix0 = ox0 * stride - pad, iy0 = oy0 * stride - pad;
+    const int tw = (CT2_TW - 1) * stride + 2 * dil + 1;
+    const int th = (CT2_TH - 1) * stride + 2 * dil + 1;
+    const long HW = (long)H * W;
+    for (int i = tid; i < IC * th * tw; i += CT2_TW * CT2_TH) {
+        const int c = i / (th * tw);
+        const int rem = i - c * th * tw;
+        const int ty = rem / tw, tx = rem - (rem / tw) * tw;
+        const int gy = iy0 + ty, gx = ix0 + tx;
+        tile[i] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(x + c * HW + (long)gy * W + gx)
+                                                            : 0.0f;
+    }
+    __syncthreads();
+    const int ox = ox0 + threadIdx.x, oy = oy0 + threadIdx.y;
+    if (ox >= OW || oy >= OH) return;
+    float acc[OCG];
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
+    const int by = threadIdx.y * stride, bx = threadIdx.x * stride;
+#pragma unroll
+    for (int c = 0; c < IC; ++c) {
+        const float *tc = tile + c * th * tw;
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            const float *row = tc + (by + ky * dil) * tw + bx;
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+                const float v = row[kx * dil];
+#pragma unroll
+                for (int o = 0; o < OCG; ++o)
+                    acc[o] = fmaf(v, sw[(o * IC + c) * 9 + ky * 3 + kx], acc[o]);
+            }
+        }
+    }
+    const long OHW = (long)OH * OW, oi = (long)oy * OW + ox;
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) {
+        float v = acc[o];
+        if (ACT == 1) v = v > 0.f ? v : v * 0.2f;
+        if (ACT == 2) {
+            v = resid[oi] + v;
+            v = v > 0.f ? v : v * 0.f;
+        }
+        y[(og * OCG + o) * OHW + oi] = v;
+    }
+}
+
+static size_t conv2d_tile_bytes(int IC, int stride, int dil) {
+    return (size_t)IC * ((CT2_TH - 1) * stride + 2 * dil + 1) *
+           ((CT2_TW - 1) * stride + 2 * dil + 1) * sizeof(float);
+}
+
+// Tiled cost volume + conv3d #1: a CTA covers 32 columns x CV_TD disparities
+// of one row for OCG output channels; fl rows y-1..y+1 and the matching fr
+// columns (shifted by every disparity the taps touch) are staged once.
+constexpr int CV_TD = 4;
+
+template <int C, int OC, int OCG>
+__global__ void __launch_bounds__(32 * CV_TD)
+    k_costvol_conv3d_tiled(const float *__restrict__ fl, const float *__restrict__ fr, int D,
+                           int h, int w, const float *__restrict__ wt,
+                           const float *__restrict__ b, float *__restrict__ y) {
+    // fr columns needed: x - d for x in [x0-1, x0+32], d in [d0-1, d0+CV_TD]
+    constexpr int FLW = 34, FRW = 34 + CV_TD + 1;
+    __shared__ float sfl[C][3][FLW];
+    __shared__ float sfr[C][3][FRW];
+    __shared__ float sw[OCG * C * 27];
+    __shared__ float sb[OCG];
+    const int og = blockIdx.z;
+    const int x0 = blockIdx.x * 32, oy = blockIdx.y / ((D + CV_TD - 1) / CV_TD);
+    const int d0 = (blockIdx.y - oy * ((D + CV_TD - 1) / CV_TD)) * CV_TD;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < OCG * C * 27; i += 32 * CV_TD) sw[i] = wt[og * OCG * C * 27 + i];
+    if (tid < OCG) sb[tid] = b[og * OCG + tid];
+    const long hw = (long)h * w;
+    // sfl[c][r][j] = fl[c][oy-1+r][x0-1+j];  sfr[c][r][j] = fr[c][oy-1+r][x0-1-(d0+CV_TD)+j]
+    const int frx0 = x0 - 1 - (d0 + CV_TD);
+    for (int i = tid; i < C * 3 * FLW; i += 32 * CV_TD) {
+        const int c = i / (3 * FLW), rem = i - c * 3 * FLW, r = rem / FLW, j = rem - r * FLW;
+        const int yy = oy - 1 + r, xx = x0 - 1 + j;
+        sfl[c][r][j] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? __ldg(fl + c * hw + yy * w + xx) : 0.f;
+    }
+    for (int i = tid; i < C * 3 * FRW; i += 32 * CV_TD) {
+        const int c = i / (3 * FRW), rem = i - c * 3 * FRW, r = rem / FRW, j = rem - r * FRW;
+        const int yy = oy - 1 + r, xx = frx0 + j;
+        sfr[c][r][j] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? __ldg(fr + c * hw + yy * w + xx) : 0.f;
+    }
+    __syncthreads();
+    const int ox = x0 + threadIdx.x, od = d0 + threadIdx.y;
+    if (ox >= w || od >= D) return;
+    float acc[OCG];
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
+    for (int c = 0; c < C; ++c) {
+#pragma unroll
+        for (int kd = 0; kd < 3; ++kd) {
+            const int dd = od + kd - 1;
+            if (dd < 0 || dd >= D) continue;
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                const int yy = oy + ky - 1;
+                if (yy < 0 || yy >= h) continue;
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) {
+                    const int xx = ox + kx - 1;
+                    if (xx < 0 || xx >= w) continue;
+                    float v;
+                    if (xx - dd < 0) {
+                        v = 2.0f;
+                    } else {
+                        // fl at column xx -> sfl index xx - (x0-1); fr at xx-dd -> xx-dd-frx0
+                        v = fabsf(sfl[c][ky][xx - x0 + 1] - sfr[c][ky][xx - dd - frx0]);
+                    }
+#pragma unroll
+                    for (int o = 0; o < OCG; ++o)
+                        acc[o] = fmaf(v, sw[(o * C + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
+                }
+            }
+        }
+    }
+    const long total = (long)D * hw;
+    const long idx = (long)od * hw + (long)oy * w + ox;
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) {
+        const float v = acc[o];
+        y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
+    }
+}
+
+// Tiled conv3d #2 (same CTA shape): stages x[c][d0-1..d0+CV_TD][y-1..y+1]
+// [x0-1..x0+32], zeros outside the volume.
+template <int IC, int OC, int OCG>
+__global__ void __launch_bounds__(32 * CV_TD)
+    k_conv3d_tiled(const float *__restrict__ x, int D, int h, int w, const float *__restrict__ wt,
+                   const float *__restrict__ b, float *__restrict__ y) {
+    __shared__ float sx[IC][CV_TD + 2][3][34];
+    __shared__ float sw[OCG * IC * 27];
+    __shared__ float sb[OCG];
+    const int og = blockIdx.z;
+    const int nd = (D + CV_TD - 1) / CV_TD;
+    const int x0 = blockIdx.x * 32, oy = blockIdx.y / nd;
+    const int d0 = (blockIdx.y - oy * nd) * CV_TD;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < OCG * IC * 27; i += 32 * CV_TD) sw[i] = wt[og * OCG * IC * 27 + i];
+    if (tid < OCG) sb[tid] = b[og * OCG + tid];
+    const long hw = (long)h * w, total = (long)D * hw;
+    constexpr int PLANE = (CV_TD + 2) * 3 * 34;
+    for (int i = tid; i < IC * PLANE; i += 32 * CV_TD) {
+        const int c = i / PLANE, rem = i - c * PLANE;
+        const int dz = rem / (3 * 34), rem2 = rem - dz * 3 * 34, r = rem2 / 34, j = rem2 - r * 34;
+        const int dd = d0 - 1 + dz, yy = oy - 1 + r, xx = x0 - 1 + j;
+        sx[c][dz][r][j] = (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w)
+                              ? __ldg(x + c * total + dd * hw + yy * w + xx)
+                              : 0.f;
+    }
+    __syncthreads();
+    const int ox = x0 + threadIdx.x, od = d0 + threadIdx.y;
+    if (ox >= w || od >= D) return;
+    float acc[OCG];
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
+#pragma unroll
+    for (int c = 0; c < IC; ++c) {
+#pragma unroll
+        for (int kd = 0; kd < 3; ++kd) {
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                const float *row = &sx[c][threadIdx.y + kd][ky][threadIdx.x];
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) {
+                    const float v = row[kx];
+#pragma unroll
+                    for (int o = 0; o < OCG; ++o)
+                        acc[o] = fmaf(v, sw[(o * IC + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
+                }
+            }
+        }
+    }
+    const long idx = (long)od * hw + (long)oy * w + ox;
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) {
+        const float v = acc[o];
+        y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
+    }
+}
+
 // -------------------------------------------------- cost volume + conv3d #1
 // CostVolume.forward (stereonet.py:771-799) fused into Conv3d #1 (596-641)
 // and its leaky ReLU: each tap of the 3x3x3 window reads |fl - fr(x-d)|
@@ -491,28 +702,32 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
     dim3 blk(32, 8);
     // FeatureNet, both images: c1 s2, c2 s2, c3, c4 (4 output channels per thread)
     constexpr int FG = C % 4 == 0 ? 4 : C;
+    const dim3 tb(CT2_TW, CT2_TH);
+    auto tgrid = [&](int OW, int OH, int z) {
+        return dim3((OW + CT2_TW - 1) / CT2_TW, (OH + CT2_TH - 1) / CT2_TH, z);
+    };
     count_launch();
-    k_conv2d<1, C, FG, 1><<<grid2d(w1, h1, blk, 2 * (C / FG)), blk, 0, st>>>(
+    k_conv2d_tiled<1, C, FG, 1><<<tgrid(w1, h1, 2 * (C / FG)), tb, conv2d_tile_bytes(1, 2, 1), st>>>(
         left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
     count_launch();
-    k_conv2d<C, C, FG, 1><<<grid2d(w, h, blk, 2 * (C / FG)), blk, 0, st>>>(
+    k_conv2d_tiled<C, C, FG, 1><<<tgrid(w, h, 2 * (C / FG)), tb, conv2d_tile_bytes(C, 2, 1), st>>>(
         b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
     count_launch();
-    k_conv2d<C, C, FG, 1><<<grid2d(w, h, blk, 2 * (C / FG)), blk, 0, st>>>(
+    k_conv2d_tiled<C, C, FG, 1><<<tgrid(w, h, 2 * (C / FG)), tb, conv2d_tile_bytes(C, 1, 1), st>>>(
         b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1], nullptr);
     count_launch();
-    k_conv2d<C, C, FG, 0><<<grid2d(w, h, blk, 2 * (C / FG)), blk, 0, st>>>(
+    k_conv2d_tiled<C, C, FG, 0><<<tgrid(w, h, 2 * (C / FG)), tb, conv2d_tile_bytes(C, 1, 1), st>>>(
         b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
     SV_LAUNCH_CHECK();
     // cost volume + CostFilter + soft-argmin (2 output channels per thread)
     constexpr int CG = CM % 2 == 0 ? 2 : CM;
-    const long vox = (long)D * h * w;
+    const dim3 vgrid((w + 31) / 32, h * ((D + CV_TD - 1) / CV_TD), CM / CG);
     count_launch();
-    k_costvol_conv3d<C, CM, CG><<<dim3(grid_for(vox, 128, 1 << 30), CM / CG), 128, 0, st>>>(
+    k_costvol_conv3d_tiled<C, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(
         b.fb[0], b.fb[1], D, h, w, n.cw[0], n.cb[0], b.v0);
     count_launch();
-    k_conv3d<CM, CM, CG><<<dim3(grid_for(vox, 128, 1 << 30), CM / CG), 128, 0, st>>>(
-        b.v0, D, h, w, n.cw[1], n.cb[1], b.v1);
+    k_conv3d_tiled<CM, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(b.v0, D, h, w, n.cw[1],
+                                                                  n.cb[1], b.v1);
     count_launch();
     k_conv3d_softargmin<CM><<<dim3((w + 31) / 32, h), dim3(32, SA_DMAX), 0, st>>>(
         b.v1, D, h, w, n.cw[2], n.cb[2], d0);
@@ -525,7 +740,8 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
     int ph = h, pw = w;
     for (int lv = 0; lv < 2; ++lv) {
         const int Hl = Hs[lv], Wl = Ws[lv];
-        count_launch(); k_upsample_concat<<<grid2d(Wl, Hl, blk), blk, 0, st>>>(prev, ph, pw, Hl, Wl, guides[lv],
+        count_launch();
+        k_upsample_concat<<<grid2d(Wl, Hl, blk), blk, 0, st>>>(prev, ph, pw, Hl, Wl, guides[lv],
                                                               b.rin);
         const float *cur = b.rin;
         float *bufs[2] = {b.ra, b.rb};
@@ -535,17 +751,19 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
             const int dl = n.dil[i];
             count_launch();
             if (i == 0)
-                k_conv2d<2, RC, RG, 1><<<grid2d(Wl, Hl, blk, RC / RG), blk, 0, st>>>(
+                k_conv2d_tiled<2, RC, RG, 1><<<tgrid(Wl, Hl, RC / RG), tb,
+                                               conv2d_tile_bytes(2, 1, dl), st>>>(
                     cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
                     nullptr);
             else
-                k_conv2d<RC, RC, RG, 1><<<grid2d(Wl, Hl, blk, RC / RG), blk, 0, st>>>(
+                k_conv2d_tiled<RC, RC, RG, 1><<<tgrid(Wl, Hl, RC / RG), tb,
+                                                conv2d_tile_bytes(RC, 1, dl), st>>>(
                     cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
                     nullptr);
             cur = dst;
         }
         count_launch();
-        k_conv2d<RC, 1, 1, 2><<<grid2d(Wl, Hl, blk), blk, 0, st>>>(
+        k_conv2d_tiled<RC, 1, 1, 2><<<tgrid(Wl, Hl, 1), tb, conv2d_tile_bytes(RC, 1, 1), st>>>(
             cur, cur, Hl, Wl, Hl, Wl, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
             outs[lv], b.rin);
         SV_LAUNCH_CHECK();

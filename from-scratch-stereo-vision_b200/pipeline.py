@@ -28,6 +28,9 @@ class PairPipeline:
         self.lib = _lib.load()
         self.W, self.H = W, H
         self.dev = torch.device("cuda", torch.cuda.current_device()) if device is None else device
+        # A stream of its own: work on it can be captured, so each predict_auto
+        # pass replays as one CUDA graph after its first run.
+        self.stream = torch.cuda.Stream(device=self.dev)
         self.net = gpu_net(net)
         self.tp = float(self.net.target_peak if target_peak is None else target_peak)
         self.probe_width, self.max_width, self.passes = probe_width, max_width, passes
@@ -53,7 +56,7 @@ class PairPipeline:
 
     # ------------------------------------------------------------------
     def predict(self, stream=None) -> None:
-        s = _stream() if stream is None else stream
+        s = self.stream.cuda_stream if stream is None else stream
         _lib.check(self.lib.sv_predict_auto(
             self.net.handle, _ptr(self.left), _ptr(self.right), self.code, self.W, self.H,
             self.tp, self.probe_width, self.max_width, self.passes, _lib.SV_FP32,
@@ -61,22 +64,26 @@ class PairPipeline:
             ctypes.byref(self._Hw), self._trace, _ptr(self.pws), self.pneed, s), "predict_auto")
 
     def refine(self, stream=None) -> None:
-        self.refiner.run(self.left, self.right, self.disp0, self.out, self.status, stream)
+        self.refiner.run(self.left, self.right, self.disp0, self.out, self.status,
+                         self.stream.cuda_stream if stream is None else stream)
 
     def run_device(self, stream=None) -> None:
-        """predict_auto + lr_refine on the images already in self.left/right."""
+        """predict_auto + lr_refine on the images already in self.left/right
+        (on self.stream unless a stream handle is given)."""
         self.predict(stream)
         self.refine(stream)
 
     def run_host(self, left: torch.Tensor, right: torch.Tensor):
         """End to end from pinned host images: H2D, the path, D2H of the
-        refined disparity and status.  Returns the pinned host tensors."""
-        self.left.copy_(left, non_blocking=True)
-        self.right.copy_(right, non_blocking=True)
-        self.run_device()
-        self.h_out.copy_(self.out, non_blocking=True)
-        self.h_status.copy_(self.status, non_blocking=True)
-        torch.cuda.current_stream().synchronize()
+        refined disparity and status, all on self.stream.  Returns the pinned
+        host tensors."""
+        with torch.cuda.stream(self.stream):
+            self.left.copy_(left, non_blocking=True)
+            self.right.copy_(right, non_blocking=True)
+            self.run_device()
+            self.h_out.copy_(self.out, non_blocking=True)
+            self.h_status.copy_(self.status, non_blocking=True)
+        self.stream.synchronize()
         return self.h_out, self.h_status
 
     @property

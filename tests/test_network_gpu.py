@@ -108,7 +108,13 @@ def test_pipeline_matches_drop_ins(svb, net):
     import torch
     p = svb.synth.config_full()
     pipe = svb.pipeline.PairPipeline(p.W, p.H, net)
-    out, st = pipe.run_host(torch.from_numpy(p.left.ravel()), torch.from_numpy(p.right.ravel()))
+    hl, hr = torch.from_numpy(p.left.ravel()), torch.from_numpy(p.right.ravel())
+    # first run records the passes as CUDA graphs, the second replays them
+    out, st = (t.clone() for t in pipe.run_host(hl, hr))
+    out2, st2 = pipe.run_host(hl, hr)
+    assert np.array_equal(bits(out.numpy()), bits(out2.numpy()))
+    assert np.array_equal(st.numpy(), st2.numpy())
+    # drop-ins on the default stream (no graphs) give the same bits
     df, _, _, _ = svb.network.predict_auto(net, p.left, p.right, p.W, p.H, verbose=False)
     o2, s2 = svb.refine.lr_refine(p.left, p.right, df, p.W, p.H, tol=2.0, R=10, P1=12.0,
                                   P2=150.0, rx=4, ry=3)

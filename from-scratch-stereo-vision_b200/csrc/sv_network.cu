@@ -794,194 +794,5 @@ int launch_forward(const NetView &n, const float *left, const float *right, int 
     return SV_ERR_NET;
 }
 
-// ------------------------------------------------------------- _peak
-// sorted(disp)[int(n*q)] (stereonet.py:3866-3869) by exact radix selection
-// on order-preserving 64-bit keys, digits of 11/11/11/11/11/9 bits from the
-// top.  Signed zeros share one key (they compare equal in the sort, and a
-// zero peak becomes 0.5 anyway).
-//
-// Multi-CTA form: pass p histograms the p-th digit of the keys that match
-// the prefix chosen by passes 0..p-1; every CTA rebuilds that prefix itself
-// from the earlier histograms (a parallel scan over 2048 bins each), so a
-// pass is one launch and no CTA waits on another.  A last one-CTA launch
-// turns the full prefix back into the double.  Small inputs use one CTA for
-// everything.
-constexpr int SEL_BINS = 2048;
-constexpr int SEL_PASSES = 6;
-__constant__ int c_sel_shift[SEL_PASSES] = {53, 42, 31, 20, 9, 0};
-__constant__ int c_sel_bits[SEL_PASSES] = {11, 11, 11, 11, 11, 9};
-
-struct SelState {
-    unsigned long long prefix;
-    long long rank;
-    double value;
-};
-
-__device__ __forceinline__ unsigned long long sel_key(double d) {
-    return ordkey(d == 0.0 ? 0.0 : d);
-}
-
-__device__ __forceinline__ double sel_unkey(unsigned long long k) {
-    unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
-    return __longlong_as_double((long long)b);
-}
-
-// Count element i (if < n and on the current prefix) into cnt[digit].  The
-// first digits are mostly exponent bits, so most lanes of a warp hit the same
-// bin: lanes with equal digits are merged (__match_any_sync) and one atomic
-// per distinct digit is issued.  Called by every lane of the warp.
-__device__ __forceinline__ void sel_count(const double *__restrict__ x, long n, long i,
-                                          unsigned long long pre, int top, int shift,
-                                          unsigned mask, unsigned *cnt) {
-    unsigned digit = 0xffffffffu;
-    if (i < n) {
-        const unsigned long long k = sel_key(x[i]);
-        if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
-    }
-    const unsigned same = __match_any_sync(kFull, digit);
-    if (digit != 0xffffffffu && (threadIdx.x & 31) == __ffs(same) - 1)
-        atomicAdd(&cnt[digit], (unsigned)__popc(same));
-}
-
-// With cnt[] (nb bins) in shared memory and a rank below their total, find
-// the bin holding that rank; every thread returns (bin, rank within bin).
-// Needs blockDim.x == 256 (8 bins per thread).
-__device__ __forceinline__ void sel_find(const unsigned *cnt, long long rank, int *bin,
-                                         long long *rem, long long *sbuf /*33*/) {
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    long long loc = 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) loc += cnt[t * 8 + i];
-    long long x = loc;                                       // inclusive warp scan
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        long long y = __shfl_up_sync(kFull, x, o);
-        if (lane >= o) x += y;
-    }
-    if (lane == 31) sbuf[wid] = x;
-    __syncthreads();
-    if (t == 0) {
-        long long run = 0;
-        for (int w = 0; w < 8; ++w) { long long v = sbuf[w]; sbuf[w] = run; run += v; }
-    }
-    __syncthreads();
-    const long long excl = sbuf[wid] + x - loc;
-    if (rank >= excl && rank < excl + loc) {
-        long long r = rank - excl;
-        int b = t * 8;
-        for (int i = 0; i < 8; ++i, ++b) {
-            if (r < (long long)cnt[b]) break;
-            r -= cnt[b];
-        }
-        sbuf[32] = ((long long)b << 40) | r;                 // r < 2^40
-    }
-    __syncthreads();
-    const long long packed = sbuf[32];
-    *bin = (int)(packed >> 40);
-    *rem = packed & ((1ll << 40) - 1);
-    __syncthreads();
-}
-
-// Rebuild prefix/rank after passes 0..upto-1 from their histograms.
-__device__ __forceinline__ void sel_replay(const unsigned *__restrict__ hist, int upto,
-                                           long long rank0, unsigned *cnt, long long *sbuf,
-                                           unsigned long long *prefix, long long *rank) {
-    unsigned long long pre = 0;
-    long long r = rank0;
-    for (int q = 0; q < upto; ++q) {
-        const int nb = 1 << c_sel_bits[q];
-        for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x)
-            cnt[i] = i < nb ? hist[q * SEL_BINS + i] : 0u;
-        __syncthreads();
-        int b;
-        long long rem;
-        sel_find(cnt, r, &b, &rem, sbuf);
-        pre |= (unsigned long long)b << c_sel_shift[q];
-        r = rem;
-    }
-    *prefix = pre;
-    *rank = r;
-}
-
-__global__ void __launch_bounds__(256)
-    k_sel_pass(const double *__restrict__ x, long n, int pass, long long rank0,
-               unsigned *__restrict__ hist, SelState *__restrict__ out) {
-    __shared__ unsigned cnt[SEL_BINS];
-    __shared__ long long sbuf[33];
-    unsigned long long pre;
-    long long r;
-    sel_replay(hist, pass, rank0, cnt, sbuf, &pre, &r);
-    if (pass == SEL_PASSES) {                                // final: the value
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            out->prefix = pre;
-            out->rank = r;
-            out->value = sel_unkey(pre);
-        }
-        return;
-    }
-    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) cnt[i] = 0u;
-    __syncthreads();
-    const int shift = c_sel_shift[pass], bits = c_sel_bits[pass];
-    const int top = shift + bits;
-    const unsigned mask = (1u << bits) - 1u;
-    const long stride = (long)gridDim.x * blockDim.x;
-    for (long i0 = blockIdx.x * (long)blockDim.x; i0 < n; i0 += stride)
-        sel_count(x, n, i0 + threadIdx.x, pre, top, shift, mask, cnt);
-    __syncthreads();
-    for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x)
-        if (cnt[i]) atomicAdd(&hist[pass * SEL_BINS + i], cnt[i]);
-}
-
-// One CTA, all passes (inputs up to a few tens of thousands of values).
-__global__ void __launch_bounds__(256)
-    k_sel_small(const double *__restrict__ x, long n, long long rank, SelState *__restrict__ out) {
-    __shared__ unsigned cnt[SEL_BINS];
-    __shared__ long long sbuf[33];
-    unsigned long long pre = 0;
-    long long r = rank;
-    for (int p = 0; p < SEL_PASSES; ++p) {
-        for (int i = threadIdx.x; i < SEL_BINS; i += blockDim.x) cnt[i] = 0u;
-        __syncthreads();
-        const int shift = c_sel_shift[p], bits = c_sel_bits[p], top = shift + bits;
-        const unsigned mask = (1u << bits) - 1u;
-        for (long i0 = 0; i0 < n; i0 += blockDim.x)
-            sel_count(x, n, i0 + threadIdx.x, pre, top, shift, mask, cnt);
-        __syncthreads();
-        int b;
-        long long rem;
-        sel_find(cnt, r, &b, &rem, sbuf);
-        pre |= (unsigned long long)b << shift;
-        r = rem;
-    }
-    if (threadIdx.x == 0) {
-        out->prefix = pre;
-        out->rank = r;
-        out->value = sel_unkey(pre);
-    }
-}
-
-int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
-                  cudaStream_t st) {
-    if (n <= 8192) {
-        count_launch();
-        k_sel_small<<<1, 256, 0, st>>>(x, n, rank, state);
-        SV_LAUNCH_CHECK();
-        return SV_OK;
-    }
-    SV_CUDA_TRY(cudaMemsetAsync(hist, 0, SEL_PASSES * SEL_BINS * sizeof(unsigned), st));
-    const int blocks = grid_for(n, 256 * 8, 148);
-    for (int p = 0; p < SEL_PASSES; ++p) {
-        count_launch();
-        k_sel_pass<<<blocks, 256, 0, st>>>(x, n, p, rank, hist, state);
-    }
-    count_launch();
-    k_sel_pass<<<1, 256, 0, st>>>(x, n, SEL_PASSES, rank, hist, state);
-    SV_LAUNCH_CHECK();
-    return SV_OK;
-}
-
-size_t select_state_bytes() { return sizeof(SelState); }
-size_t select_value_offset() { return offsetof(SelState, value); }
-size_t select_hist_words() { return (size_t)SEL_PASSES * SEL_BINS; }
 
 }  // namespace sv

@@ -249,6 +249,181 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// ------------------------------------------------- SGM, thread per scanline
+// For bands up to K = 30 (Kp <= 32) one thread owns a whole scanline: its
+// Kp slots are NR = Kp/2 u16x2 registers, the +-1 neighbour of a slot is a
+// byte_perm of adjacent registers, the path minimum a register reduction,
+// and a one-slot re-centring another byte_perm -- no shuffles, no shared
+// memory, 3-4x fewer instructions per pixel-path than the lane-group kernel
+// and a dozen independent chains per step.  Larger re-centring jumps
+// (depth edges) go through a per-thread local copy.  Same recurrence and
+// same INF conventions as k_sgm_packed.
+constexpr int SGMT_PF = 4;   // prefetch distance in pixels
+
+template <int NR>
+__device__ __forceinline__ void shift_regs(const unsigned (&t)[NR], unsigned (&o)[NR], int s) {
+    if (s == 1) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) o[r] = __byte_perm(t[r], r < NR - 1 ? t[r + 1] : kInf2, 0x5432);
+    } else if (s == -1) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) o[r] = __byte_perm(r > 0 ? t[r - 1] : kInf2, t[r], 0x5432);
+    } else {
+        unsigned short buf[2 * NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            buf[2 * r] = (unsigned short)(t[r] & 0xFFFFu);
+            buf[2 * r + 1] = (unsigned short)(t[r] >> 16);
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const int ia = 2 * r + s, ib = ia + 1;
+            const unsigned lo = (ia >= 0 && ia < 2 * NR) ? buf[ia] : 0x7FFFu;
+            const unsigned hi = (ib >= 0 && ib < 2 * NR) ? buf[ib] : 0x7FFFu;
+            o[r] = lo | (hi << 16);
+        }
+    }
+}
+
+template <int NR, typename LT>
+__global__ void __launch_bounds__(128)
+    k_sgm_thread(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
+                 const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
+                 int H, int K, int P1, int P2, LT *__restrict__ Lout, int npaths,
+                 SgmTasks tasks) {
+    constexpr int Kp = 2 * NR;
+    static_assert(Kp % 8 == 0, "slot rows are 8-byte aligned");
+    constexpr int NW = Kp / 8;                 // 64-bit words per pixel row of costs
+    const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (gid >= tasks.start[tasks.nseg]) return;
+    int sg = 0;
+    while (gid >= tasks.start[sg + 1]) ++sg;
+    const int j0 = (int)(gid - tasks.start[sg]);
+    const int view = tasks.view[sg], dir = tasks.dir[sg];
+    int dx, dy;
+    dir_of(dir, dx, dy);
+    int x0, y0, n;
+    if (dy == 0) {
+        y0 = j0; x0 = dx > 0 ? 0 : W - 1; n = W;
+    } else if (dx == 0) {
+        x0 = j0; y0 = dy > 0 ? 0 : H - 1; n = H;
+    } else {
+        if (j0 < W) {
+            x0 = j0; y0 = dy > 0 ? 0 : H - 1;
+        } else {
+            const int i = j0 - W + 1;
+            x0 = dx > 0 ? 0 : W - 1;
+            y0 = dy > 0 ? i : H - 1 - i;
+        }
+        n = min(dx > 0 ? W - x0 : x0 + 1, dy > 0 ? H - y0 : y0 + 1);
+    }
+    const long N = (long)W * H;
+    const long step = (long)dy * W + dx;
+    const long p0 = (long)y0 * W + x0;
+    const uint2 *__restrict__ Cw =
+        reinterpret_cast<const uint2 *>((view ? C1 : C0) + p0 * Kp);   // row of costs, step +stepKp
+    const long cstep = step * NW;
+    const int32_t *__restrict__ base = (view ? base1 : base0) + p0;
+    LT *__restrict__ Lo = Lout + (long)(view * npaths + dir) * N * Kp + p0 * Kp;
+    const long lstep = step * Kp;
+
+    unsigned vm[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int sa = 2 * r, sb = sa + 1;
+        vm[r] = ((sa >= 1 && sa <= K) ? 0x0000FFFFu : 0u) | ((sb >= 1 && sb <= K) ? 0xFFFF0000u : 0u);
+    }
+    const unsigned P1P1 = (unsigned)P1 * 0x10001u;
+
+    uint2 cring[SGMT_PF][NW];
+    int bring[SGMT_PF];
+#pragma unroll
+    for (int u = 0; u < SGMT_PF; ++u) {
+        if (u < n) {
+            bring[u] = __ldg(base + u * step);
+#pragma unroll
+            for (int wd = 0; wd < NW; ++wd) cring[u][wd] = __ldg(Cw + u * cstep + wd);
+        }
+    }
+    unsigned t_[NR];
+    int mq = 0, bprev = 0;
+    for (int tt = 0; tt < n; tt += SGMT_PF) {
+#pragma unroll
+        for (int u = 0; u < SGMT_PF; ++u) {
+            const int t = tt + u;
+            if (t >= n) break;
+            unsigned c[NR];
+#pragma unroll
+            for (int wd = 0; wd < NW; ++wd) {
+                c[4 * wd + 0] = __byte_perm(cring[u][wd].x, 0, 0x4140);
+                c[4 * wd + 1] = __byte_perm(cring[u][wd].x, 0, 0x4342);
+                c[4 * wd + 2] = __byte_perm(cring[u][wd].y, 0, 0x4140);
+                c[4 * wd + 3] = __byte_perm(cring[u][wd].y, 0, 0x4342);
+            }
+            const int bcur = bring[u];
+            if (t + SGMT_PF < n) {
+                bring[u] = __ldg(base + (t + SGMT_PF) * step);
+#pragma unroll
+                for (int wd = 0; wd < NW; ++wd) cring[u][wd] = __ldg(Cw + (t + SGMT_PF) * cstep + wd);
+            }
+            unsigned L[NR];
+            if (t == 0) {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) L[r] = (c[r] & vm[r]) | (kInf2 & ~vm[r]);
+            } else {
+                const int s = bcur - bprev;
+                unsigned ts[NR];
+                if (s == 0) {
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) ts[r] = t_[r];
+                } else {
+                    shift_regs<NR>(t_, ts, max(-Kp - 2, min(Kp + 2, s)));
+                }
+                const unsigned cap = (unsigned)(mq + P2) * 0x10001u;
+                const unsigned mm = (unsigned)mq * 0x10001u;
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    const unsigned v = c[r] + __vminu2(ts[r], cap) - mm;
+                    L[r] = (v & vm[r]) | (kInf2 & ~vm[r]);
+                }
+            }
+            bprev = bcur;
+            unsigned m2 = L[0];
+#pragma unroll
+            for (int r = 1; r < NR; ++r) m2 = __vminu2(m2, L[r]);
+            mq = (int)min(m2 & 0xFFFFu, m2 >> 16);
+            // store the pixel's path costs, padding slots as 0
+            LT *dst = Lo + t * lstep;
+            if (sizeof(LT) == 1) {
+#pragma unroll
+                for (int wd = 0; wd < NW; ++wd) {
+                    uint2 v;
+                    v.x = __byte_perm(L[4 * wd] & vm[4 * wd], L[4 * wd + 1] & vm[4 * wd + 1], 0x6420);
+                    v.y = __byte_perm(L[4 * wd + 2] & vm[4 * wd + 2], L[4 * wd + 3] & vm[4 * wd + 3],
+                                      0x6420);
+                    reinterpret_cast<uint2 *>(dst)[wd] = v;
+                }
+            } else {
+#pragma unroll
+                for (int wd = 0; wd < NW; ++wd) {
+                    uint4 v;
+                    v.x = L[4 * wd] & vm[4 * wd];
+                    v.y = L[4 * wd + 1] & vm[4 * wd + 1];
+                    v.z = L[4 * wd + 2] & vm[4 * wd + 2];
+                    v.w = L[4 * wd + 3] & vm[4 * wd + 3];
+                    reinterpret_cast<uint4 *>(dst)[wd] = v;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const unsigned lm = __byte_perm(r > 0 ? L[r - 1] : kInf2, L[r], 0x5432);
+                const unsigned lp = __byte_perm(L[r], r < NR - 1 ? L[r + 1] : kInf2, 0x5432);
+                t_[r] = __vimin3_u16x2(L[r], lm + P1P1, lp + P1P1);
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ WTA
 template <typename LT>
 __device__ __forceinline__ int path_sum_slot(const LT *__restrict__ L, long stride, int npaths,
@@ -385,11 +560,32 @@ static int sgm_packed_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0
     return SV_OK;
 }
 
+template <int NR, typename LT>
+static int sgm_thread_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
+                         const int32_t *b1, int W, int H, int K, int P1, int P2, void *Lout,
+                         int npaths, const SgmTasks &t, cudaStream_t st) {
+    const long threads = t.start[t.nseg];
+    const int blocks = (int)((threads + 127) / 128);
+    count_launch();
+    k_sgm_thread<NR, LT><<<blocks, 128, 0, st>>>(C0, C1, b0, b1, W, H, K, P1, P2, (LT *)Lout,
+                                                  npaths, t);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
 template <typename LT>
 static int sgm_packed_dispatch(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
                                const int32_t *b1, int W, int H, int K, int P1, int P2,
                                void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
     const SgmGeom g = geom_for(K);
+    // bands up to K = 30: one thread per scanline
+    switch (g.Kp) {
+    case 8: return sgm_thread_go<4, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+    case 16: return sgm_thread_go<8, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+    case 24: return sgm_thread_go<12, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+    case 32: return sgm_thread_go<16, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+    default: break;
+    }
 #define SV_GEOM(KP, LPV, NRV)                                                                \
     if (g.Kp == KP)                                                                          \
         return sgm_packed_go<NRV, LPV, LT>(C0, C1, b0, b1, W, H, K, KP, P1, P2, Lout, npaths, \

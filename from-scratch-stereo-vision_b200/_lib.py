@@ -55,6 +55,8 @@ SIGNATURES = {
     "sv_lr_refine_timed": (_I, [_VP, _VP, _I, _VP, _I, _I, _D, _PRM, _VP, _VP, _VP, _SZ, _VP,
                                 ctypes.POINTER(_VP), _I]),
     "sv_refine_fullres_noalloc": (_I, [_VP, _VP, _I, _VP, _I, _I, _PRM, _VP, _VP, _VP]),
+    "sv_batch_lr_refine_workspace_size": (_SZ, [_VP, _I, _PRM]),
+    "sv_batch_lr_refine": (_I, [_VP, _I, _I, _D, _PRM, _VP, _SZ, _VP]),
     "sv_net_create": (_I, [_VP, _I, _VP, ctypes.c_long, ctypes.POINTER(_VP)]),
     "sv_net_destroy": (None, [_VP]),
     "sv_resize": (_I, [_VP, _I, _I, _I, _I, _VP, _VP]),

@@ -30,13 +30,7 @@ void set_error(const char *fmt, ...) {
 }
 
 // Validated refinement parameters.
-struct RefineCfg {
-    int R, K, P1, P2, rx, ry, nbits, npaths, invalid;
-    double uniq;
-    bool l16;
-};
-
-static int check_refine(int W, int H, const sv_refine_params *p, bool rows, RefineCfg *c) {
+int check_refine(int W, int H, const sv_refine_params *p, bool rows, RefineCfg *c) {
     if (!p) { set_error("params is NULL"); return SV_ERR_NULL; }
     if (W < 1 || H < 1) { set_error("W=%d H=%d must be positive", W, H); return SV_ERR_SHAPE; }
     if (rows && W > kMaxRowW) {
@@ -110,7 +104,7 @@ static size_t carve_refine(void *ws, int W, int H, const RefineCfg &c, int nview
     return cv.off;
 }
 
-static int check_ws(void *ws, size_t have, size_t need) {
+int check_ws(void *ws, size_t have, size_t need) {
     if (!ws) { set_error("workspace is NULL"); return SV_ERR_WORKSPACE; }
     if ((uintptr_t)ws & 255) { set_error("workspace must be 256-byte aligned"); return SV_ERR_WORKSPACE; }
     if (have < need) {

@@ -51,15 +51,11 @@ __global__ void k_base(const double *__restrict__ disp0, long N,
 // the top bit, exactly as the reference builds its Python int.
 constexpr int CT_W = 32, CT_H = 8;
 
+// One CT_W x CT_H tile starting at (tx0, ty0), called by a whole CTA.
 template <typename T>
-__global__ void __launch_bounds__(CT_W *CT_H)
-    k_census(const T *__restrict__ img0, const T *__restrict__ img1, int W, int H,
-             int rx, int ry, uint64_t *__restrict__ out0, uint64_t *__restrict__ out1) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *tile = reinterpret_cast<T *>(smem_raw);
-    const T *img = blockIdx.z ? img1 : img0;
-    uint64_t *out = blockIdx.z ? out1 : out0;
-    const int tx0 = blockIdx.x * CT_W, ty0 = blockIdx.y * CT_H;
+__device__ __forceinline__ void census_tile(const T *__restrict__ img, int W, int H, int rx,
+                                            int ry, uint64_t *__restrict__ out, int tx0,
+                                            int ty0, T *tile) {
     const int sw = CT_W + 2 * rx, sh = CT_H + 2 * ry;
     const int tid = threadIdx.y * CT_W + threadIdx.x;
     for (int i = tid; i < sw * sh; i += CT_W * CT_H) {
@@ -82,6 +78,15 @@ __global__ void __launch_bounds__(CT_W *CT_H)
         }
     }
     out[(long)y * W + x] = s;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CT_W *CT_H)
+    k_census(const T *__restrict__ img0, const T *__restrict__ img1, int W, int H,
+             int rx, int ry, uint64_t *__restrict__ out0, uint64_t *__restrict__ out1) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    census_tile<T>(blockIdx.z ? img1 : img0, W, H, rx, ry, blockIdx.z ? out1 : out0,
+                   blockIdx.x * CT_W, blockIdx.y * CT_H, reinterpret_cast<T *>(smem_raw));
 }
 
 // ------------------------------------------------------------ band costs
@@ -296,16 +301,14 @@ __global__ void __launch_bounds__(256)
 // sentinels, 0.0 when neither exists; within a run of holes the reference's
 // in-place update gives every hole that same value.  base of the result is
 // written too (the right view's band centre).
-__global__ void __launch_bounds__(256)
-    k_left_to_right(const double *__restrict__ dl, int W, double *__restrict__ dr,
-                    int32_t *__restrict__ base_r) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// One row, called by a whole CTA; smem_raw holds 13*W bytes, sbuf 32 ints.
+__device__ __forceinline__ void l2r_row(const double *__restrict__ row, int W,
+                                        double *__restrict__ dr_row,
+                                        int32_t *__restrict__ base_row,
+                                        unsigned char *smem_raw, int *sbuf) {
     unsigned long long *key = reinterpret_cast<unsigned long long *>(smem_raw);
     int *win = reinterpret_cast<int *>(key + W);
     unsigned char *hole = reinterpret_cast<unsigned char *>(win + W);
-    __shared__ int sbuf[32];
-    const long r = (long)blockIdx.x * W;
-    const double *row = dl + r;
     for (int x = threadIdx.x; x < W; x += blockDim.x) {
         key[x] = 0ull;
         win[x] = INT_MAX;
@@ -357,12 +360,21 @@ __global__ void __launch_bounds__(256)
         } else {
             pv = x;
         }
-        dr[r + x] = v;
-        if (base_r) {
+        dr_row[x] = v;
+        if (base_row) {
             int b = __double2int_rz(__dadd_rn(v, 0.5));
-            base_r[r + x] = b > 0 ? b : 0;
+            base_row[x] = b > 0 ? b : 0;
         }
     }
+}
+
+__global__ void __launch_bounds__(256)
+    k_left_to_right(const double *__restrict__ dl, int W, double *__restrict__ dr,
+                    int32_t *__restrict__ base_r) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int sbuf[32];
+    const long r = (long)blockIdx.x * W;
+    l2r_row(dl + r, W, dr + r, base_r ? base_r + r : nullptr, smem_raw, sbuf);
 }
 
 // ------------------------------------------------------------- LR check
@@ -370,16 +382,17 @@ __global__ void __launch_bounds__(256)
 // mismatches (2) take disp0; occlusions (1) take min(out of the nearest
 // non-occluded pixel left / right), 1e9 sentinels, disp0 when neither exists.
 // The fill reads only non-occluded pixels, so order does not matter.
-__global__ void __launch_bounds__(256)
-    k_lr_check(const double *__restrict__ dl, const double *__restrict__ drr,
-               const double *__restrict__ disp0, int W, double tol,
-               double *__restrict__ out, uint8_t *__restrict__ status) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+// One row (all pointers at the row start), called by a whole CTA; smem_raw
+// holds 13*W bytes, sbuf 32 ints.
+__device__ __forceinline__ void lr_row(const double *__restrict__ dl,
+                                       const double *__restrict__ drr,
+                                       const double *__restrict__ disp0, int W, double tol,
+                                       double *__restrict__ out, uint8_t *__restrict__ status,
+                                       unsigned char *smem_raw, int *sbuf) {
     double *val = reinterpret_cast<double *>(smem_raw);
     int *nxt = reinterpret_cast<int *>(val + W);
     unsigned char *st = reinterpret_cast<unsigned char *>(nxt + W);
-    __shared__ int sbuf[32];
-    const long r = (long)blockIdx.x * W;
+    const long r = 0;
     for (int x = threadIdx.x; x < W; x += blockDim.x) {
         double d = dl[r + x];
         int xr = __double2int_rz(__dadd_rn(__dsub_rn((double)x, d), 0.5));
@@ -420,6 +433,16 @@ __global__ void __launch_bounds__(256)
         out[r + x] = v;
         status[r + x] = st[x];
     }
+}
+
+__global__ void __launch_bounds__(256)
+    k_lr_check(const double *__restrict__ dl, const double *__restrict__ drr,
+               const double *__restrict__ disp0, int W, double tol,
+               double *__restrict__ out, uint8_t *__restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int sbuf[32];
+    const long r = (long)blockIdx.x * W;
+    lr_row(dl + r, drr + r, disp0 + r, W, tol, out + r, status + r, smem_raw, sbuf);
 }
 
 // ====================================================================
@@ -524,6 +547,98 @@ int launch_lr_check(const double *dl, const double *dr, const double *disp0, int
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
     count_launch(); k_lr_check<<<H, 256, smem, st>>>(dl, dr, disp0, W, tol, out, status);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+// ====================================================================
+// Batched lr_refine, front and back: one launch per stage over every pair.
+// A block finds its pair (and its row / tile / pixel chunk) in the prefix
+// tables of BatchTables and runs the same per-row / per-tile code as the
+// single-pair kernels above.
+// ====================================================================
+
+__global__ void __launch_bounds__(256) k_b_base(BatchTables t) {
+    const int i = batch_find(t.px_blk, t.n, blockIdx.x);
+    const BatchPair &P = t.pairs[i];
+    const long N = (long)P.W * P.H;
+    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * kBatchPxPerBlock;
+    const long p1 = min(N, p0 + kBatchPxPerBlock);
+    for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        const double d = P.disp0[p];
+        int b = 0;
+        if (!(fabs(d) < 1073741824.0)) {
+            flag_error(t.flag, SV_ERR_DISP);
+        } else {
+            const int v = __double2int_rz(__dadd_rn(d, 0.5));
+            b = v > 0 ? v : 0;
+        }
+        P.base0[p] = b;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_b_left_to_right(BatchTables t) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int sbuf[32];
+    const int i = batch_find(t.row_blk, t.n, blockIdx.x);
+    const BatchPair &P = t.pairs[i];
+    const long r = (long)(blockIdx.x - t.row_blk[i]) * P.W;
+    l2r_row(P.disp0 + r, P.W, P.d0r + r, P.base1 + r, smem_raw, sbuf);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CT_W *CT_H) k_b_census(BatchTables t) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int i = batch_find(t.tile_blk, t.n, blockIdx.x);
+    const BatchPair &P = t.pairs[i];
+    const int tiles_x = (P.W + CT_W - 1) / CT_W;
+    const int tl = (int)(blockIdx.x - t.tile_blk[i]);
+    const int ty = tl / tiles_x, tx = tl - ty * tiles_x;
+    census_tile<T>(reinterpret_cast<const T *>(blockIdx.z ? P.right : P.left), P.W, P.H, t.rx,
+                   t.ry, blockIdx.z ? P.cen1 : P.cen0, tx * CT_W, ty * CT_H,
+                   reinterpret_cast<T *>(smem_raw));
+}
+
+__global__ void __launch_bounds__(256) k_b_lr_check(BatchTables t) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int sbuf[32];
+    const int i = batch_find(t.row_blk, t.n, blockIdx.x);
+    const BatchPair &P = t.pairs[i];
+    const long r = (long)(blockIdx.x - t.row_blk[i]) * P.W;
+    lr_row(P.dl + r, P.dr + r, P.disp0 + r, P.W, t.tol, P.out + r, P.status + r, smem_raw, sbuf);
+}
+
+int launch_batch_front(const BatchTables &t, long long px_blocks, long long rows,
+                       long long tiles, cudaStream_t st) {
+    count_launch();
+    k_b_base<<<(unsigned)px_blocks, 256, 0, st>>>(t);
+    const size_t row_smem = (size_t)t.maxW * (8 + 4 + 1) + 16;
+    if (row_smem > 48 * 1024)
+        SV_CUDA_TRY(cudaFuncSetAttribute(k_b_left_to_right,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)row_smem));
+    count_launch();
+    k_b_left_to_right<<<(unsigned)rows, 256, row_smem, st>>>(t);
+    const size_t cells = (size_t)(CT_W + 2 * t.rx) * (CT_H + 2 * t.ry);
+    const dim3 g((unsigned)tiles, 1, 2), blk(CT_W, CT_H);
+    count_launch();
+    switch (t.dtype) {
+    case SV_U8: k_b_census<uint8_t><<<g, blk, cells, st>>>(t); break;
+    case SV_F32: k_b_census<float><<<g, blk, cells * 4, st>>>(t); break;
+    case SV_F64: k_b_census<double><<<g, blk, cells * 8, st>>>(t); break;
+    default: set_error("unknown image dtype %d", t.dtype); return SV_ERR_PARAM;
+    }
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_batch_back(const BatchTables &t, long long rows, cudaStream_t st) {
+    const size_t row_smem = (size_t)t.maxW * (8 + 4 + 1) + 16;
+    if (row_smem > 48 * 1024)
+        SV_CUDA_TRY(cudaFuncSetAttribute(k_b_lr_check, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)row_smem));
+    count_launch();
+    k_b_lr_check<<<(unsigned)rows, 256, row_smem, st>>>(t);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

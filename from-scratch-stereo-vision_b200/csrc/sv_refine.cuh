@@ -48,6 +48,64 @@ inline SgmTasks make_sgm_tasks(int W, int H, int nviews, int npaths, const int *
 // slots rounded up to a multiple of 8).
 int slot_width(int K);
 
+// Validated refinement parameters (sv_api.cu).
+struct RefineCfg {
+    int R, K, P1, P2, rx, ry, nbits, npaths, invalid;
+    double uniq;
+    bool l16;
+};
+int check_refine(int W, int H, const sv_refine_params *p, bool rows, RefineCfg *c);
+int check_ws(void *ws, size_t have, size_t need);
+
+// ------------------------------------------------------------- batches
+// One pair of a batched lr_refine: its inputs/outputs and its slice of the
+// workspace (device table entry).
+struct BatchPair {
+    const void *left, *right;
+    const double *disp0;
+    double *out;
+    uint8_t *status;
+    int W, H;
+    int32_t *base0, *base1;
+    double *d0r, *dl, *dr;
+    uint64_t *cen0, *cen1;
+    uint8_t *C0, *C1;
+    void *L;
+};
+
+constexpr int kBatchPxPerBlock = 2048;   // pixels per block of the per-pixel kernels
+
+// Everything a batched kernel needs, passed by value.  Prefix tables map a
+// block (or an SGM task) to its pair by binary search.
+struct BatchTables {
+    const BatchPair *pairs;
+    int n;
+    const long long *px_blk;     // [n+1] blocks of kBatchPxPerBlock pixels
+    const long long *row_blk;    // [n+1] image rows
+    const long long *tile_blk;   // [n+1] census tiles
+    const long long *seg_start;  // [nseg+1] scanlines per (pair, view, dir) segment
+    const int *seg_pair;         // [nseg]
+    const int *seg_vd;           // [nseg] view * 8 + dir
+    int nseg;
+    int *queue;                  // SGM task counter, zeroed per call
+    int *flag;                   // data errors (first wins)
+    int R, K, Kp, P1, P2, npaths, invalid, rx, ry, dtype, maxW;
+    double tol, uniq;
+};
+
+// Largest i in [0, n) with prefix[i] <= v (prefix is non-decreasing).
+__device__ __forceinline__ int batch_find(const long long *prefix, int n, long long v) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+int launch_batch_refine(const BatchTables &t, long long px_blocks, long long rows,
+                        long long tiles, long long tasks, bool l16, cudaStream_t st);
+
 int launch_base(const double *disp0, long N, int32_t *base, int *flag, cudaStream_t st);
 int launch_census(const void *img0, const void *img1, int dtype, int W, int H, int rx,
                   int ry, uint64_t *out0, uint64_t *out1, cudaStream_t st);

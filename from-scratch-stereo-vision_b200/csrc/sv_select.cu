@@ -4,13 +4,11 @@
 // Exact selection on order-preserving 64-bit keys of the FP64 values (signed
 // zeros share one key: they compare equal in the sort, and a zero peak is
 // replaced by 0.5 anyway).
-//  * n <= 4096 (the 64-pixel probe): one CTA bitonic-sorts the keys in shared
-//    memory and reads element `rank`.
-//  * larger maps: four passes over 16-bit digits from the top.  Pass p is a
-//    histogram of digit p over the keys that match the prefix chosen so far
-//    (warp-aggregated atomics into a 65536-bin global histogram), followed
-//    by a one-CTA parallel scan that picks the bin holding the rank and
-//    extends the prefix.  After pass 3 the prefix is the key.
+//  Four passes over 16-bit digits from the top.  Pass p is a
+//  histogram of digit p over the keys that match the prefix chosen so far
+//  (warp-aggregated atomics into a 65536-bin global histogram), followed by
+//  a one-CTA parallel scan that picks the bin holding the rank and extends
+//  the prefix.  After pass 3 the prefix is the key.
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
@@ -20,7 +18,6 @@ namespace sv {
 constexpr int SEL_DIGIT = 16;
 constexpr int SEL_NB = 1 << SEL_DIGIT;
 constexpr int SEL_NPASS = 4;
-constexpr int SEL_SMALL = 4096;
 
 struct SelState {
     unsigned long long prefix;
@@ -35,38 +32,6 @@ __device__ __forceinline__ unsigned long long sel_key(double d) {
 __device__ __forceinline__ double sel_unkey(unsigned long long k) {
     const unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
     return __longlong_as_double((long long)b);
-}
-
-// ------------------------------------------------------- small: bitonic
-__global__ void __launch_bounds__(1024)
-    k_sel_sort(const double *__restrict__ x, long n, long long rank, SelState *__restrict__ out) {
-    __shared__ unsigned long long key[SEL_SMALL];
-    int m = 1;
-    while (m < n) m <<= 1;
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        key[i] = i < n ? sel_key(x[i]) : ~0ull;
-    __syncthreads();
-    for (int k = 2; k <= m; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < m; i += blockDim.x) {
-                const int l = i ^ j;
-                if (l > i) {
-                    const unsigned long long a = key[i], b = key[l];
-                    const bool up = (i & k) == 0;
-                    if ((a > b) == up) {
-                        key[i] = b;
-                        key[l] = a;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    if (threadIdx.x == 0) {
-        out->prefix = key[rank];
-        out->rank = 0;
-        out->value = sel_unkey(key[rank]);
-    }
 }
 
 // ---------------------------------------------------- large: 16-bit radix
@@ -130,34 +95,37 @@ __global__ void __launch_bounds__(1024)
     __syncthreads();
     const long long rank = s->rank;
     const long long excl = (long long)(warp_tot[wid] + x - loc);
-    if (rank >= excl && rank < excl + (long long)loc) {
-        long long r = rank - excl;
-        int b = t * 64;
-        for (int i = 0; i < 64; ++i, ++b) {
-            const long long c = hist[b];
-            if (r < c) break;
-            r -= c;
-        }
-        found[0] = b;
-        found[1] = r;
+    if (rank >= excl && rank < excl + (long long)loc) {        // exactly one thread
+        found[0] = t;
+        found[1] = rank - excl;
     }
     __syncthreads();
-    if (t == 0) {
-        const int shift = 64 - SEL_DIGIT * (pass + 1);
-        s->prefix |= (unsigned long long)found[0] << shift;
-        s->rank = found[1];
-        if (pass == SEL_NPASS - 1) s->value = sel_unkey(s->prefix);
+    // warp 0 finds the bin inside the owner's 64 (two per lane)
+    if (wid == 0) {
+        const int owner = (int)found[0];
+        const long long r = found[1];
+        const uint2 c2 = reinterpret_cast<const uint2 *>(hist)[owner * 32 + lane];
+        const unsigned long long c = (unsigned long long)c2.x + c2.y;
+        unsigned long long inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const long long ex = (long long)(inc - c);
+        if (r >= ex && r < ex + (long long)c) {
+            const long long rr = r - ex;
+            const int b = owner * 64 + lane * 2 + (rr < (long long)c2.x ? 0 : 1);
+            const int shift = 64 - SEL_DIGIT * (pass + 1);
+            s->prefix |= (unsigned long long)b << shift;
+            s->rank = rr < (long long)c2.x ? rr : rr - c2.x;
+            if (pass == SEL_NPASS - 1) s->value = sel_unkey(s->prefix);
+        }
     }
 }
 
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st) {
-    if (n <= SEL_SMALL) {
-        count_launch();
-        k_sel_sort<<<1, 1024, 0, st>>>(x, n, rank, state);
-        SV_LAUNCH_CHECK();
-        return SV_OK;
-    }
     SV_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)SEL_NPASS * SEL_NB * sizeof(unsigned), st));
     count_launch();
     k_sel_init<<<1, 1, 0, st>>>(state, rank);

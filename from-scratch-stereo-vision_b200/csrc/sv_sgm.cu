@@ -41,7 +41,39 @@ __device__ __forceinline__ void dir_of(int d, int &dx, int &dy) {
 }
 
 // ----------------------------------------------------------- band costs
-// One thread per pixel writes its Kp slots (slot 0 and padding are 0).
+// The Kp slots of pixel p (slot 0 and padding are 0).
+__device__ __forceinline__ void cost_pixel_slot(const uint64_t *__restrict__ ref,
+                                                const uint64_t *__restrict__ oth,
+                                                const int32_t *__restrict__ base, int W, long p,
+                                                int R, int K, int Kp, int invalid, int view,
+                                                uint8_t *__restrict__ C) {
+    const int x = (int)(p % W);
+    const uint64_t a = ref[p];
+    const int b = base[p] - R;
+    uint64_t *dst = reinterpret_cast<uint64_t *>(C + p * Kp);
+    for (int c = 0; c < Kp; c += 8) {
+        uint64_t word = 0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int k = c + u - 1;
+            uint64_t v = 0;
+            if (k >= 0 && k < K) {
+                const int d = b + k;
+                int cost = invalid;
+                if (view == 0) {
+                    if (d >= 0 && x - d >= 0) cost = __popcll(a ^ oth[p - d]);
+                } else {
+                    if (d >= 0 && x + d <= W - 1) cost = __popcll(a ^ oth[p + d]);
+                }
+                v = (uint64_t)cost;
+            }
+            word |= v << (8 * u);
+        }
+        dst[c >> 3] = word;
+    }
+}
+
+// One thread per pixel writes its Kp slots.
 __global__ void __launch_bounds__(256)
     k_band_costs_slot(const uint64_t *__restrict__ cl, const uint64_t *__restrict__ cr,
                       const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
@@ -53,32 +85,8 @@ __global__ void __launch_bounds__(256)
     const int32_t *base = view ? base1 : base0;
     uint8_t *C = view ? C1 : C0;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < N;
-         p += (long)gridDim.x * blockDim.x) {
-        const int x = (int)(p % W);
-        const uint64_t a = ref[p];
-        const int b = base[p] - R;
-        uint64_t *dst = reinterpret_cast<uint64_t *>(C + p * Kp);
-        for (int c = 0; c < Kp; c += 8) {
-            uint64_t word = 0;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int k = c + u - 1;
-                uint64_t v = 0;
-                if (k >= 0 && k < K) {
-                    const int d = b + k;
-                    int cost = invalid;
-                    if (view == 0) {
-                        if (d >= 0 && x - d >= 0) cost = __popcll(a ^ oth[p - d]);
-                    } else {
-                        if (d >= 0 && x + d <= W - 1) cost = __popcll(a ^ oth[p + d]);
-                    }
-                    v = (uint64_t)cost;
-                }
-                word |= v << (8 * u);
-            }
-            dst[c >> 3] = word;
-        }
-    }
+         p += (long)gridDim.x * blockDim.x)
+        cost_pixel_slot(ref, oth, base, W, p, R, K, Kp, invalid, view, C);
 }
 
 // ------------------------------------------------------------------ SGM
@@ -285,24 +293,9 @@ __device__ __forceinline__ void shift_regs(const unsigned (&t)[NR], unsigned (&o
     }
 }
 
-template <int NR, typename LT>
-__global__ void __launch_bounds__(128)
-    k_sgm_thread(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
-                 const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
-                 int H, int K, int P1, int P2, LT *__restrict__ Lout, int npaths,
-                 SgmTasks tasks) {
-    constexpr int Kp = 2 * NR;
-    static_assert(Kp % 8 == 0, "slot rows are 8-byte aligned");
-    constexpr int NW = Kp / 8;                 // 64-bit words per pixel row of costs
-    const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (gid >= tasks.start[tasks.nseg]) return;
-    int sg = 0;
-    while (gid >= tasks.start[sg + 1]) ++sg;
-    const int j0 = (int)(gid - tasks.start[sg]);
-    const int view = tasks.view[sg], dir = tasks.dir[sg];
-    int dx, dy;
-    dir_of(dir, dx, dy);
-    int x0, y0, n;
+// Start pixel and length of scanline j0 of direction (dx, dy) in a W x H image.
+__device__ __forceinline__ void scanline_of(int W, int H, int dx, int dy, int j0, int &x0,
+                                            int &y0, int &n) {
     if (dy == 0) {
         y0 = j0; x0 = dx > 0 ? 0 : W - 1; n = W;
     } else if (dx == 0) {
@@ -317,14 +310,24 @@ __global__ void __launch_bounds__(128)
         }
         n = min(dx > 0 ? W - x0 : x0 + 1, dy > 0 ? H - y0 : y0 + 1);
     }
-    const long N = (long)W * H;
+}
+
+// One scanline swept by one thread.  Cimg / base / Lo are the costs, band
+// centres and path-cost array of one view (and one direction for Lo).
+template <int NR, typename LT>
+__device__ __forceinline__ void sgm_line_thread(const uint8_t *__restrict__ Cimg,
+                                                const int32_t *__restrict__ base_img,
+                                                LT *__restrict__ Lo_img, int W, int K, int P1,
+                                                int P2, int dx, int dy, int x0, int y0, int n) {
+    constexpr int Kp = 2 * NR;
+    static_assert(Kp % 8 == 0, "slot rows are 8-byte aligned");
+    constexpr int NW = Kp / 8;                 // 64-bit words per pixel row of costs
     const long step = (long)dy * W + dx;
     const long p0 = (long)y0 * W + x0;
-    const uint2 *__restrict__ Cw =
-        reinterpret_cast<const uint2 *>((view ? C1 : C0) + p0 * Kp);   // row of costs, step +stepKp
+    const uint2 *__restrict__ Cw = reinterpret_cast<const uint2 *>(Cimg + p0 * Kp);
     const long cstep = step * NW;
-    const int32_t *__restrict__ base = (view ? base1 : base0) + p0;
-    LT *__restrict__ Lo = Lout + (long)(view * npaths + dir) * N * Kp + p0 * Kp;
+    const int32_t *__restrict__ base = base_img + p0;
+    LT *__restrict__ Lo = Lo_img + p0 * Kp;
     const long lstep = step * Kp;
 
     unsigned vm[NR];
@@ -424,6 +427,28 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+template <int NR, typename LT>
+__global__ void __launch_bounds__(128)
+    k_sgm_thread(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
+                 const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
+                 int H, int K, int P1, int P2, LT *__restrict__ Lout, int npaths,
+                 SgmTasks tasks) {
+    constexpr int Kp = 2 * NR;
+    const long gid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (gid >= tasks.start[tasks.nseg]) return;
+    int sg = 0;
+    while (gid >= tasks.start[sg + 1]) ++sg;
+    const int j0 = (int)(gid - tasks.start[sg]);
+    const int view = tasks.view[sg], dir = tasks.dir[sg];
+    int dx, dy, x0, y0, n;
+    dir_of(dir, dx, dy);
+    scanline_of(W, H, dx, dy, j0, x0, y0, n);
+    const long N = (long)W * H;
+    sgm_line_thread<NR, LT>(view ? C1 : C0, view ? base1 : base0,
+                            Lout + (long)(view * npaths + dir) * N * Kp, W, K, P1, P2, dx, dy,
+                            x0, y0, n);
+}
+
 // ------------------------------------------------------------------ WTA
 template <typename LT>
 __device__ __forceinline__ int path_sum_slot(const LT *__restrict__ L, long stride, int npaths,
@@ -434,19 +459,41 @@ __device__ __forceinline__ int path_sum_slot(const LT *__restrict__ L, long stri
 }
 
 template <typename LT>
+__device__ __forceinline__ void wta_pixel(const LT *__restrict__ Lp, long stride, int npaths,
+                                          int K, int Kp, int R, int32_t base_p,
+                                          const double *__restrict__ d0p, double uniq,
+                                          bool want_conf, double *__restrict__ outp,
+                                          double *__restrict__ confp);
+
+template <typename LT>
 __global__ void __launch_bounds__(256)
     k_wta_slot(const LT *__restrict__ Lall, int npaths, int nviews, long N, int K, int Kp, int R,
                const int32_t *__restrict__ base0, const int32_t *__restrict__ base1,
                const double *__restrict__ d00, const double *__restrict__ d01, double uniq,
                int want_conf, double *__restrict__ out0, double *__restrict__ out1,
                double *__restrict__ conf0) {
-    constexpr int PER64 = 8 / sizeof(LT);                  // slots per 64-bit load
     const long stride = N * Kp;                            // between path arrays
     for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < nviews * N;
          w += (long)gridDim.x * blockDim.x) {
         const int view = (int)(w / N);
         const long p = w - view * N;
-        const LT *Lp = Lall + (long)view * npaths * stride + p * Kp;
+        wta_pixel<LT>(Lall + (long)view * npaths * stride + p * Kp, stride, npaths, K, Kp, R,
+                      (view ? base1 : base0)[p], (view ? d01 : d00) + p, uniq,
+                      want_conf && view == 0, (view ? out1 : out0) + p,
+                      conf0 ? conf0 + p : nullptr);
+    }
+}
+
+// S = sum of the path costs at one pixel (Lp: its row in path array 0),
+// first minimum, FP64 parabola (stereonet.py:5271-5303).
+template <typename LT>
+__device__ __forceinline__ void wta_pixel(const LT *__restrict__ Lp, long stride, int npaths,
+                                          int K, int Kp, int R, int32_t base_p,
+                                          const double *__restrict__ d0p, double uniq,
+                                          bool want_conf, double *__restrict__ outp,
+                                          double *__restrict__ confp) {
+    constexpr int PER64 = 8 / sizeof(LT);                  // slots per 64-bit load
+    {
         int bv = 0x7FFFFFFF, bs = -1;                      // best value, its slot
         for (int c = 0; c < Kp; c += 8) {
             unsigned acc[4] = {0u, 0u, 0u, 0u};            // 8 slots as u16x2
@@ -476,12 +523,10 @@ __global__ void __launch_bounds__(256)
             }
         }
         const int bk = bs - 1;
-        const double *d0 = view ? d01 : d00;
-        double *out = view ? out1 : out0;
         if (bk == 0 || bk == K - 1) {
-            out[p] = d0[p];
-            if (want_conf && view == 0) conf0[p] = 0.0;
-            continue;
+            *outp = *d0p;
+            if (want_conf) *confp = 0.0;
+            return;
         }
         const int va = path_sum_slot(Lp, stride, npaths, bs - 1);
         const int vb = path_sum_slot(Lp, stride, npaths, bs + 1);
@@ -496,19 +541,18 @@ __global__ void __launch_bounds__(256)
                 const double dsv = (double)sv, dbv = (double)bv;
                 conf = __ddiv_rn(__dsub_rn(dsv, dbv), __dadd_rn(dbv, 1.0e-6));
             }
-            if (want_conf && view == 0) conf0[p] = conf;
+            if (want_conf) *confp = conf;
             use_d0 = conf < uniq;
         }
         if (use_d0) {
-            out[p] = d0[p];
-            continue;
+            *outp = *d0p;
+            return;
         }
         const double a = (double)va, b = (double)vb, dbv = (double)bv;
         const double den = __dadd_rn(__dsub_rn(a, __dmul_rn(2.0, dbv)), b);
         double off = 0.0;
         if (den > 1.0e-9) off = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(a, b)), den);
-        const int32_t *base = view ? base1 : base0;
-        out[p] = __dadd_rn((double)(base[p] - R + bk), off);
+        *outp = __dadd_rn((double)(base_p - R + bk), off);
     }
 }
 
@@ -632,6 +676,120 @@ int launch_wta_slot(const void *L, bool l16, int npaths, int nviews, int W, int 
                                                     out0, out1, conf0);
     SV_LAUNCH_CHECK();
     return SV_OK;
+}
+
+// ====================================================================
+// Batched lr_refine, middle stages.  Costs and WTA run one block per
+// kBatchPxPerBlock pixels of a pair (blockIdx.y = view).  The SGM is a
+// persistent kernel over a device-side queue: every warp takes 32 scanline
+// tasks at a time from one atomic counter, tasks ordered longest scanline
+// first (segments of (pair, view, direction) sorted by length on the host),
+// so all pairs' scanlines share one launch and finish together.
+// ====================================================================
+
+__global__ void __launch_bounds__(256) k_b_costs(BatchTables t) {
+    const int i = batch_find(t.px_blk, t.n, blockIdx.x);
+    const BatchPair &P = t.pairs[i];
+    const int view = blockIdx.y;
+    const long N = (long)P.W * P.H;
+    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * kBatchPxPerBlock;
+    const long p1 = min(N, p0 + kBatchPxPerBlock);
+    const uint64_t *ref = view ? P.cen1 : P.cen0;
+    const uint64_t *oth = view ? P.cen0 : P.cen1;
+    for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
+        cost_pixel_slot(ref, oth, view ? P.base1 : P.base0, P.W, p, t.R, t.K, t.Kp, t.invalid,
+                        view, view ? P.C1 : P.C0);
+}
+
+template <int NR, typename LT>
+__global__ void __launch_bounds__(128) k_b_sgm(BatchTables t, long long total) {
+    constexpr int Kp = 2 * NR;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        long long first = 0;
+        if (lane == 0) first = atomicAdd(t.queue, 32);
+        first = __shfl_sync(kFull, first, 0);
+        if (first >= total) return;                        // warp-uniform
+        const long long task = first + lane;
+        if (task < total) {
+            const int s = batch_find(t.seg_start, t.nseg, task);
+            const BatchPair &P = t.pairs[t.seg_pair[s]];
+            const int view = t.seg_vd[s] >> 3, dir = t.seg_vd[s] & 7;
+            int dx, dy, x0, y0, n;
+            dir_of(dir, dx, dy);
+            scanline_of(P.W, P.H, dx, dy, (int)(task - t.seg_start[s]), x0, y0, n);
+            const long N = (long)P.W * P.H;
+            sgm_line_thread<NR, LT>(view ? P.C1 : P.C0, view ? P.base1 : P.base0,
+                                    reinterpret_cast<LT *>(P.L) + (long)(view * t.npaths + dir) * N * Kp,
+                                    P.W, t.K, t.P1, t.P2, dx, dy, x0, y0, n);
+        }
+    }
+}
+
+template <typename LT>
+__global__ void __launch_bounds__(256) k_b_wta(BatchTables t) {
+    const int i = batch_find(t.px_blk, t.n, blockIdx.x);
+    const BatchPair &P = t.pairs[i];
+    const int view = blockIdx.y;
+    const long N = (long)P.W * P.H;
+    const long stride = N * t.Kp;
+    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * kBatchPxPerBlock;
+    const long p1 = min(N, p0 + kBatchPxPerBlock);
+    const LT *Lv = reinterpret_cast<const LT *>(P.L) + (long)view * t.npaths * stride;
+    for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
+        wta_pixel<LT>(Lv + p * t.Kp, stride, t.npaths, t.K, t.Kp, t.R,
+                      (view ? P.base1 : P.base0)[p], (view ? P.d0r : P.disp0) + p, t.uniq, false,
+                      (view ? P.dr : P.dl) + p, nullptr);
+}
+
+int launch_batch_front(const BatchTables &t, long long px_blocks, long long rows,
+                       long long tiles, cudaStream_t st);
+int launch_batch_back(const BatchTables &t, long long rows, cudaStream_t st);
+
+template <int NR, typename LT>
+static int batch_sgm_go(const BatchTables &t, long long tasks, cudaStream_t st) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long want = (tasks + 127) / 128;
+    const long long cap = (long long)sms * 8;              // persistent: a few CTAs per SM
+    const unsigned blocks = (unsigned)(want < cap ? (want < 1 ? 1 : want) : cap);
+    count_launch();
+    k_b_sgm<NR, LT><<<blocks, 128, 0, st>>>(t, tasks);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_batch_refine(const BatchTables &t, long long px_blocks, long long rows,
+                        long long tiles, long long tasks, bool l16, cudaStream_t st) {
+    int rc = launch_batch_front(t, px_blocks, rows, tiles, st);
+    if (rc) return rc;
+    count_launch();
+    k_b_costs<<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+    SV_LAUNCH_CHECK();
+    switch (t.Kp) {
+#define SV_BGO(KP)                                                                      \
+    case KP:                                                                            \
+        rc = l16 ? batch_sgm_go<KP / 2, uint16_t>(t, tasks, st)                         \
+                 : batch_sgm_go<KP / 2, uint8_t>(t, tasks, st);                         \
+        break;
+        SV_BGO(8)
+        SV_BGO(16)
+        SV_BGO(24)
+        SV_BGO(32)
+#undef SV_BGO
+    default:
+        set_error("batched refinement supports bands up to K = 30 (got K = %d)", t.K);
+        return SV_ERR_SHAPE;
+    }
+    if (rc) return rc;
+    count_launch();
+    if (l16)
+        k_b_wta<uint16_t><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+    else
+        k_b_wta<uint8_t><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+    SV_LAUNCH_CHECK();
+    return launch_batch_back(t, rows, st);
 }
 
 }  // namespace sv

@@ -128,6 +128,27 @@ int sv_lr_refine_timed(const void *left, const void *right, int dtype,
                        void *workspace, size_t workspace_bytes, void *stream,
                        void *const *events, int n_events);
 
+/* lr_refine over many pairs of uneven sizes (the batched form of
+ * stereonet.py:5343-5391 that serves callers such as eval_real.evaluate,
+ * eval_real.py:133-152, over a whole test split).  Each pair's outputs are
+ * bit-identical to sv_lr_refine on that pair alone; the work runs as one
+ * launch per stage, the SGM stage as a persistent kernel over a device-side
+ * queue of (pair, view, path, scanline) tasks, longest scanlines first.
+ * Bands up to K = 30 (R <= 14).  `pairs` is a host array; its pointers are
+ * device buffers.  The tables are copied from host memory during the call. */
+typedef struct sv_pair_desc {
+    const void *left, *right;   /* [H][W] of the call's dtype  */
+    const double *disp0;        /* [H][W] network disparity    */
+    double *out;                /* [H][W] refined disparity    */
+    uint8_t *status;            /* [H][W] 0 ok, 1 occluded, 2 mismatch */
+    int W, H;
+} sv_pair_desc;
+size_t sv_batch_lr_refine_workspace_size(const sv_pair_desc *pairs, int n,
+                                         const sv_refine_params *p);
+int sv_batch_lr_refine(const sv_pair_desc *pairs, int n, int dtype, double tol,
+                       const sv_refine_params *p, void *workspace,
+                       size_t workspace_bytes, void *stream);
+
 /* refine_fullres for callers that cannot allocate device memory (an engine
  * that reserves all GPU memory up front, a plugin host without an
  * allocator): same kernels and bit-identical output as sv_refine_fullres,

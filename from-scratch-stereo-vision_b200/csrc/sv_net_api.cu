@@ -10,17 +10,18 @@
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
+#include "sv_tc.cuh"
 
 // One captured predict_auto stage (a network pass, optionally with the peak
 // selection that follows it), keyed by everything its kernels' arguments
 // depend on.
 struct sv_graph_key {
-    int kind, W, H, dtype, work, with_sel;
+    int kind, W, H, dtype, work, with_sel, precision;
     const void *left, *right;
     void *disp_full, *disp_work, *ws;
     bool operator==(const sv_graph_key &o) const {
         return kind == o.kind && W == o.W && H == o.H && dtype == o.dtype && work == o.work &&
-               with_sel == o.with_sel && left == o.left && right == o.right &&
+               with_sel == o.with_sel && precision == o.precision && left == o.left && right == o.right &&
                disp_full == o.disp_full && disp_work == o.disp_work && ws == o.ws;
     }
 };
@@ -35,6 +36,7 @@ struct sv_graph_entry {
 struct sv_net {
     sv::NetView view;
     float *dev = nullptr;     // all FP32 parameters, one allocation
+    uint16_t *tc = nullptr;   // BF16 tensor-core operands of the six convolutions
     int arch[16];
     int n_arch;
     std::mutex graph_mu;      // guards graphs (the weights themselves are immutable)
@@ -90,7 +92,7 @@ static void conv_out(int H, int W, int *h1, int *w1, int *h, int *w) {
 }
 
 // Forward scratch for an (H, W) input (sizes are monotone in H and W).
-static size_t carve_fwd(Carver &cv, const NetView &n, int H, int W, FwdBufs *b) {
+static size_t carve_fwd(Carver &cv, const NetView &n, int H, int W, DevFlags *flag, FwdBufs *b) {
     int h1, w1, h, w;
     conv_out(H, W, &h1, &w1, &h, &w);
     const size_t f1 = (size_t)n.C * h1 * w1, f2 = (size_t)n.C * h * w;
@@ -106,6 +108,7 @@ static size_t carve_fwd(Carver &cv, const NetView &n, int H, int W, FwdBufs *b) 
     t.rin = cv.take<float>(2 * HW);
     t.ra = cv.take<float>((size_t)n.Rc * HW);
     t.rb = cv.take<float>((size_t)n.Rc * HW);
+    t.flag = flag ? &flag->status : nullptr;
     if (b) *b = t;
     return cv.off - start;
 }
@@ -159,7 +162,7 @@ static void predict_dims(int W, int H, int max_width, int probe_width, int *Wm, 
 static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictWs *o) {
     Carver cv(ws);
     PredictWs p{};
-    cv.take<DevFlags>(1);
+    DevFlags *flag = cv.take<DevFlags>(1);
     const size_t HW = (size_t)Wm * Hm;
     int h1, w1, h, w;
     conv_out(Hm, Wm, &h1, &w1, &h, &w);
@@ -172,28 +175,30 @@ static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictW
     p.probe64 = cv.take<double>(HW);
     p.sel = reinterpret_cast<SelState *>(cv.take<unsigned char>(select_state_bytes()));
     p.hist = cv.take<unsigned>(select_hist_words());
-    carve_fwd(cv, n, Hm, Wm, &p.fwd);
+    carve_fwd(cv, n, Hm, Wm, flag, &p.fwd);
     if (o) *o = p;
     return cv.off;
 }
 
 // predict (stereonet.py:5891-5897) on FP32 images already in lw/rw.
-static int predict_f32(const sv_net *net, const PredictWs &w, int W, int H, cudaStream_t st) {
+static int predict_f32(const sv_net *net, const PredictWs &w, int W, int H, int precision,
+                       cudaStream_t st) {
     int rc = check_net_shape(net->view, H, W);
     if (rc) return rc;
     rc = launch_avgpool2(w.lw, H, W, w.gh, st);
     if (rc) return rc;
-    return launch_forward(net->view, w.lw, w.rw, H, W, w.gh, w.lw, w.d0, w.d1, w.d2, w.fwd, st);
+    return launch_forward(net->view, w.lw, w.rw, H, W, w.gh, w.lw, w.d0, w.d1, w.d2, w.fwd,
+                          precision, st);
 }
 
 static int predict_at_scale_impl(const sv_net *net, const PredictWs &w, const void *left,
                                  const void *right, int dtype, int W, int H, int work,
-                                 double *disp_full, double *disp_work, int *pWw, int *pHw,
-                                 cudaStream_t st) {
+                                 int precision, double *disp_full, double *disp_work, int *pWw,
+                                 int *pHw, cudaStream_t st) {
     int rc;
     if (work >= W) {
         rc = launch_to_f32_pair(left, right, dtype, (long)W * H, w.lw, w.rw, st);
-        if (!rc) rc = predict_f32(net, w, W, H, st);
+        if (!rc) rc = predict_f32(net, w, W, H, precision, st);
         if (!rc) rc = launch_promote(w.d2, (long)W * H, disp_full, st);
         if (rc) return rc;
         SV_CUDA_TRY(cudaMemcpyAsync(disp_work, disp_full, sizeof(double) * W * H,
@@ -207,7 +212,7 @@ static int predict_at_scale_impl(const sv_net *net, const PredictWs &w, const vo
     int Hw = (int)(H * scale + 0.5);
     if (Hw < 8) Hw = 8;
     rc = launch_resize_pair(left, right, dtype, W, H, Ww, Hw, w.lw, w.rw, st);
-    if (!rc) rc = predict_f32(net, w, Ww, Hw, st);
+    if (!rc) rc = predict_f32(net, w, Ww, Hw, precision, st);
     if (!rc) rc = launch_promote(w.d2, (long)Ww * Hw, disp_work, st);
     if (!rc) rc = launch_upscale_disp(w.d2, Ww, Hw, W, H, 1.0 / scale, disp_full, st);
     *pWw = Ww;
@@ -299,6 +304,34 @@ static int run_stage(sv_net *net, const sv_graph_key &key, cudaStream_t st, F &&
     return SV_OK;
 }
 
+// Pack FeatureNet c1..c4 and CostFilter c1, c2 as BF16 tensor-core
+// operands (their FP64 parameters sit at the FP32 copy's offsets).
+static int pack_tc(sv_net *net, const double *params) {
+    NetView &v = net->view;
+    const float *w[6] = {v.fw[0], v.fw[1], v.fw[2], v.fw[3], v.cw[0], v.cw[1]};
+    const int K[6] = {9, v.C * 9, v.C * 9, v.C * 9, v.C * 27, v.Cm * 27};
+    const int OC[6] = {v.C, v.C, v.C, v.C, v.Cm, v.Cm};
+    size_t total = 0, off[6];
+    for (int l = 0; l < 6; ++l) {
+        off[l] = total;
+        total += tc_weight_elems(K[l]);
+    }
+    for (int l = 0; l < 6; ++l) v.tw[l] = nullptr;
+    if (v.C > 16 || v.Cm > 16) return SV_OK;         // outside the kernel: FP32 only
+    std::vector<uint16_t> h(total, 0);
+    for (int l = 0; l < 6; ++l)
+        tc_pack_weights(params + (w[l] - net->dev), OC[l], K[l], h.data() + off[l]);
+    cudaError_t e = cudaMalloc(&net->tc, total * sizeof(uint16_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(net->tc, h.data(), total * sizeof(uint16_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        set_error("BF16 weight upload failed: %s", cudaGetErrorString(e));
+        return SV_ERR_CUDA;
+    }
+    for (int l = 0; l < 6; ++l) v.tw[l] = net->tc + off[l];
+    return SV_OK;
+}
+
 }  // namespace sv
 
 using namespace sv;
@@ -332,6 +365,10 @@ int sv_net_create(const int *arch, int n_arch, const double *params, long n_para
         return SV_ERR_CUDA;
     }
     bind_view(net);
+    if (pack_tc(net, params) != SV_OK) {
+        sv_net_destroy(net);
+        return SV_ERR_CUDA;
+    }
     *out = net;
     return SV_OK;
 }
@@ -340,6 +377,7 @@ void sv_net_destroy(sv_net *net) {
     if (!net) return;
     for (auto &g : net->graphs) cudaGraphExecDestroy(g.exec);
     if (net->dev) cudaFree(net->dev);
+    if (net->tc) cudaFree(net->tc);
     delete net;
 }
 
@@ -359,7 +397,7 @@ size_t sv_forward_workspace_size(const sv_net *net, int H, int W) {
     if (!net || H < 1 || W < 1) return 0;
     Carver cv(nullptr);
     cv.take<DevFlags>(1);
-    carve_fwd(cv, net->view, H, W, nullptr);
+    carve_fwd(cv, net->view, H, W, nullptr, nullptr);
     return cv.off;
 }
 
@@ -371,7 +409,10 @@ int sv_stereonet_forward(const sv_net *net, const float *left, const float *righ
         set_error("NULL argument");
         return SV_ERR_NULL;
     }
-    if (precision != SV_FP32) { set_error("precision %d not available", precision); return SV_ERR_PARAM; }
+    if (precision != SV_FP32 && precision != SV_BF16) {
+        set_error("precision %d is neither SV_FP32 nor SV_BF16", precision);
+        return SV_ERR_PARAM;
+    }
     SV_TRY(check_net_shape(net->view, H, W));
     size_t need = sv_forward_workspace_size(net, H, W);
     if (!workspace || ((uintptr_t)workspace & 255) || workspace_bytes < need) {
@@ -379,11 +420,11 @@ int sv_stereonet_forward(const sv_net *net, const float *left, const float *righ
         return SV_ERR_WORKSPACE;
     }
     Carver cv(workspace);
-    cv.take<DevFlags>(1);
+    DevFlags *flag = cv.take<DevFlags>(1);
     FwdBufs b;
-    carve_fwd(cv, net->view, H, W, &b);
+    carve_fwd(cv, net->view, H, W, flag, &b);
     return launch_forward(net->view, left, right, H, W, guide_half, guide_full, d0, d1, d2, b,
-                          (cudaStream_t)stream);
+                          precision, (cudaStream_t)stream);
 }
 
 size_t sv_predict_workspace_size(const sv_net *net, int W, int H, int max_width) {
@@ -414,13 +455,16 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right, 
         set_error("NULL argument");
         return SV_ERR_NULL;
     }
-    if (precision != SV_FP32) { set_error("precision %d not available", precision); return SV_ERR_PARAM; }
+    if (precision != SV_FP32 && precision != SV_BF16) {
+        set_error("precision %d is neither SV_FP32 nor SV_BF16", precision);
+        return SV_ERR_PARAM;
+    }
     if (W < 1 || H < 1 || work_width < 1) { set_error("bad shape"); return SV_ERR_SHAPE; }
     PredictWs w;
     int mw = work_width > 48 ? work_width : 48;
     SV_TRY(predict_ws(net, W, H, mw, 64, workspace, workspace_bytes, &w));
-    return predict_at_scale_impl(net, w, left, right, dtype, W, H, work_width, disp_full,
-                                 disp_work, Ww, Hw, (cudaStream_t)stream);
+    return predict_at_scale_impl(net, w, left, right, dtype, W, H, work_width, precision,
+                                 disp_full, disp_work, Ww, Hw, (cudaStream_t)stream);
 }
 
 int sv_predict_auto(const sv_net *net, const void *left, const void *right, int dtype, int W,
@@ -431,7 +475,10 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
         set_error("NULL argument");
         return SV_ERR_NULL;
     }
-    if (precision != SV_FP32) { set_error("precision %d not available", precision); return SV_ERR_PARAM; }
+    if (precision != SV_FP32 && precision != SV_BF16) {
+        set_error("precision %d is neither SV_FP32 nor SV_BF16", precision);
+        return SV_ERR_PARAM;
+    }
     if (W < 1 || H < 1 || probe_width < 1 || max_width < 1 || passes < 1 ||
         !std::isfinite(target_peak)) {
         set_error("bad arguments");
@@ -445,11 +492,11 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     const int pw = probe_width < W ? probe_width : W;
     int ph = (int)(H * pw / (double)W + 0.5);
     if (ph < 8) ph = 8;
-    sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, left, right, disp_full, disp_work,
-                     workspace};
+    sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, precision, left, right, disp_full,
+                     disp_work, workspace};
     SV_TRY(run_stage(mnet, key, st, [&]() -> int {
         int rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st);
-        if (!rc) rc = predict_f32(net, w, pw, ph, st);
+        if (!rc) rc = predict_f32(net, w, pw, ph, precision, st);
         if (!rc) rc = launch_promote(w.d2, (long)pw * ph, w.probe64, st);
         if (!rc) rc = launch_select(w.probe64, (long)pw * ph, (long long)((long)pw * ph * 0.95),
                                     w.sel, w.hist, st);
@@ -465,12 +512,12 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     // when another pass may follow
     for (int pass = 1;; ++pass) {
         const bool with_sel = pass < passes;
-        sv_graph_key k{1, W, H, dtype, work, with_sel ? 1 : 0, left, right, disp_full, disp_work,
-                       workspace};
+        sv_graph_key k{1, W, H, dtype, work, with_sel ? 1 : 0, precision, left, right, disp_full,
+                       disp_work, workspace};
         int Ww, Hw;
         SV_TRY(run_stage(mnet, k, st, [&]() -> int {
-            int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, disp_full,
-                                           disp_work, &Ww, &Hw, st);
+            int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, precision,
+                                           disp_full, disp_work, &Ww, &Hw, st);
             if (!rc && with_sel)
                 rc = launch_select(disp_full, (long)W * H, (long long)((long)W * H * 0.95), w.sel,
                                    w.hist, st);

@@ -20,6 +20,7 @@
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
+#include "sv_tc.cuh"
 
 namespace sv {
 
@@ -689,45 +690,128 @@ int launch_avgpool2(const float *img, int H, int W, float *out, cudaStream_t st)
     return SV_OK;
 }
 
+// BF16 precision, FeatureNet and CostFilter c1/c2 on the tensor cores: the
+// four feature convolutions (both images per launch), the cost volume fused
+// into CostFilter c1, and CostFilter c2.  Their FP32 outputs feed the same
+// CostFilter c3 + soft-argmin and Refinement kernels as the FP32 path.
+static int forward_bf16_front(const NetView &n, const float *left, const float *right, int H,
+                              int W, int h1, int w1, int h, int w, const FwdBufs &b,
+                              cudaStream_t st) {
+    SV_CUDA_TRY(cudaMemsetAsync(b.flag, 0, sizeof(int), st));
+    const int C = n.C, Cm = n.Cm;
+    TcConv a{};
+    a.mode = 0;
+    a.nd = 2;
+    a.nimg = 2;
+    a.D = a.OD = 1;
+    a.pad = a.dil = 1;
+    a.act = 1;
+    a.err = b.flag;
+    // c1..c4: (input, in size, out size, stride)
+    const float *in[4][2] = {{left, right}, {b.fa[0], b.fa[1]}, {b.fb[0], b.fb[1]},
+                             {b.fa[0], b.fa[1]}};
+    float *out[4][2] = {{b.fa[0], b.fa[1]}, {b.fb[0], b.fb[1]}, {b.fa[0], b.fa[1]},
+                        {b.fb[0], b.fb[1]}};
+    const int ih[4] = {H, h1, h, h}, iw[4] = {W, w1, w, w};
+    const int oh[4] = {h1, h, h, h}, ow[4] = {w1, w, w, w};
+    for (int l = 0; l < 4; ++l) {
+        a.IC = l == 0 ? 1 : C;
+        a.OC = C;
+        a.K = a.IC * 9;
+        a.Kpad = tc_kpad(a.K);
+        a.H = ih[l];
+        a.W = iw[l];
+        a.OH = oh[l];
+        a.OW = ow[l];
+        a.stride = l < 2 ? 2 : 1;
+        a.act = l < 3 ? 1 : 0;
+        a.x[0] = in[l][0];
+        a.x[1] = in[l][1];
+        a.y[0] = out[l][0];
+        a.y[1] = out[l][1];
+        a.wB = n.tw[l];
+        a.bias = n.fb[l];
+        const int rc = launch_conv_tc(a, st);
+        if (rc) return rc;
+    }
+    // cost volume + CostFilter c1, then c2 (leaky ReLU after both)
+    TcConv v{};
+    v.mode = 1;
+    v.nd = 3;
+    v.nimg = 1;
+    v.IC = C;
+    v.OC = Cm;
+    v.K = C * 27;
+    v.Kpad = tc_kpad(v.K);
+    v.D = v.OD = n.D;
+    v.H = v.OH = h;
+    v.W = v.OW = w;
+    v.stride = v.pad = v.dil = 1;
+    v.act = 1;
+    v.x[0] = b.fb[0];
+    v.x[1] = b.fb[1];
+    v.y[0] = v.y[1] = b.v0;
+    v.wB = n.tw[4];
+    v.bias = n.cb[0];
+    v.err = b.flag;
+    int rc = launch_conv_tc(v, st);
+    if (rc) return rc;
+    v.mode = 0;
+    v.IC = Cm;
+    v.K = Cm * 27;
+    v.Kpad = tc_kpad(v.K);
+    v.x[0] = v.x[1] = b.v0;
+    v.y[0] = v.y[1] = b.v1;
+    v.wB = n.tw[5];
+    v.bias = n.cb[1];
+    return launch_conv_tc(v, st);
+}
+
 // The network shapes this build instantiates: the reference's shipped
 // architectures (feat_C, cost_C, refine_C) = (12, 6, 8), (8, 4, 8), (8, 4, 4),
 // (16, 8, 8) with D <= 16.
 template <int C, int CM, int RC>
 static int forward_impl(const NetView &n, const float *left, const float *right, int H, int W,
                         const float *gh, const float *gf, float *d0, float *d1, float *d2,
-                        const FwdBufs &b, cudaStream_t st) {
+                        const FwdBufs &b, int precision, cudaStream_t st) {
     const int h1 = (H - 1) / 2 + 1, w1 = (W - 1) / 2 + 1;
     const int h = (h1 - 1) / 2 + 1, w = (w1 - 1) / 2 + 1;
     const int D = n.D;
     dim3 blk(32, 8);
-    // FeatureNet, both images: c1 s2, c2 s2, c3, c4 (4 output channels per thread)
-    constexpr int FG = C % 4 == 0 ? 4 : C;
     const dim3 tb(CT2_TW, CT2_TH);
     auto tgrid = [&](int OW, int OH, int z) {
         return dim3((OW + CT2_TW - 1) / CT2_TW, (OH + CT2_TH - 1) / CT2_TH, z);
     };
-    count_launch();
-    k_conv2d_tiled<1, C, FG, 1><<<tgrid(w1, h1, 2 * (C / FG)), tb, conv2d_tile_bytes(1, 2, 1), st>>>(
-        left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
-    count_launch();
-    k_conv2d_tiled<C, C, FG, 1><<<tgrid(w, h, 2 * (C / FG)), tb, conv2d_tile_bytes(C, 2, 1), st>>>(
-        b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
-    count_launch();
-    k_conv2d_tiled<C, C, FG, 1><<<tgrid(w, h, 2 * (C / FG)), tb, conv2d_tile_bytes(C, 1, 1), st>>>(
-        b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1], nullptr);
-    count_launch();
-    k_conv2d_tiled<C, C, FG, 0><<<tgrid(w, h, 2 * (C / FG)), tb, conv2d_tile_bytes(C, 1, 1), st>>>(
-        b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
-    SV_LAUNCH_CHECK();
-    // cost volume + CostFilter + soft-argmin (2 output channels per thread)
-    constexpr int CG = CM % 2 == 0 ? 2 : CM;
-    const dim3 vgrid((w + 31) / 32, h * ((D + CV_TD - 1) / CV_TD), CM / CG);
-    count_launch();
-    k_costvol_conv3d_tiled<C, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(
-        b.fb[0], b.fb[1], D, h, w, n.cw[0], n.cb[0], b.v0);
-    count_launch();
-    k_conv3d_tiled<CM, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(b.v0, D, h, w, n.cw[1],
-                                                                  n.cb[1], b.v1);
+    if (precision == SV_BF16) {
+        const int rc = forward_bf16_front(n, left, right, H, W, h1, w1, h, w, b, st);
+        if (rc) return rc;
+    } else {
+        // FeatureNet, both images: c1 s2, c2 s2, c3, c4 (4 output channels per thread)
+        constexpr int FG = C % 4 == 0 ? 4 : C;
+        const dim3 fg1 = tgrid(w1, h1, 2 * (C / FG)), fg = tgrid(w, h, 2 * (C / FG));
+        count_launch();
+        k_conv2d_tiled<1, C, FG, 1><<<fg1, tb, conv2d_tile_bytes(1, 2, 1), st>>>(
+            left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
+        count_launch();
+        k_conv2d_tiled<C, C, FG, 1><<<fg, tb, conv2d_tile_bytes(C, 2, 1), st>>>(
+            b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
+        count_launch();
+        k_conv2d_tiled<C, C, FG, 1><<<fg, tb, conv2d_tile_bytes(C, 1, 1), st>>>(
+            b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1], nullptr);
+        count_launch();
+        k_conv2d_tiled<C, C, FG, 0><<<fg, tb, conv2d_tile_bytes(C, 1, 1), st>>>(
+            b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
+        SV_LAUNCH_CHECK();
+        // cost volume + CostFilter c1, c2 (2 output channels per thread)
+        constexpr int CG = CM % 2 == 0 ? 2 : CM;
+        const dim3 vgrid((w + 31) / 32, h * ((D + CV_TD - 1) / CV_TD), CM / CG);
+        count_launch();
+        k_costvol_conv3d_tiled<C, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(
+            b.fb[0], b.fb[1], D, h, w, n.cw[0], n.cb[0], b.v0);
+        count_launch();
+        k_conv3d_tiled<CM, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(b.v0, D, h, w, n.cw[1],
+                                                                      n.cb[1], b.v1);
+    }
     count_launch();
     k_conv3d_softargmin<CM><<<dim3((w + 31) / 32, h), dim3(32, SA_DMAX), 0, st>>>(
         b.v1, D, h, w, n.cw[2], n.cb[2], d0);
@@ -776,19 +860,31 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
 
 int launch_forward(const NetView &n, const float *left, const float *right, int H, int W,
                    const float *gh, const float *gf, float *d0, float *d1, float *d2,
-                   const FwdBufs &b, cudaStream_t st) {
+                   const FwdBufs &b, int precision, cudaStream_t st) {
+    if (precision != SV_FP32 && precision != SV_BF16) {
+        set_error("precision %d is neither SV_FP32 nor SV_BF16", precision);
+        return SV_ERR_PARAM;
+    }
+    if (precision == SV_BF16 && (!n.tw[0] || !b.flag)) {
+        set_error("BF16 forward without packed weights or an error flag");
+        return SV_ERR_PARAM;
+    }
     if (n.D < 1 || n.D > 16) {
         set_error("D=%d outside 1..16", n.D);
         return SV_ERR_NET;
     }
     if (n.C == 12 && n.Cm == 6 && n.Rc == 8)
-        return forward_impl<12, 6, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+        return forward_impl<12, 6, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, precision,
+                                         st);
     if (n.C == 8 && n.Cm == 4 && n.Rc == 8)
-        return forward_impl<8, 4, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+        return forward_impl<8, 4, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, precision,
+                                         st);
     if (n.C == 8 && n.Cm == 4 && n.Rc == 4)
-        return forward_impl<8, 4, 4>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+        return forward_impl<8, 4, 4>(n, left, right, H, W, gh, gf, d0, d1, d2, b, precision,
+                                         st);
     if (n.C == 16 && n.Cm == 8 && n.Rc == 8)
-        return forward_impl<16, 8, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, st);
+        return forward_impl<16, 8, 8>(n, left, right, H, W, gh, gf, d0, d1, d2, b, precision,
+                                         st);
     set_error("architecture feat_C=%d cost_C=%d refine_C=%d is not instantiated", n.C, n.Cm,
               n.Rc);
     return SV_ERR_NET;

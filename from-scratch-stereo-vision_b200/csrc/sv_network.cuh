@@ -15,6 +15,9 @@ struct NetView {
     const float *fw[4], *fb[4];          // FeatureNet c1..c4
     const float *cw[3], *cb[3];          // CostFilter c1..c3
     const float *rw[2][9], *rb[2][9];    // Refinement levels: ndil convs + final
+    // BF16 precision: tensor-core operand B of FeatureNet c1..c4 and
+    // CostFilter c1, c2 (sv_tc.cuh layout)
+    const uint16_t *tw[6];
 };
 
 // Scratch of one forward at (H, W).
@@ -22,6 +25,7 @@ struct FwdBufs {
     float *fa[2], *fb[2];    // feature maps, left/right
     float *v0, *v1;          // filtered cost volumes [Cm][D][h][w]
     float *rin, *ra, *rb;    // refinement input [2][H][W] and ping-pong [Rc][H][W]
+    int *flag;               // device error flag (the workspace's DevFlags)
 };
 
 int launch_resize_pair(const void *l, const void *r, int dtype, int W, int H, int W2, int H2,
@@ -37,7 +41,7 @@ int launch_avgpool2(const float *img, int H, int W, float *out, cudaStream_t st)
 int launch_avgpool2_f64(const double *img, int C, int H, int W, double *out, cudaStream_t st);
 int launch_forward(const NetView &n, const float *left, const float *right, int H, int W,
                    const float *gh, const float *gf, float *d0, float *d1, float *d2,
-                   const FwdBufs &b, cudaStream_t st);
+                   const FwdBufs &b, int precision, cudaStream_t st);
 
 struct SelState;
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,

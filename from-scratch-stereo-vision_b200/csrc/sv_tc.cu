@@ -1,0 +1,271 @@
+// sv_tc.cu -- BF16 implicit-GEMM convolutions on the sm_100a tensor cores
+// (tcgen05.mma, FP32 accumulator in tensor memory) for the network's BF16
+// path: the feature tower's 2-D convolutions (FeatureNet, stereonet.py:
+// 1022-1070) and the cost filter's first two 3-D convolutions (CostFilter,
+// 1071-1109), the first one fused with the cost volume (CostVolume,
+// 740-842).
+//
+// GEMM view: M = output positions (a CTA tile of 128), N = output channels
+// padded to 16, K = input channels x taps padded to a multiple of 16.
+//  * B (weights) is packed once at checkpoint upload into the canonical
+//    K-major, no-swizzle UMMA layout (8 x 16-byte core matrices, 128
+//    contiguous bytes each) and copied to shared memory once per CTA;
+//  * A (the im2col tile) is gathered by the CTA's 128 threads straight into
+//    that layout -- thread m owns output row m and writes 16-byte chunks of
+//    8 consecutive k -- and fenced into the async proxy; a shared table maps
+//    k to (channel, tap offsets);
+//  * one thread issues Kpad/16 tcgen05.mma (M=128, N=16, K=16) into a
+//    32-column tensor-memory accumulator and commits them to an mbarrier;
+//  * each warp reads its 32 accumulator rows back with tcgen05.ld
+//    (32x32b.x16) and applies bias + activation.
+// CTAs are persistent over tiles.  Every mbarrier wait is bounded: on
+// timeout the kernel records SV_ERR_CUDA, stops and still frees its tensor
+// memory.
+
+#include <cuda_bf16.h>
+
+#include "sv_common.cuh"
+#include "sv_tc.cuh"
+
+namespace sv {
+
+namespace {
+
+constexpr int kTcM = 128, kTcN = 16, kTmemCols = 32;
+constexpr int kTcMaxK = 432;                  // 16 channels x 27 taps
+constexpr unsigned kWaitLimit = 1u << 24;     // polls before a wait is declared failed
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory descriptor, K-major without swizzle: start address,
+// leading byte offset (between the two 8-element K halves of one MMA),
+// stride byte offset (between 8-row groups), all >> 4; version 1 (sm_100).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// kind::f16 instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) |
+                                ((uint32_t)(kTcN >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Bounded wait for phase `parity` of the barrier; true when it completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    const uint32_t a = smem_u32(bar);
+    for (unsigned it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+// ktab[k] = {channel (-1: K padding), dz, dy, dx}: mode 0 input offsets
+// (input z = od + dz, y = oy * stride + dy, x = ox * stride + dx); mode 1
+// cost-volume offsets (d = od + dz, y = oy + dy, x = ox + dx).
+__global__ void __launch_bounds__(kTcM) k_conv_tc(TcConv a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    __shared__ int4 ktab[kTcMaxK];
+    unsigned char *sA = smem;                                   // 128 x Kpad BF16
+    unsigned char *sB = smem + (size_t)a.Kpad * kTcM * 2;        // 16 x Kpad BF16
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    const uint4 *wsrc = reinterpret_cast<const uint4 *>(a.wB);
+    uint4 *wdst = reinterpret_cast<uint4 *>(sB);
+    for (int i = tid; i < a.Kpad * kTcN * 2 / 16; i += kTcM) wdst[i] = __ldg(wsrc + i);
+    const int taps = a.nd == 3 ? 27 : 9;
+    for (int k = tid; k < a.Kpad; k += kTcM) {
+        int4 e = make_int4(-1, 0, 0, 0);
+        if (k < a.K) {
+            const int c = k / taps;
+            int t = k - c * taps;
+            const int kd = a.nd == 3 ? t / 9 : 1;
+            if (a.nd == 3) t -= kd * 9;
+            const int ky = t / 3, kx = t - (t / 3) * 3;
+            if (a.mode == 0)
+                e = make_int4(c, kd - 1, ky * a.dil - a.pad, kx * a.dil - a.pad);
+            else
+                e = make_int4(c, kd - 1, ky - 1, kx - 1);
+        }
+        ktab[k] = e;
+    }
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+
+    const long M = (long)a.OD * a.OH * a.OW;
+    const long tiles_img = (M + kTcM - 1) / kTcM;
+    const long tiles = tiles_img * (a.mode == 0 ? a.nimg : 1);
+    const int ohw = a.OH * a.OW;
+    const long plane = (long)a.D * a.H * a.W;     // one input channel (mode 0)
+    const long fplane = (long)a.H * a.W;          // one feature channel (mode 1)
+    unsigned phase = 0;
+    for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int img = (int)(tile / tiles_img);
+        const long mi = (tile - img * tiles_img) * kTcM + tid;
+        const bool row_ok = mi < M;
+        int od = 0, oy = 0, ox = 0;
+        if (row_ok) {
+            od = (int)(mi / ohw);
+            const int r = (int)(mi - (long)od * ohw);
+            oy = r / a.OW;
+            ox = r - oy * a.OW;
+        }
+        // ---- gather this thread's im2col row, 8 k at a time
+        const float *x0 = img ? a.x[1] : a.x[0], *x1 = a.x[1];
+        const int by = a.mode == 0 ? oy * a.stride : oy, bx = a.mode == 0 ? ox * a.stride : ox;
+        for (int kg = 0; kg < a.Kpad / 8; ++kg) {
+            __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int4 e = ktab[kg * 8 + j];
+                float f = 0.f;
+                const int z = od + e.y, yy = by + e.z, xx = bx + e.w;
+                if (row_ok && e.x >= 0 && z >= 0 && z < a.D && yy >= 0 && yy < a.H && xx >= 0 &&
+                    xx < a.W) {
+                    if (a.mode == 0) {
+                        f = __ldg(x0 + e.x * plane + ((long)z * a.H + yy) * a.W + xx);
+                    } else if (xx < z) {
+                        f = 2.0f;
+                    } else {
+                        const long o = e.x * fplane + (long)yy * a.W + xx;
+                        f = fabsf(__ldg(x0 + o) - __ldg(x1 + o - z));
+                    }
+                }
+                v[j] = __float2bfloat16_rn(f);
+            }
+            *reinterpret_cast<uint4 *>(sA + (size_t)(kg * (kTcM / 8) + (tid >> 3)) * 128 +
+                                       (tid & 7) * 16) = *reinterpret_cast<const uint4 *>(v);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0 && !failed) {
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int ks = 0; ks < a.Kpad / 16; ++ks) {
+                const uint64_t da = umma_desc(a0 + ks * 2 * (kTcM / 8) * 128, (kTcM / 8) * 128, 128);
+                const uint64_t db = umma_desc(b0 + ks * 2 * (kTcN / 8) * 128, (kTcN / 8) * 128, 128);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(kIdescBf16), "r"(ks));
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                ::"r"(smem_u32(&mbar))
+                : "memory");
+        }
+        // ---- wait for the accumulator (bounded), then the epilogue
+        if (!failed && !mbar_wait(&mbar, phase)) {
+            failed = 1;
+            flag_error(a.err, SV_ERR_CUDA);
+        }
+        phase ^= 1u;
+        __syncthreads();
+        if (failed) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row_ok) {
+            float *y = img ? a.y[1] : a.y[0];
+#pragma unroll
+            for (int n = 0; n < kTcN; ++n) {
+                if (n < a.OC) {
+                    float v = __uint_as_float(r[n]) + __ldg(a.bias + n);
+                    if (a.act == 1) v = v > 0.f ? v : v * 0.2f;
+                    y[(long)n * M + mi] = v;
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(kTmemCols));
+}
+
+// Element (n, k) of the 16 x Kpad operand B sits in core matrix
+// (k / 8, n / 8) -- core matrices ordered k-group-major, 2 per k group --
+// at row n % 8 (16 bytes per row), column k % 8.
+void tc_pack_weights(const double *w, int OC, int K, uint16_t *out) {
+    const int Kpad = tc_kpad(K);
+    for (int n = 0; n < kTcN; ++n)
+        for (int k = 0; k < Kpad; ++k) {
+            const float v = (n < OC && k < K) ? (float)w[(long)n * K + k] : 0.f;
+            const __nv_bfloat16 b = __float2bfloat16_rn(v);
+            const size_t byte = (size_t)((k / 8) * 2 + n / 8) * 128 + (n % 8) * 16 + (k % 8) * 2;
+            out[byte / 2] = *reinterpret_cast<const uint16_t *>(&b);
+        }
+}
+
+int launch_conv_tc(const TcConv &a, cudaStream_t st) {
+    if (a.OC < 1 || a.OC > kTcN || a.K < 1 || a.K > kTcMaxK || a.Kpad != tc_kpad(a.K) ||
+        (a.mode == 0 && (a.nimg < 1 || a.nimg > 2)) || (a.mode == 1 && a.nd != 3) ||
+        !a.wB || !a.bias || !a.err) {
+        set_error("tensor-core conv: IC=%d OC=%d K=%d outside the kernel's shapes", a.IC, a.OC,
+                  a.K);
+        return SV_ERR_PARAM;
+    }
+    const size_t smem = (size_t)a.Kpad * (kTcM + kTcN) * 2;
+    SV_CUDA_TRY(
+        cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long M = (long)a.OD * a.OH * a.OW;
+    if (M == 0) return SV_OK;
+    const long tiles = (M + kTcM - 1) / kTcM * (a.mode == 0 ? a.nimg : 1);
+    int dev = 0, sms = 148;
+    SV_CUDA_TRY(cudaGetDevice(&dev));
+    SV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long per_sm = smem > 100 * 1024 ? 1 : 2;
+    const long cap = (long)sms * per_sm;
+    const unsigned blocks = (unsigned)(tiles < cap ? tiles : cap);
+    count_launch();
+    k_conv_tc<<<blocks, kTcM, smem, st>>>(a);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+}  // namespace sv

@@ -111,8 +111,26 @@ def _f32(x, n, name):
     return _to_dev(x, n, torch.float32, name=name)
 
 
-def forward(net, left, right, H, W, guide_half, guide_full):
+def _precision(precision) -> int:
+    """"fp32" (default) or "bf16": FeatureNet and CostFilter c1/c2 as BF16
+    tensor-core GEMMs with FP32 accumulation (soft-argmin and Refinement stay
+    FP32)."""
+    codes = {"fp32": _lib.SV_FP32, "bf16": _lib.SV_BF16, _lib.SV_FP32: _lib.SV_FP32,
+             _lib.SV_BF16: _lib.SV_BF16}
+    if precision not in codes:
+        raise ValueError("precision must be 'fp32' or 'bf16', not %r" % (precision,))
+    return codes[precision]
+
+
+def _flag_check(lib, ws, code, what):
+    """BF16 kernels report a stalled tensor-core wait through the workspace flag."""
+    if code == _lib.SV_BF16:
+        _lib.check(lib.sv_workspace_status(_ptr(ws), ctypes.c_void_p(_stream())), what)
+
+
+def forward(net, left, right, H, W, guide_half, guide_full, *, precision="fp32"):
     """StereoNet.forward (stereonet.py:1203-1233): (d_quarter, d_half, d_full)."""
+    code = _precision(precision)
     g = gpu_net(net)
     lib = g.lib
     h1, w1 = (H - 1) // 2 + 1, (W - 1) // 2 + 1
@@ -127,15 +145,17 @@ def forward(net, left, right, H, W, guide_half, guide_full):
     need = lib.sv_forward_workspace_size(g.handle, H, W)
     ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     _lib.check(lib.sv_stereonet_forward(g.handle, _ptr(tl), _ptr(tr), H, W, _ptr(gh), _ptr(gf),
-                                        _ptr(d0), _ptr(d1), _ptr(d2), _lib.SV_FP32, _ptr(ws),
+                                        _ptr(d0), _ptr(d1), _ptr(d2), code, _ptr(ws),
                                         need, _stream()), "forward")
+    _flag_check(lib, ws, code, "forward")
     return tuple(_ret(d.to(torch.float64), left) for d in (d0, d1, d2))
 
 
-def predict(net, left, right, W, H):
+def predict(net, left, right, W, H, *, precision="fp32"):
     """stereonet.py:5891-5897: full-resolution disparity of the network
     (guide_half = avgpool2(left), guide_full = left)."""
-    return predict_at_scale(net, left, right, W, H, work_width=W, verbose=False)[0]
+    return predict_at_scale(net, left, right, W, H, work_width=W, verbose=False,
+                            precision=precision)[0]
 
 
 # ------------------------------------------------- resolution selection
@@ -147,8 +167,9 @@ def _pair_inputs(left, right, W, H):
     return tl, tr, code
 
 
-def predict_at_scale(net, left, right, W, H, work_width=96, verbose=True):
+def predict_at_scale(net, left, right, W, H, work_width=96, verbose=True, *, precision="fp32"):
     """stereonet.py:3932-3960 -> (disp_full, disp_work, W_work, H_work)."""
+    code_p = _precision(precision)
     g = gpu_net(net)
     lib = g.lib
     tl, tr, code = _pair_inputs(left, right, W, H)
@@ -159,9 +180,10 @@ def predict_at_scale(net, left, right, W, H, work_width=96, verbose=True):
     ws = torch.empty(max(need, 256), dtype=torch.uint8, device=dev)
     Ww, Hw = ctypes.c_int(), ctypes.c_int()
     _lib.check(lib.sv_predict_at_scale(g.handle, _ptr(tl), _ptr(tr), code, W, H, int(work_width),
-                                       _lib.SV_FP32, _ptr(df), _ptr(dw), ctypes.byref(Ww),
+                                       code_p, _ptr(df), _ptr(dw), ctypes.byref(Ww),
                                        ctypes.byref(Hw), _ptr(ws), need, _stream()),
                "predict_at_scale")
+    _flag_check(lib, ws, code_p, "predict_at_scale")
     if verbose and work_width < W:
         print("  running at %dx%d (input %dx%d, scale %.3f)"
               % (Ww.value, Hw.value, W, H, work_width / float(W)))
@@ -170,11 +192,12 @@ def predict_at_scale(net, left, right, W, H, work_width=96, verbose=True):
 
 
 def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64, max_width=320,
-                 passes=3, verbose=True, return_trace=False):
+                 passes=3, verbose=True, return_trace=False, *, precision="fp32"):
     """stereonet.py:3872-3929 -> (disp_full, disp_work, W_work, H_work).
 
     The work width depends on each pass's 95% disparity quantile, so the
     call reads one number back from the GPU per pass."""
+    code_p = _precision(precision)
     g = gpu_net(net)
     lib = g.lib
     tp = float(g.target_peak if target_peak is None else target_peak)
@@ -187,9 +210,10 @@ def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64, max_w
     Ww, Hw = ctypes.c_int(), ctypes.c_int()
     trace = (ctypes.c_int * (passes + 2))()
     _lib.check(lib.sv_predict_auto(g.handle, _ptr(tl), _ptr(tr), code, W, H, tp,
-                                   int(probe_width), int(max_width), int(passes), _lib.SV_FP32,
+                                   int(probe_width), int(max_width), int(passes), code_p,
                                    _ptr(df), _ptr(dw), ctypes.byref(Ww), ctypes.byref(Hw), trace,
                                    _ptr(ws), need, _stream()), "predict_auto")
+    _flag_check(lib, ws, code_p, "predict_auto")
     widths = [int(t) for t in trace if t > 0]
     if verbose:
         for i, wd in enumerate(widths):

@@ -17,15 +17,16 @@ import numpy as np
 import torch
 
 from . import _lib
-from .network import gpu_net
+from .network import _precision, gpu_net
 from .refine import LRRefiner, _ptr, _stream
 
 
 class PairPipeline:
     def __init__(self, W: int, H: int, net, image_dtype=torch.uint8, R=10, P1=12.0, P2=150.0,
                  rx=4, ry=3, tol=2.0, probe_width=64, max_width=320, passes=3,
-                 target_peak=None, device=None):
+                 target_peak=None, device=None, precision="fp32"):
         self.lib = _lib.load()
+        self.precision = _precision(precision)
         self.W, self.H = W, H
         self.dev = torch.device("cuda", torch.cuda.current_device()) if device is None else device
         # A stream of its own: work on it can be captured, so each predict_auto
@@ -59,7 +60,7 @@ class PairPipeline:
         s = self.stream.cuda_stream if stream is None else stream
         _lib.check(self.lib.sv_predict_auto(
             self.net.handle, _ptr(self.left), _ptr(self.right), self.code, self.W, self.H,
-            self.tp, self.probe_width, self.max_width, self.passes, _lib.SV_FP32,
+            self.tp, self.probe_width, self.max_width, self.passes, self.precision,
             _ptr(self.disp0), _ptr(self.disp_work), ctypes.byref(self._Ww),
             ctypes.byref(self._Hw), self._trace, _ptr(self.pws), self.pneed, s), "predict_auto")
 

@@ -57,6 +57,20 @@ SIGNATURES = {
     "sv_refine_fullres_noalloc": (_I, [_VP, _VP, _I, _VP, _I, _I, _PRM, _VP, _VP, _VP]),
     "sv_batch_lr_refine_workspace_size": (_SZ, [_VP, _I, _PRM]),
     "sv_batch_lr_refine": (_I, [_VP, _I, _I, _D, _PRM, _VP, _SZ, _VP]),
+    "sv_lr_refine_band": (_I, [_VP, _VP, _I, _VP, _VP, _I, _I, _D, _PRM, _VP, _VP, _VP, _SZ,
+                               _VP]),
+    "sv_band_param_count": (ctypes.c_long, []),
+    "sv_band_create": (_I, [_VP, ctypes.c_long, ctypes.POINTER(_VP)]),
+    "sv_band_destroy": (None, [_VP]),
+    "sv_band_get_params": (_I, [_VP, _VP, ctypes.c_long]),
+    "sv_band_features_workspace_size": (_SZ, [_I, _I]),
+    "sv_band_features": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _VP, _VP, _SZ, _VP]),
+    "sv_band_workspace_size": (_SZ, [_I, _I, _I]),
+    "sv_band_forward": (_I, [_VP, _VP, _I, _I, _I, _VP, _VP, _SZ, _VP]),
+    "sv_band_grads": (_I, [_VP, _VP, _VP, _VP, _I, _I, _I, _VP, _VP, _VP, _SZ, _VP]),
+    "sv_band_train_step": (_I, [_VP, _VP, _VP, _VP, _I, _I, _I, _D, _VP, _VP, _SZ, _VP]),
+    "sv_band_targets": (_I, [_VP, _VP, _VP, ctypes.c_long, _D, _VP, _VP, _VP]),
+    "sv_band_apply": (_I, [_VP, _VP, _I, _I, _D, _D, _I, _I, _D, _VP, _VP, _VP]),
     "sv_net_create": (_I, [_VP, _I, _VP, ctypes.c_long, ctypes.POINTER(_VP)]),
     "sv_net_destroy": (None, [_VP]),
     "sv_resize": (_I, [_VP, _I, _I, _I, _I, _VP, _VP]),

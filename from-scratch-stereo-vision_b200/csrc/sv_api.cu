@@ -262,7 +262,8 @@ int sv_refine_fullres(const void *left, const void *right, int dtype, const doub
 static int lr_refine_impl(const void *left, const void *right, int dtype, const double *disp0,
                           int W, int H, double tol, const sv_refine_params *p, double *out,
                           uint8_t *status, void *workspace, size_t workspace_bytes,
-                          void *stream, void *const *events, int n_events) {
+                          void *stream, void *const *events, int n_events,
+                          const uint8_t *rad = nullptr) {
     if (!left || !right || !disp0 || !out || !status) {
         set_error("NULL argument");
         return SV_ERR_NULL;
@@ -292,7 +293,7 @@ static int lr_refine_impl(const void *left, const void *right, int dtype, const 
     SV_TRY(launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st));
     SV_TRY(mark());
     SV_TRY(launch_band_costs_slot(w.cen0, w.cen1, w.base0, w.base1, W, H, c.R, c.invalid, w.C0,
-                             w.C1, 2, st));
+                             w.C1, 2, st, rad));
     SV_TRY(mark());
     SV_TRY(launch_sgm_packed(w.C0, w.C1, w.base0, w.base1, W, H, c.K, c.P1, c.P2, w.L, c.l16, 2,
                       c.npaths, st));
@@ -310,6 +311,15 @@ int sv_lr_refine(const void *left, const void *right, int dtype, const double *d
                  void *workspace, size_t workspace_bytes, void *stream) {
     return lr_refine_impl(left, right, dtype, disp0, W, H, tol, p, out, status, workspace,
                           workspace_bytes, stream, nullptr, 0);
+}
+
+int sv_lr_refine_band(const void *left, const void *right, int dtype, const double *centre,
+                      const uint8_t *rad, int W, int H, double tol, const sv_refine_params *p,
+                      double *out, uint8_t *status, void *workspace, size_t workspace_bytes,
+                      void *stream) {
+    if (!rad) { set_error("NULL half-width map"); return SV_ERR_NULL; }
+    return lr_refine_impl(left, right, dtype, centre, W, H, tol, p, out, status, workspace,
+                          workspace_bytes, stream, nullptr, 0, rad);
 }
 
 int sv_lr_refine_timed(const void *left, const void *right, int dtype, const double *disp0,

@@ -114,9 +114,12 @@ int launch_band_costs(const uint64_t *cl, const uint64_t *cr, const int32_t *bas
                       uint8_t *C1, int nviews, cudaStream_t st);
 int launch_sgm_add_path(const uint8_t *C, const int32_t *base, int W, int H, int K, int P1,
                         int P2, int dir, uint16_t *S, cudaStream_t st);
+// rad0 (may be NULL): per-pixel half-width of the left view's band; slots
+// with |k - R| > rad0[p] get the invalid cost.
 int launch_band_costs_slot(const uint64_t *cl, const uint64_t *cr, const int32_t *base0,
                            const int32_t *base1, int W, int H, int R, int invalid, uint8_t *C0,
-                           uint8_t *C1, int nviews, cudaStream_t st);
+                           uint8_t *C1, int nviews, cudaStream_t st,
+                           const uint8_t *rad0 = nullptr);
 int launch_sgm_packed(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
                       const int32_t *b1, int W, int H, int K, int P1, int P2, void *Lout,
                       bool l16, int nviews, int npaths, cudaStream_t st);

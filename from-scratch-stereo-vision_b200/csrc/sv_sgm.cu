@@ -46,7 +46,7 @@ __device__ __forceinline__ void cost_pixel_slot(const uint64_t *__restrict__ ref
                                                 const uint64_t *__restrict__ oth,
                                                 const int32_t *__restrict__ base, int W, long p,
                                                 int R, int K, int Kp, int invalid, int view,
-                                                uint8_t *__restrict__ C) {
+                                                uint8_t *__restrict__ C, int rk) {
     const int x = (int)(p % W);
     const uint64_t a = ref[p];
     const int b = base[p] - R;
@@ -60,7 +60,8 @@ __device__ __forceinline__ void cost_pixel_slot(const uint64_t *__restrict__ ref
             if (k >= 0 && k < K) {
                 const int d = b + k;
                 int cost = invalid;
-                if (view == 0) {
+                if (abs(k - R) > rk) {
+                } else if (view == 0) {
                     if (d >= 0 && x - d >= 0) cost = __popcll(a ^ oth[p - d]);
                 } else {
                     if (d >= 0 && x + d <= W - 1) cost = __popcll(a ^ oth[p + d]);
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(256)
     k_band_costs_slot(const uint64_t *__restrict__ cl, const uint64_t *__restrict__ cr,
                       const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
                       long N, int R, int K, int Kp, int invalid, uint8_t *__restrict__ C0,
-                      uint8_t *__restrict__ C1) {
+                      uint8_t *__restrict__ C1, const uint8_t *__restrict__ rad0) {
     const int view = blockIdx.y;
     const uint64_t *ref = view ? cr : cl;
     const uint64_t *oth = view ? cl : cr;
@@ -86,7 +87,8 @@ __global__ void __launch_bounds__(256)
     uint8_t *C = view ? C1 : C0;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < N;
          p += (long)gridDim.x * blockDim.x)
-        cost_pixel_slot(ref, oth, base, W, p, R, K, Kp, invalid, view, C);
+        cost_pixel_slot(ref, oth, base, W, p, R, K, Kp, invalid, view, C,
+                        view == 0 && rad0 ? (int)rad0[p] : R);
 }
 
 // ------------------------------------------------------------------ SGM
@@ -578,13 +580,13 @@ int slot_width(int K) { return geom_for(K).Kp; }
 
 int launch_band_costs_slot(const uint64_t *cl, const uint64_t *cr, const int32_t *base0,
                            const int32_t *base1, int W, int H, int R, int invalid, uint8_t *C0,
-                           uint8_t *C1, int nviews, cudaStream_t st) {
+                           uint8_t *C1, int nviews, cudaStream_t st, const uint8_t *rad0) {
     const long N = (long)W * H;
     const int K = 2 * R + 1;
     dim3 grd(grid_for(N, 256, 148 * 8), nviews);
     count_launch();
     k_band_costs_slot<<<grd, 256, 0, st>>>(cl, cr, base0, base1, W, N, R, K, slot_width(K),
-                                           invalid, C0, C1);
+                                           invalid, C0, C1, rad0);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -698,7 +700,7 @@ __global__ void __launch_bounds__(256) k_b_costs(BatchTables t) {
     const uint64_t *oth = view ? P.cen0 : P.cen1;
     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
         cost_pixel_slot(ref, oth, view ? P.base1 : P.base0, P.W, p, t.R, t.K, t.Kp, t.invalid,
-                        view, view ? P.C1 : P.C0);
+                        view, view ? P.C1 : P.C0, t.R);
 }
 
 template <int NR, typename LT>

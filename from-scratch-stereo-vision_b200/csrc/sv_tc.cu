@@ -128,14 +128,16 @@ __global__ void __launch_bounds__(kTcM) k_conv_tc(TcConv a) {
 
     const long M = (long)a.OD * a.OH * a.OW;
     const long tiles_img = (M + kTcM - 1) / kTcM;
-    const long tiles = tiles_img * (a.mode == 0 ? a.nimg : 1);
+    const int nb = a.nb > 0 ? a.nb : 1;
+    const long tiles = tiles_img * (a.mode == 0 ? a.nimg : 1) * nb;
     const int ohw = a.OH * a.OW;
     const long plane = (long)a.D * a.H * a.W;     // one input channel (mode 0)
     const long fplane = (long)a.H * a.W;          // one feature channel (mode 1)
     unsigned phase = 0;
     for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int img = (int)(tile / tiles_img);
-        const long mi = (tile - img * tiles_img) * kTcM + tid;
+        const int item = (int)(tile / tiles_img);
+        const int img = item / nb, bi = item - img * nb;
+        const long mi = (tile - item * tiles_img) * kTcM + tid;
         const bool row_ok = mi < M;
         int od = 0, oy = 0, ox = 0;
         if (row_ok) {
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(kTcM) k_conv_tc(TcConv a) {
             ox = r - oy * a.OW;
         }
         // ---- gather this thread's im2col row, 8 k at a time
-        const float *x0 = img ? a.x[1] : a.x[0], *x1 = a.x[1];
+        const float *x0 = (img ? a.x[1] : a.x[0]) + bi * a.xs, *x1 = a.x[1] + bi * a.xs;
         const int by = a.mode == 0 ? oy * a.stride : oy, bx = a.mode == 0 ? ox * a.stride : ox;
         for (int kg = 0; kg < a.Kpad / 8; ++kg) {
             __align__(16) __nv_bfloat16 v[8];
@@ -208,12 +210,15 @@ __global__ void __launch_bounds__(kTcM) k_conv_tc(TcConv a) {
             : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (row_ok) {
-            float *y = img ? a.y[1] : a.y[0];
+            float *y = (img ? a.y[1] : a.y[0]) + bi * a.ys;
+            const float *aux = a.aux ? a.aux + bi * a.ys : nullptr;
 #pragma unroll
             for (int n = 0; n < kTcN; ++n) {
                 if (n < a.OC) {
-                    float v = __uint_as_float(r[n]) + __ldg(a.bias + n);
+                    float v = __uint_as_float(r[n]);
+                    if (a.bias) v += __ldg(a.bias + n);
                     if (a.act == 1) v = v > 0.f ? v : v * 0.2f;
+                    if (a.act == 2) v = __ldg(aux + (long)n * M + mi) > 0.f ? v : v * 0.2f;
                     y[(long)n * M + mi] = v;
                 }
             }
@@ -245,7 +250,7 @@ void tc_pack_weights(const double *w, int OC, int K, uint16_t *out) {
 int launch_conv_tc(const TcConv &a, cudaStream_t st) {
     if (a.OC < 1 || a.OC > kTcN || a.K < 1 || a.K > kTcMaxK || a.Kpad != tc_kpad(a.K) ||
         (a.mode == 0 && (a.nimg < 1 || a.nimg > 2)) || (a.mode == 1 && a.nd != 3) ||
-        !a.wB || !a.bias || !a.err) {
+        !a.wB || !a.err || (a.act == 2 && !a.aux) || a.nb < 0) {
         set_error("tensor-core conv: IC=%d OC=%d K=%d outside the kernel's shapes", a.IC, a.OC,
                   a.K);
         return SV_ERR_PARAM;
@@ -255,7 +260,8 @@ int launch_conv_tc(const TcConv &a, cudaStream_t st) {
         cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long M = (long)a.OD * a.OH * a.OW;
     if (M == 0) return SV_OK;
-    const long tiles = (M + kTcM - 1) / kTcM * (a.mode == 0 ? a.nimg : 1);
+    const long tiles =
+        (M + kTcM - 1) / kTcM * (a.mode == 0 ? a.nimg : 1) * (a.nb > 0 ? a.nb : 1);
     int dev = 0, sms = 148;
     SV_CUDA_TRY(cudaGetDevice(&dev));
     SV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -264,6 +270,239 @@ int launch_conv_tc(const TcConv &a, cudaStream_t st) {
     const unsigned blocks = (unsigned)(tiles < cap ? tiles : cap);
     count_launch();
     k_conv_tc<<<blocks, kTcM, smem, st>>>(a);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+// ------------------------------------------------------- weight gradient
+// D[m][n] = sum over pixels p of A[m][p] * B[n][p] with A[m = c*9 + t][p] =
+// x[c][p + tap t] (row IC*9 is all ones, giving the bias gradient) and
+// B[n = o][p] = g[o][p].  M is 1 or 2 tiles of 128 rows (IC*9 + 1 <= 256),
+// N = 16, K = the pixels, 64 per chunk.  CTAs stride over chunks with two
+// shared-memory stages: the gather of chunk i overlaps the MMAs of chunk
+// i-1, and stage reuse waits for the commit of chunk i-2.  At the end every
+// CTA adds its FP32 partial sums into gw / gb.
+constexpr int kWgK = 64;
+
+__global__ void __launch_bounds__(kTcM) k_wgrad_tc(TcWgrad a, int mtiles) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    __shared__ int4 pix[2][kWgK];                    // (item, y, x, valid)
+    const size_t a_tile = (size_t)kTcM * kWgK * 2;
+    const size_t stage = (size_t)mtiles * a_tile + (size_t)kTcN * kWgK * 2;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+    const long HW = (long)a.H * a.W;
+    const long P = HW * a.nb;
+    const long chunks = (P + kWgK - 1) / kWgK;
+    const int KR = a.IC * 9;
+    // this thread's A rows, one per M tile
+    int rc[2], rdy[2], rdx[2], rkind[2];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        const int m = mt * kTcM + tid;
+        rc[mt] = 0; rdy[mt] = 0; rdx[mt] = 0;
+        rkind[mt] = m < KR ? 0 : (m == KR ? 1 : 2);
+        if (m < KR) {
+            const int c = m / 9, t = m - (m / 9) * 9;
+            rc[mt] = c;
+            rdy[mt] = (t / 3 - 1) * a.dil;
+            rdx[mt] = (t - (t / 3) * 3 - 1) * a.dil;
+        }
+    }
+    int it = 0;
+    for (long ch = blockIdx.x; ch < chunks; ch += gridDim.x, ++it) {
+        const int s = it & 1;
+        unsigned char *sA = smem + s * stage;
+        unsigned char *sB = sA + (size_t)mtiles * a_tile;
+        if (it >= 2 && !failed && !mbar_wait(&mbar[s], ((it - 2) >> 1) & 1)) {
+            failed = 1;
+            flag_error(a.err, SV_ERR_CUDA);
+        }
+        __syncthreads();
+        if (failed) break;
+        if (tid < kWgK) {
+            const long p = ch * kWgK + tid;
+            int4 e = make_int4(0, 0, 0, 0);
+            if (p < P) {
+                const int item = (int)(p / HW);
+                const int r = (int)(p - item * HW);
+                e = make_int4(item, r / a.W, r - (r / a.W) * a.W, 1);
+            }
+            pix[s][tid] = e;
+        }
+        __syncthreads();
+        {   // B: thread (n, 8 pixels)
+            const int n = tid >> 3, kg = tid & 7;
+            __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int4 e = pix[s][kg * 8 + j];
+                float f = 0.f;
+                if (e.w && n < a.OC)
+                    f = __ldg(a.g + e.x * a.gs + n * HW + (long)e.y * a.W + e.z);
+                v[j] = __float2bfloat16_rn(f);
+            }
+            *reinterpret_cast<uint4 *>(sB + (size_t)(kg * 2 + (n >> 3)) * 128 + (n & 7) * 16) =
+                *reinterpret_cast<const uint4 *>(v);
+        }
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {        // A: this thread's row of each M tile
+            if (mt >= mtiles) break;
+            unsigned char *tA = sA + (size_t)mt * a_tile;
+            const float *xc = a.x + (long)rc[mt] * HW;
+            for (int kg = 0; kg < kWgK / 8; ++kg) {
+                __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int4 e = pix[s][kg * 8 + j];
+                    float f = 0.f;
+                    if (e.w) {
+                        if (rkind[mt] == 0) {
+                            const int yy = e.y + rdy[mt], xx = e.z + rdx[mt];
+                            if (yy >= 0 && yy < a.H && xx >= 0 && xx < a.W)
+                                f = __ldg(xc + e.x * a.xs + (long)yy * a.W + xx);
+                        } else if (rkind[mt] == 1) {
+                            f = 1.f;
+                        }
+                    }
+                    v[j] = __float2bfloat16_rn(f);
+                }
+                *reinterpret_cast<uint4 *>(tA + (size_t)(kg * (kTcM / 8) + (tid >> 3)) * 128 +
+                                           (tid & 7) * 16) = *reinterpret_cast<const uint4 *>(v);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0) {
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int mt = 0; mt < mtiles; ++mt) {
+                for (int ks = 0; ks < kWgK / 16; ++ks) {
+                    const uint64_t da = umma_desc(a0 + mt * (uint32_t)a_tile +
+                                                      ks * 2 * (kTcM / 8) * 128,
+                                                  (kTcM / 8) * 128, 128);
+                    const uint64_t db =
+                        umma_desc(b0 + ks * 2 * (kTcN / 8) * 128, (kTcN / 8) * 128, 128);
+                    const uint32_t acc = (it > 0 || ks > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                        ::"r"(tmem + mt * kTcN), "l"(da), "l"(db), "r"(kIdescBf16), "r"(acc));
+                }
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                ::"r"(smem_u32(&mbar[s]))
+                : "memory");
+        }
+    }
+    // the last commit covers every MMA this CTA issued
+    if (it > 0 && !failed && !mbar_wait(&mbar[(it - 1) & 1], ((it - 1) >> 1) & 1)) {
+        failed = 1;
+        flag_error(a.err, SV_ERR_CUDA);
+    }
+    __syncthreads();
+    if (it > 0 && !failed) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            if (mt >= mtiles) break;
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                  "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                  "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + mt * kTcN));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int m = mt * kTcM + tid;
+#pragma unroll
+            for (int n = 0; n < kTcN; ++n) {
+                if (n >= a.OC) break;
+                const float v = __uint_as_float(r[n]);
+                if (m < KR) atomicAdd(a.gw + (long)n * KR + m, v);
+                else if (m == KR) atomicAdd(a.gb + n, v);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(kTmemCols));
+}
+
+int launch_wgrad_tc(const TcWgrad &a, cudaStream_t st) {
+    if (a.IC < 1 || a.OC < 1 || a.OC > kTcN || a.IC * 9 + 1 > 2 * kTcM || a.dil < 1 ||
+        a.H < 1 || a.W < 1 || a.nb < 1 || !a.x || !a.g || !a.gw || !a.gb || !a.err) {
+        set_error("tensor-core weight gradient: IC=%d OC=%d outside the kernel's shapes", a.IC,
+                  a.OC);
+        return SV_ERR_PARAM;
+    }
+    const int mtiles = (a.IC * 9 + 1 + kTcM - 1) / kTcM;
+    const size_t smem = 2 * ((size_t)mtiles * kTcM * kWgK * 2 + (size_t)kTcN * kWgK * 2);
+    SV_CUDA_TRY(
+        cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long chunks = ((long)a.H * a.W * a.nb + kWgK - 1) / kWgK;
+    int dev = 0, sms = 148;
+    SV_CUDA_TRY(cudaGetDevice(&dev));
+    SV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long cap = (long)sms * 2;
+    const unsigned blocks = (unsigned)(chunks < cap ? chunks : cap);
+    count_launch();
+    k_wgrad_tc<<<blocks, kTcM, smem, st>>>(a, mtiles);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+__global__ void k_pack_weights(const float *__restrict__ w, int OC, int IC, int transpose,
+                               int K, int Kpad, uint16_t *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kTcN * Kpad) return;
+    const int n = i / Kpad, k = i - (i / Kpad) * Kpad;
+    float v = 0.f;
+    if (!transpose) {
+        if (n < OC && k < K) v = w[n * K + k];
+    } else if (n < IC && k < K) {
+        const int o = k / 9, t = k - (k / 9) * 9;
+        v = w[(o * IC + n) * 9 + (8 - t)];
+    }
+    const __nv_bfloat16 b = __float2bfloat16_rn(v);
+    out[((size_t)((k >> 3) * 2 + (n >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) / 2] =
+        *reinterpret_cast<const uint16_t *>(&b);
+}
+
+int launch_pack_weights(const float *w, int OC, int IC, int transpose, uint16_t *out,
+                        cudaStream_t st) {
+    const int K = (transpose ? OC : IC) * 9;
+    if ((transpose ? IC : OC) > kTcN) {
+        set_error("packed operand has more than 16 rows");
+        return SV_ERR_PARAM;
+    }
+    const int Kpad = tc_kpad(K);
+    count_launch();
+    k_pack_weights<<<(kTcN * Kpad + 255) / 256, 256, 0, st>>>(w, OC, IC, transpose, K, Kpad,
+                                                              out);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

@@ -222,6 +222,69 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right,
                         double *disp_full, double *disp_work, int *Ww, int *Hw,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Learned adaptive band (no counterpart in the reference: it extends
+ * lr_refine, stereonet.py:5343-5391, whose band is fixed at +-R around the
+ * network disparity).  A 4-layer convolutional band net (5810 parameters,
+ * BF16 tensor-core kernels with FP32 accumulation) reads SV_BAND_FEATURES
+ * per-pixel features and predicts a shift of the band centre and a Laplace
+ * scale; confident pixels get the shifted centre and a narrower band, the
+ * rest keep the fixed band.  Trained with Adam (stereonet.py:1354-1387) on
+ * full-range SGM disparities.  All tensors are device buffers, [item][c][H][W].
+ * ---------------------------------------------------------------------- */
+#define SV_BAND_FEATURES 6
+#define SV_BAND_OUTPUTS 2
+typedef struct sv_band sv_band;
+long sv_band_param_count(void);
+int sv_band_create(const double *params, long n_params, sv_band **out);
+void sv_band_destroy(sv_band *band);
+/* copies the (FP32 master) parameters to host memory as doubles; syncs */
+int sv_band_get_params(const sv_band *band, double *out, long n_params);
+
+/* features [6][H][W] FP32 from the two views (9x7 census) and disp0 (FP64),
+ * disparities searched over 0..dmax (dmax <= 255) */
+size_t sv_band_features_workspace_size(int W, int H);
+int sv_band_features(const void *left, const void *right, int dtype,
+                     const double *disp0, int W, int H, int dmax, float *feat,
+                     void *workspace, size_t workspace_bytes, void *stream);
+
+/* forward of nb items: feat [nb][6][H][W] -> out [nb][2][H][W] */
+size_t sv_band_workspace_size(int nb, int W, int H);
+int sv_band_forward(const sv_band *band, const float *feat, int nb, int W, int H,
+                    float *out, void *workspace, size_t workspace_bytes,
+                    void *stream);
+/* loss and gradients (FP32, parameter order) of target [nb][H][W] shifts on
+ * the mask [nb][H][W] (1 = labelled); grads / loss (device) may be NULL */
+int sv_band_grads(sv_band *band, const float *feat, const float *target,
+                  const uint8_t *mask, int nb, int W, int H, float *grads,
+                  double *loss, void *workspace, size_t workspace_bytes,
+                  void *stream);
+/* sv_band_grads followed by one Adam step (b1 0.9, b2 0.999, eps 1e-8,
+ * gradient clip 5) at learning rate lr */
+int sv_band_train_step(sv_band *band, const float *feat, const float *target,
+                       const uint8_t *mask, int nb, int W, int H, double lr,
+                       double *loss, void *workspace, size_t workspace_bytes,
+                       void *stream);
+/* target = clamp(label - disp0, +-shift_max), mask = (status == 0) */
+int sv_band_targets(const double *label, const uint8_t *status,
+                    const double *disp0, long n, double shift_max, float *target,
+                    uint8_t *mask, void *stream);
+/* out [2][H][W] of one item -> band centre (FP64) and half-width per pixel:
+ * b = exp(clamp(out1 + 1)); b <= b_thr: centre = disp0 + clamp(32 out0),
+ * half-width = clamp(ceil(rad_k * b), rad_min, R); else centre = disp0,
+ * half-width R */
+int sv_band_apply(const float *out, const double *disp0, int W, int H,
+                  double b_thr, double rad_k, int rad_min, int R,
+                  double shift_max, double *centre, uint8_t *rad, void *stream);
+/* lr_refine around `centre` with the left view's band restricted to
+ * |k - R| <= rad[p] (other slots cost the invalid value); same workspace as
+ * sv_lr_refine.  rad[p] = R everywhere gives sv_lr_refine's result. */
+int sv_lr_refine_band(const void *left, const void *right, int dtype,
+                      const double *centre, const uint8_t *rad, int W, int H,
+                      double tol, const sv_refine_params *p, double *out,
+                      uint8_t *status, void *workspace, size_t workspace_bytes,
+                      void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,8 +37,9 @@ def build() -> str:
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_SO) or os.path.getmtime(_SO) < os.path.getmtime(
-                os.path.join(_HERE, "sv_oracle.c")):
+        if not os.path.exists(_SO) or os.path.getmtime(_SO) < max(
+                os.path.getmtime(os.path.join(_HERE, f))
+                for f in ("sv_oracle.c", "sv_band_oracle.c")):
             build()
         L = ctypes.CDLL(_SO)
         L.orc_fexp.restype = _dbl
@@ -46,6 +47,8 @@ def lib():
         L.orc_peak.restype = _dbl
         L.orc_peak.argtypes = [_d, ctypes.c_long, _dbl]
         L.orc_param_count.restype = ctypes.c_long
+        L.orc_band_param_count.restype = ctypes.c_long
+        L.orc_band_loss.restype = _dbl
         _lib = L
     return _lib
 
@@ -226,3 +229,99 @@ def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64,
     if return_trace:
         return res, [int(t) for t in trace if t > 0]
     return res
+
+
+# ------------------------------------------------------------ learned band
+# FP64 definition of the band predictor (sv_band_oracle.c): features, the
+# 4-layer net's forward / loss / gradients, Adam, band application and the
+# masked lr_refine.
+_u8 = ctypes.POINTER(ctypes.c_uint8)
+
+
+def band_param_count() -> int:
+    return int(lib().orc_band_param_count())
+
+
+def band_features(left, right, disp0, W, H, dmax) -> np.ndarray:
+    """[6][H][W] features (census 9x7 of both views, disparity, gray)."""
+    gl, gr = _f64(left), _f64(right)
+    cl, cr = census(gl, W, H, 4, 3), census(gr, W, H, 4, 3)
+    d0 = _f64(disp0)
+    out = np.zeros(6 * W * H)
+    _check(lib().orc_band_features(_p(cl, _u64), _p(cr, _u64), _p(d0), _p(gl), W, H,
+                                   int(dmax), _p(out)), "band_features")
+    return out
+
+
+def band_forward(params, feat, nb, W, H) -> np.ndarray:
+    params, feat = _f64(params), _f64(feat)
+    out = np.zeros(nb * 2 * W * H)
+    _check(lib().orc_band_forward(_p(params), _p(feat), nb, W, H, _p(out)), "band_forward")
+    return out
+
+
+def band_grads(params, feat, target, mask, nb, W, H):
+    """-> (gradients in parameter order, loss)."""
+    params, feat, target = _f64(params), _f64(feat), _f64(target)
+    mask = np.ascontiguousarray(mask, dtype=np.uint8)
+    g = np.zeros(band_param_count())
+    loss = _dbl()
+    _check(lib().orc_band_grads(_p(params), _p(feat), _p(target), _p(mask, _u8), nb, W, H,
+                                _p(g), ctypes.byref(loss)), "band_grads")
+    return g, loss.value
+
+
+def band_loss(out, target, mask, nb, W, H) -> float:
+    out, target = _f64(out), _f64(target)
+    mask = np.ascontiguousarray(mask, dtype=np.uint8)
+    return float(lib().orc_band_loss(_p(out), _p(target), _p(mask, _u8), nb, W, H, None))
+
+
+class Adam:
+    """Adam.step of stereonet.py:1354-1387 over one flat parameter vector."""
+
+    def __init__(self, params, lr=5e-4, b1=0.9, b2=0.999, eps=1e-8, clip=5.0):
+        self.p = np.array(params, dtype=np.float64)
+        self.m = np.zeros_like(self.p)
+        self.v = np.zeros_like(self.p)
+        self.lr, self.b1, self.b2, self.eps, self.clip = lr, b1, b2, eps, clip
+        self.b1t, self.b2t = _dbl(1.0), _dbl(1.0)
+
+    def step(self, g):
+        g = _f64(g)
+        lib().orc_adam_step(_p(self.p), _p(g), _p(self.m), _p(self.v),
+                            ctypes.c_long(self.p.size), _dbl(self.lr), _dbl(self.b1),
+                            _dbl(self.b2), _dbl(self.eps), _dbl(self.clip),
+                            ctypes.byref(self.b1t), ctypes.byref(self.b2t))
+        return self.p
+
+
+def band_apply(out, disp0, W, H, b_thr=3.0, rad_k=3.0, rad_min=3, R=10, shift_max=160.0):
+    out, d0 = _f64(out), _f64(disp0)
+    centre = np.zeros(W * H)
+    rad = np.zeros(W * H, dtype=np.uint8)
+    lib().orc_band_apply(_p(out), _p(d0), W, H, _dbl(b_thr), _dbl(rad_k), int(rad_min), int(R),
+                         _dbl(shift_max), _p(centre), _p(rad, _u8))
+    return centre, rad
+
+
+def band_targets(label, status, disp0, shift_max=160.0):
+    label, d0 = _f64(label), _f64(disp0)
+    status = np.ascontiguousarray(status, dtype=np.int32)
+    t = np.zeros(label.size)
+    m = np.zeros(label.size, dtype=np.uint8)
+    lib().orc_band_targets(_p(label), _p(status, _i32), _p(d0), ctypes.c_long(label.size),
+                           _dbl(shift_max), _p(t), _p(m, _u8))
+    return t, m
+
+
+def lr_refine_band(left, right, centre, rad, W, H, tol=2.0, R=10, P1=12.0, P2=150.0, rx=4,
+                   ry=3):
+    gl, gr, c = _f64(left), _f64(right), _f64(centre)
+    rad = None if rad is None else np.ascontiguousarray(rad, dtype=np.uint8)
+    out = np.zeros(W * H)
+    st = np.zeros(W * H, dtype=np.int32)
+    _check(lib().orc_lr_refine_band(_p(gl), _p(gr), _p(c), None if rad is None else _p(rad, _u8),
+                                    W, H, _dbl(tol), R, _dbl(P1), _dbl(P2), rx, ry, _p(out),
+                                    _p(st, _i32)), "lr_refine_band")
+    return out, st

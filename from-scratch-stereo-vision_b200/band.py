@@ -159,7 +159,8 @@ class BandNet:
 
     def train_step(self, feat, target, mask, nb, W, H, lr=5e-4, stream=None):
         """One Adam step on a batch of device tensors (no host sync); the
-        batch loss accumulates into self.loss[0] (zero it to read a mean)."""
+        batch's loss (before the step) is left in a device scalar that
+        ``last_loss`` reads."""
         ws, need = self._workspace(nb, W, H)
         _lib.check(self.lib.sv_band_train_step(self.handle, _ptr(feat), _ptr(target), _ptr(mask),
                                                nb, W, H, float(lr), _ptr(self._step_loss()),

@@ -29,7 +29,7 @@ constexpr int kBandDil[kBandL] = {1, 2, 4, 1};
 constexpr float kShiftScale = 32.f, kRho0 = 1.f;
 constexpr float kRhoMin = -1.3862943611198906f, kRhoMax = 4.852030263919617f;
 constexpr double kRhoMinD = -1.3862943611198906, kRhoMaxD = 4.852030263919617;
-constexpr int kFeatRows = 8;          // output rows per feature thread
+constexpr int kFeatRows = 4;          // output rows per feature thread
 constexpr int kAggHalf = 4;           // vertical aggregation: 9 rows
 constexpr int kBandInvalid = 66;
 
@@ -65,66 +65,112 @@ __device__ __forceinline__ double gray_of<double>(const double *img, long p) {
     return img[p];
 }
 
-// One thread per (column, 8 output rows).  For every d in [0, dmax] the
-// thread forms the 16 row costs of its window once and slides the 9-row sum
-// down its 8 rows, keeping per row the first minimum (as a packed key
-// agg << 8 | d), the minimum inside the +-10 band around d0 and the cost at
-// round(d0).
+// Thread (column, 8 output rows, disparity group): the disparity range is
+// split over kFeatDG groups.  For each of its d the thread forms the 16 row
+// costs of its window once and slides the 9-row sum down its 8 rows, keeping
+// per row the first minimum (as a packed key agg << 8 | d, so the smallest d
+// wins ties), the minimum inside the +-10 band around d0 and the cost at
+// round(d0); the groups combine with shared-memory atomicMin.  The right
+// view's census words the block reads (its 16 rows, columns x0 - dmax ..
+// x0 + 31) are staged in shared memory first.
+constexpr int kFeatDG = 4, kFeatSeg = 2;
+constexpr int kFeatBR = kFeatSeg * kFeatRows + 2 * kAggHalf;   // staged rows
+
+static size_t band_features_smem(int dmax) { return (size_t)kFeatBR * (32 + dmax) * 8; }
+
 template <typename T>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(32 * kFeatSeg * kFeatDG)
     k_band_features(const uint64_t *__restrict__ cl, const uint64_t *__restrict__ cr,
                     const double *__restrict__ d0, const T *__restrict__ left, int W, int H,
                     int dmax, float *__restrict__ feat, int *__restrict__ err) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y0 = (blockIdx.y * blockDim.y + threadIdx.y) * kFeatRows;
-    if (x >= W || y0 >= H) return;
-    constexpr int NR = kFeatRows + 2 * kAggHalf;
-    uint64_t clv[NR];
-    long rowoff[NR];
-#pragma unroll
-    for (int i = 0; i < NR; ++i) {
-        int yy = y0 - kAggHalf + i;
-        yy = yy < 0 ? 0 : (yy >= H ? H - 1 : yy);
-        rowoff[i] = (long)yy * W + x;
-        clv[i] = __ldg(cl + rowoff[i]);
-    }
-    int r0[kFeatRows];
-    unsigned best[kFeatRows];
-    int band[kFeatRows], cd0[kFeatRows];
-#pragma unroll
-    for (int j = 0; j < kFeatRows; ++j) {
-        const int y = y0 + j < H ? y0 + j : H - 1;
-        const double t = __dadd_rn(d0[(long)y * W + x], 0.5);
-        int r = 0;
-        if (!(t > -9.0e15 && t < 9.0e15)) {
-            flag_error(err, SV_ERR_DISP);
-        } else if (t >= (double)dmax) {
-            r = dmax;
-        } else if (t >= 1.0) {
-            r = __double2int_rz(t);
+    __shared__ unsigned s_best[kFeatSeg][kFeatRows][32];
+    __shared__ int s_band[kFeatSeg][kFeatRows][32];
+    __shared__ int s_cd0[kFeatSeg][kFeatRows][32];
+    extern __shared__ uint64_t s_cr[];                 // [kFeatBR][32 + dmax]
+    const int tx = threadIdx.x, ty = threadIdx.y, g = threadIdx.z;
+    const int x = blockIdx.x * 32 + tx;
+    const int y0 = (blockIdx.y * kFeatSeg + ty) * kFeatRows;
+    const bool active = x < W && y0 < H;
+    const int CW = 32 + dmax;
+    {
+        const int yb = blockIdx.y * kFeatSeg * kFeatRows - kAggHalf;
+        const int xb = blockIdx.x * 32 - dmax;
+        const int tid = (g * kFeatSeg + ty) * 32 + tx;
+        for (int i = tid; i < kFeatBR * CW; i += 32 * kFeatSeg * kFeatDG) {
+            const int r = i / CW, c = i - (i / CW) * CW;
+            int yy = yb + r;
+            yy = yy < 0 ? 0 : (yy >= H ? H - 1 : yy);
+            const int gx = xb + c;
+            s_cr[i] = gx >= 0 && gx < W ? __ldg(cr + (long)yy * W + gx) : 0ull;
         }
-        r0[j] = r;
-        best[j] = 0xffffffffu;
-        band[j] = 1 << 30;
-        cd0[j] = 0;
     }
-    for (int d = 0; d <= dmax; ++d) {
-        int c[NR];
-        const bool in = x - d >= 0;
-#pragma unroll
-        for (int i = 0; i < NR; ++i)
-            c[i] = in ? __popcll(clv[i] ^ __ldg(cr + rowoff[i] - d)) : kBandInvalid;
-        int s = 0;
-#pragma unroll
-        for (int i = 0; i < 2 * kAggHalf + 1; ++i) s += c[i];
+    if (g == 0) {
 #pragma unroll
         for (int j = 0; j < kFeatRows; ++j) {
-            if (j > 0) s += c[j + 2 * kAggHalf] - c[j - 1];
-            best[j] = min(best[j], ((unsigned)s << 8) | (unsigned)d);
-            if (abs(d - r0[j]) <= 10) band[j] = min(band[j], s);
-            if (d == r0[j]) cd0[j] = s;
+            s_best[ty][j][tx] = 0xffffffffu;
+            s_band[ty][j][tx] = 1 << 30;
+            s_cd0[ty][j][tx] = 0;
         }
     }
+    __syncthreads();
+    if (active) {
+        constexpr int NR = kFeatRows + 2 * kAggHalf;
+        uint64_t clv[NR];
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            int yy = y0 - kAggHalf + i;
+            yy = yy < 0 ? 0 : (yy >= H ? H - 1 : yy);
+            clv[i] = __ldg(cl + (long)yy * W + x);
+        }
+        const uint64_t *crow = s_cr + ty * kFeatRows * CW + tx + dmax;   // column x - d at -d
+        int r0[kFeatRows];
+        unsigned best[kFeatRows];
+        int band[kFeatRows], cd0[kFeatRows];
+#pragma unroll
+        for (int j = 0; j < kFeatRows; ++j) {
+            const int y = y0 + j < H ? y0 + j : H - 1;
+            const double t = __dadd_rn(d0[(long)y * W + x], 0.5);
+            int r = 0;
+            if (!(t > -9.0e15 && t < 9.0e15)) {
+                if (g == 0) flag_error(err, SV_ERR_DISP);
+            } else if (t >= (double)dmax) {
+                r = dmax;
+            } else if (t >= 1.0) {
+                r = __double2int_rz(t);
+            }
+            r0[j] = r;
+            best[j] = 0xffffffffu;
+            band[j] = 1 << 30;
+            cd0[j] = -1;
+        }
+        const int chunk = (dmax + kFeatDG) / kFeatDG;
+        const int dlo = g * chunk, dhi = min(dmax, dlo + chunk - 1);
+        for (int d = dlo; d <= dhi; ++d) {
+            int c[NR];
+            const bool in = x - d >= 0;
+#pragma unroll
+            for (int i = 0; i < NR; ++i)
+                c[i] = in ? __popcll(clv[i] ^ crow[i * CW - d]) : kBandInvalid;
+            int s = 0;
+#pragma unroll
+            for (int i = 0; i < 2 * kAggHalf + 1; ++i) s += c[i];
+#pragma unroll
+            for (int j = 0; j < kFeatRows; ++j) {
+                if (j > 0) s += c[j + 2 * kAggHalf] - c[j - 1];
+                best[j] = min(best[j], ((unsigned)s << 8) | (unsigned)d);
+                if (abs(d - r0[j]) <= 10) band[j] = min(band[j], s);
+                if (d == r0[j]) cd0[j] = s;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kFeatRows; ++j) {
+            atomicMin(&s_best[ty][j][tx], best[j]);
+            atomicMin(&s_band[ty][j][tx], band[j]);
+            if (cd0[j] >= 0) s_cd0[ty][j][tx] = cd0[j];     // one group owns d == r0
+        }
+    }
+    __syncthreads();
+    if (!active || g != 0) return;
     const long N = (long)W * H;
 #pragma unroll
     for (int j = 0; j < kFeatRows; ++j) {
@@ -132,12 +178,13 @@ __global__ void __launch_bounds__(128)
         if (y >= H) break;
         const long p = (long)y * W + x;
         const double dd = d0[p];
-        const int dw = (int)(best[j] & 0xffu), aw = (int)(best[j] >> 8);
+        const unsigned bk = s_best[ty][j][tx];
+        const int dw = (int)(bk & 0xffu), aw = (int)(bk >> 8);
         feat[p] = (float)__ddiv_rn(dd, 64.0);
         feat[N + p] = (float)__ddiv_rn(__dsub_rn((double)dw, dd), 64.0);
         feat[2 * N + p] = (float)__ddiv_rn((double)aw, 558.0);
-        feat[3 * N + p] = (float)__ddiv_rn((double)cd0[j], 558.0);
-        feat[4 * N + p] = (float)__ddiv_rn((double)band[j], 558.0);
+        feat[3 * N + p] = (float)__ddiv_rn((double)s_cd0[ty][j][tx], 558.0);
+        feat[4 * N + p] = (float)__ddiv_rn((double)s_band[ty][j][tx], 558.0);
         feat[5 * N + p] = (float)__dsub_rn(gray_of<T>(left, p), 0.5);
     }
 }
@@ -476,17 +523,17 @@ int sv_band_features(const void *left, const void *right, int dtype, const doubl
     cudaStream_t st = (cudaStream_t)stream;
     SV_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(DevFlags), st));
     SV_TRY(launch_census(left, right, dtype, W, H, 4, 3, cl, cr, st));
-    const dim3 blk(32, 4);
-    const dim3 grd((W + 31) / 32, ((H + kFeatRows - 1) / kFeatRows + 3) / 4);
+    const dim3 blk(32, kFeatSeg, kFeatDG);
+    const dim3 grd((W + 31) / 32, ((H + kFeatRows - 1) / kFeatRows + kFeatSeg - 1) / kFeatSeg);
     count_launch();
     if (dtype == SV_U8)
-        k_band_features<uint8_t><<<grd, blk, 0, st>>>(cl, cr, disp0, (const uint8_t *)left, W, H,
+        k_band_features<uint8_t><<<grd, blk, band_features_smem(dmax), st>>>(cl, cr, disp0, (const uint8_t *)left, W, H,
                                                       dmax, feat, &flags->status);
     else if (dtype == SV_F32)
-        k_band_features<float><<<grd, blk, 0, st>>>(cl, cr, disp0, (const float *)left, W, H,
+        k_band_features<float><<<grd, blk, band_features_smem(dmax), st>>>(cl, cr, disp0, (const float *)left, W, H,
                                                     dmax, feat, &flags->status);
     else
-        k_band_features<double><<<grd, blk, 0, st>>>(cl, cr, disp0, (const double *)left, W, H,
+        k_band_features<double><<<grd, blk, band_features_smem(dmax), st>>>(cl, cr, disp0, (const double *)left, W, H,
                                                       dmax, feat, &flags->status);
     SV_LAUNCH_CHECK();
     return SV_OK;

@@ -24,6 +24,8 @@
 
 #include <cuda_bf16.h>
 
+#include <mutex>
+
 #include "sv_common.cuh"
 #include "sv_tc.cuh"
 
@@ -247,6 +249,231 @@ void tc_pack_weights(const double *w, int OC, int K, uint16_t *out) {
         }
 }
 
+// 2-D convolutions (mode 0, nd 2).  A CTA tile is 32 x 4 output pixels.
+// The input patch the tile reads -- every channel, the tile's rows and
+// columns scaled by the stride plus the dilated halo -- is first staged in
+// shared memory as BF16 by whole warps reading rows (coalesced, all loads
+// independent), and the im2col operand A is then built from shared memory:
+// element (m, k) is patch[ktab[k] + base(m)].  The MMA issue, the bounded
+// wait and the epilogue are those of k_conv_tc.
+constexpr int kT2W = 32, kT2H = 4;
+constexpr int kT2Cols = 3;              // patch columns per lane: PW <= 96
+
+__global__ void __launch_bounds__(kTcM) k_conv2d_tc(TcConv a, int PH, int PW) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    __shared__ int ktab[kTcMaxK];                  // patch offset of k, -1 for K padding
+    unsigned char *sA = smem;                                   // 128 x Kpad BF16
+    unsigned char *sB = smem + (size_t)a.Kpad * kTcM * 2;        // 16 x Kpad BF16
+    __nv_bfloat16 *patch = reinterpret_cast<__nv_bfloat16 *>(sB + (size_t)a.Kpad * kTcN * 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    const uint4 *wsrc = reinterpret_cast<const uint4 *>(a.wB);
+    uint4 *wdst = reinterpret_cast<uint4 *>(sB);
+    for (int i = tid; i < a.Kpad * kTcN * 2 / 16; i += kTcM) wdst[i] = __ldg(wsrc + i);
+    const int pplane = PH * PW;
+    for (int k = tid; k < a.Kpad; k += kTcM) {
+        int e = -1;
+        if (k < a.K) {
+            const int c = k / 9, t = k - (k / 9) * 9;
+            const int ky = t / 3, kx = t - (t / 3) * 3;
+            e = c * pplane + ky * a.dil * PW + kx * a.dil;
+        }
+        ktab[k] = e;
+    }
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+
+    const int tiles_x = (a.OW + kT2W - 1) / kT2W, tiles_y = (a.OH + kT2H - 1) / kT2H;
+    const long tiles_img = (long)tiles_x * tiles_y;
+    const int nb = a.nb > 0 ? a.nb : 1;
+    const long tiles = tiles_img * a.nimg * nb;
+    const long plane = (long)a.H * a.W, M = (long)a.OH * a.OW;
+    const int my = tid / kT2W, mx = tid - (tid / kT2W) * kT2W;
+    const int base = my * a.stride * PW + mx * a.stride;
+    unsigned phase = 0;
+    for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int item = (int)(tile / tiles_img);
+        const int img = item / nb, bi = item - img * nb;
+        const int t2 = (int)(tile - item * tiles_img);
+        const int ty0 = (t2 / tiles_x) * kT2H, tx0 = (t2 - (t2 / tiles_x) * tiles_x) * kT2W;
+        const float *x0 = (img ? a.x[1] : a.x[0]) + bi * a.xs;
+        const int iy0 = ty0 * a.stride - a.pad, ix0 = tx0 * a.stride - a.pad;
+        // ---- stage the patch: each warp takes 8 patch rows at a time, every
+        // lane up to kT2Cols columns of each, all loads issued before the stores
+        const int nrows = a.IC * PH;
+        for (int r0 = warp; r0 < nrows; r0 += (kTcM / 32) * 8) {
+            float v[8][kT2Cols];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int r = r0 + u * (kTcM / 32);
+                const int c = r / PH, py = r - (r / PH) * PH;
+                const int gy = iy0 + py;
+                const bool rok = r < nrows && gy >= 0 && gy < a.H;
+                const float *src = x0 + c * plane + (long)gy * a.W;
+#pragma unroll
+                for (int q = 0; q < kT2Cols; ++q) {
+                    const int px = lane + 32 * q, gx = ix0 + px;
+                    v[u][q] = rok && px < PW && gx >= 0 && gx < a.W ? __ldg(src + gx) : 0.f;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int r = r0 + u * (kTcM / 32);
+                if (r >= nrows) break;
+#pragma unroll
+                for (int q = 0; q < kT2Cols; ++q) {
+                    const int px = lane + 32 * q;
+                    if (px < PW) patch[(long)r * PW + px] = __float2bfloat16_rn(v[u][q]);
+                }
+            }
+        }
+        __syncthreads();
+        const int oy = ty0 + my, ox = tx0 + mx;
+        const bool row_ok = oy < a.OH && ox < a.OW;
+        for (int kg = 0; kg < a.Kpad / 8; ++kg) {
+            __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int e = ktab[kg * 8 + j];
+                v[j] = row_ok && e >= 0 ? patch[e + base] : __float2bfloat16_rn(0.f);
+            }
+            *reinterpret_cast<uint4 *>(sA + (size_t)(kg * (kTcM / 8) + (tid >> 3)) * 128 +
+                                       (tid & 7) * 16) = *reinterpret_cast<const uint4 *>(v);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0 && !failed) {
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int ks = 0; ks < a.Kpad / 16; ++ks) {
+                const uint64_t da = umma_desc(a0 + ks * 2 * (kTcM / 8) * 128, (kTcM / 8) * 128, 128);
+                const uint64_t db = umma_desc(b0 + ks * 2 * (kTcN / 8) * 128, (kTcN / 8) * 128, 128);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(kIdescBf16), "r"(ks));
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                ::"r"(smem_u32(&mbar))
+                : "memory");
+        }
+        if (!failed && !mbar_wait(&mbar, phase)) {
+            failed = 1;
+            flag_error(a.err, SV_ERR_CUDA);
+        }
+        phase ^= 1u;
+        __syncthreads();
+        if (failed) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row_ok) {
+            const long mi = (long)oy * a.OW + ox;
+            float *y = (img ? a.y[1] : a.y[0]) + bi * a.ys;
+            const float *aux = a.aux ? a.aux + bi * a.ys : nullptr;
+#pragma unroll
+            for (int n = 0; n < kTcN; ++n) {
+                if (n < a.OC) {
+                    float v = __uint_as_float(r[n]);
+                    if (a.bias) v += __ldg(a.bias + n);
+                    if (a.act == 1) v = v > 0.f ? v : v * 0.2f;
+                    if (a.act == 2) v = __ldg(aux + (long)n * M + mi) > 0.f ? v : v * 0.2f;
+                    y[(long)n * M + mi] = v;
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(kTmemCols));
+}
+
+// Per-device launch set-up, done once: the SM count and each kernel's
+// dynamic shared-memory limit (raised to kTcSmemMax; every launch checks
+// its own size against it).  Launches stay free of attribute calls.
+constexpr size_t kTcSmemMax = 200 * 1024;
+enum { kKConv = 0, kKConv2d = 1, kKWgrad = 2, kKCount = 3 };
+
+static int tc_setup(int which, const void *fn, int *sms) {
+    static std::mutex mu;
+    static int cached_sms[64];
+    static bool attr_done[64][kKCount];
+    int dev = 0;
+    SV_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("device ordinal %d out of range", dev);
+        return SV_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cached_sms[dev])
+        SV_CUDA_TRY(cudaDeviceGetAttribute(&cached_sms[dev], cudaDevAttrMultiProcessorCount, dev));
+    if (!attr_done[dev][which]) {
+        SV_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmemMax));
+        attr_done[dev][which] = true;
+    }
+    *sms = cached_sms[dev];
+    return SV_OK;
+}
+
+// CTAs per SM for a kernel using `smem` bytes of dynamic shared memory.
+static long tc_ctas_per_sm(size_t smem) {
+    const long per = (long)((220 * 1024) / (smem + 8 * 1024));
+    return per < 1 ? 1 : (per > 4 ? 4 : per);
+}
+
+static int launch_conv2d_tc(const TcConv &a, cudaStream_t st) {
+    const int PH = (kT2H - 1) * a.stride + 2 * a.dil + 1;
+    const int PW = (kT2W - 1) * a.stride + 2 * a.dil + 1;
+    const size_t patch = ((size_t)a.IC * PH * PW * 2 + 15) / 16 * 16;
+    const size_t smem = (size_t)a.Kpad * (kTcM + kTcN) * 2 + patch;
+    if (smem > kTcSmemMax || PW > 32 * kT2Cols) {
+        set_error("tensor-core conv: IC=%d dil=%d stride=%d patch too large", a.IC, a.dil,
+                  a.stride);
+        return SV_ERR_PARAM;
+    }
+    const long tiles = (long)((a.OW + kT2W - 1) / kT2W) * ((a.OH + kT2H - 1) / kT2H) * a.nimg *
+                       (a.nb > 0 ? a.nb : 1);
+    if (tiles == 0) return SV_OK;
+    int sms = 148;
+    const int rc = tc_setup(kKConv2d, (const void *)k_conv2d_tc, &sms);
+    if (rc) return rc;
+    const long cap = (long)sms * tc_ctas_per_sm(smem);
+    const unsigned blocks = (unsigned)(tiles < cap ? tiles : cap);
+    count_launch();
+    k_conv2d_tc<<<blocks, kTcM, smem, st>>>(a, PH, PW);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
 int launch_conv_tc(const TcConv &a, cudaStream_t st) {
     if (a.OC < 1 || a.OC > kTcN || a.K < 1 || a.K > kTcMaxK || a.Kpad != tc_kpad(a.K) ||
         (a.mode == 0 && (a.nimg < 1 || a.nimg > 2)) || (a.mode == 1 && a.nd != 3) ||
@@ -255,18 +482,22 @@ int launch_conv_tc(const TcConv &a, cudaStream_t st) {
                   a.K);
         return SV_ERR_PARAM;
     }
+    if (a.mode == 0 && a.nd == 2) {
+        if (a.K != a.IC * 9 || a.D != 1 || a.OD != 1 || a.stride < 1 || a.dil < 1) {
+            set_error("tensor-core conv2d: inconsistent shape");
+            return SV_ERR_PARAM;
+        }
+        return launch_conv2d_tc(a, st);
+    }
     const size_t smem = (size_t)a.Kpad * (kTcM + kTcN) * 2;
-    SV_CUDA_TRY(
-        cudaFuncSetAttribute(k_conv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long M = (long)a.OD * a.OH * a.OW;
     if (M == 0) return SV_OK;
     const long tiles =
         (M + kTcM - 1) / kTcM * (a.mode == 0 ? a.nimg : 1) * (a.nb > 0 ? a.nb : 1);
-    int dev = 0, sms = 148;
-    SV_CUDA_TRY(cudaGetDevice(&dev));
-    SV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long per_sm = smem > 100 * 1024 ? 1 : 2;
-    const long cap = (long)sms * per_sm;
+    int sms = 148;
+    const int rc = tc_setup(kKConv, (const void *)k_conv_tc, &sms);
+    if (rc) return rc;
+    const long cap = (long)sms * tc_ctas_per_sm(smem);
     const unsigned blocks = (unsigned)(tiles < cap ? tiles : cap);
     count_launch();
     k_conv_tc<<<blocks, kTcM, smem, st>>>(a);
@@ -461,12 +692,10 @@ int launch_wgrad_tc(const TcWgrad &a, cudaStream_t st) {
     }
     const int mtiles = (a.IC * 9 + 1 + kTcM - 1) / kTcM;
     const size_t smem = 2 * ((size_t)mtiles * kTcM * kWgK * 2 + (size_t)kTcN * kWgK * 2);
-    SV_CUDA_TRY(
-        cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const long chunks = ((long)a.H * a.W * a.nb + kWgK - 1) / kWgK;
-    int dev = 0, sms = 148;
-    SV_CUDA_TRY(cudaGetDevice(&dev));
-    SV_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int sms = 148;
+    const int rc = tc_setup(kKWgrad, (const void *)k_wgrad_tc, &sms);
+    if (rc) return rc;
     const long cap = (long)sms * 2;
     const unsigned blocks = (unsigned)(chunks < cap ? chunks : cap);
     count_launch();

@@ -251,7 +251,11 @@ class Evaluator:
 
 
 def _timed(torch, stream, fn):
-    """(result, device ms) of fn() on `stream` (host syncs inside included)."""
+    """(result, device ms) of a second fn() on `stream` (host syncs inside
+    included).  The untimed first run records the CUDA graphs of a new
+    predict_auto work width and allocates any new workspace, so every method
+    is timed in the same steady state."""
+    fn()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     r = fn()

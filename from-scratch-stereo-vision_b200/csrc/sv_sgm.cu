@@ -279,19 +279,43 @@ __device__ __forceinline__ void shift_regs(const unsigned (&t)[NR], unsigned (&o
 #pragma unroll
         for (int r = 0; r < NR; ++r) o[r] = __byte_perm(r > 0 ? t[r - 1] : kInf2, t[r], 0x5432);
     } else {
-        unsigned short buf[2 * NR];
+        // Any other jump, in registers: an odd jump first moves one slot
+        // towards its sign (byte_perm of adjacent registers, so no slot the
+        // rest still needs is dropped), the even rest is a barrel shift by
+        // whole registers (2 slots each) in stages of 1, 2, 4, 8, 16.
+        unsigned a[NR];
+        if ((s & 1) && s > 0) {
 #pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            buf[2 * r] = (unsigned short)(t[r] & 0xFFFFu);
-            buf[2 * r + 1] = (unsigned short)(t[r] >> 16);
+            for (int r = 0; r < NR; ++r) a[r] = __byte_perm(t[r], r < NR - 1 ? t[r + 1] : kInf2, 0x5432);
+            s -= 1;
+        } else if (s & 1) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) a[r] = __byte_perm(r > 0 ? t[r - 1] : kInf2, t[r], 0x5432);
+            s += 1;
+        } else {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) a[r] = t[r];
+        }
+        const int q = s / 2;                      // s is even here
+        if (q > 0) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                if (q & (1 << k)) {
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) a[r] = r + (1 << k) < NR ? a[r + (1 << k)] : kInf2;
+                }
+            }
+        } else if (q < 0) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) {
+                if ((-q) & (1 << k)) {
+#pragma unroll
+                    for (int r = NR - 1; r >= 0; --r) a[r] = r - (1 << k) >= 0 ? a[r - (1 << k)] : kInf2;
+                }
+            }
         }
 #pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            const int ia = 2 * r + s, ib = ia + 1;
-            const unsigned lo = (ia >= 0 && ia < 2 * NR) ? buf[ia] : 0x7FFFu;
-            const unsigned hi = (ib >= 0 && ib < 2 * NR) ? buf[ib] : 0x7FFFu;
-            o[r] = lo | (hi << 16);
-        }
+        for (int r = 0; r < NR; ++r) o[r] = a[r];
     }
 }
 
@@ -393,9 +417,15 @@ __device__ __forceinline__ void sgm_line_thread(const uint8_t *__restrict__ Cimg
                 }
             }
             bprev = bcur;
-            unsigned m2 = L[0];
+            unsigned mt[NR];                       // path minimum, as a depth-log2(NR) tree
 #pragma unroll
-            for (int r = 1; r < NR; ++r) m2 = __vminu2(m2, L[r]);
+            for (int r = 0; r < NR; ++r) mt[r] = L[r];
+#pragma unroll
+            for (int w = 1; w < NR; w *= 2) {
+#pragma unroll
+                for (int r = 0; r + w < NR; r += 2 * w) mt[r] = __vminu2(mt[r], mt[r + w]);
+            }
+            const unsigned m2 = mt[0];
             mq = (int)min(m2 & 0xFFFFu, m2 >> 16);
             // store the pixel's path costs, padding slots as 0
             LT *dst = Lo + t * lstep;

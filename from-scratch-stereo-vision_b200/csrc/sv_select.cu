@@ -3,26 +3,29 @@
 //
 // Exact selection on order-preserving 64-bit keys of the FP64 values (signed
 // zeros share one key: they compare equal in the sort, and a zero peak is
-// replaced by 0.5 anyway).
-//  Four passes over 16-bit digits from the top.  Pass p is a
-//  histogram of digit p over the keys that match the prefix chosen so far
-//  (warp-aggregated atomics into a 65536-bin global histogram), followed by
-//  a one-CTA parallel scan that picks the bin holding the rank and extends
-//  the prefix.  After pass 3 the prefix is the key.
+// replaced by 0.5 anyway).  Six passes over digits of 11, 11, 11, 11, 10 and
+// 10 bits from the top.  Pass p: every CTA histograms digit p of the keys
+// that match the prefix chosen so far into 2048 shared-memory bins
+// (warp-aggregated), adds its non-zero bins into a global histogram, and the
+// last CTA to finish (a device-scope counter) scans that histogram, picks the
+// bin holding the rank and extends the prefix.  One launch per pass; after
+// pass 5 the prefix is the key.
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
 
 namespace sv {
 
-constexpr int SEL_DIGIT = 16;
-constexpr int SEL_NB = 1 << SEL_DIGIT;
-constexpr int SEL_NPASS = 4;
+constexpr int SEL_NPASS = 6;
+constexpr int SEL_NB = 2048;
+__constant__ int kSelBits[SEL_NPASS] = {11, 11, 11, 11, 10, 10};
+__constant__ int kSelShift[SEL_NPASS] = {53, 42, 31, 20, 10, 0};
 
 struct SelState {
     unsigned long long prefix;
     long long rank;
     double value;
+    unsigned done[SEL_NPASS];          // CTAs finished per pass
 };
 
 __device__ __forceinline__ unsigned long long sel_key(double d) {
@@ -34,107 +37,105 @@ __device__ __forceinline__ double sel_unkey(unsigned long long k) {
     return __longlong_as_double((long long)b);
 }
 
-// ---------------------------------------------------- large: 16-bit radix
 __global__ void k_sel_init(SelState *s, long long rank) {
     s->prefix = 0ull;
     s->rank = rank;
     s->value = 0.0;
+    for (int p = 0; p < SEL_NPASS; ++p) s->done[p] = 0u;
 }
 
-__global__ void __launch_bounds__(256)
-    k_sel_hist16(const double *__restrict__ x, long n, int pass, const SelState *__restrict__ s,
-                 unsigned *__restrict__ hist) {
-    const int shift = 64 - SEL_DIGIT * (pass + 1);
-    const int top = shift + SEL_DIGIT;
+__global__ void __launch_bounds__(1024)
+    k_sel_pass(const double *__restrict__ x, long n, int pass, SelState *__restrict__ s,
+               unsigned *__restrict__ ghist) {
+    __shared__ unsigned hist[SEL_NB];
+    __shared__ unsigned wsum[32];
+    __shared__ int owner;
+    __shared__ unsigned long long owner_excl;
+    __shared__ bool last;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
+    const int shift = kSelShift[pass], bits = kSelBits[pass];
+    const int top = shift + bits;
+    const unsigned mask = (1u << bits) - 1u;
+    for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
+    __syncthreads();
     const unsigned long long pre = s->prefix;
-    const long stride = (long)gridDim.x * blockDim.x;
-    for (long i0 = blockIdx.x * (long)blockDim.x; i0 < n; i0 += stride) {
-        const long i = i0 + threadIdx.x;
+    const long stride = (long)gridDim.x * nt;
+    for (long i0 = blockIdx.x * (long)nt; i0 < n; i0 += stride) {
+        const long i = i0 + t;
         unsigned digit = 0xffffffffu;
         if (i < n) {
             const unsigned long long k = sel_key(x[i]);
-            if (top >= 64 || (k >> top) == (pre >> top))
-                digit = (unsigned)(k >> shift) & (SEL_NB - 1);
+            if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
         }
         const unsigned same = __match_any_sync(kFull, digit);
-        if (digit != 0xffffffffu && (threadIdx.x & 31) == __ffs(same) - 1)
-            atomicAdd(&hist[digit], (unsigned)__popc(same));
+        if (digit != 0xffffffffu && lane == __ffs(same) - 1) atomicAdd(&hist[digit], __popc(same));
     }
-}
-
-// One CTA of 1024 threads, 64 bins each: find the bin holding s->rank.
-__global__ void __launch_bounds__(1024)
-    k_sel_pick16(const unsigned *__restrict__ hist, int pass, SelState *__restrict__ s) {
-    __shared__ unsigned long long warp_tot[32];
-    __shared__ long long found[2];
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    const uint4 *h4 = reinterpret_cast<const uint4 *>(hist) + t * 16;
+    __syncthreads();
+    for (int i = t; i < SEL_NB; i += nt)
+        if (hist[i]) atomicAdd(&ghist[i], hist[i]);
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(&s->done[pass], 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // ---- last CTA: find the bin holding s->rank (2 bins per thread at 1024)
+    const int per = SEL_NB / nt;
     unsigned long long loc = 0;
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const uint4 v = h4[i];
-        loc += (unsigned long long)v.x + v.y + v.z + v.w;
-    }
-    unsigned long long x = loc;
+    for (int j = 0; j < per; ++j) loc += __ldcg(ghist + t * per + j);
+    unsigned long long incl = loc;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(kFull, x, o);
-        if (lane >= o) x += y;
+        const unsigned long long y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
     }
-    if (lane == 31) warp_tot[wid] = x;
+    if (lane == 31) wsum[wid] = (unsigned)incl;    // at most n < 2^32 keys
     __syncthreads();
     if (wid == 0) {
-        unsigned long long w = warp_tot[lane], v = w;
+        const int nw = nt >> 5;
+        unsigned long long w = lane < nw ? wsum[lane] : 0ull, v = w;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const unsigned long long y = __shfl_up_sync(kFull, v, o);
             if (lane >= o) v += y;
         }
-        warp_tot[lane] = v - w;                     // exclusive
+        if (lane < nw) wsum[lane] = (unsigned)(v - w);
     }
     __syncthreads();
     const long long rank = s->rank;
-    const long long excl = (long long)(warp_tot[wid] + x - loc);
-    if (rank >= excl && rank < excl + (long long)loc) {        // exactly one thread
-        found[0] = t;
-        found[1] = rank - excl;
+    const long long excl = (long long)(wsum[wid] + incl - loc);
+    if (rank >= excl && rank < excl + (long long)loc) {
+        owner = t;
+        owner_excl = (unsigned long long)excl;
     }
     __syncthreads();
-    // warp 0 finds the bin inside the owner's 64 (two per lane)
-    if (wid == 0) {
-        const int owner = (int)found[0];
-        const long long r = found[1];
-        const uint2 c2 = reinterpret_cast<const uint2 *>(hist)[owner * 32 + lane];
-        const unsigned long long c = (unsigned long long)c2.x + c2.y;
-        unsigned long long inc = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long y = __shfl_up_sync(kFull, inc, o);
-            if (lane >= o) inc += y;
+    if (t == owner) {
+        long long r = rank - (long long)owner_excl;
+        int b = t * per;
+        for (int j = 0; j < per; ++j) {
+            const long long c = __ldcg(ghist + t * per + j);
+            if (r < c) { b = t * per + j; break; }
+            r -= c;
         }
-        const long long ex = (long long)(inc - c);
-        if (r >= ex && r < ex + (long long)c) {
-            const long long rr = r - ex;
-            const int b = owner * 64 + lane * 2 + (rr < (long long)c2.x ? 0 : 1);
-            const int shift = 64 - SEL_DIGIT * (pass + 1);
-            s->prefix |= (unsigned long long)b << shift;
-            s->rank = rr < (long long)c2.x ? rr : rr - c2.x;
-            if (pass == SEL_NPASS - 1) s->value = sel_unkey(s->prefix);
-        }
+        s->prefix |= (unsigned long long)b << shift;
+        s->rank = r;
+        if (pass == SEL_NPASS - 1) s->value = sel_unkey(s->prefix);
     }
 }
 
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st) {
+    if (n < 1 || n >= (1l << 32) || rank < 0 || rank >= n) {
+        set_error("select: n=%ld rank=%lld", n, rank);
+        return SV_ERR_PARAM;
+    }
     SV_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)SEL_NPASS * SEL_NB * sizeof(unsigned), st));
     count_launch();
     k_sel_init<<<1, 1, 0, st>>>(state, rank);
-    const int blocks = grid_for(n, 256 * 4, 148 * 2);
+    const int blocks = grid_for(n, 1024 * 4, 148);
     for (int p = 0; p < SEL_NPASS; ++p) {
         count_launch();
-        k_sel_hist16<<<blocks, 256, 0, st>>>(x, n, p, state, hist + (size_t)p * SEL_NB);
-        count_launch();
-        k_sel_pick16<<<1, 1024, 0, st>>>(hist + (size_t)p * SEL_NB, p, state);
+        k_sel_pass<<<blocks, 1024, 0, st>>>(x, n, p, state, hist + (size_t)p * SEL_NB);
     }
     SV_LAUNCH_CHECK();
     return SV_OK;

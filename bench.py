@@ -156,7 +156,7 @@ def hbm_peak():
 def sgm_traffic(K, N):
     """DRAM bytes per SGM launch from the committed ncu summary, scaled to
     this launch's pixel count (traffic grows with the pixels swept)."""
-    p = os.path.join(REPO, "profiles", "ncu_sgm.md")
+    p = os.path.join(REPO, "profiles", "ncu_sgm_thread_450x375.md")
     if not os.path.exists(p):
         return None
     per_px = None
@@ -282,7 +282,7 @@ def run_ours(args, rank, world, local):
                        "parallelism": "replicas x%d" % world},
             "stages_ms": {"predict_auto": round(ms / args.steps - sum(stage_ms), 4),
                           **{s: round(v, 4) for s, v in zip(stages, stage_ms)}},
-            "roofline": {"kernel": "k_sgm (8 paths x 2 views)", "bound": "hbm",
+            "roofline": {"kernel": "k_sgm_thread (8 paths x 2 views)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind

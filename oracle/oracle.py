@@ -325,3 +325,54 @@ def lr_refine_band(left, right, centre, rad, W, H, tol=2.0, R=10, P1=12.0, P2=15
                                     W, H, _dbl(tol), R, _dbl(P1), _dbl(P2), rx, ry, _p(out),
                                     _p(st, _i32)), "lr_refine_band")
     return out, st
+
+
+# --------------------------------------------- rest of refine_disparity
+def _m2(compactness, step):
+    # the reference computes (compactness / step) ** 2 with CPython's float
+    # power, which calls the C library's pow()
+    return (float(compactness) / step) ** 2
+
+
+def slic(rgb, W, H, step=12, compactness=10.0, iters=5):
+    rgb = _f64(rgb)
+    lab = np.zeros(W * H, dtype=np.int32)
+    nseg = _int()
+    _check(lib().orc_slic(_p(rgb), W, H, int(step), _dbl(_m2(compactness, step)), int(iters),
+                          _p(lab, _i32), ctypes.byref(nseg)), "slic")
+    return lab, nseg.value
+
+
+def plane_snap(disp, rgb, W, H, valid=None, step=12, thr=1.0, min_inl=0.6, trials=40,
+               seed=12345):
+    disp, rgb = _f64(disp), _f64(rgb)
+    v = None if valid is None else np.ascontiguousarray(np.asarray(valid, dtype=bool), np.uint8)
+    out = np.zeros(W * H)
+    _check(lib().orc_plane_snap(_p(disp), _p(rgb), W, H,
+                                None if v is None else _p(v, ctypes.POINTER(ctypes.c_uint8)),
+                                int(step), _dbl(_m2(10.0, step)), _dbl(thr), _dbl(min_inl),
+                                int(trials), ctypes.c_uint32(seed), _p(out)), "plane_snap")
+    return out
+
+
+def median_filter(disp, W, H, radius=1, passes=1):
+    disp = _f64(disp)
+    out = np.zeros(W * H)
+    _check(lib().orc_median_filter(_p(disp), W, H, int(radius), int(passes), _p(out)),
+           "median_filter")
+    return out
+
+
+def refine_disparity(left, right, rgb, disp0, W, H, R=10, P1=12.0, P2=150.0, rx=4, ry=3,
+                     tol=2.0, planes=True, plane_step=12, plane_thr=1.0, plane_min_inl=0.4):
+    left, right, d0 = _f64(left), _f64(right), _f64(disp0)
+    rgbv = None if rgb is None else _f64(rgb)
+    out = np.zeros(W * H)
+    st = np.zeros(W * H, dtype=np.int32)
+    _check(lib().orc_refine_disparity(_p(left), _p(right), None if rgbv is None else _p(rgbv),
+                                      _p(d0), W, H, R, _dbl(P1), _dbl(P2), rx, ry, _dbl(tol),
+                                      int(bool(planes)), int(plane_step),
+                                      _dbl(_m2(10.0, plane_step)), _dbl(plane_thr),
+                                      _dbl(plane_min_inl), _p(out), _p(st, _i32)),
+           "refine_disparity")
+    return out, st

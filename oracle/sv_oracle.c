@@ -882,3 +882,267 @@ int orc_lr_refine(const double *left, const double *right, const double *disp0,
     free(dl); free(d0r); free(m1); free(m2); free(m3); free(drm); free(dr);
     return ORC_OK;
 }
+
+/* ----------------------------------------------------------------------
+ * The rest of refine_disparity (stereonet.py:5865-5883): SLIC superpixels,
+ * plane_snap (RANSAC + least-squares plane per segment) and median_filter.
+ * ---------------------------------------------------------------------- */
+
+/* slic -- stereonet.py:5394-5455.  m2 is (compactness / step) ** 2 as the
+ * caller's libm pow computes it (CPython's float ** int calls pow()). */
+int orc_slic(const double *rgb, int W, int H, int step, double m2, int iters,
+             int32_t *lab, int *nseg) {
+    if (W < 1 || H < 1 || step < 1) return ORC_EBADARG;
+    int ncx = 0, ncy = 0;
+    for (int x = step / 2; x < W; x += step) ncx++;
+    for (int y = step / 2; y < H; y += step) ncy++;
+    int nc = ncx * ncy;
+    long N = (long)W * H;
+    double *cs = (double *)malloc(sizeof(double) * 5 * (nc > 0 ? nc : 1));
+    double *dist = (double *)malloc(sizeof(double) * N);
+    double *acc = (double *)malloc(sizeof(double) * 6 * (nc > 0 ? nc : 1));
+    if (!cs || !dist || !acc) { free(cs); free(dist); free(acc); return ORC_ENOMEM; }
+    int k = 0;
+    for (int y = step / 2; y < H; y += step)
+        for (int x = step / 2; x < W; x += step) {
+            long i = (long)y * W + x;
+            cs[5 * k + 0] = rgb[3 * i] * 255.0;
+            cs[5 * k + 1] = rgb[3 * i + 1] * 255.0;
+            cs[5 * k + 2] = rgb[3 * i + 2] * 255.0;
+            cs[5 * k + 3] = (double)x;
+            cs[5 * k + 4] = (double)y;
+            k++;
+        }
+    for (long i = 0; i < N; i++) lab[i] = -1;
+    for (int it = 0; it < iters; it++) {
+        for (long i = 0; i < N; i++) dist[i] = 1.0e30;
+        for (int ci = 0; ci < nc; ci++) {
+            double cr = cs[5 * ci], cg = cs[5 * ci + 1], cb = cs[5 * ci + 2];
+            double cx = cs[5 * ci + 3], cy = cs[5 * ci + 4];
+            int x0 = (int)cx - step, x1 = (int)cx + step;
+            int y0 = (int)cy - step, y1 = (int)cy + step;
+            if (x0 < 0) x0 = 0;
+            if (y0 < 0) y0 = 0;
+            if (x1 >= W) x1 = W - 1;
+            if (y1 >= H) y1 = H - 1;
+            for (int yy = y0; yy <= y1; yy++) {
+                double dy = yy - cy;
+                for (int xx = x0; xx <= x1; xx++) {
+                    long i = (long)yy * W + xx;
+                    double a = rgb[3 * i] * 255.0 - cr;
+                    double b = rgb[3 * i + 1] * 255.0 - cg;
+                    double c = rgb[3 * i + 2] * 255.0 - cb;
+                    double dx = xx - cx;
+                    double dd = a * a + b * b + c * c + m2 * (dx * dx + dy * dy);
+                    if (dd < dist[i]) { dist[i] = dd; lab[i] = ci; }
+                }
+            }
+        }
+        for (int ci = 0; ci < 6 * nc; ci++) acc[ci] = 0.0;
+        for (long i = 0; i < N; i++) {
+            int l = lab[i];
+            if (l < 0) continue;
+            double *a = acc + 6 * l;
+            a[0] += rgb[3 * i];
+            a[1] += rgb[3 * i + 1];
+            a[2] += rgb[3 * i + 2];
+            a[3] += (double)(i % W);
+            a[4] += (double)(i / W);
+            a[5] += 1.0;
+        }
+        for (int ci = 0; ci < nc; ci++) {
+            double *a = acc + 6 * ci;
+            if (a[5] != 0.0) {
+                double n = a[5];
+                cs[5 * ci + 0] = a[0] / n * 255.0;
+                cs[5 * ci + 1] = a[1] / n * 255.0;
+                cs[5 * ci + 2] = a[2] / n * 255.0;
+                cs[5 * ci + 3] = a[3] / n;
+                cs[5 * ci + 4] = a[4] / n;
+            }
+        }
+    }
+    *nseg = nc;
+    free(cs); free(dist); free(acc);
+    return ORC_OK;
+}
+
+/* _solve3 -- stereonet.py:5458-5469; returns 0 when |det| < 1e-9. */
+static int solve3(const double A[3][3], const double bv[3], double out[3]) {
+    double a = A[0][0], bb = A[0][1], c = A[0][2];
+    double d = A[1][0], e = A[1][1], f = A[1][2];
+    double g = A[2][0], h = A[2][1], k = A[2][2];
+    double det = a * (e * k - f * h) - bb * (d * k - f * g) + c * (d * h - e * g);
+    if (fabs(det) < 1.0e-9) return 0;
+    out[0] = (bv[0] * (e * k - f * h) - bb * (bv[1] * k - f * bv[2]) +
+              c * (bv[1] * h - e * bv[2])) / det;
+    out[1] = (a * (bv[1] * k - f * bv[2]) - bv[0] * (d * k - f * g) +
+              c * (d * bv[2] - bv[1] * g)) / det;
+    out[2] = (a * (e * bv[2] - bv[1] * h) - bb * (d * bv[2] - bv[1] * g) +
+              bv[0] * (d * h - e * g)) / det;
+    return 1;
+}
+
+/* _lsq_plane -- stereonet.py:5472-5502 (sequential sums in list order). */
+static void lsq_plane(const long *idx, long n, const double *disp, int W, double out[3]) {
+    double nn = (double)n, sx = 0.0, sy = 0.0, sd = 0.0;
+    for (long j = 0; j < n; j++) sx += (double)(idx[j] % W);
+    for (long j = 0; j < n; j++) sy += (double)(idx[j] / W);
+    for (long j = 0; j < n; j++) sd += disp[idx[j]];
+    double mx = sx / nn, my = sy / nn, md = sd / nn;
+    double sxx = 0.0, sxy = 0.0, syy = 0.0, sxd = 0.0, syd = 0.0;
+    for (long j = 0; j < n; j++) {
+        double u = (double)(idx[j] % W) - mx;
+        double v = (double)(idx[j] / W) - my;
+        double w = disp[idx[j]] - md;
+        sxx += u * u;
+        sxy += u * v;
+        syy += v * v;
+        sxd += u * w;
+        syd += v * w;
+    }
+    double det = sxx * syy - sxy * sxy;
+    if (fabs(det) < 1.0e-9) { out[0] = 0.0; out[1] = 0.0; out[2] = md; return; }
+    double a = (sxd * syy - syd * sxy) / det;
+    double b = (syd * sxx - sxd * sxy) / det;
+    out[0] = a; out[1] = b; out[2] = md - a * mx - b * my;
+}
+
+static inline uint32_t xorshift32(uint32_t s) {
+    s ^= s << 13;
+    s ^= s >> 17;
+    s ^= s << 5;
+    return s;
+}
+
+/* plane_snap -- stereonet.py:5505-5563.  valid may be NULL. */
+int orc_plane_snap(const double *disp, const double *rgb, int W, int H, const uint8_t *valid,
+                   int step, double m2, double thr, double min_inl, int trials,
+                   uint32_t seed, double *out) {
+    long N = (long)W * H;
+    int32_t *lab = (int32_t *)malloc(sizeof(int32_t) * N);
+    long *order = (long *)malloc(sizeof(long) * N);
+    long *pts = (long *)malloc(sizeof(long) * N);
+    if (!lab || !order || !pts) { free(lab); free(order); free(pts); return ORC_ENOMEM; }
+    int nseg = 0;
+    int rc = orc_slic(rgb, W, H, step, m2, 5, lab, &nseg);
+    if (rc) { free(lab); free(order); free(pts); return rc; }
+    long *start = (long *)calloc((size_t)nseg + 1, sizeof(long));
+    long *fill = (long *)calloc((size_t)nseg + 1, sizeof(long));
+    for (long i = 0; i < N; i++) if (lab[i] >= 0) start[lab[i] + 1]++;
+    for (int g = 0; g < nseg; g++) start[g + 1] += start[g];
+    for (long i = 0; i < N; i++)
+        if (lab[i] >= 0) order[start[lab[i]] + fill[lab[i]]++] = i;     /* index order */
+    for (long i = 0; i < N; i++) out[i] = disp[i];
+    uint32_t s = seed;
+    for (int g = 0; g < nseg; g++) {
+        const long *grp = order + start[g];
+        long gn = start[g + 1] - start[g], n = 0;
+        for (long j = 0; j < gn; j++)
+            if (!valid || valid[grp[j]]) pts[n++] = grp[j];
+        if (n < 12) continue;
+        int have = 0;
+        long bestc = -1;
+        double best[3] = {0.0, 0.0, 0.0};
+        for (int t = 0; t < trials; t++) {
+            long tri[3];
+            for (int u = 0; u < 3; u++) {
+                s = xorshift32(s);
+                tri[u] = pts[s % (uint32_t)n];
+            }
+            double A[3][3], bv[3], pl[3];
+            for (int u = 0; u < 3; u++) {
+                A[u][0] = (double)(tri[u] % W);
+                A[u][1] = (double)(tri[u] / W);
+                A[u][2] = 1.0;
+                bv[u] = disp[tri[u]];
+            }
+            if (!solve3(A, bv, pl)) continue;
+            long cnt = 0;
+            for (long j = 0; j < n; j++) {
+                long i = pts[j];
+                if (fabs(pl[0] * (double)(i % W) + pl[1] * (double)(i / W) + pl[2] - disp[i]) <= thr)
+                    cnt++;
+            }
+            if (cnt > bestc) {
+                bestc = cnt;
+                best[0] = pl[0]; best[1] = pl[1]; best[2] = pl[2];
+                have = 1;
+            }
+        }
+        if (!have || (double)bestc < min_inl * (double)n) continue;
+        long ni = 0;
+        for (long j = 0; j < n; j++) {
+            long i = pts[j];
+            if (fabs(best[0] * (double)(i % W) + best[1] * (double)(i / W) + best[2] - disp[i]) <= thr)
+                pts[ni++] = i;             /* inliers, in order, compacted in place */
+        }
+        double pl[3];
+        lsq_plane(pts, ni, disp, W, pl);
+        for (long j = 0; j < gn; j++) {
+            long i = grp[j];
+            double v = pl[0] * (double)(i % W) + pl[1] * (double)(i / W) + pl[2];
+            if (fabs(v - disp[i]) <= thr || (valid && !valid[i])) out[i] = v > 0.0 ? v : 0.0;
+        }
+    }
+    free(lab); free(order); free(pts); free(start); free(fill);
+    return ORC_OK;
+}
+
+/* median_filter -- stereonet.py:2231-2259 (upper median of the clipped window). */
+int orc_median_filter(const double *disp, int W, int H, int radius, int passes, double *out) {
+    long N = (long)W * H;
+    int side = 2 * radius + 1;
+    double *cur = (double *)malloc(sizeof(double) * N);
+    double *vals = (double *)malloc(sizeof(double) * side * side);
+    if (!cur || !vals) { free(cur); free(vals); return ORC_ENOMEM; }
+    memcpy(cur, disp, sizeof(double) * N);
+    for (int p = 0; p < passes; p++) {
+        for (int y = 0; y < H; y++) {
+            int y0 = y - radius > 0 ? y - radius : 0;
+            int y1 = y + radius < H - 1 ? y + radius : H - 1;
+            for (int x = 0; x < W; x++) {
+                int x0 = x - radius > 0 ? x - radius : 0;
+                int x1 = x + radius < W - 1 ? x + radius : W - 1;
+                int n = 0;
+                for (int yy = y0; yy <= y1; yy++)
+                    for (int xx = x0; xx <= x1; xx++) vals[n++] = cur[(long)yy * W + xx];
+                for (int a = 1; a < n; a++) {             /* insertion sort */
+                    double v = vals[a];
+                    int b = a - 1;
+                    while (b >= 0 && vals[b] > v) { vals[b + 1] = vals[b]; b--; }
+                    vals[b + 1] = v;
+                }
+                out[(long)y * W + x] = vals[n / 2];
+            }
+        }
+        memcpy(cur, out, sizeof(double) * N);
+    }
+    if (passes < 1) memcpy(out, disp, sizeof(double) * N);
+    free(cur); free(vals);
+    return ORC_OK;
+}
+
+/* refine_disparity -- stereonet.py:5865-5883.  rgb may be NULL (no planes). */
+int orc_refine_disparity(const double *left, const double *right, const double *rgb,
+                         const double *disp0, int W, int H, int R, double P1, double P2,
+                         int rx, int ry, double tol, int planes, int plane_step, double m2,
+                         double plane_thr, double plane_min_inl, double *out,
+                         int32_t *status) {
+    long N = (long)W * H;
+    double *d = (double *)malloc(sizeof(double) * N);
+    double *e = (double *)malloc(sizeof(double) * N);
+    uint8_t *valid = (uint8_t *)malloc(N);
+    if (!d || !e || !valid) { free(d); free(e); free(valid); return ORC_ENOMEM; }
+    int rc = orc_lr_refine(left, right, disp0, W, H, tol, R, P1, P2, 0.0, 20.0, 8, 0.0, rx, ry,
+                           0.0, 4.0, d, status);
+    if (!rc && planes && rgb) {
+        for (long i = 0; i < N; i++) valid[i] = status[i] == 0;
+        rc = orc_plane_snap(d, rgb, W, H, valid, plane_step, m2, plane_thr, plane_min_inl, 40,
+                            12345u, e);
+        if (!rc) memcpy(d, e, sizeof(double) * N);
+    }
+    if (!rc) rc = orc_median_filter(d, W, H, 1, 1, out);
+    free(d); free(e); free(valid);
+    return rc;
+}

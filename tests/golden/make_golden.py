@@ -199,6 +199,54 @@ def main(ref_dir):
     print("all fixtures written (%.1fs)" % (time.time() - t0))
 
 
+def pseudo_rgb(pair):
+    """A deterministic colour image for the plane_snap / SLIC inputs
+    (interleaved RGB in [0, 1], as read_image gives): the left gray level
+    and two smooth transforms of it."""
+    g = pair.left.astype(np.float64) / 255.0
+    h, w = g.shape
+    yy, xx = np.mgrid[0:h, 0:w]
+    rgb = np.stack([g, 0.5 * g + 0.5 * (xx / max(1, w - 1)), 1.0 - 0.7 * g * (yy / max(1, h - 1))],
+                   axis=-1)
+    return np.round(rgb * 255.0) / 255.0
+
+
+def postproc(ref_dir):
+    """The rest of refine_disparity (stereonet.py:5865-5883): SLIC, plane_snap,
+    median_filter and refine_disparity itself, on small seeded pairs."""
+    SN = load_reference(ref_dir)
+    out = {}
+    for tag, (W, H, seed, step) in {"a": (64, 48, 31, 12), "b": (90, 70, 32, 8)}.items():
+        p = synth.make_pair(seed, W, H, 2.0, 24.0, n_planes=(3, 5))
+        L = list(p.gray("left").ravel())
+        R = list(p.gray("right").ravel())
+        rgb = pseudo_rgb(p)
+        rl = list(rgb.ravel())
+        rng = np.random.default_rng(seed)
+        d0 = list(p.disp.ravel() + rng.uniform(-2.5, 2.5, W * H))
+        d, st = SN["lr_refine"](L, R, d0, W, H, tol=2.0, R=10, P1=12.0, P2=150.0, rx=4, ry=3)
+        valid = [s == 0 for s in st]
+        lab, nseg = SN["slic"](rl, W, H, step)
+        out[tag + "_left"], out[tag + "_right"] = p.left, p.right
+        out[tag + "_rgb"], out[tag + "_disp0"] = rgb.ravel(), np.array(d0)
+        out[tag + "_lr"], out[tag + "_status"] = np.array(d), np.array(st, dtype=np.int8)
+        out[tag + "_slic"] = np.array(lab, dtype=np.int32)
+        out[tag + "_slic_c20_it3"] = np.array(SN["slic"](rl, W, H, step, 20.0, 3)[0], dtype=np.int32)
+        out[tag + "_snap"] = np.array(SN["plane_snap"](d, rl, W, H, valid=valid, step=step,
+                                                       thr=1.0, min_inl=0.4))
+        out[tag + "_snap_novalid"] = np.array(SN["plane_snap"](d, rl, W, H, step=step))
+        out[tag + "_median"] = np.array(SN["median_filter"](d, W, H))
+        out[tag + "_median_r2p2"] = np.array(SN["median_filter"](d, W, H, radius=2, passes=2))
+        rd, rs = SN["refine_disparity"](L, R, rl, d0, W, H, plane_step=step)
+        out[tag + "_refine_disparity"] = np.array(rd)
+        out[tag + "_refine_disparity_status"] = np.array(rs, dtype=np.int8)
+        rd2, _ = SN["refine_disparity"](L, R, rl, d0, W, H, planes=False)
+        out[tag + "_refine_disparity_noplanes"] = np.array(rd2)
+        out[tag + "_dims"] = np.array([W, H, step])
+    np.savez_compressed(os.path.join(HERE, "postproc.npz"), **out)
+    print("postproc fixtures written")
+
+
 HOT_PATH = ["census", "band_costs", "_aggregate_path", "refine_fullres", "left_to_right",
             "lr_refine", "resize_gray", "avgpool2", "predict", "predict_at_scale",
             "predict_auto", "refine_disparity"]
@@ -219,6 +267,9 @@ def signatures(ref_dir):
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
     ref = args[0] if args else "/root/reference"
-    if "--signatures-only" not in sys.argv:
+    if "--postproc-only" in sys.argv:
+        postproc(ref)
+    elif "--signatures-only" not in sys.argv:
         main(ref)
+        postproc(ref)
     signatures(ref)

@@ -154,3 +154,27 @@ def test_config_full_digests(orc, net, svb, golden_meta):
     out, st = orc.lr_refine(L, R, df, p.W, p.H, tol=2.0, R=10, P1=12.0, P2=150.0, rx=4, ry=3)
     assert sha(out) == m["out_sha256"]
     assert sha(st, np.int8) == m["status_sha256"]
+
+
+# ------------------------------------------- rest of refine_disparity
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_postproc_oracle_vs_reference(orc, tag):
+    """slic, plane_snap, median_filter and refine_disparity (stereonet.py:
+    2231-2259, 5394-5563, 5865-5883) bit-for-bit against the reference."""
+    g = golden("postproc.npz")
+    W, H, step = map(int, g[tag + "_dims"])
+    rgb, d, st = g[tag + "_rgb"], g[tag + "_lr"], g[tag + "_status"]
+    assert np.array_equal(orc.slic(rgb, W, H, step)[0], g[tag + "_slic"])
+    assert np.array_equal(orc.slic(rgb, W, H, step, 20.0, 3)[0], g[tag + "_slic_c20_it3"])
+    snap = orc.plane_snap(d, rgb, W, H, valid=st == 0, step=step, thr=1.0, min_inl=0.4)
+    assert np.array_equal(bits(snap), bits(g[tag + "_snap"]))
+    assert np.array_equal(bits(orc.plane_snap(d, rgb, W, H, step=step)),
+                          bits(g[tag + "_snap_novalid"]))
+    assert np.array_equal(bits(orc.median_filter(d, W, H)), bits(g[tag + "_median"]))
+    assert np.array_equal(bits(orc.median_filter(d, W, H, 2, 2)), bits(g[tag + "_median_r2p2"]))
+    L, R = g[tag + "_left"].ravel() / 255.0, g[tag + "_right"].ravel() / 255.0
+    rd, rs = orc.refine_disparity(L, R, rgb, g[tag + "_disp0"], W, H, plane_step=step)
+    assert np.array_equal(bits(rd), bits(g[tag + "_refine_disparity"]))
+    assert np.array_equal(rs, g[tag + "_refine_disparity_status"])
+    rd2, _ = orc.refine_disparity(L, R, rgb, g[tag + "_disp0"], W, H, planes=False)
+    assert np.array_equal(bits(rd2), bits(g[tag + "_refine_disparity_noplanes"]))

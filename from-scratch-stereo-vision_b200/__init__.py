@@ -24,6 +24,6 @@ __all__ = ["_lib", "synth", "weights"]
 def __getattr__(name):
     # heavy modules (torch) load on first use
     import importlib
-    if name in ("refine", "network", "pipeline", "shim", "shard", "batch", "band"):
+    if name in ("refine", "network", "pipeline", "shim", "shard", "batch", "band", "post"):
         return importlib.import_module("." + name, __name__)
     raise AttributeError(name)

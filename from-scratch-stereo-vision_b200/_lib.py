@@ -57,6 +57,16 @@ SIGNATURES = {
     "sv_refine_fullres_noalloc": (_I, [_VP, _VP, _I, _VP, _I, _I, _PRM, _VP, _VP, _VP]),
     "sv_batch_lr_refine_workspace_size": (_SZ, [_VP, _I, _PRM]),
     "sv_batch_lr_refine": (_I, [_VP, _I, _I, _D, _PRM, _VP, _SZ, _VP]),
+    "sv_median_workspace_size": (_SZ, [_I, _I]),
+    "sv_median_filter": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _SZ, _VP]),
+    "sv_postproc_workspace_size": (_SZ, [_I, _I, _I]),
+    "sv_slic_count": (_I, [_I, _I, _I]),
+    "sv_slic": (_I, [_VP, _I, _I, _I, _D, _I, _VP, _VP, _SZ, _VP]),
+    "sv_plane_snap": (_I, [_VP, _VP, _I, _I, _VP, _I, _D, _D, _I, ctypes.c_uint32, _VP, _VP, _SZ,
+                           _VP]),
+    "sv_refine_disparity_workspace_size": (_SZ, [_I, _I, _PRM, _I]),
+    "sv_refine_disparity": (_I, [_VP, _VP, _I, _VP, _VP, _I, _I, _D, _PRM, _I, _I, _D, _D, _VP,
+                                 _VP, _VP, _SZ, _VP]),
     "sv_lr_refine_band": (_I, [_VP, _VP, _I, _VP, _VP, _I, _I, _D, _PRM, _VP, _VP, _VP, _SZ,
                                _VP]),
     "sv_band_param_count": (ctypes.c_long, []),

@@ -5,7 +5,7 @@ stereonet.py into a dict and looks functions up there (eval_real.py:41-44,
 serve.py:34-37, test_stereonet.py:18-22).  Inside that dict the reference's
 functions call each other through the same dict, so rebinding a name
 redirects every caller, e.g. ``lr_refine`` -> ``refine_fullres`` and
-``refine_disparity`` -> ``lr_refine``:
+``reconstruct_from_pair`` -> ``refine_disparity``:
 
     SN = {}
     exec(open("stereonet.py").read(), SN)
@@ -19,7 +19,7 @@ reference's own path).  ``uninstall(SN)`` restores the originals.
 
 from __future__ import annotations
 
-from . import network, refine
+from . import network, post, refine
 
 # reference name -> drop-in
 DROP_INS = {
@@ -34,6 +34,10 @@ DROP_INS = {
     "predict": network.predict,
     "predict_at_scale": network.predict_at_scale,
     "predict_auto": network.predict_auto,
+    "median_filter": post.median_filter,
+    "slic": post.slic,
+    "plane_snap": post.plane_snap,
+    "refine_disparity": post.refine_disparity,
 }
 
 _SAVED = "__sv_b200_saved__"

@@ -223,6 +223,40 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right,
                         void *workspace, size_t workspace_bytes, void *stream);
 
 /* ------------------------------------------------------------------------
+ * The rest of refine_disparity (stereonet.py:5865-5883), bit-identical.
+ * disp / out are FP64 [H][W]; rgb is interleaved FP64 RGB in [0, 1] as
+ * read_image gives it; out must not alias the input disparity.
+ * ---------------------------------------------------------------------- */
+/* median_filter, stereonet.py:2231-2259 (radius <= 3) */
+size_t sv_median_workspace_size(int W, int H);
+int sv_median_filter(const double *disp, int W, int H, int radius, int passes,
+                     double *out, void *workspace, size_t workspace_bytes,
+                     void *stream);
+/* slic, stereonet.py:5394-5455: labels [H][W] (-1 where no cluster ever
+ * covered the pixel); sv_slic_count gives the number of clusters */
+size_t sv_postproc_workspace_size(int W, int H, int step);
+int sv_slic_count(int W, int H, int step);
+int sv_slic(const double *rgb, int W, int H, int step, double compactness,
+            int iters, int32_t *labels, void *workspace, size_t workspace_bytes,
+            void *stream);
+/* plane_snap, stereonet.py:5505-5563 (SLIC with compactness 10, 5 iterations;
+ * valid may be NULL; trials <= 64) */
+int sv_plane_snap(const double *disp, const double *rgb, int W, int H,
+                  const uint8_t *valid, int step, double thr, double min_inl,
+                  int trials, uint32_t seed, double *out, void *workspace,
+                  size_t workspace_bytes, void *stream);
+/* refine_disparity, stereonet.py:5865-5883: lr_refine, plane_snap on the
+ * status-0 pixels when planes != 0 and rgb != NULL, 3x3 median */
+size_t sv_refine_disparity_workspace_size(int W, int H, const sv_refine_params *p,
+                                          int plane_step);
+int sv_refine_disparity(const void *left, const void *right, int dtype,
+                        const double *rgb, const double *disp0, int W, int H,
+                        double tol, const sv_refine_params *p, int planes,
+                        int plane_step, double plane_thr, double plane_min_inl,
+                        double *out, uint8_t *status, void *workspace,
+                        size_t workspace_bytes, void *stream);
+
+/* ------------------------------------------------------------------------
  * Learned adaptive band (no counterpart in the reference: it extends
  * lr_refine, stereonet.py:5343-5391, whose band is fixed at +-R around the
  * network disparity).  A 4-layer convolutional band net (5810 parameters,

@@ -243,13 +243,33 @@ def postproc(ref_dir):
         rd2, _ = SN["refine_disparity"](L, R, rl, d0, W, H, planes=False)
         out[tag + "_refine_disparity_noplanes"] = np.array(rd2)
         out[tag + "_dims"] = np.array([W, H, step])
+    # An 11x17 binary image where some pixels lie in no cluster window in
+    # SLIC iterations 3 and 4 (they keep their labels): found by a seeded
+    # search, regenerated here from its seed.
+    rng = np.random.default_rng(0)
+    for trial in range(111):
+        W, H, step = (int(rng.integers(8, 40)), int(rng.integers(8, 40)), int(rng.integers(3, 12)))
+        img = rng.random((H, W, 3))
+        if trial % 3 == 1:
+            img[:, :W // 2] = 0.0
+            img[:, W // 2:] = 1.0
+        if trial % 3 == 2:
+            img = (rng.random((H, W, 1)) > 0.5) * np.ones((1, 1, 3))
+        comp = float(rng.choice([0.1, 1.0, 10.0]))
+    rgb = (np.round(img * 255) / 255.0).ravel()
+    d = np.random.default_rng(7).uniform(0, 20, W * H)
+    out["u_rgb"], out["u_disp"], out["u_dims"] = rgb, d, np.array([W, H, step])
+    out["u_comp"] = np.array(comp)
+    out["u_slic"] = np.array(SN["slic"](list(rgb), W, H, step, comp)[0], dtype=np.int32)
+    out["u_snap"] = np.array(SN["plane_snap"](list(d), list(rgb), W, H, step=step, thr=5.0,
+                                              min_inl=0.3))
     np.savez_compressed(os.path.join(HERE, "postproc.npz"), **out)
     print("postproc fixtures written")
 
 
 HOT_PATH = ["census", "band_costs", "_aggregate_path", "refine_fullres", "left_to_right",
             "lr_refine", "resize_gray", "avgpool2", "predict", "predict_at_scale",
-            "predict_auto", "refine_disparity"]
+            "predict_auto", "refine_disparity", "median_filter", "slic", "plane_snap"]
 
 
 def signatures(ref_dir):

@@ -178,3 +178,13 @@ def test_postproc_oracle_vs_reference(orc, tag):
     assert np.array_equal(rs, g[tag + "_refine_disparity_status"])
     rd2, _ = orc.refine_disparity(L, R, rgb, g[tag + "_disp0"], W, H, planes=False)
     assert np.array_equal(bits(rd2), bits(g[tag + "_refine_disparity_noplanes"]))
+
+
+def test_slic_uncovered_pixels_oracle_vs_reference(orc):
+    """Pixels no cluster window covers keep their labels (stereonet.py:
+    5409-5432); on this image that happens in SLIC iterations 3 and 4."""
+    g = golden("postproc.npz")
+    W, H, step = map(int, g["u_dims"])
+    assert np.array_equal(orc.slic(g["u_rgb"], W, H, step, float(g["u_comp"]))[0], g["u_slic"])
+    snap = orc.plane_snap(g["u_disp"], g["u_rgb"], W, H, step=step, thr=5.0, min_inl=0.3)
+    assert np.array_equal(bits(snap), bits(g["u_snap"]))

@@ -20,8 +20,7 @@ def _params(sig_str):
     return [(p.name, p.default, p.kind) for p in inspect.signature(ns["f"]).parameters.values()]
 
 
-@pytest.mark.parametrize("name", sorted(n for n in REF_SIGS if n not in ("refine_disparity",
-                                                                         "StereoNet.forward")))
+@pytest.mark.parametrize("name", sorted(n for n in REF_SIGS if n != "StereoNet.forward"))
 def test_signature_kept(svb, name):
     fn = svb.shim.DROP_INS[name]
     ref = _params(REF_SIGS[name])

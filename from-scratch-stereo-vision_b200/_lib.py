@@ -57,6 +57,12 @@ SIGNATURES = {
     "sv_refine_fullres_noalloc": (_I, [_VP, _VP, _I, _VP, _I, _I, _PRM, _VP, _VP, _VP]),
     "sv_batch_lr_refine_workspace_size": (_SZ, [_VP, _I, _PRM]),
     "sv_batch_lr_refine": (_I, [_VP, _I, _I, _D, _PRM, _VP, _SZ, _VP]),
+    "sv_predict_consistent_workspace_size": (_SZ, [_VP, _I, _I, _I, _I]),
+    "sv_predict_consistent": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _D, _I, _I, _I, _D, _I, _VP,
+                                   ctypes.POINTER(ctypes.c_longlong), _VP, _SZ, _VP]),
+    "sv_lr_consistency": (_I, [_VP, _VP, _I, _I, _D, _VP, _VP, _VP]),
+    "sv_fill_invalid_workspace_size": (_SZ, [_I, _I]),
+    "sv_fill_invalid": (_I, [_VP, _VP, _I, _I, _VP, _VP, _SZ, _VP]),
     "sv_median_workspace_size": (_SZ, [_I, _I]),
     "sv_median_filter": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _SZ, _VP]),
     "sv_postproc_workspace_size": (_SZ, [_I, _I, _I]),

@@ -539,3 +539,100 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
 }
 
 }  // extern "C"
+
+// ------------------------------------------- network-level LR consistency
+#include "sv_post.cuh"
+
+namespace {
+
+size_t dtype_size(int dtype) {
+    return dtype == SV_U8 ? 1 : dtype == SV_F32 ? 4 : dtype == SV_F64 ? 8 : 0;
+}
+
+struct ConsistWs {
+    unsigned char *ml, *mr;
+    double *dl, *dwork, *drm, *dr;
+    uint8_t *valid;
+    int *scratch;
+    unsigned long long *kept;
+    void *pws;
+};
+
+size_t carve_consist(void *ws, const sv_net *net, int W, int H, int dtype, int max_width,
+                     size_t *pneed, ConsistWs *o) {
+    Carver cv(ws);
+    ConsistWs c{};
+    const size_t N = (size_t)W * H, es = dtype_size(dtype);
+    c.ml = cv.take<unsigned char>(N * es);
+    c.mr = cv.take<unsigned char>(N * es);
+    c.dl = cv.take<double>(N);
+    c.dwork = cv.take<double>(N > 4096 ? N : 4096);
+    c.drm = cv.take<double>(N);
+    c.dr = cv.take<double>(N);
+    c.valid = cv.take<uint8_t>(N);
+    c.scratch = cv.take<int>(N);
+    c.kept = cv.take<unsigned long long>(1);
+    const size_t pn = sv_predict_workspace_size(net, W, H, max_width);
+    c.pws = cv.take<unsigned char>(pn);
+    if (pneed) *pneed = pn;
+    if (o) *o = c;
+    return cv.off;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t sv_predict_consistent_workspace_size(const sv_net *net, int W, int H, int dtype,
+                                            int max_width) {
+    if (!net || W < 1 || H < 1 || !dtype_size(dtype)) return 0;
+    return carve_consist(nullptr, net, W, H, dtype, max_width < 48 ? 48 : max_width, nullptr,
+                         nullptr);
+}
+
+int sv_predict_consistent(const sv_net *net, const void *left, const void *right, int dtype,
+                          int W, int H, int work_width, double target_peak, int probe_width,
+                          int max_width, int passes, double tol, int precision,
+                          double *disp_out, long long *kept, void *workspace,
+                          size_t workspace_bytes, void *stream) {
+    if (!net || !left || !right || !disp_out || !kept) {
+        set_error("NULL argument");
+        return SV_ERR_NULL;
+    }
+    if (W < 1 || H < 1 || !dtype_size(dtype)) { set_error("bad shape or dtype"); return SV_ERR_SHAPE; }
+    if (!std::isfinite(tol)) { set_error("tol must be finite"); return SV_ERR_PARAM; }
+    const int mw = work_width > 0 ? (work_width > 48 ? work_width : 48) : max_width;
+    const size_t need = sv_predict_consistent_workspace_size(net, W, H, dtype, mw);
+    if (!workspace || ((uintptr_t)workspace & 255) || workspace_bytes < need) {
+        set_error("workspace needs %zu bytes, 256-aligned", need);
+        return SV_ERR_WORKSPACE;
+    }
+    ConsistWs c;
+    size_t pn = 0;
+    carve_consist(workspace, net, W, H, dtype, mw < 48 ? 48 : mw, &pn, &c);
+    cudaStream_t st = (cudaStream_t)stream;
+    int Ww = 0, Hw = 0;
+    // predict_consistent, stereonet.py:5048-5076
+    if (work_width <= 0)
+        SV_TRY(sv_predict_auto(net, left, right, dtype, W, H, target_peak, probe_width, max_width,
+                               passes, precision, c.dl, c.dwork, &Ww, &Hw, nullptr, c.pws, pn,
+                               stream));
+    else
+        SV_TRY(sv_predict_at_scale(net, left, right, dtype, W, H, work_width, precision, c.dl,
+                                   c.dwork, &Ww, &Hw, c.pws, pn, stream));
+    const int es = (int)dtype_size(dtype);
+    SV_TRY(launch_mirror(left, es, W, H, c.ml, st));
+    SV_TRY(launch_mirror(right, es, W, H, c.mr, st));
+    SV_TRY(sv_predict_at_scale(net, c.mr, c.ml, dtype, W, H, Ww, precision, c.drm, c.dwork, &Ww,
+                               &Hw, c.pws, pn, stream));
+    SV_TRY(launch_mirror(c.drm, 8, W, H, c.dr, st));
+    SV_TRY(launch_lr_consistency(c.dl, c.dr, W, H, tol, c.valid, c.kept, st));
+    SV_TRY(launch_fill_invalid(c.dl, c.valid, W, H, c.scratch, disp_out, st));
+    unsigned long long k = 0;
+    SV_CUDA_TRY(cudaMemcpyAsync(&k, c.kept, sizeof(k), cudaMemcpyDeviceToHost, st));
+    SV_CUDA_TRY(cudaStreamSynchronize(st));
+    *kept = (long long)k;
+    return SV_OK;
+}
+
+}  // extern "C"

@@ -651,3 +651,128 @@ int launch_status_valid(const uint8_t *status, long N, uint8_t *valid, cudaStrea
 }
 
 }  // namespace sv
+
+namespace sv {
+
+// ====================================== network-level LR consistency
+// mirror_h (stereonet.py:4974-4983) of one [H][W] plane of esize-byte values
+__global__ void k_mirror(const unsigned char *__restrict__ in, int esize, int W, int H,
+                         unsigned char *__restrict__ out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W || y >= H) return;
+    const long src = ((long)y * W + (W - 1 - x)) * esize, dst = ((long)y * W + x) * esize;
+    for (int b = 0; b < esize; ++b) out[dst + b] = in[src + b];
+}
+
+// lr_consistency, stereonet.py:4986-5009 (FP64, the reference's order)
+__global__ void k_lr_consistency(const double *__restrict__ dl, const double *__restrict__ dr,
+                                 int W, int H, double tol, uint8_t *__restrict__ valid,
+                                 unsigned long long *__restrict__ kept) {
+    const long N = (long)W * H;
+    const long p = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    int ok = 0;
+    if (p < N) {
+        const int x = (int)(p % W);
+        const long row = p - x;
+        const double d = dl[p];
+        const double xr = __dsub_rn((double)x, d);
+        ok = 1;
+        if (xr < 0.0 || xr > (double)(W - 1)) {
+            ok = 0;
+        } else {
+            const int x0 = __double2int_rz(xr);
+            const int x1 = x0 + 1 < W ? x0 + 1 : x0;
+            const double f = __dsub_rn(xr, (double)x0);
+            const double e = __dadd_rn(__dmul_rn(dr[row + x0], __dsub_rn(1.0, f)),
+                                       __dmul_rn(dr[row + x1], f));
+            double diff = __dsub_rn(d, e);
+            if (diff < 0.0) diff = -diff;
+            if (diff > tol) ok = 0;
+        }
+        valid[p] = (uint8_t)ok;
+    }
+    unsigned c = __popc(__ballot_sync(kFull, ok));
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(kept, (unsigned long long)c);
+}
+
+// fill_invalid, stereonet.py:5012-5045: one CTA per row.  Pass 1 records the
+// nearest valid column to the left of each pixel (chunked block scans),
+// pass 2 walks from the right with the nearest valid column to the right
+// and fills.
+__global__ void __launch_bounds__(1024)
+    k_fill_invalid(const double *__restrict__ disp, const uint8_t *__restrict__ valid, int W,
+                   int H, int *__restrict__ left_idx, double *__restrict__ out) {
+    __shared__ int sbuf[32];
+    __shared__ int carry;
+    const int y = blockIdx.x, t = threadIdx.x, bd = blockDim.x;
+    const long row = (long)y * W;
+    if (t == 0) carry = -1;
+    __syncthreads();
+    for (int c0 = 0; c0 < W; c0 += bd) {
+        const int x = c0 + t;
+        const int v = x < W && valid[row + x] ? x : -1;
+        const int ex = block_excl_max(v, -1, sbuf);
+        const int c = carry;
+        if (x < W) left_idx[row + x] = max(c, ex);
+        __syncthreads();
+        if (t == bd - 1) carry = max(c, max(ex, v));
+        __syncthreads();
+    }
+    if (t == 0) carry = W;
+    __syncthreads();
+    const int nch = (W + bd - 1) / bd;
+    for (int ci = nch - 1; ci >= 0; --ci) {
+        const int x = ci * bd + t;
+        const int v = x < W && valid[row + x] ? x : W;
+        const int ex = block_excl_min_suffix(v, W, sbuf);
+        const int c = carry;
+        if (x < W) {
+            double r = disp[row + x];
+            if (!valid[row + x]) {
+                const int lf = left_idx[row + x], rt = min(c, ex);
+                const bool hl = lf >= 0, hr = rt < W;
+                if (hl && hr) {
+                    const double lv = disp[row + lf], rv = disp[row + rt];
+                    r = lv < rv ? lv : rv;
+                } else if (hl) {
+                    r = disp[row + lf];
+                } else if (hr) {
+                    r = disp[row + rt];
+                }
+            }
+            out[row + x] = r;
+        }
+        __syncthreads();
+        if (t == 0) carry = min(c, min(ex, v));
+        __syncthreads();
+    }
+}
+
+int launch_mirror(const void *in, int esize, int W, int H, void *out, cudaStream_t st) {
+    count_launch();
+    k_mirror<<<dim3((W + 255) / 256, H), 256, 0, st>>>((const unsigned char *)in, esize, W, H,
+                                                       (unsigned char *)out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_lr_consistency(const double *dl, const double *dr, int W, int H, double tol,
+                          uint8_t *valid, unsigned long long *kept, cudaStream_t st) {
+    SV_CUDA_TRY(cudaMemsetAsync(kept, 0, sizeof(unsigned long long), st));
+    const long N = (long)W * H;
+    count_launch();
+    k_lr_consistency<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(dl, dr, W, H, tol, valid, kept);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_fill_invalid(const double *disp, const uint8_t *valid, int W, int H, int *scratch,
+                        double *out, cudaStream_t st) {
+    count_launch();
+    const int bd = W >= 1024 ? 1024 : (W + 31) / 32 * 32;
+    k_fill_invalid<<<H, bd, 0, st>>>(disp, valid, W, H, scratch, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+}  // namespace sv

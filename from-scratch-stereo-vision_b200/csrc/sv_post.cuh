@@ -43,5 +43,10 @@ int launch_plane_snap(const double *disp, const double *rgb, int W, int H, const
                       int step, double thr, double min_inl, int trials, uint32_t seed,
                       double *out, const PostWs &w, cudaStream_t st);
 int launch_status_valid(const uint8_t *status, long N, uint8_t *valid, cudaStream_t st);
+int launch_mirror(const void *in, int esize, int W, int H, void *out, cudaStream_t st);
+int launch_lr_consistency(const double *dl, const double *dr, int W, int H, double tol,
+                          uint8_t *valid, unsigned long long *kept, cudaStream_t st);
+int launch_fill_invalid(const double *disp, const uint8_t *valid, int W, int H, int *scratch,
+                        double *out, cudaStream_t st);
 
 }  // namespace sv

@@ -131,3 +131,31 @@ int sv_refine_disparity(const void *left, const void *right, int dtype, const do
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int sv_lr_consistency(const double *disp_l, const double *disp_r, int W, int H, double tol,
+                      uint8_t *valid, unsigned long long *kept, void *stream) {
+    if (!disp_l || !disp_r || !valid || !kept) { set_error("NULL argument"); return SV_ERR_NULL; }
+    SV_TRY_POST(check_shape(W, H));
+    return launch_lr_consistency(disp_l, disp_r, W, H, tol, valid, kept, (cudaStream_t)stream);
+}
+
+size_t sv_fill_invalid_workspace_size(int W, int H) {
+    if (W < 1 || H < 1) return 0;
+    Carver cv(nullptr);
+    cv.take<int>((size_t)W * H);
+    return cv.off;
+}
+
+int sv_fill_invalid(const double *disp, const uint8_t *valid, int W, int H, double *out,
+                    void *workspace, size_t workspace_bytes, void *stream) {
+    if (!disp || !valid || !out) { set_error("NULL argument"); return SV_ERR_NULL; }
+    if (disp == out) { set_error("fill_invalid: out must not alias disp"); return SV_ERR_PARAM; }
+    SV_TRY_POST(check_shape(W, H));
+    SV_TRY_POST(check_ws_post(workspace, workspace_bytes, sv_fill_invalid_workspace_size(W, H)));
+    return launch_fill_invalid(disp, valid, W, H, static_cast<int *>(workspace), out,
+                               (cudaStream_t)stream);
+}
+
+}  // extern "C"

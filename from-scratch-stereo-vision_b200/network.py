@@ -222,3 +222,33 @@ def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64, max_w
     if return_trace:
         return res, widths
     return res
+
+
+# ----------------------------------------- network-level LR consistency
+def predict_consistent(net, left, right, W, H, work_width=None, tol=1.5, verbose=True, *,
+                       precision="fp32"):
+    """stereonet.py:5048-5076 -> (disparity, valid fraction): the network on
+    the pair and on the mirrored pair at the same work width, the left-right
+    check and the row fill of the rejected pixels."""
+    code_p = _precision(precision)
+    g = gpu_net(net)
+    lib = g.lib
+    tl, tr, code = _pair_inputs(left, right, W, H)
+    dev = tl.device
+    mw = 320 if work_width is None else max(int(work_width), 48)
+    need = lib.sv_predict_consistent_workspace_size(g.handle, W, H, code, mw)
+    if need == 0:
+        raise ValueError("predict_consistent: bad shape")
+    ws = torch.empty(need, dtype=torch.uint8, device=dev)
+    out = torch.empty(W * H, dtype=torch.float64, device=dev)
+    kept = ctypes.c_longlong()
+    _lib.check(lib.sv_predict_consistent(g.handle, _ptr(tl), _ptr(tr), code, W, H,
+                                         0 if work_width is None else int(work_width),
+                                         float(g.target_peak), 64, 320, 3, float(tol), code_p,
+                                         _ptr(out), ctypes.byref(kept), _ptr(ws), need,
+                                         _stream()), "predict_consistent")
+    frac = kept.value / float(W * H)
+    if verbose:
+        print("  left-right consistency: %.1f%% of pixels agree within %.1f px"
+              % (100.0 * frac, tol))
+    return _ret(out, left), frac

@@ -100,3 +100,33 @@ def refine_disparity(left, right, rgb, disp0, W, H, R=10, P1=12.0, P2=150.0, rx=
         print("  full-res refinement: %.1f%% occluded, %.1f%% mismatched"
               % (100.0 * (s == 1).mean(), 100.0 * (s == 2).mean()))
     return _ret(out, left), _ret(st, left, as_int=True)
+
+
+def lr_consistency(disp_l, disp_r, W, H, tol=1.5):
+    """stereonet.py:4986-5009 -> list of bools (or a bool array / tensor)."""
+    lib = _lib.load()
+    N = W * H
+    dl, dr = _f64(disp_l, N, "disp_l"), _f64(disp_r, N, "disp_r")
+    v = torch.empty(N, dtype=torch.uint8, device=dl.device)
+    kept = torch.zeros(1, dtype=torch.int64, device=dl.device)
+    _lib.check(lib.sv_lr_consistency(_ptr(dl), _ptr(dr), W, H, float(tol), _ptr(v), _ptr(kept),
+                                     _stream()), "lr_consistency")
+    vb = v.bool()
+    if isinstance(disp_l, list):
+        return [bool(x) for x in vb.cpu().numpy()]
+    return _ret(vb, disp_l)
+
+
+def fill_invalid(disp, valid, W, H):
+    """stereonet.py:5012-5045."""
+    lib = _lib.load()
+    N = W * H
+    d = _f64(disp, N, "disp")
+    v = _to_dev([bool(x) for x in valid] if isinstance(valid, list) else valid, N, torch.uint8,
+                name="valid")
+    out = torch.empty_like(d)
+    need = lib.sv_fill_invalid_workspace_size(W, H)
+    ws = _workspace(need)
+    _lib.check(lib.sv_fill_invalid(_ptr(d), _ptr(v), W, H, _ptr(out), _ptr(ws), need, _stream()),
+               "fill_invalid")
+    return _ret(out, disp)

@@ -38,6 +38,9 @@ DROP_INS = {
     "slic": post.slic,
     "plane_snap": post.plane_snap,
     "refine_disparity": post.refine_disparity,
+    "predict_consistent": network.predict_consistent,
+    "lr_consistency": post.lr_consistency,
+    "fill_invalid": post.fill_invalid,
 }
 
 _SAVED = "__sv_b200_saved__"

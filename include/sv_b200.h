@@ -222,6 +222,33 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right,
                         double *disp_full, double *disp_work, int *Ww, int *Hw,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* predict_consistent, stereonet.py:5048-5076 (with mirror_h 4974-4983,
+ * lr_consistency 4986-5009, fill_invalid 5012-5045): the network on the pair
+ * (predict_auto when work_width <= 0, else predict_at_scale) and on the
+ * mirrored pair at the same work width, the left-right check with `tol`, and
+ * the row fill of the rejected pixels.  *kept (host) receives the number of
+ * consistent pixels (valid fraction = kept / (W H)); the call synchronises
+ * the stream. */
+size_t sv_predict_consistent_workspace_size(const sv_net *net, int W, int H,
+                                            int dtype, int max_width);
+int sv_predict_consistent(const sv_net *net, const void *left, const void *right,
+                          int dtype, int W, int H, int work_width,
+                          double target_peak, int probe_width, int max_width,
+                          int passes, double tol, int precision, double *disp_out,
+                          long long *kept, void *workspace,
+                          size_t workspace_bytes, void *stream);
+
+/* lr_consistency, stereonet.py:4986-5009 (disp_r in the right image's frame):
+ * valid[p] = 1 where the two maps agree within tol; *kept (device) receives
+ * the count of valid pixels */
+int sv_lr_consistency(const double *disp_l, const double *disp_r, int W, int H,
+                      double tol, uint8_t *valid, unsigned long long *kept,
+                      void *stream);
+/* fill_invalid, stereonet.py:5012-5045 */
+size_t sv_fill_invalid_workspace_size(int W, int H);
+int sv_fill_invalid(const double *disp, const uint8_t *valid, int W, int H,
+                    double *out, void *workspace, size_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------------------
  * The rest of refine_disparity (stereonet.py:5865-5883), bit-identical.
  * disp / out are FP64 [H][W]; rgb is interleaved FP64 RGB in [0, 1] as

@@ -376,3 +376,33 @@ def refine_disparity(left, right, rgb, disp0, W, H, R=10, P1=12.0, P2=150.0, rx=
                                       _dbl(plane_min_inl), _p(out), _p(st, _i32)),
            "refine_disparity")
     return out, st
+
+
+# ------------------------------------------- network-level LR consistency
+def lr_consistency(disp_l, disp_r, W, H, tol=1.5):
+    dl, dr = _f64(disp_l), _f64(disp_r)
+    v = np.zeros(W * H, dtype=np.uint8)
+    lib().orc_lr_consistency(_p(dl), _p(dr), W, H, _dbl(tol), _p(v, ctypes.POINTER(ctypes.c_uint8)))
+    return v.astype(bool)
+
+
+def fill_invalid(disp, valid, W, H):
+    d = _f64(disp)
+    v = np.ascontiguousarray(np.asarray(valid, dtype=bool), dtype=np.uint8)
+    out = np.zeros(W * H)
+    lib().orc_fill_invalid(_p(d), _p(v, ctypes.POINTER(ctypes.c_uint8)), W, H, _p(out))
+    return out
+
+
+def predict_consistent(net, left, right, W, H, work_width=None, tol=1.5, target_peak=None,
+                       probe_width=64, max_width=320, passes=3):
+    arch, params = _net_args(net)
+    left, right = _f64(left), _f64(right)
+    tp = float(net.target_peak if target_peak is None else target_peak)
+    out = np.zeros(W * H)
+    kept = ctypes.c_long()
+    _check(lib().orc_predict_consistent(_p(arch, _i32), _p(params), _p(left), _p(right), W, H,
+                                        0 if work_width is None else int(work_width), _dbl(tp),
+                                        probe_width, max_width, passes, _dbl(tol), _p(out),
+                                        ctypes.byref(kept)), "predict_consistent")
+    return out, kept.value / float(W * H)

@@ -1146,3 +1146,87 @@ int orc_refine_disparity(const double *left, const double *right, const double *
     free(d); free(e); free(valid);
     return rc;
 }
+
+/* ----------------------------------------------------------------------
+ * Network-level left-right consistency (stereonet.py:4974-5076).
+ * ---------------------------------------------------------------------- */
+
+/* lr_consistency -- stereonet.py:4986-5009 */
+void orc_lr_consistency(const double *dl, const double *dr, int W, int H, double tol,
+                        uint8_t *valid) {
+    for (int y = 0; y < H; y++) {
+        long row = (long)y * W;
+        for (int x = 0; x < W; x++) {
+            double d = dl[row + x];
+            double xr = x - d;
+            valid[row + x] = 1;
+            if (xr < 0.0 || xr > W - 1) { valid[row + x] = 0; continue; }
+            int x0 = (int)xr;
+            int x1 = x0 + 1 < W ? x0 + 1 : x0;
+            double f = xr - x0;
+            double e = dr[row + x0] * (1.0 - f) + dr[row + x1] * f;
+            double diff = d - e;
+            if (diff < 0.0) diff = -diff;
+            if (diff > tol) valid[row + x] = 0;
+        }
+    }
+}
+
+/* fill_invalid -- stereonet.py:5012-5045 */
+void orc_fill_invalid(const double *disp, const uint8_t *valid, int W, int H, double *out) {
+    for (long i = 0; i < (long)W * H; i++) out[i] = disp[i];
+    for (int y = 0; y < H; y++) {
+        long row = (long)y * W;
+        int x = 0;
+        while (x < W) {
+            if (valid[row + x]) { x++; continue; }
+            int start = x;
+            while (x < W && !valid[row + x]) x++;
+            int end = x;
+            int hl = start > 0, hr = end < W;
+            if (!hl && !hr) continue;
+            double fillv;
+            if (!hl) fillv = disp[row + end];
+            else if (!hr) fillv = disp[row + start - 1];
+            else {
+                double lv = disp[row + start - 1], rv = disp[row + end];
+                fillv = lv < rv ? lv : rv;
+            }
+            for (int i = start; i < end; i++) out[row + i] = fillv;
+        }
+    }
+}
+
+/* predict_consistent -- stereonet.py:5048-5076.  work_width <= 0: predict_auto
+ * with the given target_peak / probe_width / max_width / passes. */
+int orc_predict_consistent(const int *arch, const double *params, const double *left,
+                           const double *right, int W, int H, int work_width,
+                           double target_peak, int probe_width, int max_width, int passes,
+                           double tol, double *out, long *kept) {
+    long N = (long)W * H;
+    double *dl = (double *)malloc(sizeof(double) * N), *dw = (double *)malloc(sizeof(double) * N);
+    double *ml = (double *)malloc(sizeof(double) * N), *mr = (double *)malloc(sizeof(double) * N);
+    double *drm = (double *)malloc(sizeof(double) * N), *dr = (double *)malloc(sizeof(double) * N);
+    uint8_t *valid = (uint8_t *)malloc(N);
+    int Ww = 0, Hw = 0, rc;
+    if (work_width <= 0)
+        rc = orc_predict_auto(arch, params, left, right, W, H, target_peak, probe_width,
+                              max_width, passes, dl, dw, &Ww, &Hw, NULL);
+    else
+        rc = orc_predict_at_scale(arch, params, left, right, W, H, work_width, dl, dw, &Ww, &Hw);
+    if (!rc) {
+        orc_mirror(left, W, H, ml);
+        orc_mirror(right, W, H, mr);
+        rc = orc_predict_at_scale(arch, params, mr, ml, W, H, Ww, drm, dw, &Ww, &Hw);
+    }
+    if (!rc) {
+        orc_mirror(drm, W, H, dr);
+        orc_lr_consistency(dl, dr, W, H, tol, valid);
+        long k = 0;
+        for (long i = 0; i < N; i++) k += valid[i];
+        *kept = k;
+        orc_fill_invalid(dl, valid, W, H, out);
+    }
+    free(dl); free(dw); free(ml); free(mr); free(drm); free(dr); free(valid);
+    return rc;
+}

@@ -263,13 +263,30 @@ def postproc(ref_dir):
     out["u_slic"] = np.array(SN["slic"](list(rgb), W, H, step, comp)[0], dtype=np.int32)
     out["u_snap"] = np.array(SN["plane_snap"](list(d), list(rgb), W, H, step=step, thr=5.0,
                                               min_inl=0.3))
+    # network-level left-right consistency (stereonet.py:4974-5076)
+    net = SN["load_model"](os.path.join(ref_dir, "stereonet_weights.txt"))
+    for tag, (W, H, seed, ww) in {"c": (112, 80, 41, None), "d": (96, 72, 42, 64)}.items():
+        p = synth.make_pair(seed, W, H, 2.0, 30.0, n_planes=(3, 5))
+        L, R = list(p.gray("left").ravel()), list(p.gray("right").ravel())
+        dc, frac = SN["predict_consistent"](net, L, R, W, H, work_width=ww, verbose=False)
+        out[tag + "_left"], out[tag + "_right"] = p.left, p.right
+        out[tag + "_consistent"], out[tag + "_frac"] = np.array(dc), np.array(frac)
+        out[tag + "_dims"] = np.array([W, H, 0 if ww is None else ww])
+        rng = np.random.default_rng(seed)
+        dl = list(p.disp.ravel() + rng.normal(0, 1.0, W * H))
+        dr = list(rng.uniform(0, 30, W * H))
+        v = SN["lr_consistency"](dl, dr, W, H, 1.5)
+        out[tag + "_lrc_in"] = np.array([dl, dr])
+        out[tag + "_lrc"] = np.array(v)
+        out[tag + "_fill"] = np.array(SN["fill_invalid"](dl, v, W, H))
     np.savez_compressed(os.path.join(HERE, "postproc.npz"), **out)
     print("postproc fixtures written")
 
 
 HOT_PATH = ["census", "band_costs", "_aggregate_path", "refine_fullres", "left_to_right",
             "lr_refine", "resize_gray", "avgpool2", "predict", "predict_at_scale",
-            "predict_auto", "refine_disparity", "median_filter", "slic", "plane_snap"]
+            "predict_auto", "refine_disparity", "median_filter", "slic", "plane_snap",
+            "predict_consistent", "lr_consistency", "fill_invalid"]
 
 
 def signatures(ref_dir):

@@ -188,3 +188,18 @@ def test_slic_uncovered_pixels_oracle_vs_reference(orc):
     assert np.array_equal(orc.slic(g["u_rgb"], W, H, step, float(g["u_comp"]))[0], g["u_slic"])
     snap = orc.plane_snap(g["u_disp"], g["u_rgb"], W, H, step=step, thr=5.0, min_inl=0.3)
     assert np.array_equal(bits(snap), bits(g["u_snap"]))
+
+
+@pytest.mark.parametrize("tag", ["c", "d"])
+def test_predict_consistent_oracle_vs_reference(orc, net, tag):
+    """predict_consistent, lr_consistency, fill_invalid (stereonet.py:4974-5076)."""
+    g = golden("postproc.npz")
+    W, H, ww = map(int, g[tag + "_dims"])
+    dl, dr = g[tag + "_lrc_in"]
+    v = orc.lr_consistency(dl, dr, W, H, 1.5)
+    assert np.array_equal(v, g[tag + "_lrc"])
+    assert np.array_equal(bits(orc.fill_invalid(dl, v, W, H)), bits(g[tag + "_fill"]))
+    d, frac = orc.predict_consistent(net, g[tag + "_left"].ravel() / 255.0,
+                                     g[tag + "_right"].ravel() / 255.0, W, H,
+                                     work_width=None if ww == 0 else ww)
+    assert np.array_equal(bits(d), bits(g[tag + "_consistent"])) and frac == float(g[tag + "_frac"])

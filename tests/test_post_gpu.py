@@ -88,3 +88,67 @@ def test_rejects(svb):
         svb.post.median_filter(np.zeros(12), 4, 3, radius=4)
     with pytest.raises(ValueError):
         svb.post.plane_snap(np.zeros(12), np.zeros(36), 4, 3, trials=65)
+
+
+@pytest.mark.parametrize("tag", ["c", "d"])
+def test_predict_consistent_vs_reference(svb, net, tag):
+    """stereonet.py:5048-5076; the network is FP32 here, FP64 in the
+    reference, so the disparity is compared within the network tolerance
+    (2e-3 px) and the valid fraction exactly."""
+    g = golden("postproc.npz")
+    W, H, ww = map(int, g[tag + "_dims"])
+    d, frac = svb.network.predict_consistent(net, g[tag + "_left"], g[tag + "_right"], W, H,
+                                             work_width=None if ww == 0 else ww, verbose=False)
+    assert frac == float(g[tag + "_frac"])
+    assert np.max(np.abs(np.asarray(d) - g[tag + "_consistent"])) < 2e-3
+
+
+def test_predict_consistent_vs_oracle_large(svb, orc, net):
+    p = svb.synth.make_pair(77, 450, 375, 0.0, 80.0, n_planes=(8, 15), lowtex_frac=0.2)
+    W, H = p.W, p.H
+    ref, rf = orc.predict_consistent(net, p.gray("left").ravel(), p.gray("right").ravel(), W, H)
+    got, gf = svb.network.predict_consistent(net, p.left, p.right, W, H, verbose=False)
+    # a pixel whose left-right difference sits within FP32 noise of tol may flip
+    assert abs(gf - rf) < 1e-3
+    close = np.abs(np.asarray(got) - ref) < 2e-3
+    assert close.mean() > 0.995
+
+
+def test_lr_consistency_and_fill_vs_reference(svb):
+    """lr_consistency and fill_invalid (stereonet.py:4986-5045) bit-exact."""
+    g = golden("postproc.npz")
+    for tag in "cd":
+        W, H, _ = map(int, g[tag + "_dims"])
+        dl, dr = g[tag + "_lrc_in"]
+        v = svb.post.lr_consistency(dl, dr, W, H, 1.5)
+        assert np.array_equal(np.asarray(v), g[tag + "_lrc"])
+        f = svb.post.fill_invalid(dl, g[tag + "_lrc"], W, H)
+        assert np.array_equal(bits(f), bits(g[tag + "_fill"]))
+    # rows without any valid pixel keep their values; single-pixel rows
+    rng = np.random.default_rng(3)
+    for W, H in ((1, 5), (7, 1), (2000, 3)):
+        d = rng.uniform(0, 9, W * H)
+        v = rng.random(W * H) < 0.3
+        v[:W] = False
+        assert np.array_equal(bits(svb.post.fill_invalid(d, v, W, H)),
+                              bits(_fill_ref(d, v, W, H)))
+
+
+def _fill_ref(d, v, W, H):
+    out = d.copy()
+    for y in range(H):
+        x = 0
+        while x < W:
+            if v[y * W + x]:
+                x += 1
+                continue
+            s = x
+            while x < W and not v[y * W + x]:
+                x += 1
+            lv = d[y * W + s - 1] if s > 0 else None
+            rv = d[y * W + x] if x < W else None
+            if lv is None and rv is None:
+                continue
+            f = rv if lv is None else lv if rv is None else (lv if lv < rv else rv)
+            out[y * W + s:y * W + x] = f
+    return out

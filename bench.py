@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="full", choices=["full", "small", "batched"])
+    ap.add_argument("--workload", default="full",
+                    choices=["full", "small", "batched", "refine_disparity"])
     ap.add_argument("--pairs", type=int, default=256, help="pairs of the batched workload")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound on the CPU-baseline sample")
@@ -424,6 +425,152 @@ def run_batched(args, rank, world, local):
     return res
 
 
+def pseudo_rgb(pair):
+    """An RGB image for plane_snap's SLIC: the left gray level and two smooth
+    transforms of it, interleaved, in [0, 1] (as read_image returns)."""
+    import numpy as np
+    g = pair.left.astype(np.float64) / 255.0
+    h, w = g.shape
+    yy, xx = np.mgrid[0:h, 0:w]
+    rgb = np.stack([g, 0.5 * g + 0.5 * (xx / max(1, w - 1)), 1.0 - 0.7 * g * (yy / max(1, h - 1))],
+                   axis=-1)
+    return (np.round(rgb * 255.0) / 255.0).ravel()
+
+
+def run_refdisp(args, rank, world, local):
+    """The refine_disparity workload: the 450x375 pair with an RGB image;
+    a step is predict_auto and refine_disparity (lr_refine, plane_snap on
+    the left-right-consistent pixels, 3x3 median; stereonet.py:5865-5883),
+    from images in HBM."""
+    import ctypes
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    lib = pkg._lib.load()
+    net = pkg.weights.load_model()
+    pair = pkg.synth.config_full()
+    W, H, N = pair.W, pair.H, pair.W * pair.H
+    rgb_h = pseudo_rgb(pair)
+    rgb = torch.from_numpy(rgb_h).cuda()
+    pipe = pkg.pipeline.PairPipeline(W, H, net, **PARAMS, tol=TOL)
+    hl = torch.from_numpy(pair.left.ravel()).pin_memory()
+    hr = torch.from_numpy(pair.right.ravel()).pin_memory()
+    pipe.left.copy_(hl)
+    pipe.right.copy_(hr)
+    prm = pkg.refine._params(**PARAMS)
+    need = lib.sv_refine_disparity_workspace_size(W, H, ctypes.byref(prm), 12)
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+    out = torch.empty(N, dtype=torch.float64, device="cuda")
+    st = torch.empty(N, dtype=torch.uint8, device="cuda")
+    hout = torch.empty(N, dtype=torch.float64).pin_memory()
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())                         # noqa: E731
+    s = pipe.stream.cuda_stream
+
+    def refdisp():
+        pkg._lib.check(lib.sv_refine_disparity(vp(pipe.left), vp(pipe.right), pipe.code, vp(rgb),
+                                               vp(pipe.disp0), W, H, TOL, ctypes.byref(prm), 1, 12,
+                                               1.0, 0.4, vp(out), vp(st), vp(ws), need, s),
+                       "refine_disparity")
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    with torch.cuda.stream(pipe.stream):
+        for _ in range(args.warmup):
+            pipe.predict()
+            refdisp()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.sv_launch_count()
+    with ClockSampler(local) as clk, torch.cuda.stream(pipe.stream):
+        for i in range(args.steps):
+            flush.zero_()
+            ev[i][0].record()
+            pipe.predict()
+            ev[i][1].record()
+            refdisp()
+            ev[i][2].record()
+        torch.cuda.synchronize()
+    launches = lib.sv_launch_count() - launches0
+    ms = sum(ev[i][0].elapsed_time(ev[i][2]) for i in range(args.steps))
+    st_pred = sum(ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)) / args.steps
+    st_ref = sum(ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)) / args.steps
+    # lr_refine alone on the same disparity, for the post-processing share
+    with torch.cuda.stream(pipe.stream):
+        for _ in range(3):
+            pipe.refine()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            pipe.refine()
+        e1.record()
+        torch.cuda.synchronize()
+    st_lr = e0.elapsed_time(e1) / args.steps
+    ms = pkg.shard.max_over_ranks(ms, device="cuda")
+    value = world * N * args.steps / (ms / 1e3) / 1e6
+    # end to end: pinned host images in, refined disparity out, every step
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(pipe.stream):
+        for i in range(args.steps):
+            flush.zero_()
+            e0[i].record()
+            pipe.left.copy_(hl, non_blocking=True)
+            pipe.right.copy_(hr, non_blocking=True)
+            pipe.predict()
+            refdisp()
+            hout.copy_(out, non_blocking=True)
+            e1[i].record()
+        torch.cuda.synchronize()
+    ems = sum(e0[i].elapsed_time(e1[i]) for i in range(args.steps))
+    ems = pkg.shard.max_over_ranks(ems, device="cuda")
+    evalue = world * N * args.steps / (ems / 1e3) / 1e6
+    if rank != 0:
+        return None
+    threads = os.cpu_count() or 1
+    import __graft_entry__ as ge
+    orc = ge.load_oracle()
+    orc.set_threads(threads)
+    L, R = pair.gray("left").ravel(), pair.gray("right").ravel()
+    t0 = time.time()
+    n = 0
+    while n < 1 or time.time() - t0 < min(args.cpu_seconds, 20.0):
+        df = orc.predict_auto(net, L, R, W, H)[0]
+        orc.refine_disparity(L, R, rgb_h, df, W, H, **PARAMS, tol=TOL)
+        n += 1
+    el = time.time() - t0
+    return {"metric": "refine_disparity Mpix/s per B200 (bit-exact post-processing)",
+            "value": round(value, 3), "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 network, integer refinement, f64 planes and median",
+            "data": "synthetic (seeded generator; pseudo-RGB from the left image)",
+            "config": {"workload": "450x375 pair: predict_auto + refine_disparity (lr_refine R=10, "
+                                   "plane_snap step 12 thr 1 min_inl 0.4, 3x3 median)",
+                       "l2": "flushed before every step (256 MB write, untimed)",
+                       "parallelism": "replicas x%d" % world},
+            "stages_ms": {"predict_auto": round(st_pred, 4), "refine_disparity": round(st_ref, 4),
+                          "of_which_lr_refine": round(st_lr, 4),
+                          "of_which_plane_snap_and_median": round(st_ref - st_lr, 4)},
+            "cpu_baseline": {"value": round(n * N / el / 1e6, 6), "unit": "Mpix/s",
+                             "cores": threads, "kind": "port",
+                             "sample": "%d whole pairs through the FP64 C port of predict_auto + "
+                                       "refine_disparity, %.1f s, OpenMP over %d threads"
+                                       % (n, el, threads)},
+            "e2e": {"value": round(evalue, 3), "unit": "Mpix/s", "h2d_bytes_per_step": 2 * N,
+                    "d2h_bytes_per_step": 8 * N},
+            "gpu_launches": int(launches), "clocks": clk.summary()}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -431,6 +578,8 @@ def main():
         res = run_reference(args, rank, world)
     elif args.workload == "batched":
         res = run_batched(args, rank, world, local)
+    elif args.workload == "refine_disparity":
+        res = run_refdisp(args, rank, world, local)
     else:
         res = run_ours(args, rank, world, local)
     if res is not None and rank == 0:

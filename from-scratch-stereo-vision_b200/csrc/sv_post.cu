@@ -158,16 +158,23 @@ __global__ void k_slic_commit(long N, const int *__restrict__ labtmp, int *__res
     else atomicExch(flag, 1);                          // not covered: keeps its label
 }
 
-// One thread per cluster (window order == index order), or one thread for
-// everything when some pixel was not covered.  win[] keeps the windows of
-// the assignment for the segment lists.
-__global__ void k_slic_update(const double *__restrict__ rgb, int W, int H, int step, int nc,
-                              SlicCenter *__restrict__ cs, const int *__restrict__ lab,
-                              const int *__restrict__ flag, int4 *__restrict__ win,
-                              double *__restrict__ acc) {
-    const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per cluster (window order == index order): the lanes stage 32
+// pixels of a window row at a time in shared memory and lane 0 adds the
+// cluster's ones in order -- or one thread for everything when some pixel
+// was not covered.  win[] keeps the windows of the assignment for the
+// segment lists.
+constexpr int kUpdWarps = 4;
+
+__global__ void __launch_bounds__(32 * kUpdWarps)
+    k_slic_update(const double *__restrict__ rgb, int W, int H, int step, int nc,
+                  SlicCenter *__restrict__ cs, const int *__restrict__ lab,
+                  const int *__restrict__ flag, int4 *__restrict__ win,
+                  double *__restrict__ acc) {
+    __shared__ double sv[kUpdWarps][32][3];
+    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (*flag) {
-        if (ci != 0) return;
+        if (blockIdx.x != 0 || threadIdx.x != 0) return;
         for (int k = 0; k < nc; ++k) win[k] = slic_window(cs[k], step, W, H);
         for (int k = 0; k < 6 * nc; ++k) acc[k] = 0.0;
         const long N = (long)W * H;
@@ -193,24 +200,39 @@ __global__ void k_slic_update(const double *__restrict__ rgb, int W, int H, int 
         }
         return;
     }
-    if (ci >= nc) return;
+    if (ci >= nc) return;                              // whole warps leave together
     const int4 w = slic_window(cs[ci], step, W, H);
-    win[ci] = w;
+    if (lane == 0) win[ci] = w;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
     long cnt = 0;
     for (int yy = w.z; yy <= w.w; ++yy) {
-        for (int xx = w.x; xx <= w.y; ++xx) {
+        for (int xb = w.x; xb <= w.y; xb += 32) {
+            const int xx = xb + lane;
             const long i = (long)yy * W + xx;
-            if (lab[i] != ci) continue;
-            s0 = __dadd_rn(s0, rgb[3 * i]);
-            s1 = __dadd_rn(s1, rgb[3 * i + 1]);
-            s2 = __dadd_rn(s2, rgb[3 * i + 2]);
-            s3 = __dadd_rn(s3, (double)xx);
-            s4 = __dadd_rn(s4, (double)yy);
-            ++cnt;
+            const bool ok = xx <= w.y && lab[i] == ci;
+            if (ok) {
+                sv[wi][lane][0] = rgb[3 * i];
+                sv[wi][lane][1] = rgb[3 * i + 1];
+                sv[wi][lane][2] = rgb[3 * i + 2];
+            }
+            unsigned m = __ballot_sync(kFull, ok);
+            __syncwarp();
+            if (lane == 0) {
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    s0 = __dadd_rn(s0, sv[wi][b][0]);
+                    s1 = __dadd_rn(s1, sv[wi][b][1]);
+                    s2 = __dadd_rn(s2, sv[wi][b][2]);
+                    s3 = __dadd_rn(s3, (double)(xb + b));
+                    s4 = __dadd_rn(s4, (double)yy);
+                    ++cnt;
+                }
+            }
+            __syncwarp();
         }
     }
-    if (cnt) {
+    if (lane == 0 && cnt) {
         const double n = (double)cnt;
         cs[ci] = {__dmul_rn(__ddiv_rn(s0, n), 255.0), __dmul_rn(__ddiv_rn(s1, n), 255.0),
                   __dmul_rn(__ddiv_rn(s2, n), 255.0), __ddiv_rn(s3, n), __ddiv_rn(s4, n)};
@@ -245,13 +267,14 @@ __device__ __forceinline__ int block_excl_sum(int v, int *total, int *sbuf) {
     return pre + x - v;
 }
 
-// Segment sizes (pass 0) and ordered pixel lists (pass 1) from the windows
-// of the last assignment; the exact single-thread path when some pixel was
-// not covered in that assignment.
+// Segment sizes (pass 0), then ordered pixel lists and valid counts
+// (pass 1), from the windows of the last assignment; the exact single-thread
+// path when some pixel was not covered in that assignment.
 __global__ void __launch_bounds__(256)
     k_seg_lists(int W, int H, int nseg, const int *__restrict__ lab, const int4 *__restrict__ win,
                 const int *__restrict__ flag, int pass, int *__restrict__ count,
-                const int *__restrict__ start, int *__restrict__ list) {
+                const int *__restrict__ start, int *__restrict__ list,
+                const uint8_t *__restrict__ valid, int *__restrict__ nvalid) {
     __shared__ int sbuf[32];
     if (*flag) {
         if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -261,10 +284,12 @@ __global__ void __launch_bounds__(256)
             for (long i = 0; i < N; ++i)
                 if (lab[i] >= 0) ++count[lab[i]];
         } else {
-            for (int g = 0; g < nseg; ++g) count[g] = 0;   // reused as fill cursors
+            for (int g = 0; g < nseg; ++g) count[g] = nvalid[g] = 0;   // count: fill cursors
             for (long i = 0; i < N; ++i) {
                 const int l = lab[i];
-                if (l >= 0) list[start[l] + count[l]++] = (int)i;
+                if (l < 0) continue;
+                list[start[l] + count[l]++] = (int)i;
+                nvalid[l] += valid ? (int)valid[i] : 1;
             }
         }
         return;
@@ -272,7 +297,7 @@ __global__ void __launch_bounds__(256)
     const int g = blockIdx.x;
     const int4 w = win[g];
     const int ww = w.y - w.x + 1, n = ww * (w.w - w.z + 1);
-    int base = 0;
+    int base = 0, nv = 0;
     for (int t0 = 0; t0 < n; t0 += blockDim.x) {
         const int t = t0 + threadIdx.x;
         int i = -1;
@@ -282,10 +307,18 @@ __global__ void __launch_bounds__(256)
         }
         int tot;
         const int pos = block_excl_sum(i >= 0, &tot, sbuf);
-        if (pass == 1 && i >= 0) list[start[g] + base + pos] = i;
+        if (pass == 1) {
+            if (i >= 0) list[start[g] + base + pos] = i;
+            int vt;
+            block_excl_sum(i >= 0 && (!valid || valid[i]), &vt, sbuf);
+            nv += vt;
+        }
         base += tot;
     }
-    if (pass == 0 && threadIdx.x == 0) count[g] = base;
+    if (threadIdx.x == 0) {
+        if (pass == 0) count[g] = base;
+        else nvalid[g] = nv;
+    }
 }
 
 // Exclusive scan of count[] into start[] (one CTA of 1024 threads).
@@ -327,9 +360,8 @@ constexpr int kJumpBits = 24;                // up to 2^24 segments
 // the jump matrices J_j = M^(3*trials*2^j) by squaring, then a scan of the
 // eligibility and one matrix product per set bit of each segment's count.
 __global__ void __launch_bounds__(1024)
-    k_seg_rng(int nseg, const int *__restrict__ start, const int *__restrict__ list,
-              const uint8_t *__restrict__ valid, int trials, uint32_t seed,
-              uint32_t *__restrict__ state, int *__restrict__ nvalid) {
+    k_seg_rng(int nseg, const int *__restrict__ nvalid, int trials, uint32_t seed,
+              uint32_t *__restrict__ state) {
     __shared__ uint32_t J[kJumpBits][32];
     __shared__ uint32_t T[2][32];
     __shared__ int sbuf[32];
@@ -364,11 +396,7 @@ __global__ void __launch_bounds__(1024)
     int base = 0;
     for (int g0 = 0; g0 < nseg; g0 += blockDim.x) {
         const int g = g0 + t;
-        int nv = 0;
-        if (g < nseg) {
-            for (int k = start[g]; k < start[g + 1]; ++k) nv += valid ? (int)valid[list[k]] : 1;
-            nvalid[g] = nv;
-        }
+        const int nv = g < nseg ? nvalid[g] : 0;
         int tot;
         const int c = base + block_excl_sum(g < nseg && nv >= 12, &tot, sbuf);
         if (g < nseg) {
@@ -411,8 +439,13 @@ __device__ __forceinline__ double plane_at(const double *pl, int i, int W) {
 }
 
 constexpr int kMaxTrials = 64;
+constexpr int kSnapCap = 2048;          // segment points staged in shared memory
 
-// One CTA per segment: RANSAC, least squares over the inliers, snap.
+// One CTA per segment: RANSAC, least squares over the inliers, snap.  The
+// segment's valid points (x, y, d) are staged in shared memory so the
+// sequential parts (the draws and planes of thread 0, the ordered
+// least-squares sums) read shared memory; segments larger than kSnapCap
+// read global memory instead (same values, same order).
 __global__ void __launch_bounds__(256)
     k_seg_snap(const double *__restrict__ disp, int W, const uint8_t *__restrict__ valid,
                const int *__restrict__ start, const int *__restrict__ list,
@@ -424,6 +457,9 @@ __global__ void __launch_bounds__(256)
     __shared__ int sbuf[32];
     __shared__ int s_best;
     __shared__ double fit[3];
+    __shared__ int2 sxy[kSnapCap];
+    __shared__ double sdv[kSnapCap];
+    __shared__ int sinl[kSnapCap];
     const int g = blockIdx.x, t = threadIdx.x;
     const int s0 = start[g], gn = start[g + 1] - s0;
     if (nvalid[g] < 12) return;
@@ -439,17 +475,43 @@ __global__ void __launch_bounds__(256)
         base += tot;
     }
     const int n = base;
+    const bool staged = n <= kSnapCap;
+    __syncthreads();
+    if (staged) {
+        for (int j = t; j < n; j += blockDim.x) {
+            const int i = pts[s0 + j];
+            sxy[j] = make_int2(i % W, i / W);
+            sdv[j] = disp[i];
+        }
+    }
+    __syncthreads();
+    auto P = [&](int j, double &x, double &y, double &d) {
+        if (staged) {
+            const int2 q = sxy[j];
+            x = (double)q.x;
+            y = (double)q.y;
+            d = sdv[j];
+        } else {
+            const int i = pts[s0 + j];
+            x = (double)(i % W);
+            y = (double)(i / W);
+            d = disp[i];
+        }
+    };
+    auto resid_ok = [&](const double *pl, int j) {
+        double x, y, d;
+        P(j, x, y, d);
+        const double v = __dadd_rn(__dadd_rn(__dmul_rn(pl[0], x), __dmul_rn(pl[1], y)), pl[2]);
+        return fabs(__dsub_rn(v, d)) <= thr;
+    };
     if (t == 0) {
         uint32_t s = state[g];
         for (int tr = 0; tr < trials; ++tr) {
             double A[3][3], bv[3];
             for (int u = 0; u < 3; ++u) {
                 s = xorshift32(s);
-                const int i = pts[s0 + (int)(s % (uint32_t)n)];
-                A[u][0] = (double)(i % W);
-                A[u][1] = (double)(i / W);
+                P((int)(s % (uint32_t)n), A[u][0], A[u][1], bv[u]);
                 A[u][2] = 1.0;
-                bv[u] = disp[i];
             }
             ok[tr] = solve3_dev(A, bv, planes[tr]);
             cnt[tr] = 0;
@@ -458,9 +520,7 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     for (long q = t; q < (long)trials * n; q += blockDim.x) {
         const int tr = (int)(q / n), j = (int)(q - (long)tr * n);
-        if (!ok[tr]) continue;
-        const int i = pts[s0 + j];
-        if (fabs(__dsub_rn(plane_at(planes[tr], i, W), disp[i])) <= thr) atomicAdd(&cnt[tr], 1);
+        if (ok[tr] && resid_ok(planes[tr], j)) atomicAdd(&cnt[tr], 1);
     }
     __syncthreads();
     if (t == 0) {
@@ -478,41 +538,52 @@ __global__ void __launch_bounds__(256)
     base = 0;
     for (int k0 = 0; k0 < n; k0 += blockDim.x) {
         const int k = k0 + t;
-        const int i = k < n ? pts[s0 + k] : -1;
-        const int take = i >= 0 && fabs(__dsub_rn(plane_at(planes[best], i, W), disp[i])) <= thr;
+        const int take = k < n && resid_ok(planes[best], k);
         int tot;
         const int pos = block_excl_sum(take, &tot, sbuf);
-        if (take) inl[s0 + base + pos] = i;
+        if (take) {
+            if (staged) sinl[base + pos] = k;
+            else inl[s0 + base + pos] = k;
+        }
         base += tot;
     }
+    __syncthreads();
     if (t == 0) {
         // _lsq_plane, stereonet.py:5472-5502: sums in inlier order
         const int ni = base;
         const double nn = (double)ni;
-        double sx = 0.0, sy = 0.0, sd = 0.0;
-        for (int k = 0; k < ni; ++k) sx = __dadd_rn(sx, (double)(inl[s0 + k] % W));
-        for (int k = 0; k < ni; ++k) sy = __dadd_rn(sy, (double)(inl[s0 + k] / W));
-        for (int k = 0; k < ni; ++k) sd = __dadd_rn(sd, disp[inl[s0 + k]]);
-        const double mx = __ddiv_rn(sx, nn), my = __ddiv_rn(sy, nn), md = __ddiv_rn(sd, nn);
-        double sxx = 0.0, sxy = 0.0, syy = 0.0, sxd = 0.0, syd = 0.0;
+        double sx = 0.0, sy = 0.0, sd = 0.0, x, y, d;
         for (int k = 0; k < ni; ++k) {
-            const int i = inl[s0 + k];
-            const double u = __dsub_rn((double)(i % W), mx), v = __dsub_rn((double)(i / W), my);
-            const double w = __dsub_rn(disp[i], md);
+            P(staged ? sinl[k] : inl[s0 + k], x, y, d);
+            sx = __dadd_rn(sx, x);
+        }
+        for (int k = 0; k < ni; ++k) {
+            P(staged ? sinl[k] : inl[s0 + k], x, y, d);
+            sy = __dadd_rn(sy, y);
+        }
+        for (int k = 0; k < ni; ++k) {
+            P(staged ? sinl[k] : inl[s0 + k], x, y, d);
+            sd = __dadd_rn(sd, d);
+        }
+        const double mx = __ddiv_rn(sx, nn), my = __ddiv_rn(sy, nn), md = __ddiv_rn(sd, nn);
+        double sxx = 0.0, sxy_ = 0.0, syy = 0.0, sxd = 0.0, syd = 0.0;
+        for (int k = 0; k < ni; ++k) {
+            P(staged ? sinl[k] : inl[s0 + k], x, y, d);
+            const double u = __dsub_rn(x, mx), v = __dsub_rn(y, my), w = __dsub_rn(d, md);
             sxx = __dadd_rn(sxx, __dmul_rn(u, u));
-            sxy = __dadd_rn(sxy, __dmul_rn(u, v));
+            sxy_ = __dadd_rn(sxy_, __dmul_rn(u, v));
             syy = __dadd_rn(syy, __dmul_rn(v, v));
             sxd = __dadd_rn(sxd, __dmul_rn(u, w));
             syd = __dadd_rn(syd, __dmul_rn(v, w));
         }
-        const double det = __dsub_rn(__dmul_rn(sxx, syy), __dmul_rn(sxy, sxy));
+        const double det = __dsub_rn(__dmul_rn(sxx, syy), __dmul_rn(sxy_, sxy_));
         if (fabs(det) < 1.0e-9) {
             fit[0] = 0.0;
             fit[1] = 0.0;
             fit[2] = md;
         } else {
-            const double a = __ddiv_rn(__dsub_rn(__dmul_rn(sxd, syy), __dmul_rn(syd, sxy)), det);
-            const double b = __ddiv_rn(__dsub_rn(__dmul_rn(syd, sxx), __dmul_rn(sxd, sxy)), det);
+            const double a = __ddiv_rn(__dsub_rn(__dmul_rn(sxd, syy), __dmul_rn(syd, sxy_)), det);
+            const double b = __ddiv_rn(__dsub_rn(__dmul_rn(syd, sxx), __dmul_rn(sxd, sxy_)), det);
             fit[0] = a;
             fit[1] = b;
             fit[2] = __dsub_rn(__dsub_rn(md, __dmul_rn(a, mx)), __dmul_rn(b, my));
@@ -608,8 +679,8 @@ int launch_slic(const double *rgb, int W, int H, int step, double compactness, i
         count_launch();
         k_slic_commit<<<nb, 256, 0, st>>>(N, w.labtmp, w.lab, w.flag);
         count_launch();
-        k_slic_update<<<(nc + 127) / 128, 128, 0, st>>>(rgb, W, H, step, nc, cs, w.lab, w.flag,
-                                                        w.win, w.acc);
+        k_slic_update<<<(nc + kUpdWarps - 1) / kUpdWarps, 32 * kUpdWarps, 0, st>>>(
+            rgb, W, H, step, nc, cs, w.lab, w.flag, w.win, w.acc);
     }
     SV_LAUNCH_CHECK();
     return SV_OK;
@@ -629,13 +700,15 @@ int launch_plane_snap(const double *disp, const double *rgb, int W, int H, const
     SV_TRY_POST(launch_slic(rgb, W, H, step, 10.0, 5, w, st));
     if (nc == 0 || trials == 0) return SV_OK;
     count_launch();
-    k_seg_lists<<<nc, 256, 0, st>>>(W, H, nc, w.lab, w.win, w.flag, 0, w.count, w.start, w.list);
+    k_seg_lists<<<nc, 256, 0, st>>>(W, H, nc, w.lab, w.win, w.flag, 0, w.count, w.start, w.list,
+                                    valid, w.nvalid);
     count_launch();
     k_seg_scan<<<1, 1024, 0, st>>>(nc, w.count, w.start);
     count_launch();
-    k_seg_lists<<<nc, 256, 0, st>>>(W, H, nc, w.lab, w.win, w.flag, 1, w.count, w.start, w.list);
+    k_seg_lists<<<nc, 256, 0, st>>>(W, H, nc, w.lab, w.win, w.flag, 1, w.count, w.start, w.list,
+                                    valid, w.nvalid);
     count_launch();
-    k_seg_rng<<<1, 1024, 0, st>>>(nc, w.start, w.list, valid, trials, seed, w.state, w.nvalid);
+    k_seg_rng<<<1, 1024, 0, st>>>(nc, w.nvalid, trials, seed, w.state);
     count_launch();
     k_seg_snap<<<nc, 256, 0, st>>>(disp, W, valid, w.start, w.list, w.nvalid, w.state, trials,
                                    thr, min_inl, w.pts, w.inl, out);

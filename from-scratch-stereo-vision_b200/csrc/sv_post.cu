@@ -169,8 +169,9 @@ __global__ void __launch_bounds__(32 * kUpdWarps)
     k_slic_update(const double *__restrict__ rgb, int W, int H, int step, int nc,
                   SlicCenter *__restrict__ cs, const int *__restrict__ lab,
                   const int *__restrict__ flag, int4 *__restrict__ win,
-                  double *__restrict__ acc) {
+                  double *__restrict__ acc, int cap) {
     __shared__ double sv[kUpdWarps][32][3];
+    extern __shared__ __align__(16) unsigned char upd_smem[];   // [warps][cap] staged pixels
     const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
     const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (*flag) {
@@ -205,7 +206,54 @@ __global__ void __launch_bounds__(32 * kUpdWarps)
     if (lane == 0) win[ci] = w;
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, s4 = 0.0;
     long cnt = 0;
-    for (int yy = w.z; yy <= w.w; ++yy) {
+    const int ww = w.y - w.x + 1, wn = ww * (w.w - w.z + 1);
+    if (wn <= cap) {
+        // stage the cluster's pixels, compacted in window (= index) order
+        const int nw = blockDim.x >> 5;
+        double *cv = reinterpret_cast<double *>(upd_smem) + (size_t)wi * cap * 3;
+        int2 *cxy = reinterpret_cast<int2 *>(reinterpret_cast<double *>(upd_smem) +
+                                             (size_t)nw * cap * 3) + (size_t)wi * cap;
+        int base = 0;
+        for (int t0 = 0; t0 < wn; t0 += 4 * 32) {
+            int xx[4], yy[4];
+            bool ok[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int t = t0 + 32 * u + lane;
+                ok[u] = false;
+                xx[u] = yy[u] = 0;
+                if (t < wn) {
+                    yy[u] = w.z + t / ww;
+                    xx[u] = w.x + t % ww;
+                    ok[u] = lab[(long)yy[u] * W + xx[u]] == ci;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const unsigned m = __ballot_sync(kFull, ok[u]);
+                if (ok[u]) {
+                    const int pos = base + __popc(m & ((1u << lane) - 1u));
+                    const long i = (long)yy[u] * W + xx[u];
+                    cv[3 * pos] = rgb[3 * i];
+                    cv[3 * pos + 1] = rgb[3 * i + 1];
+                    cv[3 * pos + 2] = rgb[3 * i + 2];
+                    cxy[pos] = make_int2(xx[u], yy[u]);
+                }
+                base += __popc(m);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            for (int k = 0; k < base; ++k) {
+                s0 = __dadd_rn(s0, cv[3 * k]);
+                s1 = __dadd_rn(s1, cv[3 * k + 1]);
+                s2 = __dadd_rn(s2, cv[3 * k + 2]);
+                s3 = __dadd_rn(s3, (double)cxy[k].x);
+                s4 = __dadd_rn(s4, (double)cxy[k].y);
+            }
+            cnt = base;
+        }
+    } else for (int yy = w.z; yy <= w.w; ++yy) {
         for (int xb = w.x; xb <= w.y; xb += 32) {
             const int xx = xb + lane;
             const long i = (long)yy * W + xx;
@@ -460,6 +508,7 @@ __global__ void __launch_bounds__(256)
     __shared__ int2 sxy[kSnapCap];
     __shared__ double sdv[kSnapCap];
     __shared__ int sinl[kSnapCap];
+    __shared__ int sbuf_draw[3 * kMaxTrials];
     const int g = blockIdx.x, t = threadIdx.x;
     const int s0 = start[g], gn = start[g + 1] - s0;
     if (nvalid[g] < 12) return;
@@ -504,18 +553,23 @@ __global__ void __launch_bounds__(256)
         const double v = __dadd_rn(__dadd_rn(__dmul_rn(pl[0], x), __dmul_rn(pl[1], y)), pl[2]);
         return fabs(__dsub_rn(v, d)) <= thr;
     };
+    // the draws are one sequential stream (thread 0); the planes are not
     if (t == 0) {
         uint32_t s = state[g];
-        for (int tr = 0; tr < trials; ++tr) {
-            double A[3][3], bv[3];
-            for (int u = 0; u < 3; ++u) {
-                s = xorshift32(s);
-                P((int)(s % (uint32_t)n), A[u][0], A[u][1], bv[u]);
-                A[u][2] = 1.0;
-            }
-            ok[tr] = solve3_dev(A, bv, planes[tr]);
-            cnt[tr] = 0;
+        for (int k = 0; k < 3 * trials; ++k) {
+            s = xorshift32(s);
+            sbuf_draw[k] = (int)(s % (uint32_t)n);
         }
+    }
+    __syncthreads();
+    if (t < trials) {
+        double A[3][3], bv[3];
+        for (int u = 0; u < 3; ++u) {
+            P(sbuf_draw[3 * t + u], A[u][0], A[u][1], bv[u]);
+            A[u][2] = 1.0;
+        }
+        ok[t] = solve3_dev(A, bv, planes[t]);
+        cnt[t] = 0;
     }
     __syncthreads();
     for (long q = t; q < (long)trials * n; q += blockDim.x) {
@@ -669,6 +723,12 @@ int launch_slic(const double *rgb, int W, int H, int step, double compactness, i
     count_launch();
     k_slic_init<<<(nc + 127) / 128, 128, 0, st>>>(rgb, W, step, ncx, nc, cs);
     const int nb = grid_for(N, 256, 1 << 30);
+    // SLIC update staging: (2 step + 1)^2 pixels of 32 bytes per warp
+    const long wmax = (long)(2 * step + 1) * (2 * step + 1);
+    // within the 48 KB default, next to the kernel's 3 KB of static shared memory
+    const int wpb0 = (int)((44l * 1024) / (wmax * 32));
+    const int wpb = wpb0 < 1 ? kUpdWarps : (wpb0 > kUpdWarps ? kUpdWarps : wpb0);
+    const int cap = wpb0 < 1 ? 0 : (int)wmax;
     for (int it = 0; it < iters; ++it) {
         count_launch();
         k_slic_reset<<<nb, 256, 0, st>>>(N, w.dist, w.labtmp, w.flag);
@@ -679,8 +739,8 @@ int launch_slic(const double *rgb, int W, int H, int step, double compactness, i
         count_launch();
         k_slic_commit<<<nb, 256, 0, st>>>(N, w.labtmp, w.lab, w.flag);
         count_launch();
-        k_slic_update<<<(nc + kUpdWarps - 1) / kUpdWarps, 32 * kUpdWarps, 0, st>>>(
-            rgb, W, H, step, nc, cs, w.lab, w.flag, w.win, w.acc);
+        k_slic_update<<<(nc + wpb - 1) / wpb, 32 * wpb, (size_t)wpb * cap * 32, st>>>(
+            rgb, W, H, step, nc, cs, w.lab, w.flag, w.win, w.acc, cap);
     }
     SV_LAUNCH_CHECK();
     return SV_OK;

@@ -11,6 +11,10 @@ with ``importlib`` the same way.  Modules:
 * ``pipeline``-- the network + refinement path for one pair, device resident;
 * ``shim``    -- ``install(SN)`` rebinds those names in an exec'd reference
   namespace, so the reference's own callers use the GPU versions;
+* ``post``    -- median_filter / slic / plane_snap / refine_disparity /
+  lr_consistency / fill_invalid drop-ins; ``band`` -- the learned band;
+* ``image``   -- read_png / read_pnm / read_image drop-ins (host decode,
+  GPU FP64 conversion);
 * ``synth``   -- seeded synthetic stereo pairs; ``weights`` -- checkpoints.
 
 All compute goes through libsv_b200.so; there is no CPU fallback.
@@ -24,6 +28,7 @@ __all__ = ["_lib", "synth", "weights"]
 def __getattr__(name):
     # heavy modules (torch) load on first use
     import importlib
-    if name in ("refine", "network", "pipeline", "shim", "shard", "batch", "band", "post"):
+    if name in ("refine", "network", "pipeline", "shim", "shard", "batch", "band", "post",
+                "image"):
         return importlib.import_module("." + name, __name__)
     raise AttributeError(name)

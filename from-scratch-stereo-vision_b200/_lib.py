@@ -29,6 +29,18 @@ class RefineParams(ctypes.Structure):
                 ("prior_t", ctypes.c_double)]
 
 
+SV_IMAGE_PNG, SV_IMAGE_PNM = 1, 2
+
+
+class RawImage(ctypes.Structure):
+    """sv_raw_image (a decoded file's raw samples)."""
+    _fields_ = [("kind", ctypes.c_int), ("width", ctypes.c_int), ("height", ctypes.c_int),
+                ("depth", ctypes.c_int), ("colortype", ctypes.c_int), ("channels", ctypes.c_int),
+                ("stride", ctypes.c_int), ("interlace", ctypes.c_int), ("maxval", ctypes.c_int),
+                ("ascii", ctypes.c_int), ("palette_len", ctypes.c_int), ("inv", ctypes.c_double),
+                ("palette", ctypes.c_uint8 * 768)]
+
+
 # name -> (restype, argtypes)
 _VP = ctypes.c_void_p
 _I = ctypes.c_int
@@ -63,6 +75,9 @@ SIGNATURES = {
     "sv_lr_consistency": (_I, [_VP, _VP, _I, _I, _D, _VP, _VP, _VP]),
     "sv_fill_invalid_workspace_size": (_SZ, [_I, _I]),
     "sv_fill_invalid": (_I, [_VP, _VP, _I, _I, _VP, _VP, _SZ, _VP]),
+    "sv_image_info": (_I, [ctypes.c_char_p, _SZ, ctypes.POINTER(RawImage)]),
+    "sv_image_decode_raw": (_I, [ctypes.c_char_p, _SZ, _VP, _SZ, ctypes.POINTER(RawImage)]),
+    "sv_raw_to_float": (_I, [_VP, ctypes.POINTER(RawImage), _VP, _VP, _VP]),
     "sv_median_workspace_size": (_SZ, [_I, _I]),
     "sv_median_filter": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _SZ, _VP]),
     "sv_postproc_workspace_size": (_SZ, [_I, _I, _I]),

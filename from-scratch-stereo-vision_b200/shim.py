@@ -19,7 +19,7 @@ reference's own path).  ``uninstall(SN)`` restores the originals.
 
 from __future__ import annotations
 
-from . import network, post, refine
+from . import image, network, post, refine
 
 # reference name -> drop-in
 DROP_INS = {
@@ -41,6 +41,9 @@ DROP_INS = {
     "predict_consistent": network.predict_consistent,
     "lr_consistency": post.lr_consistency,
     "fill_invalid": post.fill_invalid,
+    "read_png": image.read_png,
+    "read_pnm": image.read_pnm,
+    "read_image": image.read_image,
 }
 
 _SAVED = "__sv_b200_saved__"

@@ -257,3 +257,77 @@ def config_learned_crop(seed: int, W: int = 256, H: int = 192) -> StereoPair:
     rng = np.random.default_rng(seed)
     return make_pair(seed, W, H, 30.0, 150.0, n_planes=(2, 5),
                      lowtex_frac=0.3, bars=int(rng.integers(1, 4)))
+
+
+# ------------------------------------------------------- file formats
+def _png_chunk(tag: bytes, body: bytes) -> bytes:
+    import zlib
+    return (len(body).to_bytes(4, "big") + tag + body +
+            (zlib.crc32(tag + body) & 0xFFFFFFFF).to_bytes(4, "big"))
+
+
+def _filter_rows(rows, bpp, filters):
+    """PNG row filters 0-4 applied forward (PNG 1.2 section 6)."""
+    out = bytearray()
+    prev = bytes(len(rows[0]))
+    for y, row in enumerate(rows):
+        ft = filters[y % len(filters)]
+        out.append(ft)
+        for i, x in enumerate(row):
+            a = row[i - bpp] if i >= bpp else 0
+            b = prev[i] if y > 0 else 0
+            c = prev[i - bpp] if (y > 0 and i >= bpp) else 0
+            if ft == 0:
+                pr = 0
+            elif ft == 1:
+                pr = a
+            elif ft == 2:
+                pr = b
+            elif ft == 3:
+                pr = (a + b) >> 1
+            else:
+                p = a + b - c
+                pa, pb, pc = abs(p - a), abs(p - b), abs(p - c)
+                pr = a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)
+            out.append((x - pr) & 0xFF)
+        prev = row
+    return bytes(out)
+
+
+def make_png(W, H, depth, ct, samples, filters=(0,), level=9, strategy=0, palette=None,
+             idat_parts=1, extra=False, interlace=0, zlib_stream=None):
+    """A PNG of `samples` ([H][W*channels] ints) encoded with Python's zlib."""
+    import zlib
+    ch = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}[ct]
+    rows = []
+    for y in range(H):
+        vals = samples[y]
+        if depth == 16:
+            r = b"".join(int(v).to_bytes(2, "big") for v in vals)
+        elif depth == 8:
+            r = bytes(int(v) for v in vals)
+        else:
+            bits = 0
+            r = bytearray((W * depth + 7) // 8)
+            for v in vals:
+                r[bits >> 3] |= int(v) << (8 - depth - (bits & 7))
+                bits += depth
+            r = bytes(r)
+        rows.append(r)
+    raw = _filter_rows(rows, max(1, ch * depth // 8), list(filters))
+    if zlib_stream is None:
+        co = zlib.compressobj(level, zlib.DEFLATED, 15, 9, strategy)
+        zlib_stream = co.compress(raw) + co.flush()
+    ihdr = W.to_bytes(4, "big") + H.to_bytes(4, "big") + bytes([depth, ct, 0, 0, interlace])
+    out = b"\x89PNG\r\n\x1a\n" + _png_chunk(b"IHDR", ihdr)
+    if extra:
+        out += _png_chunk(b"tEXt", b"Comment\x00golden fixture")
+    if palette is not None:
+        out += _png_chunk(b"PLTE", bytes(palette))
+    step = (len(zlib_stream) + idat_parts - 1) // idat_parts
+    for k in range(idat_parts):
+        out += _png_chunk(b"IDAT", zlib_stream[k * step:(k + 1) * step])
+    out += _png_chunk(b"IEND", b"")
+    if extra:
+        out += b"trailing bytes after IEND"
+    return out, raw

@@ -346,6 +346,41 @@ int sv_lr_refine_band(const void *left, const void *right, int dtype,
                       uint8_t *status, void *workspace, size_t workspace_bytes,
                       void *stream);
 
+/* ------------------------------------------------------------------------
+ * Input images: PNG (stereonet.py:3499-3601 read_png, with zlib_decompress
+ * 3421, inflate 3335 and _unfilter 3456) and PGM/PPM (stereonet.py:265-324
+ * read_pnm); read_image (3604) picks by the magic bytes.  Decoding runs on
+ * the host into raw samples; sv_raw_to_float forms the FP64 images on the
+ * GPU, bit-identical to the reference's (gray = 0.299 r + 0.587 g + 0.114 b;
+ * a PGM keeps its sample as gray).
+ * ---------------------------------------------------------------------- */
+#define SV_IMAGE_PNG 1
+#define SV_IMAGE_PNM 2
+typedef struct sv_raw_image {
+    int kind;        /* SV_IMAGE_PNG or SV_IMAGE_PNM                          */
+    int width, height;
+    int depth;       /* bits per sample in `raw` (PNM: 8, or 16 big-endian)   */
+    int colortype;   /* PNG colour type; PNM: 0 (P2/P5) or 2 (P3/P6)          */
+    int channels;    /* samples per pixel in `raw`                            */
+    int stride;      /* bytes per row of `raw`                                */
+    int interlace;   /* PNG IHDR interlace method (only 0 is decoded)         */
+    int maxval;      /* PNM maxval                                            */
+    int ascii;       /* PNM P2/P3                                             */
+    int palette_len; /* PLTE bytes                                            */
+    double inv;      /* 1 / (2^depth - 1) for PNG, 1 / maxval for PNM         */
+    uint8_t palette[768];
+} sv_raw_image;
+/* header only (no decompression): fills desc; raw bytes = stride * height */
+int sv_image_info(const uint8_t *data, size_t n, sv_raw_image *desc);
+/* decodes the file held in host memory into raw samples (host memory,
+ * stride * height bytes), rejecting what the reference rejects */
+int sv_image_decode_raw(const uint8_t *data, size_t n, uint8_t *raw,
+                        size_t raw_bytes, sv_raw_image *desc);
+/* device raw samples -> gray [H][W] and rgb [H][W][3] (FP64 device buffers;
+ * either may be NULL) */
+int sv_raw_to_float(const uint8_t *raw, const sv_raw_image *desc, double *gray,
+                    double *rgb, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -283,10 +283,152 @@ def postproc(ref_dir):
     print("postproc fixtures written")
 
 
+# ------------------------------------------------------------------ images
+def image_cases():
+    """(name, file bytes) of every decoded case, and of the error cases."""
+    import zlib
+    make_png = synth.make_png
+    rng = np.random.default_rng(8086)
+
+    def noise(W, H, ch, hi):
+        return rng.integers(0, hi + 1, size=(H, W * ch)).tolist()
+
+    def smooth(W, H, ch, hi):
+        yy, xx = np.mgrid[0:H, 0:W * ch]
+        v = (np.sin(xx / 7.0) + np.cos(yy / 5.0) + 2) / 4 * hi
+        v = v + rng.integers(0, 3, size=v.shape)
+        return np.clip(v, 0, hi).astype(int).tolist()
+
+    ok = []
+    F = (0, 1, 2, 3, 4)
+    ok.append(("rgb8_dyn", make_png(37, 23, 8, 2, noise(37, 23, 3, 255), F, 9)[0]))
+    ok.append(("gray8_rle", make_png(40, 30, 8, 0, smooth(40, 30, 1, 255), (4,), 6,
+                                     zlib.Z_RLE)[0]))
+    ok.append(("rgb16_fixed", make_png(21, 13, 16, 2, noise(21, 13, 3, 65535), F, 6,
+                                       zlib.Z_FIXED)[0]))
+    ok.append(("gray16_stored", make_png(19, 11, 16, 0, noise(19, 11, 1, 65535), (2, 1), 0)[0]))
+    ok.append(("ga8", make_png(17, 9, 8, 4, noise(17, 9, 2, 255), F, 6)[0]))
+    ok.append(("rgba8_huff", make_png(23, 15, 8, 6, noise(23, 15, 4, 255), (3,), 6,
+                                      zlib.Z_HUFFMAN_ONLY)[0]))
+    ok.append(("rgba16", make_png(9, 7, 16, 6, noise(9, 7, 4, 65535), F, 9)[0]))
+    ok.append(("ga16", make_png(11, 5, 16, 4, noise(11, 5, 2, 65535), (4, 3), 9)[0]))
+    for d, W, H in ((1, 29, 7), (2, 27, 9), (4, 13, 11)):
+        ok.append(("gray%d" % d, make_png(W, H, d, 0, noise(W, H, 1, (1 << d) - 1), F, 9)[0]))
+    for d, W, H, n in ((1, 21, 6, 2), (2, 19, 7, 4), (4, 15, 9, 16), (8, 33, 12, 200)):
+        pal = rng.integers(0, 256, size=3 * n).tolist()
+        ok.append(("pal%d" % d, make_png(W, H, d, 3, noise(W, H, 1, n - 1), F, 9,
+                                         palette=pal)[0]))
+    ok.append(("rgb8_smooth_split", make_png(96, 64, 8, 2, smooth(96, 64, 3, 255), F, 9,
+                                             idat_parts=3, extra=True)[0]))
+    ok.append(("gray8_stored_multi", make_png(300, 230, 8, 0, smooth(300, 230, 1, 255),
+                                              (0,), 0)[0]))
+
+    def pnm(magic, W, H, maxval, vals, comment=True, sep=b" "):
+        hdr = magic + b"\n" + (b"# golden fixture\n" if comment else b"")
+        hdr += b"%d %d\n%d\n" % (W, H, maxval)
+        if magic in (b"P2", b"P3"):
+            body = b""
+            for i, v in enumerate(vals):
+                body += b"%d" % v + (b"\n" if i % 11 == 10 else sep)
+            return hdr + body
+        if maxval < 256:
+            return hdr + bytes(vals)
+        return hdr + b"".join(int(v).to_bytes(2, "big") for v in vals)
+
+    def flat(W, H, ch, hi):
+        return rng.integers(0, hi + 1, size=W * H * ch).tolist()
+
+    ok.append(("p5_8", pnm(b"P5", 25, 20, 255, flat(25, 20, 1, 255))))
+    ok.append(("p5_16", pnm(b"P5", 17, 13, 65535, flat(17, 13, 1, 65535), comment=False)))
+    ok.append(("p5_1000", pnm(b"P5", 12, 9, 1000, flat(12, 9, 1, 1000))))
+    ok.append(("p6_8", pnm(b"P6", 19, 11, 255, flat(19, 11, 3, 255))))
+    ok.append(("p6_100", pnm(b"P6", 14, 8, 100, flat(14, 8, 3, 100))))
+    ok.append(("p6_4095", pnm(b"P6", 9, 6, 4095, flat(9, 6, 3, 4095))))
+    ok.append(("p2_15", pnm(b"P2", 13, 7, 15, flat(13, 7, 1, 15), sep=b"\t ")))
+    ok.append(("p3_255", pnm(b"P3", 8, 5, 255, flat(8, 5, 3, 255), sep=b"\r\n")))
+    ok.append(("p2_65535", pnm(b"P2", 6, 4, 65535, flat(6, 4, 1, 65535))))
+
+    err = []
+    base, raw = make_png(8, 4, 8, 0, noise(8, 4, 1, 255), (0,), 9)
+    good = zlib.compress(raw, 9)
+    err.append(("interlaced", make_png(8, 4, 8, 0, noise(8, 4, 1, 255), interlace=1)[0]))
+    err.append(("depth3", make_png(8, 4, 8, 0, noise(8, 4, 1, 255))[0].replace(
+        b"IHDR" + (8).to_bytes(4, "big") + (4).to_bytes(4, "big") + bytes([8, 0]),
+        b"IHDR" + (8).to_bytes(4, "big") + (4).to_bytes(4, "big") + bytes([3, 0]))))
+    err.append(("colortype5", make_png(8, 4, 8, 0, noise(8, 4, 1, 255))[0].replace(
+        b"IHDR" + (8).to_bytes(4, "big") + (4).to_bytes(4, "big") + bytes([8, 0]),
+        b"IHDR" + (8).to_bytes(4, "big") + (4).to_bytes(4, "big") + bytes([8, 5]))))
+    err.append(("zlib_method", make_png(8, 4, 8, 0, noise(8, 4, 1, 255),
+                                        zlib_stream=bytes([0x77, 0x01]) + good[2:])[0]))
+    err.append(("zlib_check", make_png(8, 4, 8, 0, noise(8, 4, 1, 255),
+                                       zlib_stream=bytes([0x78, 0x02]) + good[2:])[0]))
+    err.append(("zlib_dict", make_png(8, 4, 8, 0, noise(8, 4, 1, 255),
+                                      zlib_stream=bytes([0x78, 0xBB]) + good[2:])[0]))
+    bad_filter = bytearray(raw)
+    bad_filter[9] = 5                           # second row's filter byte
+    err.append(("filter5", make_png(8, 4, 8, 0, noise(8, 4, 1, 255),
+                                    zlib_stream=zlib.compress(bytes(bad_filter), 9))[0]))
+    err.append(("btype3", make_png(8, 4, 8, 0, noise(8, 4, 1, 255),
+                                   zlib_stream=bytes([0x78, 0x01, 0x07]) + bytes(40))[0]))
+    stored = zlib.compress(raw, 0)
+    bad_len = bytearray(stored)
+    bad_len[5] ^= 0xFF                          # NLEN no longer the complement
+    err.append(("stored_len", make_png(8, 4, 8, 0, noise(8, 4, 1, 255),
+                                       zlib_stream=bytes(bad_len))[0]))
+    # fixed block whose first code is a length/distance pair (distance 1
+    # with empty output): literal/length 257 = 7-bit code 0000001
+    err.append(("backref", make_png(8, 4, 8, 0, noise(8, 4, 1, 255),
+                                    zlib_stream=bytes([0x78, 0x01, 0x03, 0x02, 0x00, 0x00]))[0]))
+    err.append(("not_png_magic", b"P4\n8 4\n" + bytes(4)))
+    return ok, err
+
+
+def images(ref_dir):
+    """read_png / read_pnm / read_image of the reference on every case."""
+    import shutil
+    import tempfile
+    SN = load_reference(ref_dir)
+    ok, err = image_cases()
+    tmp = tempfile.mkdtemp(dir=HERE)
+    out = {}
+    errors = {}
+    try:
+        for name, data in ok:
+            path = os.path.join(tmp, name)
+            with open(path, "wb") as f:
+                f.write(data)
+            g, c, W, H = SN["read_image"](path)
+            out[name + "_file"] = np.frombuffer(data, dtype=np.uint8)
+            out[name + "_wh"] = np.array([W, H])
+            if W * H > 2000:                    # large: digests of the FP64 bytes
+                out[name + "_gray_sha"] = np.array(sha(g))
+                out[name + "_rgb_sha"] = np.array(sha(c))
+            else:
+                out[name + "_gray"] = np.asarray(g, dtype=np.float64)
+                out[name + "_rgb"] = np.asarray(c, dtype=np.float64)
+        for name, data in err:
+            path = os.path.join(tmp, name)
+            with open(path, "wb") as f:
+                f.write(data)
+            try:
+                SN["read_image"](path)
+                kind = "none"
+            except Exception as e:          # the reference's own exception type
+                kind = type(e).__name__
+            out["err_" + name + "_file"] = np.frombuffer(data, dtype=np.uint8)
+            errors[name] = kind
+    finally:
+        shutil.rmtree(tmp)
+    out["err_kinds"] = np.array(json.dumps(errors, sort_keys=True))
+    np.savez_compressed(os.path.join(HERE, "images.npz"), **out)
+    print("image fixtures written:", len(ok), "decoded,", errors)
+
+
 HOT_PATH = ["census", "band_costs", "_aggregate_path", "refine_fullres", "left_to_right",
             "lr_refine", "resize_gray", "avgpool2", "predict", "predict_at_scale",
             "predict_auto", "refine_disparity", "median_filter", "slic", "plane_snap",
-            "predict_consistent", "lr_consistency", "fill_invalid"]
+            "predict_consistent", "lr_consistency", "fill_invalid", "read_png", "read_pnm",
+            "read_image"]
 
 
 def signatures(ref_dir):
@@ -306,7 +448,10 @@ if __name__ == "__main__":
     ref = args[0] if args else "/root/reference"
     if "--postproc-only" in sys.argv:
         postproc(ref)
+    elif "--images-only" in sys.argv:
+        images(ref)
     elif "--signatures-only" not in sys.argv:
         main(ref)
         postproc(ref)
+        images(ref)
     signatures(ref)

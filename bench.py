@@ -614,17 +614,27 @@ def run_image(args, rank, world, local):
     vp = lambda t: ctypes.c_void_p(t.data_ptr())                         # noqa: E731
     host_ms = []
 
+    nv = len(views)
+    c_data = (ctypes.c_char_p * nv)(*views)
+    c_sizes = (ctypes.c_size_t * nv)(*[len(v) for v in views])
+    c_raw = (ctypes.c_void_p * nv)(*[r.data_ptr() for r in raw_h])
+    c_rb = (ctypes.c_size_t * nv)(*nraw)
+    c_desc = (pkg._lib.RawImage * nv)(*descs)
+
     def step(timed_host=False):
-        for k, v in enumerate(views):
+        # the views decode concurrently on two host threads (the library's
+        # batch call), then copy and convert on the stream
+        for k in range(nv):
             done[k].synchronize()              # the previous copy out of raw_h[k] is over
-            t0 = time.perf_counter()
-            pkg._lib.check(lib.sv_image_decode_raw(v, len(v), vp(raw_h[k]), nraw[k],
-                                                   ctypes.byref(descs[k])), "decode")
-            if timed_host:
-                host_ms.append((time.perf_counter() - t0) * 1e3)
+        t0 = time.perf_counter()
+        pkg._lib.check(lib.sv_image_decode_batch(nv, c_data, c_sizes, c_raw, c_rb, c_desc, None,
+                                                 nv), "decode")
+        if timed_host:
+            host_ms.append((time.perf_counter() - t0) * 1e3)
+        for k in range(nv):
             raw_d[k].copy_(raw_h[k], non_blocking=True)
             done[k].record()
-            pkg._lib.check(lib.sv_raw_to_float(vp(raw_d[k]), ctypes.byref(descs[k]), vp(gray[k]),
+            pkg._lib.check(lib.sv_raw_to_float(vp(raw_d[k]), ctypes.byref(c_desc[k]), vp(gray[k]),
                                                vp(rgbd[k]), s.cuda_stream), "raw_to_float")
 
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -655,21 +665,30 @@ def run_image(args, rank, world, local):
         k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         k0.record()
         for _ in range(args.steps):
-            lib.sv_raw_to_float(vp(raw_d[0]), ctypes.byref(descs[0]), vp(gray[0]), vp(rgbd[0]),
+            lib.sv_raw_to_float(vp(raw_d[0]), ctypes.byref(c_desc[0]), vp(gray[0]), vp(rgbd[0]),
                                 s.cuda_stream)
         k1.record()
         torch.cuda.synchronize()
     kms = k0.elapsed_time(k1) / args.steps
-    # end to end through the public API: bytes in host memory -> numpy FP64
-    # gray and rgb back on the host (the reference's return values)
+    # end to end through the public API: both files -> numpy FP64 gray and
+    # rgb back on the host (the reference's return values)
+    tmpd = tempfile.mkdtemp()
+    paths = []
+    for k, v in enumerate(views):
+        paths.append(os.path.join(tmpd, "view%d.png" % k))
+        with open(paths[-1], "wb") as f:
+            f.write(v)
     x0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     x1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for _ in range(2):
+        image.read_images(paths, out="numpy")
     for i in range(args.steps):
         x0[i].record()
-        for v in views:
-            image.decode_image(v, out="numpy")
+        image.read_images(paths, out="numpy")
         x1[i].record()
     torch.cuda.synchronize()
+    import shutil
+    shutil.rmtree(tmpd, ignore_errors=True)
     ems = sum(x0[i].elapsed_time(x1[i]) for i in range(args.steps))
     ems = pkg.shard.max_over_ranks(ems, device="cuda")
     evalue = world * 2 * N * args.steps / (ems / 1e3) / 1e6
@@ -699,7 +718,7 @@ def run_image(args, rank, world, local):
                                    "bytes)" % (len(views[0]), len(views[1])),
                        "l2": "flushed before every step (256 MB write, untimed)",
                        "parallelism": "replicas x%d" % world},
-            "stages_ms": {"host_decode_per_view": round(statistics.median(host_ms), 4),
+            "stages_ms": {"host_decode_both_views_2_threads": round(statistics.median(host_ms), 4),
                           "raw_to_float_kernel_per_view": round(kms, 4)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
@@ -712,7 +731,8 @@ def run_image(args, rank, world, local):
                                        "inflate, Python row filters, numpy FP64), %.1f s"
                                        % (n, el)},
             "e2e": {"value": round(evalue, 3), "unit": "Mpix/s",
-                    "h2d_bytes_per_step": sum(nraw), "d2h_bytes_per_step": 2 * 32 * N},
+                    "h2d_bytes_per_step": sum(nraw), "d2h_bytes_per_step": 2 * 32 * N,
+                    "api": "read_images([left.png, right.png], out='numpy')"},
             "gpu_launches": int(launches), "clocks": clk.summary()}
 
 

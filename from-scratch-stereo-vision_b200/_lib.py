@@ -77,6 +77,9 @@ SIGNATURES = {
     "sv_fill_invalid": (_I, [_VP, _VP, _I, _I, _VP, _VP, _SZ, _VP]),
     "sv_image_info": (_I, [ctypes.c_char_p, _SZ, ctypes.POINTER(RawImage)]),
     "sv_image_decode_raw": (_I, [ctypes.c_char_p, _SZ, _VP, _SZ, ctypes.POINTER(RawImage)]),
+    "sv_image_decode_batch": (_I, [_I, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_SZ),
+                                   ctypes.POINTER(_VP), ctypes.POINTER(_SZ),
+                                   ctypes.POINTER(RawImage), _IP, _I]),
     "sv_raw_to_float": (_I, [_VP, ctypes.POINTER(RawImage), _VP, _VP, _VP]),
     "sv_median_workspace_size": (_SZ, [_I, _I]),
     "sv_median_filter": (_I, [_VP, _I, _I, _I, _I, _VP, _VP, _SZ, _VP]),

@@ -15,7 +15,11 @@
 // does and, like it, ignores the Adler-32 trailer and the chunk CRCs.
 
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "sv_common.cuh"
@@ -162,28 +166,92 @@ struct Out {
     }
 };
 
+// The symbols of one Huffman block.  The bit buffer and the output cursor
+// live in locals for the loop (stores of output bytes may alias anything
+// reachable through a pointer); the slow bit-at-a-time decode and buffer
+// growth write them back first.
 bool codes(BitIn &b, const Code &lit, const Code &dist, Out &out) {
+    uint64_t buf = b.buf;
+    int cnt = b.cnt;
+    size_t pos = b.pos, size = out.size;
+    const uint8_t *const p = b.p;
+    const size_t n = b.n;
+    uint8_t *o = out.v.data();
+    size_t cap = out.v.size();
+    bool ok = false;
+    auto refill = [&]() {
+        if (pos + 8 <= n) {                 // whole-word refill; bytes past cnt are
+            uint64_t w;                     // re-read at the same bit position later
+            memcpy(&w, p + pos, 8);
+            buf |= w << cnt;
+            pos += (size_t)((63 - cnt) >> 3);
+            cnt |= 56;
+        } else {
+            while (cnt <= 56 && pos < n) {
+                buf |= (uint64_t)p[pos++] << cnt;
+                cnt += 8;
+            }
+        }
+    };
+    auto sync_out = [&]() { b.buf = buf; b.cnt = cnt; b.pos = pos; };
+    auto sync_in = [&]() { buf = b.buf; cnt = b.cnt; pos = b.pos; };
+    auto sym = [&](const Code &c) -> int {
+        if (cnt < 15) refill();
+        const int e = c.fast[buf & ((1u << kFast) - 1)];
+        if (e && (e >> 9) <= cnt) {
+            buf >>= e >> 9;
+            cnt -= e >> 9;
+            return e & 511;
+        }
+        sync_out();
+        const int s = decode(b, c);
+        sync_in();
+        return s;
+    };
+    auto bits = [&](int k) -> uint32_t {      // k <= 13 after a refill to >= 15
+        if (cnt < k) {
+            refill();
+            if (cnt < k) { cnt = -1; return 0; }
+        }
+        const uint32_t v = (uint32_t)(buf & ((1u << k) - 1));
+        buf >>= k;
+        cnt -= k;
+        return v;
+    };
     for (;;) {
-        const int s = decode(b, lit);
-        if (s < 0) return false;
+        const int s = sym(lit);
+        if (s < 0) break;
+        if (size + 258 > cap) {                 // room for the longest match, or
+            out.size = size;                    // as much as the limit leaves
+            const size_t want = std::min(out.limit, size + 258) - size;
+            if (want == 0 || !out.room(want)) break;
+            o = out.v.data();
+            cap = out.v.size();
+        }
         if (s < 256) {
-            if (!out.room(1)) return false;
-            out.v[out.size++] = (uint8_t)s;
+            if (size >= cap) break;
+            o[size++] = (uint8_t)s;
         } else if (s == 256) {
-            return true;
+            ok = true;
+            break;
         } else {
             const int li = s - 257;
-            if (li >= 29) return false;
-            const int len = kLenBase[li] + (int)b.get(kLenExtra[li]);
-            const int ds = decode(b, dist);
-            if (ds < 0 || ds >= 30) return false;
-            const size_t d = (size_t)kDistBase[ds] + b.get(kDistExtra[ds]);
-            if (b.fail || d > out.size || !out.room((size_t)len)) return false;
-            uint8_t *o = out.v.data() + out.size;
-            for (int k = 0; k < len; ++k) o[k] = o[(ptrdiff_t)k - (ptrdiff_t)d];  // may overlap
-            out.size += (size_t)len;
+            if (li >= 29) break;
+            const int len = kLenBase[li] + (int)bits(kLenExtra[li]);
+            if (cnt < 0) break;
+            const int ds = sym(dist);
+            if (ds < 0 || ds >= 30) break;
+            const size_t d = (size_t)kDistBase[ds] + bits(kDistExtra[ds]);
+            if (cnt < 0 || d > size || size + (size_t)len > cap) break;
+            uint8_t *q = o + size;
+            for (int k = 0; k < len; ++k) q[k] = q[(ptrdiff_t)k - (ptrdiff_t)d];  // may overlap
+            size += (size_t)len;
         }
     }
+    if (cnt < 0) return false;
+    sync_out();
+    out.size = size;
+    return ok;
 }
 
 bool inflate_raw(const uint8_t *p, size_t n, Out &out) {
@@ -197,6 +265,7 @@ bool inflate_raw(const uint8_t *p, size_t n, Out &out) {
             if (b.fail || (len ^ 0xffffu) != nlen || !out.room(len)) return false;
             uint32_t k = 0;
             for (; k < len && b.cnt >= 8; ++k) out.v[out.size++] = (uint8_t)b.get(8);
+            b.buf &= b.cnt ? ((1ull << b.cnt) - 1) : 0;   // drop read-ahead bytes
             const uint32_t rest = len - k;
             if (b.pos + rest > b.n) return false;
             memcpy(out.v.data() + out.size, b.p + b.pos, rest);
@@ -247,11 +316,75 @@ bool inflate_raw(const uint8_t *p, size_t n, Out &out) {
     }
 }
 
-int paeth(int a, int b, int c) {
-    const int p = a + b - c;
-    const int pa = p > a ? p - a : a - p, pb = p > b ? p - b : b - p, pc = p > c ? p - c : c - p;
-    if (pa <= pb && pa <= pc) return a;
-    return pb <= pc ? b : c;
+// PNG's Paeth predictor (stereonet.py:3436-3453), written with the
+// distances |b - c|, |a - c| and |a + b - 2c| so it compiles to selects.
+inline int paeth(int a, int b, int c) {
+    const int pa = abs(b - c), pb = abs(a - c), pc = abs(a + b - 2 * c);
+    const int bc = pb <= pc ? b : c;
+    return ((pa <= pb) & (pa <= pc)) ? a : bc;      // no branch on pixel data
+}
+
+// The sequential filters (Sub, Average, Paeth) for BPP bytes per pixel:
+// the left pixel (a) and the upper-left one (c) ride in registers, so the
+// dependency along the row does not go through memory.  i < BPP is done by
+// the caller.
+template <int BPP>
+void unfilter_seq(int ft, const uint8_t *__restrict__ row, const uint8_t *__restrict__ up,
+                  uint8_t *__restrict__ o, int stride) {
+    int a[BPP], c[BPP];
+    for (int k = 0; k < BPP; ++k) {
+        a[k] = o[k];
+        c[k] = up ? up[k] : 0;
+    }
+    int i = BPP;
+    for (; i + BPP <= stride; i += BPP) {
+        for (int k = 0; k < BPP; ++k) {
+            const int b = up ? up[i + k] : 0;
+            int v;
+            if (ft == 1) v = row[i + k] + a[k];
+            else if (ft == 3) v = row[i + k] + ((a[k] + b) >> 1);
+            else v = row[i + k] + paeth(a[k], b, c[k]);
+            a[k] = v & 0xFF;
+            c[k] = b;
+            o[i + k] = (uint8_t)v;
+        }
+    }
+    for (int k = 0; i + k < stride; ++k) {      // a partial pixel (sub-byte rows)
+        const int b = up ? up[i + k] : 0;
+        const int v = ft == 1 ? row[i + k] + a[k]
+                    : ft == 3 ? row[i + k] + ((a[k] + b) >> 1)
+                              : row[i + k] + paeth(a[k], b, c[k]);
+        o[i + k] = (uint8_t)v;
+    }
+}
+
+// One row of _unfilter (stereonet.py:3456-3496); `up` is NULL on row 0,
+// where the row above reads as zeros.  The filter type selects the loop.
+void unfilter_row(int ft, const uint8_t *__restrict__ row, const uint8_t *__restrict__ up,
+                  uint8_t *__restrict__ o, int stride, int bpp) {
+    const int head = bpp < stride ? bpp : stride;
+    if (ft == 0 || (ft == 2 && !up)) {
+        memcpy(o, row, (size_t)stride);
+        return;
+    }
+    if (ft == 2) {
+        for (int i = 0; i < stride; ++i) o[i] = (uint8_t)(row[i] + up[i]);
+        return;
+    }
+    // first pixel: a = c = 0, so Sub gives row, Average row + b/2, Paeth row + b
+    for (int i = 0; i < head; ++i) {
+        const int b = up ? up[i] : 0;
+        o[i] = (uint8_t)(row[i] + (ft == 1 ? 0 : ft == 3 ? (b >> 1) : b));
+    }
+    if (ft == 4 && !up) ft = 1;                     // paeth(a, 0, 0) = a
+    switch (bpp) {
+    case 1: unfilter_seq<1>(ft, row, up, o, stride); break;
+    case 2: unfilter_seq<2>(ft, row, up, o, stride); break;
+    case 3: unfilter_seq<3>(ft, row, up, o, stride); break;
+    case 4: unfilter_seq<4>(ft, row, up, o, stride); break;
+    case 6: unfilter_seq<6>(ft, row, up, o, stride); break;
+    default: unfilter_seq<8>(ft, row, up, o, stride); break;
+    }
 }
 
 uint32_t be32(const uint8_t *p) {
@@ -505,24 +638,12 @@ int sv_image_decode_raw(const uint8_t *data, size_t n, uint8_t *raw, size_t raw_
     const uint8_t *src = z.v.data();
     for (int y = 0; y < H; ++y) {
         const int ft = src[0];
-        const uint8_t *row = src + 1;
-        uint8_t *o = raw + (size_t)y * stride;
-        const uint8_t *up = y > 0 ? raw + (size_t)(y - 1) * stride : nullptr;
-        for (int i = 0; i < stride; ++i) {
-            const int a = i >= bpp ? o[i - bpp] : 0;
-            const int b = up ? up[i] : 0;
-            const int c = (up && i >= bpp) ? up[i - bpp] : 0;
-            int v;
-            switch (ft) {
-            case 0: v = row[i]; break;
-            case 1: v = row[i] + a; break;
-            case 2: v = row[i] + b; break;
-            case 3: v = row[i] + ((a + b) >> 1); break;
-            case 4: v = row[i] + paeth(a, b, c); break;
-            default: set_error("unknown PNG filter type %d on row %d", ft, y); return SV_ERR_PARAM;
-            }
-            o[i] = (uint8_t)(v & 0xFF);
+        if (ft > 4) {
+            set_error("unknown PNG filter type %d on row %d", ft, y);
+            return SV_ERR_PARAM;
         }
+        unfilter_row(ft, src + 1, y > 0 ? raw + (size_t)(y - 1) * stride : nullptr,
+                     raw + (size_t)y * stride, stride, bpp);
         src += stride + 1;
     }
     if (desc->colortype == 3) {               // palette[3 p + 2] must exist
@@ -539,6 +660,39 @@ int sv_image_decode_raw(const uint8_t *data, size_t n, uint8_t *raw, size_t raw_
             }
     }
     return SV_OK;
+}
+
+int sv_image_decode_batch(int n, const uint8_t *const *data, const size_t *sizes,
+                          uint8_t *const *raw, const size_t *raw_bytes, sv_raw_image *descs,
+                          int *status, int threads) {
+    if (n < 0 || (n > 0 && (!data || !sizes || !raw || !raw_bytes || !descs))) {
+        set_error("NULL argument");
+        return SV_ERR_NULL;
+    }
+    if (n == 0) return SV_OK;
+    const int nt = std::max(1, std::min(threads > 0 ? threads : 1, n));
+    std::vector<int> st((size_t)n, SV_OK);
+    std::vector<std::string> msg((size_t)n);
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (int i; (i = next.fetch_add(1)) < n;) {
+            st[i] = sv_image_decode_raw(data[i], sizes[i], raw[i], raw_bytes[i], &descs[i]);
+            if (st[i] != SV_OK) msg[i] = sv_last_error();   // this thread's message
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    int rc = SV_OK;
+    for (int i = 0; i < n; ++i) {
+        if (status) status[i] = st[i];
+        if (st[i] != SV_OK && rc == SV_OK) {
+            rc = st[i];
+            set_error("file %d: %s", i, msg[i].c_str());
+        }
+    }
+    return rc;
 }
 
 int sv_raw_to_float(const uint8_t *raw, const sv_raw_image *desc, double *gray, double *rgb,

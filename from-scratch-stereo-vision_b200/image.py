@@ -14,6 +14,7 @@ leaving the device).  Files the reference rejects raise ValueError.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -85,6 +86,56 @@ def read_image(path, out: str = "list"):
     if data[:2] not in (b"P2", b"P3", b"P5", b"P6"):
         raise ValueError("not a PGM/PPM file: " + str(path))
     return _decode(data, out, "read_pnm")
+
+
+def _decode_many(blobs, out, threads, what):
+    """Host decode of every file on `threads` threads, then one H2D copy and
+    one conversion launch per file on the current stream."""
+    lib = _lib.load()
+    n = len(blobs)
+    descs = (_lib.RawImage * n)()
+    for i, b in enumerate(blobs):
+        _lib.check(lib.sv_image_info(b, len(b), ctypes.byref(descs[i])), "%s[%d]" % (what, i))
+    sizes = [d.stride * d.height for d in descs]
+    raws = [torch.empty(max(sz, 1), dtype=torch.uint8, pin_memory=True) for sz in sizes]
+    c_data = (ctypes.c_char_p * n)(*blobs)
+    c_sizes = (ctypes.c_size_t * n)(*[len(b) for b in blobs])
+    c_raw = (ctypes.c_void_p * n)(*[r.data_ptr() for r in raws])
+    c_rb = (ctypes.c_size_t * n)(*sizes)
+    st = (ctypes.c_int * n)()
+    _lib.check(lib.sv_image_decode_batch(n, c_data, c_sizes, c_raw, c_rb, descs, st,
+                                         int(threads)), what)
+    dev = _device()
+    res = []
+    for i in range(n):
+        W, H = descs[i].width, descs[i].height
+        raw_d = raws[i].to(dev, non_blocking=True)
+        gray = torch.empty(W * H, dtype=torch.float64, device=dev)
+        rgb = torch.empty(3 * W * H, dtype=torch.float64, device=dev)
+        _lib.check(lib.sv_raw_to_float(_ptr(raw_d), ctypes.byref(descs[i]), _ptr(gray), _ptr(rgb),
+                                       ctypes.c_void_p(_stream())), what)
+        res.append((gray, rgb, W, H))
+    torch.cuda.current_stream().synchronize()
+    if out == "cuda":
+        return res
+    conv = (lambda t: t.cpu().numpy()) if out == "numpy" else (lambda t: t.cpu().numpy().tolist())
+    return [(conv(g), conv(c), W, H) for g, c, W, H in res]
+
+
+def read_images(paths, out: str = "list", threads: int = 0):
+    """read_image of several files (e.g. the two views of a pair, or a test
+    split), decoded concurrently on host threads (default: one per file, up
+    to the CPU count).  Returns a list of (gray, rgb, width, height)."""
+    if out not in ("list", "numpy", "cuda"):
+        raise ValueError("out must be 'list', 'numpy' or 'cuda'")
+    blobs = [_read(p) for p in paths]
+    for p, b in zip(paths, blobs):
+        if b[:8] != PNG_SIGNATURE and b[:2] not in (b"P2", b"P3", b"P5", b"P6"):
+            raise ValueError("not a PGM/PPM file: " + str(p))
+    if not blobs:
+        return []
+    threads = threads or min(len(blobs), os.cpu_count() or 1)
+    return _decode_many(blobs, out, threads, "read_images")
 
 
 def decode_raw(data: bytes):

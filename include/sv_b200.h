@@ -376,6 +376,13 @@ int sv_image_info(const uint8_t *data, size_t n, sv_raw_image *desc);
  * stride * height bytes), rejecting what the reference rejects */
 int sv_image_decode_raw(const uint8_t *data, size_t n, uint8_t *raw,
                         size_t raw_bytes, sv_raw_image *desc);
+/* sv_image_decode_raw of n files on up to `threads` host threads (decoding
+ * is serial within a file; the files are independent).  status[i] (may be
+ * NULL) receives each file's code; the first failure is returned and its
+ * message is kept for sv_last_error. */
+int sv_image_decode_batch(int n, const uint8_t *const *data, const size_t *sizes,
+                          uint8_t *const *raw, const size_t *raw_bytes,
+                          sv_raw_image *descs, int *status, int threads);
 /* device raw samples -> gray [H][W] and rgb [H][W][3] (FP64 device buffers;
  * either may be NULL) */
 int sv_raw_to_float(const uint8_t *raw, const sv_raw_image *desc, double *gray,

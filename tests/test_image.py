@@ -128,3 +128,34 @@ def test_host_decoder_large_stored_and_dynamic(svb):
         want = io_orc.unfilter(filtered, H, 3, 3 * W)
         assert np.array_equal(raw, want)
         assert np.array_equal(raw, np.array(samples, dtype=np.uint8))
+
+
+def test_batch_decode_threads(svb):
+    """sv_image_decode_batch on 4 threads gives each file's samples exactly
+    as the single-file call does, and reports the failing file."""
+    import ctypes
+    from importlib import import_module
+    image = import_module(svb.__name__ + ".image")
+    lib = svb._lib.load()
+    names = CASES + CASES
+    blobs = [G[nm + "_file"].tobytes() for nm in names]
+    blobs[5] = G["err_filter5_file"].tobytes()
+    n = len(blobs)
+    descs = (svb._lib.RawImage * n)()
+    sizes = []
+    for i, b in enumerate(blobs):
+        assert lib.sv_image_info(b, len(b), ctypes.byref(descs[i])) == 0
+        sizes.append(descs[i].stride * descs[i].height)
+    raws = [np.zeros(max(s, 1), dtype=np.uint8) for s in sizes]
+    st = (ctypes.c_int * n)()
+    rc = lib.sv_image_decode_batch(
+        n, (ctypes.c_char_p * n)(*blobs), (ctypes.c_size_t * n)(*[len(b) for b in blobs]),
+        (ctypes.c_void_p * n)(*[r.ctypes.data for r in raws]), (ctypes.c_size_t * n)(*sizes),
+        descs, st, 4)
+    assert rc == svb._lib.SV_ERR_PARAM and list(st).count(0) == n - 1 and st[5] != 0
+    assert lib.sv_last_error().decode().startswith("file 5: unknown PNG filter type 5")
+    for i, b in enumerate(blobs):
+        if i == 5:
+            continue
+        want, _ = image.decode_raw(b)
+        assert np.array_equal(raws[i][:sizes[i]].reshape(want.shape), want)

@@ -79,3 +79,17 @@ def test_feeds_the_device_path(svb, image, tmp_path):
     b = refine.refine_fullres(ll, rl, d0.tolist(), W, H)
     assert a.is_cuda and isinstance(b, list)
     assert np.array_equal(bits(a.cpu().numpy()), bits(b))
+
+
+def test_read_images_batch(image, tmp_path):
+    paths = []
+    for nm in CASES:
+        p = tmp_path / nm
+        p.write_bytes(G[nm + "_file"].tobytes())
+        paths.append(str(p))
+    for out in ("list", "numpy", "cuda"):
+        res = image.read_images(paths, out=out, threads=3)
+        for nm, (g, c, W, H) in zip(CASES, res):
+            if out == "cuda":
+                g, c = g.cpu().numpy(), c.cpu().numpy()
+            check_against_golden(nm, g, c, W, H)

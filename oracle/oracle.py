@@ -39,7 +39,7 @@ def lib():
     if _lib is None:
         if not os.path.exists(_SO) or os.path.getmtime(_SO) < max(
                 os.path.getmtime(os.path.join(_HERE, f))
-                for f in ("sv_oracle.c", "sv_band_oracle.c")):
+                for f in ("sv_oracle.c", "sv_band_oracle.c", "sv_train_oracle.c")):
             build()
         L = ctypes.CDLL(_SO)
         L.orc_fexp.restype = _dbl
@@ -49,6 +49,10 @@ def lib():
         L.orc_param_count.restype = ctypes.c_long
         L.orc_band_param_count.restype = ctypes.c_long
         L.orc_band_loss.restype = _dbl
+        L.orc_fsqrt.restype = _dbl
+        L.orc_fsqrt.argtypes = [_dbl]
+        L.orc_flog.restype = _dbl
+        L.orc_flog.argtypes = [_dbl]
         _lib = L
     return _lib
 
@@ -406,3 +410,43 @@ def predict_consistent(net, left, right, W, H, work_width=None, tol=1.5, target_
                                         probe_width, max_width, passes, _dbl(tol), _p(out),
                                         ctypes.byref(kept)), "predict_consistent")
     return out, kept.value / float(W * H)
+
+
+# ------------------------------------------------------------------ training
+def train_grads(net, left, right, disp, valid, W, H, params=None):
+    """train_grads (stereonet.py:1619-1653) on one sample: returns (loss,
+    gradient in all_params() order, full-resolution prediction).  `params`
+    (flat, all_params() order) overrides the network's own."""
+    arch, p0 = _net_args(net)
+    params = _f64(p0 if params is None else params)
+    n = int(lib().orc_param_count(_p(arch, _i32)))
+    g = np.zeros(n)
+    d2 = np.zeros(W * H)
+    loss = ctypes.c_double()
+    l_, r_, d_ = _f64(left), _f64(right), _f64(disp)
+    v_ = np.ascontiguousarray(np.asarray(valid).ravel().astype(np.uint8))
+    _check(lib().orc_train_grads(_p(arch, _i32), _p(params), _p(l_), _p(r_), _p(d_),
+                                 v_.ctypes.data_as(ctypes.c_void_p), W, H, _p(g),
+                                 ctypes.byref(loss), _p(d2)), "train_grads")
+    return loss.value, g, d2
+
+
+class AdamState:
+    """Adam (stereonet.py:1354-1387) over a flat parameter vector, with the
+    reference's own fsqrt (bit-identical steps)."""
+
+    def __init__(self, params, lr=1.0e-3):
+        self.p = _f64(params).copy()
+        self.m = np.zeros_like(self.p)
+        self.v = np.zeros_like(self.p)
+        self.lr = lr
+        self.b1t = ctypes.c_double(1.0)
+        self.b2t = ctypes.c_double(1.0)
+
+    def step(self, grads, clip=5.0):
+        g = _f64(grads)
+        lib().orc_train_adam_step(_p(self.p), _p(g), _p(self.m), _p(self.v),
+                                  ctypes.c_long(self.p.size), ctypes.c_double(self.lr),
+                                  ctypes.byref(self.b1t), ctypes.byref(self.b2t),
+                                  ctypes.c_double(clip))
+        return self.p

@@ -424,6 +424,37 @@ def images(ref_dir):
     print("image fixtures written:", len(ok), "decoded,", errors)
 
 
+# ---------------------------------------------------------------- training
+def training(ref_dir):
+    """train_grads (stereonet.py:1619-1653) and two Adam steps of the
+    reference on seeded 48x32 crops with its own checkpoint."""
+    t0 = time.time()
+    SN = load_reference(ref_dir)
+    net = SN["load_model"](os.path.join(ref_dir, "stereonet_weights.txt"))
+    out = {"params0": np.array(SN["flat_params"](net))}
+    opt = SN["Adam"](net.all_params(), lr=1.0e-3)
+    for k, (seed, dmax) in enumerate(((61, 20.0), (62, 34.0))):
+        pair = synth.make_pair(seed, 48, 32, 2.0, dmax, n_planes=(2, 3))
+        W, H = pair.W, pair.H
+        sample = {"left": list(pair.gray("left").ravel()),
+                  "right": list(pair.gray("right").ravel()),
+                  "disp": [float(v) for v in pair.disp.ravel()],
+                  "valid": [bool(v) for v in pair.valid.ravel()], "W": W, "H": H}
+        total, pred, tgt = SN["train_grads"](net, sample)
+        out["s%d_left" % k] = pair.left
+        out["s%d_right" % k] = pair.right
+        out["s%d_disp" % k] = pair.disp
+        out["s%d_valid" % k] = pair.valid
+        out["s%d_loss" % k] = np.array([total])
+        out["s%d_grads" % k] = np.array(SN["flat_grads"](net))
+        out["s%d_d2" % k] = np.array(pred)
+        opt.step()
+        out["s%d_params_after" % k] = np.array(SN["flat_params"](net))
+        print("training sample %d: loss %.6f (%.1fs)" % (k, total, time.time() - t0))
+    np.savez_compressed(os.path.join(HERE, "training.npz"), **out)
+    print("training fixtures written")
+
+
 HOT_PATH = ["census", "band_costs", "_aggregate_path", "refine_fullres", "left_to_right",
             "lr_refine", "resize_gray", "avgpool2", "predict", "predict_at_scale",
             "predict_auto", "refine_disparity", "median_filter", "slic", "plane_snap",
@@ -450,8 +481,11 @@ if __name__ == "__main__":
         postproc(ref)
     elif "--images-only" in sys.argv:
         images(ref)
+    elif "--training-only" in sys.argv:
+        training(ref)
     elif "--signatures-only" not in sys.argv:
         main(ref)
         postproc(ref)
         images(ref)
+        training(ref)
     signatures(ref)

@@ -52,8 +52,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="full",
-                    choices=["full", "small", "batched", "refine_disparity", "read_image"])
+                    choices=["full", "small", "batched", "refine_disparity", "read_image",
+                             "train"])
     ap.add_argument("--pairs", type=int, default=256, help="pairs of the batched workload")
+    ap.add_argument("--batch", type=int, default=64, help="crops per step of the train workload")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound on the CPU-baseline sample")
     return ap.parse_args()
@@ -736,6 +738,108 @@ def run_image(args, rank, world, local):
             "gpu_launches": int(launches), "clocks": clk.summary()}
 
 
+def run_train(args, rank, world, local):
+    """The training workload: a step is train_grads over a batch of 96x64
+    crops (the crop size of the reference's harness, train_parallel.py:33)
+    with the batch mean of the per-sample gradients, then Adam.step -- what
+    the harness does with one CPU process per sample (train_parallel.py
+    144-156)."""
+    import numpy as np
+    import torch
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from importlib import import_module
+    train = import_module(pkg.__name__ + ".train")
+    lib = pkg._lib.load()
+    net = pkg.weights.load_model()
+    B, W, H = args.batch, 96, 64
+    crops = [pkg.synth.make_pair(9000 + 1000 * rank + k, W, H, 2.0, 36.0, n_planes=(2, 4),
+                                 lowtex_frac=0.3, bars=1) for k in range(B)]
+    hl = torch.from_numpy(np.stack([c.gray("left") for c in crops]).astype(np.float32)).pin_memory()
+    hr = torch.from_numpy(np.stack([c.gray("right") for c in crops]).astype(np.float32)).pin_memory()
+    hd = torch.from_numpy(np.stack([c.disp for c in crops]).astype(np.float32)).pin_memory()
+    hv = torch.from_numpy(np.stack([c.valid for c in crops]).astype(np.uint8)).pin_memory()
+    dl, dr, dd, dv = (t.cuda() for t in (hl, hr, hd, hv))
+    t = train.Trainer(net, lr=1.0e-4)
+    s = torch.cuda.Stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    with torch.cuda.stream(s):
+        for _ in range(args.warmup):
+            t.step(dl, dr, dd, dv)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = lib.sv_launch_count()
+    with ClockSampler(local) as clk, torch.cuda.stream(s):
+        for i in range(args.steps):
+            flush.zero_()
+            e0[i].record()
+            t.step(dl, dr, dd, dv)
+            e1[i].record()
+        torch.cuda.synchronize()
+    launches = lib.sv_launch_count() - launches0
+    ms = sum(e0[i].elapsed_time(e1[i]) for i in range(args.steps))
+    ms = pkg.shard.max_over_ranks(ms, device="cuda")
+    value = world * B * args.steps / (ms / 1e3)
+    # end to end: the batch from pinned host memory, the losses back
+    x0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    x1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    hloss = torch.empty(B, dtype=torch.float64).pin_memory()
+    with torch.cuda.stream(s):
+        for i in range(args.steps):
+            flush.zero_()
+            x0[i].record()
+            for dst, src in ((dl, hl), (dr, hr), (dd, hd), (dv, hv)):
+                dst.copy_(src, non_blocking=True)
+            loss = t.step(dl, dr, dd, dv)
+            hloss.copy_(loss, non_blocking=True)
+            x1[i].record()
+        torch.cuda.synchronize()
+    ems = sum(x0[i].elapsed_time(x1[i]) for i in range(args.steps))
+    ems = pkg.shard.max_over_ranks(ems, device="cuda")
+    evalue = world * B * args.steps / (ems / 1e3)
+    if rank != 0:
+        return None
+    import __graft_entry__ as ge
+    orc = ge.load_oracle()
+    t0 = time.time()
+    n = 0
+    while n < 1 or time.time() - t0 < min(args.cpu_seconds, 20.0):
+        c = crops[n % B]
+        orc.train_grads(net, c.gray("left"), c.gray("right"), c.disp, c.valid, W, H)
+        n += 1
+    el = time.time() - t0
+    return {"metric": "StereoNet training samples/s per B200 (train_grads + Adam, 96x64 crops)",
+            "value": round(value, 1), "unit": "samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 activations and gradients, f64 parameters and Adam",
+            "data": "synthetic (seeded 96x64 crops, disparities 2-36 px, a thin bar, 30% low "
+                    "texture)",
+            "config": {"workload": "batch of %d crops 96x64 per step, reference checkpoint "
+                                   "(12/6/12/8)" % B,
+                       "l2": "flushed before every step (256 MB write, untimed)",
+                       "parallelism": "replicas x%d" % world},
+            "cpu_baseline": {"value": round(n / el, 3), "unit": "samples/s", "cores": 1,
+                             "kind": "port",
+                             "sample": "%d crops through the FP64 C port of train_grads, %.1f s, "
+                                       "1 thread" % (n, el)},
+            "e2e": {"value": round(evalue, 1), "unit": "samples/s",
+                    "h2d_bytes_per_step": int(B * W * H * (4 * 3 + 1)),
+                    "d2h_bytes_per_step": 8 * B},
+            "gpu_launches": int(launches), "clocks": clk.summary()}
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -747,6 +851,8 @@ def main():
         res = run_refdisp(args, rank, world, local)
     elif args.workload == "read_image":
         res = run_image(args, rank, world, local)
+    elif args.workload == "train":
+        res = run_train(args, rank, world, local)
     else:
         res = run_ours(args, rank, world, local)
     if res is not None and rank == 0:

@@ -15,6 +15,8 @@ with ``importlib`` the same way.  Modules:
   lr_consistency / fill_invalid drop-ins; ``band`` -- the learned band;
 * ``image``   -- read_png / read_pnm / read_image drop-ins (host decode,
   GPU FP64 conversion);
+* ``train``   -- StereoNet training (train_grads / train_step drop-ins and a
+  device-resident batched ``Trainer``);
 * ``synth``   -- seeded synthetic stereo pairs; ``weights`` -- checkpoints.
 
 All compute goes through libsv_b200.so; there is no CPU fallback.
@@ -29,6 +31,6 @@ def __getattr__(name):
     # heavy modules (torch) load on first use
     import importlib
     if name in ("refine", "network", "pipeline", "shim", "shard", "batch", "band", "post",
-                "image"):
+                "image", "train"):
         return importlib.import_module("." + name, __name__)
     raise AttributeError(name)

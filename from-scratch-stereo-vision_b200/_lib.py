@@ -105,6 +105,17 @@ SIGNATURES = {
     "sv_band_train_step": (_I, [_VP, _VP, _VP, _VP, _I, _I, _I, _D, _VP, _VP, _SZ, _VP]),
     "sv_band_targets": (_I, [_VP, _VP, _VP, ctypes.c_long, _D, _VP, _VP, _VP]),
     "sv_band_apply": (_I, [_VP, _VP, _I, _I, _D, _D, _I, _I, _D, _VP, _VP, _VP]),
+    "sv_trainer_create": (_I, [_VP, _I, _VP, ctypes.c_long, ctypes.POINTER(_VP)]),
+    "sv_trainer_destroy": (None, [_VP]),
+    "sv_trainer_param_count": (ctypes.c_long, [_VP]),
+    "sv_trainer_get_params": (_I, [_VP, _VP, ctypes.c_long]),
+    "sv_trainer_get_grads": (_I, [_VP, _VP, ctypes.c_long]),
+    "sv_trainer_set_params": (_I, [_VP, _VP, ctypes.c_long]),
+    "sv_trainer_set_grads": (_I, [_VP, _VP, ctypes.c_long]),
+    "sv_train_workspace_size": (_SZ, [_VP, _I, _I, _I]),
+    "sv_train_grads": (_I, [_VP, _VP, _VP, _VP, _VP, _I, _I, _I, _VP, _VP, _VP, _SZ, _VP]),
+    "sv_train_adam": (_I, [_VP, _D, _D, _VP]),
+    "sv_trainer_reset_adam": (_I, [_VP]),
     "sv_net_create": (_I, [_VP, _I, _VP, ctypes.c_long, ctypes.POINTER(_VP)]),
     "sv_net_destroy": (None, [_VP]),
     "sv_resize": (_I, [_VP, _I, _I, _I, _I, _VP, _VP]),

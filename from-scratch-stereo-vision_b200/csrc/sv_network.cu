@@ -25,39 +25,6 @@
 namespace sv {
 
 // ---------------------------------------------------------------- resample
-struct Taps {
-    int i00, i01, i10, i11;
-    double w00, w01, w10, w11;
-};
-
-// BilinearUpsample.forward tap computation, stereonet.py:921-949.
-__device__ __forceinline__ Taps bilinear_taps(int oy, int ox, int H, int W, int H2,
-                                              int W2) {
-    double sy = __ddiv_rn((double)H, (double)H2);
-    double sx = __ddiv_rn((double)W, (double)W2);
-    double fy = __dsub_rn(__dmul_rn(__dadd_rn((double)oy, 0.5), sy), 0.5);
-    if (fy < 0.0) fy = 0.0;
-    int y0 = (int)fy;
-    if (y0 > H - 1) y0 = H - 1;
-    int y1 = y0 + 1 < H ? y0 + 1 : y0;
-    double wy = __dsub_rn(fy, (double)y0);
-    double fx = __dsub_rn(__dmul_rn(__dadd_rn((double)ox, 0.5), sx), 0.5);
-    if (fx < 0.0) fx = 0.0;
-    int x0 = (int)fx;
-    if (x0 > W - 1) x0 = W - 1;
-    int x1 = x0 + 1 < W ? x0 + 1 : x0;
-    double wx = __dsub_rn(fx, (double)x0);
-    Taps t;
-    t.w00 = __dmul_rn(__dsub_rn(1.0, wy), __dsub_rn(1.0, wx));
-    t.w01 = __dmul_rn(__dsub_rn(1.0, wy), wx);
-    t.w10 = __dmul_rn(wy, __dsub_rn(1.0, wx));
-    t.w11 = __dmul_rn(wy, wx);
-    t.i00 = y0 * W + x0;
-    t.i01 = y0 * W + x1;
-    t.i10 = y1 * W + x0;
-    t.i11 = y1 * W + x1;
-    return t;
-}
 
 template <typename T>
 __device__ __forceinline__ double gray_at(const T *img, int i);

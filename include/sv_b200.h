@@ -388,6 +388,44 @@ int sv_image_decode_batch(int n, const uint8_t *const *data, const size_t *sizes
 int sv_raw_to_float(const uint8_t *raw, const sv_raw_image *desc, double *gray,
                     double *rgb, void *stream);
 
+/* ------------------------------------------------------------------------
+ * StereoNet training: train_grads (stereonet.py:1619-1653, with
+ * build_targets 1572-1611, pseudo_huber 1326-1351, disparity_ce 1274-1323,
+ * StereoNet.backward 1235-1267) over a batch of B crops, and Adam.step
+ * (1368-1387).  The batch gradient is the mean of the per-sample gradients,
+ * as the reference's data-parallel harness forms it (train_parallel.py
+ * 144-156); B = 1 is train_grads itself.  FP32 activations and gradients,
+ * FP64 parameters, weight-gradient sums and Adam state; deterministic.
+ * Architectures: feat_C/cost_C/refine_C 12/6/8 or 8/4/8, D <= 16,
+ * dilations <= 8.  Crops: W, H multiples of 4 (the reference's targets
+ * line up with its outputs only then) and W/4 > D - 2.
+ * ---------------------------------------------------------------------- */
+typedef struct sv_trainer sv_trainer;
+/* arch as sv_net_create; params (host, FP64) in all_params() order */
+int sv_trainer_create(const int *arch, int n_arch, const double *params, long n_params,
+                      sv_trainer **out);
+void sv_trainer_destroy(sv_trainer *t);
+long sv_trainer_param_count(const sv_trainer *t);
+/* host copies of the parameters / the last gradient (synchronise) */
+int sv_trainer_get_params(const sv_trainer *t, double *out, long n);
+int sv_trainer_get_grads(const sv_trainer *t, double *out, long n);
+int sv_trainer_set_params(sv_trainer *t, const double *params, long n);
+int sv_trainer_set_grads(sv_trainer *t, const double *grads, long n);
+size_t sv_train_workspace_size(const sv_trainer *t, int B, int W, int H);
+/* left, right, disp: FP32 [B][H][W] (gray in [0, 1], ground-truth
+ * disparity); valid: [B][H][W] (nonzero = known).  Leaves the batch
+ * gradient in the trainer; loss (device FP64 [B], may be NULL) gets each
+ * sample's total loss, pred (device FP32 [B][H][W], may be NULL) the
+ * full-resolution prediction. */
+int sv_train_grads(sv_trainer *t, const float *left, const float *right, const float *disp,
+                   const uint8_t *valid, int B, int W, int H, double *loss, float *pred,
+                   void *workspace, size_t workspace_bytes, void *stream);
+/* one Adam step (b1 0.9, b2 0.999, eps 1e-8, per-element clip) on the
+ * trainer's gradient at learning rate lr */
+int sv_train_adam(sv_trainer *t, double lr, double clip, void *stream);
+/* zero Adam's moments and restart its bias correction */
+int sv_trainer_reset_adam(sv_trainer *t);
+
 #ifdef __cplusplus
 }
 #endif

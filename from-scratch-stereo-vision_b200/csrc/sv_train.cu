@@ -429,6 +429,62 @@ __global__ void __launch_bounds__(256)
     gx[((long)img * out_ch + c) * HW + p] = acc;
 }
 
+// The same for stride 1, tiled: the input gradient of a stride-1 3x3
+// convolution is a convolution of gy with the flipped taps, so a CTA stages
+// the gy tile (kTR x kTC inputs plus a dil halo, all OC channels) in shared
+// memory and each thread computes ICG input channels of one pixel.
+template <int IC, int OC, int ICG, int MASK>
+__global__ void __launch_bounds__(kTC *kTR)
+    k_tdgrad2d_s1(const float *__restrict__ gy, int H, int W, int dil,
+                  const float *__restrict__ w, const float *__restrict__ xin, int cmax,
+                  int out_ch, float *__restrict__ gx) {
+    extern __shared__ __align__(16) float gt[];
+    __shared__ float sw[OC * IC * 9];
+    const int ng = (cmax + ICG - 1) / ICG;
+    const int img = blockIdx.z / ng, c0 = (blockIdx.z - img * ng) * ICG;
+    const int tid = threadIdx.y * kTC + threadIdx.x;
+    for (int i = tid; i < OC * IC * 9; i += kTC * kTR) sw[i] = w[i];
+    const long HW = (long)H * W;
+    const int x0 = blockIdx.x * kTC, y0 = blockIdx.y * kTR;
+    const int th = kTR + 2 * dil, tw = kTC + 2 * dil;
+    const float *g = gy + (long)img * OC * HW;
+    for (int i = tid; i < OC * th * tw; i += kTC * kTR) {
+        const int o = i / (th * tw), r = i - o * th * tw, ty = r / tw, tx = r - ty * tw;
+        const int yy = y0 - dil + ty, xx = x0 - dil + tx;
+        gt[i] = (yy >= 0 && yy < H && xx >= 0 && xx < W) ? g[o * HW + (long)yy * W + xx] : 0.f;
+    }
+    __syncthreads();
+    const int ix = x0 + threadIdx.x, iy = y0 + threadIdx.y;
+    if (ix >= W || iy >= H) return;
+    float acc[ICG];
+#pragma unroll
+    for (int j = 0; j < ICG; ++j) acc[j] = 0.f;
+#pragma unroll
+    for (int o = 0; o < OC; ++o)
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            // output row iy + dil - ky*dil sits at tile row threadIdx.y + (2 - ky) * dil
+            const float *row = gt + (o * th + threadIdx.y + (2 - ky) * dil) * tw + threadIdx.x;
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+                const float gv = row[(2 - kx) * dil];
+#pragma unroll
+                for (int j = 0; j < ICG; ++j)
+                    if (c0 + j < cmax)
+                        acc[j] = fmaf(sw[(o * IC + c0 + j) * 9 + ky * 3 + kx], gv, acc[j]);
+            }
+        }
+    const long p = (long)iy * W + ix;
+#pragma unroll
+    for (int j = 0; j < ICG; ++j) {
+        const int c = c0 + j;
+        if (c >= cmax) break;
+        float v = acc[j];
+        if (MASK) v = xin[((long)img * IC + c) * HW + p] > 0.f ? v : v * 0.2f;
+        gx[((long)img * out_ch + c) * HW + p] = v;
+    }
+}
+
 // Conv3d input gradient (643-693), same form, with the leaky-ReLU
 // derivative of the input when MASK.
 template <int IC, int OC, int MASK>
@@ -472,54 +528,78 @@ __global__ void __launch_bounds__(256)
     gx[i] = acc;
 }
 
-// Conv2d weight gradient, per-tile partial sums: the CTA of tile t (image,
-// 4 x 32 outputs) writes partial[t][o][k], k < IC*9 the taps (c*9 + ky*3 +
-// kx), k == IC*9 the bias.
+// Weight gradients, per-CTA partial sums.  A CTA walks tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... (a fixed assignment, so the sums are
+// deterministic), stages each tile's input patch and output gradients in
+// shared memory and accumulates, for the KPT (out of K) weight rows
+// k = tid, tid + 128, ... it owns, all OC outputs in registers; at the end it
+// writes partial[cta][o][k].  Rows k < K-1 are the taps, k == K-1 the bias.
+constexpr int kWgCtas = 4 * 148;
+
+// 2-D: a tile is one image's kTR x kTC outputs; taps k = c*9 + ky*3 + kx.
 template <int IC, int OC>
 __global__ void __launch_bounds__(128)
-    k_twgrad2d(const float *__restrict__ x, const float *__restrict__ gy, int H, int W, int OH,
-               int OW, int s, int dil, float *__restrict__ partial) {
-    constexpr int K = IC * 9 + 1, P = kTR * kTC;
+    k_twgrad2d(const float *__restrict__ x, const float *__restrict__ gy, int nimg, int H, int W,
+               int OH, int OW, int s, int dil, float *__restrict__ partial) {
+    constexpr int K = IC * 9 + 1, P = kTR * kTC, KPT = (K + 127) / 128;
     extern __shared__ __align__(16) float sm[];
     float *gyt = sm;                      // [OC][P]
     float *xt = sm + OC * P;              // [IC][th][tw]
-    const int img = blockIdx.z, tid = threadIdx.x;
-    const long blk = ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    const int tid = threadIdx.x;
     const long HW = (long)H * W, OHW = (long)OH * OW;
-    const int ox0 = blockIdx.x * kTC, oy0 = blockIdx.y * kTR;
-    for (int i = tid; i < OC * P; i += 128) {
-        const int o = i / P, q = i - o * P, oy = oy0 + q / kTC, ox = ox0 + q % kTC;
-        gyt[i] = (oy < OH && ox < OW) ? gy[((long)img * OC + o) * OHW + (long)oy * OW + ox] : 0.f;
-    }
+    const int tx_n = (OW + kTC - 1) / kTC, ty_n = (OH + kTR - 1) / kTR;
+    const long ntiles = (long)nimg * tx_n * ty_n;
     const int th = (kTR - 1) * s + 2 * dil + 1, tw = (kTC - 1) * s + 2 * dil + 1;
-    const int ix0 = ox0 * s - dil, iy0 = oy0 * s - dil;
-    for (int i = tid; i < IC * th * tw; i += 128) {
-        const int c = i / (th * tw), rem = i - c * th * tw, ty = rem / tw, tx = rem - ty * tw;
-        const int yy = iy0 + ty, xx = ix0 + tx;
-        xt[i] = (yy >= 0 && yy < H && xx >= 0 && xx < W) ? x[((long)img * IC + c) * HW +
-                                                             (long)yy * W + xx]
-                                                       : 0.f;
-    }
-    __syncthreads();
-    for (int k = tid; k < K; k += 128) {
-        float acc[OC];
+    float acc[KPT][OC];
 #pragma unroll
-        for (int o = 0; o < OC; ++o) acc[o] = 0.f;
-        if (k < IC * 9) {
-            const int c = k / 9, ky = (k % 9) / 3, kx = k % 3;
-            const float *xc = xt + c * th * tw + ky * dil * tw + kx * dil;
-            for (int q = 0; q < P; ++q) {
-                const float xv = xc[(q / kTC) * s * tw + (q % kTC) * s];
+    for (int j = 0; j < KPT; ++j)
 #pragma unroll
-                for (int o = 0; o < OC; ++o) acc[o] = fmaf(xv, gyt[o * P + q], acc[o]);
-            }
-        } else {
-            for (int q = 0; q < P; ++q)
-#pragma unroll
-                for (int o = 0; o < OC; ++o) acc[o] += gyt[o * P + q];
+        for (int o = 0; o < OC; ++o) acc[j][o] = 0.f;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int img = (int)(tile / (tx_n * ty_n));
+        const int rem = (int)(tile - (long)img * tx_n * ty_n);
+        const int oy0 = (rem / tx_n) * kTR, ox0 = (rem % tx_n) * kTC;
+        __syncthreads();                  // the previous tile's reads are done
+        for (int i = tid; i < OC * P; i += 128) {
+            const int o = i / P, q = i - o * P, oy = oy0 + q / kTC, ox = ox0 + q % kTC;
+            gyt[i] = (oy < OH && ox < OW)
+                         ? gy[((long)img * OC + o) * OHW + (long)oy * OW + ox]
+                         : 0.f;
         }
+        const int ix0 = ox0 * s - dil, iy0 = oy0 * s - dil;
+        for (int i = tid; i < IC * th * tw; i += 128) {
+            const int c = i / (th * tw), r2 = i - c * th * tw, ty = r2 / tw, tx = r2 - ty * tw;
+            const int yy = iy0 + ty, xx = ix0 + tx;
+            xt[i] = (yy >= 0 && yy < H && xx >= 0 && xx < W)
+                        ? x[((long)img * IC + c) * HW + (long)yy * W + xx]
+                        : 0.f;
+        }
+        __syncthreads();
 #pragma unroll
-        for (int o = 0; o < OC; ++o) partial[(blk * OC + o) * K + k] = acc[o];
+        for (int j = 0; j < KPT; ++j) {
+            const int k = tid + 128 * j;
+            if (k >= K) break;
+            if (k < K - 1) {
+                const int c = k / 9, ky = (k % 9) / 3, kx = k % 3;
+                const float *xc = xt + c * th * tw + ky * dil * tw + kx * dil;
+                for (int q = 0; q < P; ++q) {
+                    const float xv = xc[(q / kTC) * s * tw + (q % kTC) * s];
+#pragma unroll
+                    for (int o = 0; o < OC; ++o) acc[j][o] = fmaf(xv, gyt[o * P + q], acc[j][o]);
+                }
+            } else {
+                for (int q = 0; q < P; ++q)
+#pragma unroll
+                    for (int o = 0; o < OC; ++o) acc[j][o] += gyt[o * P + q];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        const int k = tid + 128 * j;
+        if (k < K)
+#pragma unroll
+            for (int o = 0; o < OC; ++o) partial[((long)blockIdx.x * OC + o) * K + k] = acc[j][o];
     }
 }
 
@@ -528,68 +608,95 @@ size_t twgrad2d_smem(int IC, int OC, int s, int dil) {
                             IC * ((kTR - 1) * s + 2 * dil + 1) * ((kTC - 1) * s + 2 * dil + 1));
 }
 
-// Conv3d weight gradient, per-tile partial sums (tile: one sample, kTD
-// disparities x 1 row x 32 columns; k < IC*27 the taps, k == IC*27 the bias).
+// 3-D: a tile is one sample's kTD disparities x 1 row x 32 columns; taps
+// k = c*27 + kd*9 + ky*3 + kx.
 template <int IC, int OC>
 __global__ void __launch_bounds__(128)
-    k_twgrad3d(const float *__restrict__ x, const float *__restrict__ gy, int D, int h, int w,
-               float *__restrict__ partial) {
-    constexpr int K = IC * 27 + 1, P = kTD * 32;
+    k_twgrad3d(const float *__restrict__ x, const float *__restrict__ gy, int B, int D, int h,
+               int w, float *__restrict__ partial) {
+    constexpr int K = IC * 27 + 1, P = kTD * 32, KPT = (K + 127) / 128;
     __shared__ float xt[IC][kTD + 2][3][34];
     __shared__ float gyt[OC][P];
-    const int b = blockIdx.z, tid = threadIdx.x;
-    const long blk = ((long)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    const int nd = (D + kTD - 1) / kTD;
-    const int x0 = blockIdx.x * 32, oy = blockIdx.y / nd, d0 = (blockIdx.y - oy * nd) * kTD;
+    const int tid = threadIdx.x;
+    const int nd = (D + kTD - 1) / kTD, nx = (w + 31) / 32;
+    const long ntiles = (long)B * h * nd * nx;
     const long hw = (long)h * w, total = (long)D * hw;
-    for (int i = tid; i < OC * P; i += 128) {
-        const int o = i / P, q = i - o * P, od = d0 + q / 32, ox = x0 + q % 32;
-        gyt[o][q] = (od < D && ox < w) ? gy[((long)b * OC + o) * total + (long)od * hw +
-                                            (long)oy * w + ox]
-                                      : 0.f;
-    }
-    constexpr int PLANE = (kTD + 2) * 3 * 34;
-    for (int i = tid; i < IC * PLANE; i += 128) {
-        const int c = i / PLANE, rem = i - c * PLANE;
-        const int dz = rem / 102, rem2 = rem - dz * 102, r = rem2 / 34, j = rem2 - r * 34;
-        const int dd = d0 - 1 + dz, yy = oy - 1 + r, xx = x0 - 1 + j;
-        xt[c][dz][r][j] = (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w)
-                              ? x[((long)b * IC + c) * total + dd * hw + yy * w + xx]
-                              : 0.f;
-    }
-    __syncthreads();
-    for (int k = tid; k < K; k += 128) {
-        float acc[OC];
+    float acc[KPT][OC];
 #pragma unroll
-        for (int o = 0; o < OC; ++o) acc[o] = 0.f;
-        if (k < IC * 27) {
-            const int c = k / 27, kd = (k % 27) / 9, ky = (k % 9) / 3, kx = k % 3;
-            for (int q = 0; q < P; ++q) {
-                const float xv = xt[c][q / 32 + kd][ky][q % 32 + kx];
+    for (int j = 0; j < KPT; ++j)
 #pragma unroll
-                for (int o = 0; o < OC; ++o) acc[o] = fmaf(xv, gyt[o][q], acc[o]);
-            }
-        } else {
-            for (int q = 0; q < P; ++q)
-#pragma unroll
-                for (int o = 0; o < OC; ++o) acc[o] += gyt[o][q];
+        for (int o = 0; o < OC; ++o) acc[j][o] = 0.f;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int b = (int)(tile / ((long)h * nd * nx));
+        const int rem = (int)(tile - (long)b * h * nd * nx);
+        const int oy = rem / (nd * nx), r2 = rem - oy * nd * nx;
+        const int d0 = (r2 / nx) * kTD, x0 = (r2 % nx) * 32;
+        __syncthreads();
+        for (int i = tid; i < OC * P; i += 128) {
+            const int o = i / P, q = i - o * P, od = d0 + q / 32, ox = x0 + q % 32;
+            gyt[o][q] = (od < D && ox < w) ? gy[((long)b * OC + o) * total + (long)od * hw +
+                                                (long)oy * w + ox]
+                                          : 0.f;
         }
+        constexpr int PLANE = (kTD + 2) * 3 * 34;
+        for (int i = tid; i < IC * PLANE; i += 128) {
+            const int c = i / PLANE, r3 = i - c * PLANE;
+            const int dz = r3 / 102, r4 = r3 - dz * 102, r = r4 / 34, jx = r4 - r * 34;
+            const int dd = d0 - 1 + dz, yy = oy - 1 + r, xx = x0 - 1 + jx;
+            xt[c][dz][r][jx] = (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w)
+                                   ? x[((long)b * IC + c) * total + dd * hw + yy * w + xx]
+                                   : 0.f;
+        }
+        __syncthreads();
 #pragma unroll
-        for (int o = 0; o < OC; ++o) partial[(blk * OC + o) * K + k] = acc[o];
+        for (int j = 0; j < KPT; ++j) {
+            const int k = tid + 128 * j;
+            if (k >= K) break;
+            if (k < K - 1) {
+                const int c = k / 27, kd = (k % 27) / 9, ky = (k % 9) / 3, kx = k % 3;
+                for (int q = 0; q < P; ++q) {
+                    const float xv = xt[c][q / 32 + kd][ky][q % 32 + kx];
+#pragma unroll
+                    for (int o = 0; o < OC; ++o) acc[j][o] = fmaf(xv, gyt[o][q], acc[j][o]);
+                }
+            } else {
+                for (int q = 0; q < P; ++q)
+#pragma unroll
+                    for (int o = 0; o < OC; ++o) acc[j][o] += gyt[o][q];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < KPT; ++j) {
+        const int k = tid + 128 * j;
+        if (k < K)
+#pragma unroll
+            for (int o = 0; o < OC; ++o) partial[((long)blockIdx.x * OC + o) * K + k] = acc[j][o];
     }
 }
 
-// Tile partials -> one layer's weight and bias gradient, added over tiles in
-// order in FP64.  Parameter layout: weights [o][taps], then bias [o].
-__global__ void k_treduce(const float *__restrict__ partial, long nblk, int OC, int K,
-                          double *__restrict__ gw, double *__restrict__ gb) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= OC * K) return;
+// CTA partials -> one layer's weight and bias gradient in FP64.  A block
+// takes 32 weights (threadIdx.x); its 32 rows (threadIdx.y) add the partials
+// t = y, y + 32, ... in order, and row sums are then added in row order, so
+// the result does not depend on scheduling.  Parameter layout: weights
+// [o][taps], then bias [o].
+__global__ void __launch_bounds__(1024)
+    k_treduce(const float *__restrict__ partial, long nblk, int OC, int K,
+              double *__restrict__ gw, double *__restrict__ gb) {
+    __shared__ double rs[32][33];
+    const int j = blockIdx.x * 32 + threadIdx.x;
+    const long stride = (long)OC * K;
     double s = 0.0;
-    for (long t = 0; t < nblk; ++t) s += (double)partial[t * OC * K + j];
+    if (j < OC * K)
+        for (long t = threadIdx.y; t < nblk; t += 32) s += (double)partial[t * stride + j];
+    rs[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y != 0 || j >= OC * K) return;
+    double tot = 0.0;
+    for (int y = 0; y < 32; ++y) tot += rs[y][threadIdx.x];
     const int o = j / K, k = j - o * K;
-    if (k < K - 1) gw[o * (K - 1) + k] = s;
-    else gb[o] = s;
+    if (k < K - 1) gw[o * (K - 1) + k] = tot;
+    else gb[o] = tot;
 }
 
 // CostVolume.backward (801-824) as a gather: gfl[c][y][x] sums over d the
@@ -765,22 +872,18 @@ long tiles2d(int nimg, int OH, int OW) {
 }
 
 long partial_floats(const sv_trainer *t, const Dims &d) {
-    const int C = t->C, Cm = t->Cm, Rc = t->Rc, D = t->D;
+    (void)d;
+    // at most kWgCtas CTAs per weight-gradient launch; the widest layer
+    // (OC x K) bounds the rest
+    const int C = t->C, Cm = t->Cm, Rc = t->Rc;
     long m = 0;
     auto upd = [&](long v) { m = v > m ? v : m; };
-    upd(tiles2d(2 * d.B, d.h1, d.w1) * C * (1 * 9 + 1));
-    upd(tiles2d(2 * d.B, d.h, d.w) * C * (C * 9 + 1));
-    const long t3 = (long)d.B * ((d.w + 31) / 32) * d.h * ((D + kTD - 1) / kTD);
-    upd(t3 * Cm * (C * 27 + 1));
-    upd(t3 * Cm * (Cm * 27 + 1));
-    const int Hs[2] = {d.H2, d.H}, Ws[2] = {d.W2, d.W};
-    for (int lv = 0; lv < 2; ++lv) {
-        const long tl = tiles2d(d.B, Hs[lv], Ws[lv]);
-        upd(tl * Rc * (2 * 9 + 1));
-        upd(tl * Rc * (Rc * 9 + 1));
-        upd(tl * 1 * (Rc * 9 + 1));
-    }
-    return m;
+    upd((long)C * (C * 9 + 1));
+    upd((long)Cm * (C * 27 + 1));
+    upd((long)Cm * (Cm * 27 + 1));
+    upd((long)Rc * (Rc * 9 + 1));
+    upd((long)Rc * (2 * 9 + 1));
+    return m * kWgCtas;
 }
 
 void carve(const sv_trainer *t, const Dims &d, Carver &cv, TrainBufs &b) {
@@ -852,6 +955,22 @@ int fconv2d(const float *x, int nimg, int H, int W, int OH, int OW, int s, int d
     return SV_OK;
 }
 
+template <int IC, int OC, int ICG, int MASK>
+int dgrad2d_s1(const float *gy, int nimg, int H, int W, int dil, const float *w,
+               const float *xin, int cmax, int out_ch, float *gx, cudaStream_t st) {
+    const size_t sm = sizeof(float) * OC * (kTR + 2 * dil) * (kTC + 2 * dil);
+    if (sm > 48 * 1024) {
+        set_error("input-gradient tile needs %zu bytes of shared memory", sm);
+        return SV_ERR_SHAPE;
+    }
+    const dim3 g((W + kTC - 1) / kTC, (H + kTR - 1) / kTR, nimg * ((cmax + ICG - 1) / ICG));
+    count_launch();
+    k_tdgrad2d_s1<IC, OC, ICG, MASK><<<g, dim3(kTC, kTR), sm, st>>>(gy, H, W, dil, w, xin, cmax,
+                                                                   out_ch, gx);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
 template <int IC, int OC>
 int wgrad2d(const float *x, const float *gy, int nimg, int H, int W, int OH, int OW, int s,
             int dil, float *partial, double *gw, double *gb, cudaStream_t st) {
@@ -860,13 +979,13 @@ int wgrad2d(const float *x, const float *gy, int nimg, int H, int W, int OH, int
         set_error("weight-gradient tile needs %zu bytes of shared memory", sm);
         return SV_ERR_SHAPE;
     }
-    const dim3 g((OW + kTC - 1) / kTC, (OH + kTR - 1) / kTR, nimg);
-    const long nblk = (long)g.x * g.y * g.z;
+    const long ntiles = tiles2d(nimg, OH, OW);
+    const int nblk = (int)(ntiles < kWgCtas ? ntiles : kWgCtas);
     constexpr int K = IC * 9 + 1;
     count_launch();
-    k_twgrad2d<IC, OC><<<g, 128, sm, st>>>(x, gy, H, W, OH, OW, s, dil, partial);
+    k_twgrad2d<IC, OC><<<nblk, 128, sm, st>>>(x, gy, nimg, H, W, OH, OW, s, dil, partial);
     count_launch();
-    k_treduce<<<nblocks((long)OC * K, 128), 128, 0, st>>>(partial, nblk, OC, K, gw, gb);
+    k_treduce<<<(OC * K + 31) / 32, dim3(32, 32), 0, st>>>(partial, nblk, OC, K, gw, gb);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -874,13 +993,13 @@ int wgrad2d(const float *x, const float *gy, int nimg, int H, int W, int OH, int
 template <int IC, int OC>
 int wgrad3d(const float *x, const float *gy, int B, int D, int h, int w, float *partial,
             double *gw, double *gb, cudaStream_t st) {
-    const dim3 g((w + 31) / 32, h * ((D + kTD - 1) / kTD), B);
-    const long nblk = (long)g.x * g.y * g.z;
+    const long ntiles = (long)B * h * ((D + kTD - 1) / kTD) * ((w + 31) / 32);
+    const int nblk = (int)(ntiles < kWgCtas ? ntiles : kWgCtas);
     constexpr int K = IC * 27 + 1;
     count_launch();
-    k_twgrad3d<IC, OC><<<g, 128, 0, st>>>(x, gy, D, h, w, partial);
+    k_twgrad3d<IC, OC><<<nblk, 128, 0, st>>>(x, gy, B, D, h, w, partial);
     count_launch();
-    k_treduce<<<nblocks((long)OC * K, 128), 128, 0, st>>>(partial, nblk, OC, K, gw, gb);
+    k_treduce<<<(OC * K + 31) / 32, dim3(32, 32), 0, st>>>(partial, nblk, OC, K, gw, gb);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -995,19 +1114,18 @@ int train_impl(sv_trainer *t, const float *left, const float *right, const float
         if ((rc = wgrad2d<RC, 1>(b.r[lv][nd - 1], gs, B, Hl, Wl, Hl, Wl, 1, 1, b.partial,
                                  G + t->off_rw[lv][nd], G + t->off_rb[lv][nd], st)))
             return rc;
-        count_launch();
-        k_tdgrad2d<RC, 1, 1><<<nblocks((long)B * RC * HWl[lv]), 256, 0, st>>>(
-            gs, B, Hl, Wl, Hl, Wl, 1, 1, P + t->off_rw[lv][nd], b.r[lv][nd - 1], RC, RC, b.gA);
+        if ((rc = dgrad2d_s1<RC, 1, RG, 1>(gs, B, Hl, Wl, 1, P + t->off_rw[lv][nd],
+                                           b.r[lv][nd - 1], RC, RC, b.gA, st)))
+            return rc;
         float *gcur = b.gA, *gnext = b.gB;
         for (int i = nd - 1; i >= 1; --i) {
             const int dl = t->dil[i];
             if ((rc = wgrad2d<RC, RC>(b.r[lv][i - 1], gcur, B, Hl, Wl, Hl, Wl, 1, dl, b.partial,
                                       G + t->off_rw[lv][i], G + t->off_rb[lv][i], st)))
                 return rc;
-            count_launch();
-            k_tdgrad2d<RC, RC, 1><<<nblocks((long)B * RC * HWl[lv]), 256, 0, st>>>(
-                gcur, B, Hl, Wl, Hl, Wl, 1, dl, P + t->off_rw[lv][i], b.r[lv][i - 1], RC, RC,
-                gnext);
+            if ((rc = dgrad2d_s1<RC, RC, RG, 1>(gcur, B, Hl, Wl, dl, P + t->off_rw[lv][i],
+                                                b.r[lv][i - 1], RC, RC, gnext, st)))
+                return rc;
             float *tmp = gcur;
             gcur = gnext;
             gnext = tmp;
@@ -1016,9 +1134,9 @@ int train_impl(sv_trainer *t, const float *left, const float *right, const float
                                  G + t->off_rw[lv][0], G + t->off_rb[lv][0], st)))
             return rc;
         // only the disparity channel of the input gradient is needed
-        count_launch();
-        k_tdgrad2d<2, RC, 0><<<nblocks((long)B * HWl[lv]), 256, 0, st>>>(
-            gcur, B, Hl, Wl, Hl, Wl, 1, t->dil[0], P + t->off_rw[lv][0], nullptr, 1, 1, b.grin);
+        if ((rc = dgrad2d_s1<2, RC, 1, 0>(gcur, B, Hl, Wl, t->dil[0], P + t->off_rw[lv][0],
+                                          nullptr, 1, 1, b.grin, st)))
+            return rc;
         // up-sample backward of 2 * (input gradient + skip) to the previous
         // level, plus that level's loss gradient, through its output ReLU
         const int sh = lv ? d.H2 : d.h, sw = lv ? d.W2 : d.w;
@@ -1059,15 +1177,15 @@ int train_impl(sv_trainer *t, const float *left, const float *right, const float
     if ((rc = wgrad2d<C, C>(b.a3, b.gf, 2 * B, d.h, d.w, d.h, d.w, 1, 1, b.partial,
                             G + t->off_fw[3], G + t->off_fb[3], st)))
         return rc;
-    count_launch();
-    k_tdgrad2d<C, C, 1><<<nblocks(2L * B * C * d.hw), 256, 0, st>>>(
-        b.gf, 2 * B, d.h, d.w, d.h, d.w, 1, 1, P + t->off_fw[3], b.a3, C, C, b.gF4);
+    if ((rc = dgrad2d_s1<C, C, FG, 1>(b.gf, 2 * B, d.h, d.w, 1, P + t->off_fw[3], b.a3, C, C,
+                                      b.gF4, st)))
+        return rc;
     if ((rc = wgrad2d<C, C>(b.a2, b.gF4, 2 * B, d.h, d.w, d.h, d.w, 1, 1, b.partial,
                             G + t->off_fw[2], G + t->off_fb[2], st)))
         return rc;
-    count_launch();
-    k_tdgrad2d<C, C, 1><<<nblocks(2L * B * C * d.hw), 256, 0, st>>>(
-        b.gF4, 2 * B, d.h, d.w, d.h, d.w, 1, 1, P + t->off_fw[2], b.a2, C, C, b.gf);
+    if ((rc = dgrad2d_s1<C, C, FG, 1>(b.gF4, 2 * B, d.h, d.w, 1, P + t->off_fw[2], b.a2, C, C,
+                                      b.gf, st)))
+        return rc;
     if ((rc = wgrad2d<C, C>(b.a1, b.gf, 2 * B, d.h1, d.w1, d.h, d.w, 2, 1, b.partial,
                             G + t->off_fw[1], G + t->off_fb[1], st)))
         return rc;

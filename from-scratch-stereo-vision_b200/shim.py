@@ -19,7 +19,7 @@ reference's own path).  ``uninstall(SN)`` restores the originals.
 
 from __future__ import annotations
 
-from . import image, network, post, refine
+from . import image, network, post, refine, train
 
 # reference name -> drop-in
 DROP_INS = {
@@ -44,6 +44,8 @@ DROP_INS = {
     "read_png": image.read_png,
     "read_pnm": image.read_pnm,
     "read_image": image.read_image,
+    "train_grads": train.train_grads,
+    "train_step": train.train_step,
 }
 
 _SAVED = "__sv_b200_saved__"

@@ -146,3 +146,43 @@ size_t select_value_offset() { return offsetof(SelState, value); }
 size_t select_hist_words() { return (size_t)SEL_NPASS * SEL_NB; }
 
 }  // namespace sv
+
+namespace {
+__global__ void k_peak_out(const sv::SelState *s, double *out) {
+    const double v = s->value;
+    *out = v > 0.5 ? v : 0.5;
+}
+}  // namespace
+
+extern "C" {
+
+size_t sv_peak_workspace_size(void) {
+    return sv::align256(sizeof(sv::SelState)) + sv::select_hist_words() * sizeof(unsigned) + 256;
+}
+
+// _peak (stereonet.py:3866-3869): sorted(disp)[int(len(disp) * q)], floored
+// at 0.5, into *out (device FP64).
+int sv_peak(const double *disp, long n, double q, double *out, void *workspace,
+            size_t workspace_bytes, void *stream) {
+    if (!disp || !out) { sv::set_error("NULL argument"); return SV_ERR_NULL; }
+    if (!(q >= 0.0 && q < 1.0)) { sv::set_error("q=%g outside [0, 1)", q); return SV_ERR_PARAM; }
+    if (!workspace || workspace_bytes < sv_peak_workspace_size() ||
+        ((uintptr_t)workspace & 255)) {
+        sv::set_error("workspace must be 256-byte aligned and hold %zu bytes",
+                      sv_peak_workspace_size());
+        return SV_ERR_WORKSPACE;
+    }
+    const long long rank = (long long)((double)n * q);   // Python int(): toward zero
+    cudaStream_t st = (cudaStream_t)stream;
+    sv::SelState *s = static_cast<sv::SelState *>(workspace);
+    unsigned *hist = reinterpret_cast<unsigned *>(static_cast<char *>(workspace) +
+                                                  sv::align256(sizeof(sv::SelState)));
+    const int rc = sv::launch_select(disp, n, rank, s, hist, st);
+    if (rc) return rc;
+    sv::count_launch();
+    k_peak_out<<<1, 1, 0, st>>>(s, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+}  // extern "C"

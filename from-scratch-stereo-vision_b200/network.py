@@ -191,6 +191,20 @@ def predict_at_scale(net, left, right, W, H, work_width=96, verbose=True, *, pre
     return _ret(df, left), _ret(dwv, left), Ww.value, Hw.value
 
 
+def _peak(disp, q=0.95):
+    """stereonet.py:3866-3869: sorted(disp)[int(len(disp) * q)], at least
+    0.5 -- an exact radix select on the GPU."""
+    lib = _lib.load()
+    d = disp if isinstance(disp, torch.Tensor) else np.asarray(disp, dtype=np.float64)
+    n = int(d.numel() if isinstance(d, torch.Tensor) else d.size)
+    t = _to_dev(d, n, torch.float64, name="disp")
+    out = torch.empty(1, dtype=torch.float64, device=t.device)
+    need = lib.sv_peak_workspace_size()
+    ws = torch.empty(need, dtype=torch.uint8, device=t.device)
+    _lib.check(lib.sv_peak(_ptr(t), n, float(q), _ptr(out), _ptr(ws), need, _stream()), "_peak")
+    return float(out.item())
+
+
 def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64, max_width=320,
                  passes=3, verbose=True, return_trace=False, *, precision="fp32"):
     """stereonet.py:3872-3929 -> (disp_full, disp_work, W_work, H_work).

@@ -34,6 +34,7 @@ DROP_INS = {
     "predict": network.predict,
     "predict_at_scale": network.predict_at_scale,
     "predict_auto": network.predict_auto,
+    "_peak": network._peak,
     "median_filter": post.median_filter,
     "slic": post.slic,
     "plane_snap": post.plane_snap,

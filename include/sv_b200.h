@@ -346,6 +346,13 @@ int sv_lr_refine_band(const void *left, const void *right, int dtype,
                       uint8_t *status, void *workspace, size_t workspace_bytes,
                       void *stream);
 
+/* _peak (stereonet.py:3866-3869): sorted(disp)[int(len(disp) * q)], floored
+ * at 0.5, written to *out (device FP64), exact; disp is device FP64 [n],
+ * n < 2^32 (six radix passes over order-preserving 64-bit keys). */
+size_t sv_peak_workspace_size(void);
+int sv_peak(const double *disp, long n, double q, double *out, void *workspace,
+            size_t workspace_bytes, void *stream);
+
 /* ------------------------------------------------------------------------
  * Input images: PNG (stereonet.py:3499-3601 read_png, with zlib_decompress
  * 3421, inflate 3335 and _unfilter 3456) and PGM/PPM (stereonet.py:265-324

@@ -459,7 +459,7 @@ HOT_PATH = ["census", "band_costs", "_aggregate_path", "refine_fullres", "left_t
             "lr_refine", "resize_gray", "avgpool2", "predict", "predict_at_scale",
             "predict_auto", "refine_disparity", "median_filter", "slic", "plane_snap",
             "predict_consistent", "lr_consistency", "fill_invalid", "read_png", "read_pnm",
-            "read_image", "train_grads", "train_step"]
+            "read_image", "train_grads", "train_step", "_peak"]
 
 
 def signatures(ref_dir):

@@ -69,6 +69,8 @@ SIGNATURES = {
     "sv_refine_fullres_noalloc": (_I, [_VP, _VP, _I, _VP, _I, _I, _PRM, _VP, _VP, _VP]),
     "sv_batch_lr_refine_workspace_size": (_SZ, [_VP, _I, _PRM]),
     "sv_batch_lr_refine": (_I, [_VP, _I, _I, _D, _PRM, _VP, _SZ, _VP]),
+    "sv_batch_config_default": (None, [_VP]),
+    "sv_batch_lr_refine_ex": (_I, [_VP, _I, _I, _D, _PRM, _VP, _VP, _SZ, _VP]),
     "sv_predict_consistent_workspace_size": (_SZ, [_VP, _I, _I, _I, _I]),
     "sv_predict_consistent": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _D, _I, _I, _I, _D, _I, _VP,
                                    ctypes.POINTER(ctypes.c_longlong), _VP, _SZ, _VP]),

@@ -7,11 +7,20 @@ bit-identical to ``refine.lr_refine`` on that pair alone.  ``BatchRefiner``
 is the device-resident form: the images, disparities and outputs stay in
 HBM and one call enqueues the whole batch (seven launches; the SGM stage is
 a persistent kernel over a device-side queue of scanline tasks).
+
+``BatchRefiner.autotune()`` picks the batch's scheduling (pixels per CTA of
+the per-pixel stages, the persistent SGM kernel's CTA size, CTAs per SM and
+tasks per queue fetch) by timing the batch itself, one knob at a time from
+the defaults, and remembers the choice per device, band and batch shape in
+a small JSON file (``$SV_B200_CACHE`` or ``~/.cache/sv_b200``).  Every
+configuration gives the same bits; only the time changes.
 """
 
 from __future__ import annotations
 
 import ctypes
+import json
+import os
 
 import numpy as np
 import torch
@@ -26,12 +35,45 @@ class PairDesc(ctypes.Structure):
                 ("status", ctypes.c_void_p), ("W", ctypes.c_int), ("H", ctypes.c_int)]
 
 
+class BatchConfig(ctypes.Structure):
+    """sv_batch_config: the batched refinement's scheduling."""
+    _fields_ = [("px_per_block", ctypes.c_int), ("sgm_threads", ctypes.c_int),
+                ("sgm_ctas_per_sm", ctypes.c_int), ("sgm_fetch", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+    @classmethod
+    def from_dict(cls, d):
+        return cls(*(int(d[k]) for k, _ in cls._fields_))
+
+
+def default_config() -> BatchConfig:
+    c = BatchConfig()
+    _lib.load().sv_batch_config_default(ctypes.byref(c))
+    return c
+
+
+# candidate values per knob, tried one knob at a time
+TUNE_SPACE = {"px_per_block": (512, 1024, 2048, 4096),
+              "sgm_threads": (64, 128, 256),
+              "sgm_ctas_per_sm": (4, 8, 16),
+              "sgm_fetch": (32, 64)}
+
+
+def _cache_path() -> str:
+    root = os.environ.get("SV_B200_CACHE") or os.path.join(os.path.expanduser("~"), ".cache",
+                                                            "sv_b200")
+    return os.path.join(root, "batch_tune.json")
+
+
 class BatchRefiner:
     """lr_refine for a fixed list of (W, H) sizes; buffers allocated once."""
 
     def __init__(self, sizes, dtype=torch.uint8, tol=2.0, R=10, P1=12.0, P2=150.0, rx=4, ry=3,
-                 paths=8, uniq=0.0):
+                 paths=8, uniq=0.0, config: BatchConfig | None = None):
         self.lib = _lib.load()
+        self.config = config if config is not None else default_config()
         self.sizes = [(int(W), int(H)) for W, H in sizes]
         self.tol = float(tol)
         self.p = _params(R=R, P1=P1, P2=P2, rx=rx, ry=ry, paths=paths, uniq=uniq)
@@ -59,10 +101,78 @@ class BatchRefiner:
         return sum(W * H for W, H in self.sizes)
 
     def run(self, stream=None) -> None:
-        _lib.check(self.lib.sv_batch_lr_refine(self.descs, len(self.sizes), self.code, self.tol,
-                                               ctypes.byref(self.p), _ptr(self.ws), self.need,
-                                               _stream() if stream is None else stream),
+        _lib.check(self.lib.sv_batch_lr_refine_ex(self.descs, len(self.sizes), self.code,
+                                                  self.tol, ctypes.byref(self.p),
+                                                  ctypes.byref(self.config), _ptr(self.ws),
+                                                  self.need,
+                                                  _stream() if stream is None else stream),
                    "lr_refine_batch")
+
+    def _key(self) -> str:
+        props = torch.cuda.get_device_properties(torch.cuda.current_device())
+        mpix = self.pixels / 1e6
+        bucket = 1 << max(0, int(np.ceil(np.log2(max(mpix, 1e-6)))) + 20)   # pixels, next 2^k
+        return "%s|sm%d|R%d|paths%d|n%d|px%d" % (props.name, props.multi_processor_count,
+                                                 self.p.R, self.p.paths, len(self.sizes), bucket)
+
+    def time_config(self, cfg: BatchConfig, reps: int = 3) -> float:
+        """Median device milliseconds of one batched call with `cfg`."""
+        old = self.config
+        self.config = cfg
+        try:
+            self.run()
+            times = []
+            for _ in range(reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                self.run()
+                e1.record()
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+            return float(np.median(times))
+        finally:
+            self.config = old
+
+    def autotune(self, reps: int = 3, use_cache: bool = True) -> dict:
+        """Pick the scheduling by timing this batch (the buffers' current
+        contents are used as they are); returns the choice and its times."""
+        key = self._key()
+        path = _cache_path()
+        cache = {}
+        if use_cache and os.path.exists(path):
+            try:
+                with open(path) as f:
+                    cache = json.load(f)
+            except (OSError, ValueError):
+                cache = {}
+        if use_cache and key in cache:
+            self.config = BatchConfig.from_dict(cache[key]["config"])
+            return dict(cache[key], cached=True)
+        best = default_config()
+        best_ms = self.time_config(best, reps)
+        base_ms = best_ms
+        tried = {json.dumps(best.as_dict(), sort_keys=True): best_ms}
+        for knob, values in TUNE_SPACE.items():
+            for v in values:
+                cand = BatchConfig.from_dict(dict(best.as_dict(), **{knob: v}))
+                k = json.dumps(cand.as_dict(), sort_keys=True)
+                if k not in tried:
+                    tried[k] = self.time_config(cand, reps)
+                if tried[k] < best_ms:
+                    best, best_ms = cand, tried[k]
+        self.config = best
+        entry = {"config": best.as_dict(), "ms": best_ms, "default_ms": base_ms,
+                 "candidates": len(tried)}
+        if use_cache:
+            try:
+                os.makedirs(os.path.dirname(path), exist_ok=True)
+                cache[key] = entry
+                with open(path, "w") as f:
+                    json.dump(cache, f, indent=1, sort_keys=True)
+            except OSError:
+                pass
+        return dict(entry, cached=False)
 
     def data_status(self) -> None:
         rc = self.lib.sv_workspace_status(_ptr(self.ws), ctypes.c_void_p(_stream()))

@@ -34,7 +34,8 @@ struct BatchPlan {
 };
 
 // Sizes and offsets; with ws != nullptr also fills the per-pair pointers.
-int plan_batch(const sv_pair_desc *in, int n, const RefineCfg &c, char *ws, BatchPlan *pl) {
+int plan_batch(const sv_pair_desc *in, int n, const RefineCfg &c, int px_per_block, char *ws,
+               BatchPlan *pl) {
     BatchPlan &P = *pl;
     const int Kp = slot_width(c.K);
     const size_t lt = c.l16 ? 2 : 1;
@@ -89,7 +90,7 @@ int plan_batch(const sv_pair_desc *in, int n, const RefineCfg &c, char *ws, Batc
         b.C0 = cv.take<uint8_t>(N * Kp);
         b.C1 = cv.take<uint8_t>(N * Kp);
         b.L = cv.take<uint8_t>(2 * (size_t)c.npaths * N * Kp * lt);
-        P.px_blk[i + 1] = P.px_blk[i] + (long long)((N + kBatchPxPerBlock - 1) / kBatchPxPerBlock);
+        P.px_blk[i + 1] = P.px_blk[i] + (long long)((N + px_per_block - 1) / px_per_block);
         P.row_blk[i + 1] = P.row_blk[i] + d.H;
         P.tile_blk[i + 1] = P.tile_blk[i] + (long long)((d.W + kTileW - 1) / kTileW) *
                                                 ((d.H + kTileH - 1) / kTileH);
@@ -143,14 +144,43 @@ size_t sv_batch_lr_refine_workspace_size(const sv_pair_desc *pairs, int n,
         return 0;
     }
     BatchPlan pl;
-    if (plan_batch(pairs, n, c, nullptr, &pl) != SV_OK) return 0;
+    if (plan_batch(pairs, n, c, kBatchPxPerBlock, nullptr, &pl) != SV_OK) return 0;
     return pl.total;
+}
+
+void sv_batch_config_default(sv_batch_config *cfg) {
+    if (!cfg) return;
+    cfg->px_per_block = kBatchPxPerBlock;
+    cfg->sgm_threads = 128;
+    cfg->sgm_ctas_per_sm = 8;
+    cfg->sgm_fetch = 32;
 }
 
 int sv_batch_lr_refine(const sv_pair_desc *pairs, int n, int dtype, double tol,
                        const sv_refine_params *p, void *workspace, size_t workspace_bytes,
                        void *stream) {
+    sv_batch_config cfg;
+    sv_batch_config_default(&cfg);
+    return sv_batch_lr_refine_ex(pairs, n, dtype, tol, p, &cfg, workspace, workspace_bytes,
+                                 stream);
+}
+
+int sv_batch_lr_refine_ex(const sv_pair_desc *pairs, int n, int dtype, double tol,
+                          const sv_refine_params *p, const sv_batch_config *cfg,
+                          void *workspace, size_t workspace_bytes, void *stream) {
     if (!pairs || n < 1) { set_error("no pairs"); return SV_ERR_NULL; }
+    if (!cfg) { set_error("NULL config"); return SV_ERR_NULL; }
+    {
+        const int px = cfg->px_per_block, th = cfg->sgm_threads, f = cfg->sgm_fetch;
+        if (px < 256 || px > 8192 || (px & (px - 1)) || (th != 32 && th != 64 && th != 128 &&
+                                                          th != 256) ||
+            cfg->sgm_ctas_per_sm < 1 || cfg->sgm_ctas_per_sm > 32 ||
+            (f != 32 && f != 64 && f != 128)) {
+            set_error("batch config: px_per_block a power of 2 in 256..8192, sgm_threads "
+                      "32/64/128/256, sgm_ctas_per_sm 1..32, sgm_fetch 32/64/128");
+            return SV_ERR_PARAM;
+        }
+    }
     RefineCfg c;
     int rc = check_refine(1, 1, p, true, &c);
     if (rc) return rc;
@@ -164,9 +194,10 @@ int sv_batch_lr_refine(const sv_pair_desc *pairs, int n, int dtype, double tol,
         return SV_ERR_PARAM;
     }
     BatchPlan pl;
-    if ((rc = plan_batch(pairs, n, c, nullptr, &pl))) return rc;
+    if ((rc = plan_batch(pairs, n, c, cfg->px_per_block, nullptr, &pl))) return rc;
     if ((rc = check_ws(workspace, workspace_bytes, pl.total))) return rc;
-    if ((rc = plan_batch(pairs, n, c, static_cast<char *>(workspace), &pl))) return rc;
+    if ((rc = plan_batch(pairs, n, c, cfg->px_per_block, static_cast<char *>(workspace), &pl)))
+        return rc;
     char *ws = static_cast<char *>(workspace);
     cudaStream_t st = (cudaStream_t)stream;
     // tables to the device (pageable copies are staged before the call returns)
@@ -211,7 +242,10 @@ int sv_batch_lr_refine(const sv_pair_desc *pairs, int n, int dtype, double tol,
     t.maxW = pl.maxW;
     t.tol = tol;
     t.uniq = c.uniq;
-    return launch_batch_refine(t, pl.px_blocks, pl.rows, pl.tiles, pl.tasks, c.l16, st);
+    t.px_per_block = cfg->px_per_block;
+    t.sgm_fetch = cfg->sgm_fetch;
+    return launch_batch_refine(t, pl.px_blocks, pl.rows, pl.tiles, pl.tasks, c.l16,
+                               cfg->sgm_threads, cfg->sgm_ctas_per_sm, st);
 }
 
 }  // extern "C"

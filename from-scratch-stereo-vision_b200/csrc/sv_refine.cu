@@ -562,8 +562,8 @@ __global__ void __launch_bounds__(256) k_b_base(BatchTables t) {
     const int i = batch_find(t.px_blk, t.n, blockIdx.x);
     const BatchPair &P = t.pairs[i];
     const long N = (long)P.W * P.H;
-    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * kBatchPxPerBlock;
-    const long p1 = min(N, p0 + kBatchPxPerBlock);
+    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * t.px_per_block;
+    const long p1 = min(N, p0 + (long)t.px_per_block);
     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
         const double d = P.disp0[p];
         int b = 0;

@@ -73,14 +73,14 @@ struct BatchPair {
     void *L;
 };
 
-constexpr int kBatchPxPerBlock = 2048;   // pixels per block of the per-pixel kernels
+constexpr int kBatchPxPerBlock = 2048;   // default pixels per block of the per-pixel kernels
 
 // Everything a batched kernel needs, passed by value.  Prefix tables map a
 // block (or an SGM task) to its pair by binary search.
 struct BatchTables {
     const BatchPair *pairs;
     int n;
-    const long long *px_blk;     // [n+1] blocks of kBatchPxPerBlock pixels
+    const long long *px_blk;     // [n+1] blocks of px_per_block pixels
     const long long *row_blk;    // [n+1] image rows
     const long long *tile_blk;   // [n+1] census tiles
     const long long *seg_start;  // [nseg+1] scanlines per (pair, view, dir) segment
@@ -90,6 +90,8 @@ struct BatchTables {
     int *queue;                  // SGM task counter, zeroed per call
     int *flag;                   // data errors (first wins)
     int R, K, Kp, P1, P2, npaths, invalid, rx, ry, dtype, maxW;
+    int px_per_block;            // pixels per CTA of the per-pixel stages
+    int sgm_fetch;               // scanline tasks a warp claims per queue fetch
     double tol, uniq;
 };
 
@@ -104,7 +106,8 @@ __device__ __forceinline__ int batch_find(const long long *prefix, int n, long l
 }
 
 int launch_batch_refine(const BatchTables &t, long long px_blocks, long long rows,
-                        long long tiles, long long tasks, bool l16, cudaStream_t st);
+                        long long tiles, long long tasks, bool l16, int sgm_threads,
+                        int sgm_ctas_per_sm, cudaStream_t st);
 
 int launch_base(const double *disp0, long N, int32_t *base, int *flag, cudaStream_t st);
 int launch_census(const void *img0, const void *img1, int dtype, int W, int H, int rx,

@@ -712,10 +712,10 @@ int launch_wta_slot(const void *L, bool l16, int npaths, int nviews, int W, int 
 
 // ====================================================================
 // Batched lr_refine, middle stages.  Costs and WTA run one block per
-// kBatchPxPerBlock pixels of a pair (blockIdx.y = view).  The SGM is a
-// persistent kernel over a device-side queue: every warp takes 32 scanline
-// tasks at a time from one atomic counter, tasks ordered longest scanline
-// first (segments of (pair, view, direction) sorted by length on the host),
+// px_per_block pixels of a pair (blockIdx.y = view).  The SGM is a
+// persistent kernel over a device-side queue: every warp takes sgm_fetch
+// (32 by default) scanline tasks at a time from one atomic counter, tasks
+// ordered longest scanline first (segments of (pair, view, direction) sorted by length on the host),
 // so all pairs' scanlines share one launch and finish together.
 // ====================================================================
 
@@ -724,8 +724,8 @@ __global__ void __launch_bounds__(256) k_b_costs(BatchTables t) {
     const BatchPair &P = t.pairs[i];
     const int view = blockIdx.y;
     const long N = (long)P.W * P.H;
-    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * kBatchPxPerBlock;
-    const long p1 = min(N, p0 + kBatchPxPerBlock);
+    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * t.px_per_block;
+    const long p1 = min(N, p0 + (long)t.px_per_block);
     const uint64_t *ref = view ? P.cen1 : P.cen0;
     const uint64_t *oth = view ? P.cen0 : P.cen1;
     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
@@ -734,16 +734,18 @@ __global__ void __launch_bounds__(256) k_b_costs(BatchTables t) {
 }
 
 template <int NR, typename LT>
-__global__ void __launch_bounds__(128) k_b_sgm(BatchTables t, long long total) {
+__global__ void __launch_bounds__(256) k_b_sgm(BatchTables t, long long total) {
     constexpr int Kp = 2 * NR;
     const int lane = threadIdx.x & 31;
+    const int fetch = t.sgm_fetch;                         // a multiple of 32
     for (;;) {
         long long first = 0;
-        if (lane == 0) first = atomicAdd(t.queue, 32);
+        if (lane == 0) first = atomicAdd(t.queue, fetch);
         first = __shfl_sync(kFull, first, 0);
         if (first >= total) return;                        // warp-uniform
-        const long long task = first + lane;
-        if (task < total) {
+        for (int j = lane; j < fetch; j += 32) {
+            const long long task = first + j;
+            if (task >= total) break;
             const int s = batch_find(t.seg_start, t.nseg, task);
             const BatchPair &P = t.pairs[t.seg_pair[s]];
             const int view = t.seg_vd[s] >> 3, dir = t.seg_vd[s] & 7;
@@ -765,8 +767,8 @@ __global__ void __launch_bounds__(256) k_b_wta(BatchTables t) {
     const int view = blockIdx.y;
     const long N = (long)P.W * P.H;
     const long stride = N * t.Kp;
-    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * kBatchPxPerBlock;
-    const long p1 = min(N, p0 + kBatchPxPerBlock);
+    const long p0 = (long)(blockIdx.x - t.px_blk[i]) * t.px_per_block;
+    const long p1 = min(N, p0 + (long)t.px_per_block);
     const LT *Lv = reinterpret_cast<const LT *>(P.L) + (long)view * t.npaths * stride;
     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
         wta_pixel<LT>(Lv + p * t.Kp, stride, t.npaths, t.K, t.Kp, t.R,
@@ -779,21 +781,23 @@ int launch_batch_front(const BatchTables &t, long long px_blocks, long long rows
 int launch_batch_back(const BatchTables &t, long long rows, cudaStream_t st);
 
 template <int NR, typename LT>
-static int batch_sgm_go(const BatchTables &t, long long tasks, cudaStream_t st) {
+static int batch_sgm_go(const BatchTables &t, long long tasks, int threads, int ctas_per_sm,
+                        cudaStream_t st) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    long long want = (tasks + 127) / 128;
-    const long long cap = (long long)sms * 8;              // persistent: a few CTAs per SM
+    long long want = (tasks + threads - 1) / threads;
+    const long long cap = (long long)sms * ctas_per_sm;    // persistent: a few CTAs per SM
     const unsigned blocks = (unsigned)(want < cap ? (want < 1 ? 1 : want) : cap);
     count_launch();
-    k_b_sgm<NR, LT><<<blocks, 128, 0, st>>>(t, tasks);
+    k_b_sgm<NR, LT><<<blocks, threads, 0, st>>>(t, tasks);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
 
 int launch_batch_refine(const BatchTables &t, long long px_blocks, long long rows,
-                        long long tiles, long long tasks, bool l16, cudaStream_t st) {
+                        long long tiles, long long tasks, bool l16, int sgm_threads,
+                        int sgm_ctas_per_sm, cudaStream_t st) {
     int rc = launch_batch_front(t, px_blocks, rows, tiles, st);
     if (rc) return rc;
     count_launch();
@@ -802,8 +806,8 @@ int launch_batch_refine(const BatchTables &t, long long px_blocks, long long row
     switch (t.Kp) {
 #define SV_BGO(KP)                                                                      \
     case KP:                                                                            \
-        rc = l16 ? batch_sgm_go<KP / 2, uint16_t>(t, tasks, st)                         \
-                 : batch_sgm_go<KP / 2, uint8_t>(t, tasks, st);                         \
+        rc = l16 ? batch_sgm_go<KP / 2, uint16_t>(t, tasks, sgm_threads, sgm_ctas_per_sm, st) \
+                 : batch_sgm_go<KP / 2, uint8_t>(t, tasks, sgm_threads, sgm_ctas_per_sm, st);  \
         break;
         SV_BGO(8)
         SV_BGO(16)

@@ -149,6 +149,24 @@ int sv_batch_lr_refine(const sv_pair_desc *pairs, int n, int dtype, double tol,
                        const sv_refine_params *p, void *workspace,
                        size_t workspace_bytes, void *stream);
 
+/* Scheduling of sv_batch_lr_refine_ex (results do not depend on it): pixels
+ * per CTA of the per-pixel stages (base, band costs, WTA, left-right check;
+ * a power of 2 in 256..8192), threads per CTA of the persistent SGM kernel
+ * (32/64/128/256), its CTAs per SM (1..32), and the scanline tasks a warp
+ * claims per fetch from the queue (32/64/128).  batch.autotune picks them by
+ * timing the caller's batch.  No reference counterpart. */
+typedef struct sv_batch_config {
+    int px_per_block;
+    int sgm_threads;
+    int sgm_ctas_per_sm;
+    int sgm_fetch;
+} sv_batch_config;
+/* 2048, 128, 8, 32: what sv_batch_lr_refine uses */
+void sv_batch_config_default(sv_batch_config *cfg);
+int sv_batch_lr_refine_ex(const sv_pair_desc *pairs, int n, int dtype, double tol,
+                          const sv_refine_params *p, const sv_batch_config *cfg,
+                          void *workspace, size_t workspace_bytes, void *stream);
+
 /* refine_fullres for callers that cannot allocate device memory (an engine
  * that reserves all GPU memory up front, a plugin host without an
  * allocator): same kernels and bit-identical output as sv_refine_fullres,

@@ -81,3 +81,62 @@ def test_batch_nan_flagged(svb):
     pairs[1] = (L, R, d0, W, H)
     with pytest.raises(ValueError):
         svb.batch.lr_refine_batch(pairs, tol=2.0, **PIPE)
+
+
+def _loaded_refiner(svb, pairs, **kw):
+    import torch
+    b = svb.batch.BatchRefiner([(p[3], p[4]) for p in pairs], **kw)
+    for i, (L, R, d0, W, H) in enumerate(pairs):
+        b.left[i].copy_(torch.from_numpy(L.ravel()))
+        b.right[i].copy_(torch.from_numpy(R.ravel()))
+        b.disp0[i].copy_(torch.from_numpy(d0))
+    return b
+
+
+def test_every_schedule_gives_the_same_bits(svb):
+    """The scheduling knobs the autotuner moves change time only: each value
+    of each knob reproduces lr_refine on every pair bit for bit."""
+    import torch
+    shapes = [(1, 1), (333, 201), (41, 300), (1000, 31), (256, 192), (5, 200)]
+    pairs = _pairs(svb, shapes, 4400)
+    b = _loaded_refiner(svb, pairs, **PIPE)
+    ref = [svb.refine.lr_refine(L, R, d0, W, H, tol=2.0, **PIPE) for (L, R, d0, W, H) in pairs]
+    for knob, values in svb.batch.TUNE_SPACE.items():
+        for v in values + ((256, 8192) if knob == "px_per_block" else
+                           (32,) if knob == "sgm_threads" else (1, 32) if knob == "sgm_ctas_per_sm"
+                           else (128,)):
+            cfg = svb.batch.BatchConfig.from_dict(dict(svb.batch.default_config().as_dict(),
+                                                       **{knob: v}))
+            b.config = cfg
+            b.run()
+            b.data_status()
+            for i, (ro, rs) in enumerate(ref):
+                assert np.array_equal(bits(b.out[i].cpu().numpy()), bits(ro)), (knob, v, i)
+                assert np.array_equal(b.status[i].cpu().numpy(), rs), (knob, v, i)
+    assert torch.cuda.is_available()
+
+
+def test_autotune_picks_caches_and_keeps_results(svb, tmp_path, monkeypatch):
+    monkeypatch.setenv("SV_B200_CACHE", str(tmp_path))
+    pairs = _pairs(svb, [(450, 375), (200, 150), (640, 480), (97, 61)], 4500)
+    b = _loaded_refiner(svb, pairs, **PIPE)
+    b.run()
+    want = [o.cpu().numpy().copy() for o in b.out]
+    res = b.autotune(reps=2)
+    assert not res["cached"] and res["ms"] <= res["default_ms"] and res["candidates"] >= 8
+    assert b.config.as_dict() == res["config"]
+    b.run()
+    for a, o in zip(want, b.out):
+        assert np.array_equal(bits(a), bits(o.cpu().numpy()))
+    c = _loaded_refiner(svb, pairs, **PIPE)
+    again = c.autotune()
+    assert again["cached"] and again["config"] == res["config"]
+    assert (tmp_path / "batch_tune.json").exists()
+
+
+def test_bad_schedule_rejected(svb):
+    pairs = _pairs(svb, [(64, 48)], 4600)
+    b = _loaded_refiner(svb, pairs, **PIPE)
+    b.config = svb.batch.BatchConfig(3000, 128, 8, 32)
+    with pytest.raises(ValueError):
+        b.run()

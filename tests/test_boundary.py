@@ -90,3 +90,21 @@ def test_null_and_workspace_checks(svb):
     assert rc == svb._lib.SV_ERR_WORKSPACE     # misaligned
     assert lib.sv_aggregate_path(ctypes.c_void_p(256), ctypes.c_void_p(256), 8, 8, 21, 1, 2, 2,
                                  0, ctypes.c_void_p(256), None) == svb._lib.SV_ERR_PARAM
+
+
+def test_batch_schedule_defaults_and_validation(svb):
+    """sv_batch_config_default and the argument check of
+    sv_batch_lr_refine_ex (rejected before any device work)."""
+    import ctypes
+    c = svb.batch.default_config()
+    assert c.as_dict() == {"px_per_block": 2048, "sgm_threads": 128, "sgm_ctas_per_sm": 8,
+                           "sgm_fetch": 32}
+    lib = svb._lib.load()
+    d = (svb.batch.PairDesc * 1)()
+    d[0] = svb.batch.PairDesc(1, 1, 1, 1, 1, 8, 8)
+    p = svb._lib.default_params()
+    for bad in ((3000, 128, 8, 32), (2048, 96, 8, 32), (2048, 128, 0, 32), (2048, 128, 8, 48)):
+        cfg = svb.batch.BatchConfig(*bad)
+        rc = lib.sv_batch_lr_refine_ex(d, 1, 0, 2.0, ctypes.byref(p), ctypes.byref(cfg), None, 0,
+                                       None)
+        assert rc == svb._lib.SV_ERR_PARAM, bad

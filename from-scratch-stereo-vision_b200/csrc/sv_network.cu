@@ -126,71 +126,13 @@ __global__ void k_avgpool2_f64(const double *__restrict__ img, int C, int H, int
 }
 
 // ------------------------------------------------------------- conv 2d
-// One thread per (output pixel, group of OCG output channels); blockIdx.z =
-// image * (OC / OCG) + channel group, so the small maps of this network still
-// fill the GPU.  act: 0 none, 1 leaky 0.2, 2 residual + relu0 (the
-// Refinement output, v > 0 ? v : v * 0).
-template <int IC, int OC, int OCG, int ACT>
-__global__ void __launch_bounds__(256)
-    k_conv2d(const float *__restrict__ x0, const float *__restrict__ x1, int H, int W, int OH,
-             int OW, int stride, int pad, int dil, const float *__restrict__ w,
-             const float *__restrict__ b, float *y0, float *y1, const float *__restrict__ resid) {
-    constexpr int NG = OC / OCG;
-    const int img = blockIdx.z / NG, og = blockIdx.z - img * NG;
-    __shared__ float sw[OCG * IC * 9];
-    __shared__ float sb[OCG];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    for (int i = tid; i < OCG * IC * 9; i += blockDim.x * blockDim.y)
-        sw[i] = w[og * OCG * IC * 9 + i];
-    if (tid < OCG) sb[tid] = b[og * OCG + tid];
-    __syncthreads();
-    const float *x = img ? x1 : x0;
-    float *y = img ? y1 : y0;
-    const int ox = blockIdx.x * blockDim.x + threadIdx.x;
-    const int oy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ox >= OW || oy >= OH) return;
-    float acc[OCG];
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
-    const int iy0 = oy * stride - pad, ix0 = ox * stride - pad;
-    const long HW = (long)H * W;
-#pragma unroll
-    for (int c = 0; c < IC; ++c) {
-        const float *xc = x + c * HW;
-#pragma unroll
-        for (int ky = 0; ky < 3; ++ky) {
-            const int iy = iy0 + ky * dil;
-            if (iy < 0 || iy >= H) continue;
-#pragma unroll
-            for (int kx = 0; kx < 3; ++kx) {
-                const int ix = ix0 + kx * dil;
-                if (ix < 0 || ix >= W) continue;
-                const float v = __ldg(xc + (long)iy * W + ix);
-#pragma unroll
-                for (int o = 0; o < OCG; ++o)
-                    acc[o] = fmaf(v, sw[(o * IC + c) * 9 + ky * 3 + kx], acc[o]);
-            }
-        }
-    }
-    const long OHW = (long)OH * OW, oi = (long)oy * OW + ox;
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) {
-        float v = acc[o];
-        if (ACT == 1) v = v > 0.f ? v : v * 0.2f;
-        if (ACT == 2) {
-            v = resid[oi] + v;
-            v = v > 0.f ? v : v * 0.f;
-        }
-        y[(og * OCG + o) * OHW + oi] = v;
-    }
-}
-
 // Shared-memory tiled 3x3 conv2d: a CTA of CT_TW x CT_TH threads computes a
 // CT_TW x CT_TH output tile for OCG output channels (blockIdx.z = image *
 // OC/OCG + group).  The input tile with its halo, for every input channel,
 // is staged once in shared memory (zeros outside the image, which adds
 // exactly what the reference's skipped taps add: nothing); weights are read
-// by broadcast.  Same arithmetic as k_conv2d, ~8x fewer global loads.
+// by broadcast.  act: 0 none, 1 leaky 0.2, 2 residual + relu0 (the
+// Refinement output, v > 0 ? v : v * 0).
 constexpr int CT2_TW = 32, CT2_TH = 4;
 
 template <int IC, int OC, int OCG, int ACT>
@@ -262,40 +204,51 @@ static size_t conv2d_tile_bytes(int IC, int stride, int dil) {
            ((CT2_TW - 1) * stride + 2 * dil + 1) * sizeof(float);
 }
 
-// Tiled cost volume + conv3d #1: a CTA covers 32 columns x CV_TD disparities
-// of one row for OCG output channels; fl rows y-1..y+1 and the matching fr
-// columns (shifted by every disparity the taps touch) are staged once.
-constexpr int CV_TD = 4;
+constexpr int CV_TD = 4;    // disparities per CTA of the 3-D convolutions
 
+// Cost volume + conv3d #1, staged: the CTA (32 columns x CV_TD disparities
+// of one row, OCG of the OC output channels) first writes the cost-volume tile it
+// reads -- |fl - fr(x - d)|, 2.0 where x - d < 0, 0 outside the volume --
+// into shared memory once, then every tap is one shared load and OCG FMAs.
+// CostVolume.forward (stereonet.py:771-799) fused into Conv3d #1 (596-641)
+// and its leaky ReLU; taps outside the volume are skipped, as in the
+// reference's loops.
 template <int C, int OC, int OCG>
 __global__ void __launch_bounds__(32 * CV_TD)
-    k_costvol_conv3d_tiled(const float *__restrict__ fl, const float *__restrict__ fr, int D,
-                           int h, int w, const float *__restrict__ wt,
-                           const float *__restrict__ b, float *__restrict__ y) {
-    // fr columns needed: x - d for x in [x0-1, x0+32], d in [d0-1, d0+CV_TD]
-    constexpr int FLW = 34, FRW = 34 + CV_TD + 1;
-    __shared__ float sfl[C][3][FLW];
-    __shared__ float sfr[C][3][FRW];
-    __shared__ float sw[OCG * C * 27];
+    k_costvol_conv3d_staged(const float *__restrict__ fl, const float *__restrict__ fr, int D,
+                            int h, int w, const float *__restrict__ wt,
+                            const float *__restrict__ b, float *__restrict__ y) {
+    // the weights join the tile in shared memory when both fit the static
+    // 48 KB; otherwise every lane reads the same weight through the
+    // read-only cache (one broadcast transaction)
+    constexpr bool kWs = (C * (CV_TD + 2) * 102 + OCG * C * 27 + OCG) * 4 <= 48 * 1024;
+    __shared__ float sv[C][CV_TD + 2][3][34];
+    __shared__ float sw[kWs ? OCG * C * 27 : 1];
     __shared__ float sb[OCG];
-    const int og = blockIdx.z;
-    const int x0 = blockIdx.x * 32, oy = blockIdx.y / ((D + CV_TD - 1) / CV_TD);
-    const int d0 = (blockIdx.y - oy * ((D + CV_TD - 1) / CV_TD)) * CV_TD;
+    const int og = blockIdx.z;                     // output channels og*OCG ..
+    const int nd = (D + CV_TD - 1) / CV_TD;
+    const int x0 = blockIdx.x * 32, oy = blockIdx.y / nd, d0 = (blockIdx.y - oy * nd) * CV_TD;
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int i = tid; i < OCG * C * 27; i += 32 * CV_TD) sw[i] = wt[og * OCG * C * 27 + i];
+    const float *wg = wt + og * OCG * C * 27;
+    if (kWs)
+        for (int i = tid; i < OCG * C * 27; i += 32 * CV_TD) sw[i] = wg[i];
     if (tid < OCG) sb[tid] = b[og * OCG + tid];
     const long hw = (long)h * w;
-    // sfl[c][r][j] = fl[c][oy-1+r][x0-1+j];  sfr[c][r][j] = fr[c][oy-1+r][x0-1-(d0+CV_TD)+j]
-    const int frx0 = x0 - 1 - (d0 + CV_TD);
-    for (int i = tid; i < C * 3 * FLW; i += 32 * CV_TD) {
-        const int c = i / (3 * FLW), rem = i - c * 3 * FLW, r = rem / FLW, j = rem - r * FLW;
-        const int yy = oy - 1 + r, xx = x0 - 1 + j;
-        sfl[c][r][j] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? __ldg(fl + c * hw + yy * w + xx) : 0.f;
-    }
-    for (int i = tid; i < C * 3 * FRW; i += 32 * CV_TD) {
-        const int c = i / (3 * FRW), rem = i - c * 3 * FRW, r = rem / FRW, j = rem - r * FRW;
-        const int yy = oy - 1 + r, xx = frx0 + j;
-        sfr[c][r][j] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? __ldg(fr + c * hw + yy * w + xx) : 0.f;
+    constexpr int PLANE = (CV_TD + 2) * 3 * 34;
+    for (int i = tid; i < C * PLANE; i += 32 * CV_TD) {
+        const int c = i / PLANE, rem = i - c * PLANE;
+        const int dz = rem / 102, rem2 = rem - dz * 102, r = rem2 / 34, j = rem2 - r * 34;
+        const int dd = d0 - 1 + dz, yy = oy - 1 + r, xx = x0 - 1 + j;
+        float v = 0.f;
+        if (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w) {
+            if (xx - dd < 0) {
+                v = 2.0f;
+            } else {
+                const long row = c * hw + (long)yy * w;
+                v = fabsf(__ldg(fl + row + xx) - __ldg(fr + row + xx - dd));
+            }
+        }
+        sv[c][dz][r][j] = v;
     }
     __syncthreads();
     const int ox = x0 + threadIdx.x, od = d0 + threadIdx.y;
@@ -312,20 +265,17 @@ __global__ void __launch_bounds__(32 * CV_TD)
             for (int ky = 0; ky < 3; ++ky) {
                 const int yy = oy + ky - 1;
                 if (yy < 0 || yy >= h) continue;
+                const float *row = &sv[c][threadIdx.y + kd][ky][threadIdx.x];
 #pragma unroll
                 for (int kx = 0; kx < 3; ++kx) {
                     const int xx = ox + kx - 1;
                     if (xx < 0 || xx >= w) continue;
-                    float v;
-                    if (xx - dd < 0) {
-                        v = 2.0f;
-                    } else {
-                        // fl at column xx -> sfl index xx - (x0-1); fr at xx-dd -> xx-dd-frx0
-                        v = fabsf(sfl[c][ky][xx - x0 + 1] - sfr[c][ky][xx - dd - frx0]);
-                    }
+                    const float v = row[kx];
 #pragma unroll
-                    for (int o = 0; o < OCG; ++o)
-                        acc[o] = fmaf(v, sw[(o * C + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
+                    for (int o = 0; o < OCG; ++o) {
+                        const int wi = (o * C + c) * 27 + kd * 9 + ky * 3 + kx;
+                        acc[o] = fmaf(v, kWs ? sw[wi] : __ldg(wg + wi), acc[o]);
+                    }
                 }
             }
         }
@@ -389,116 +339,6 @@ __global__ void __launch_bounds__(32 * CV_TD)
         }
     }
     const long idx = (long)od * hw + (long)oy * w + ox;
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) {
-        const float v = acc[o];
-        y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
-    }
-}
-
-// -------------------------------------------------- cost volume + conv3d #1
-// CostVolume.forward (stereonet.py:771-799) fused into Conv3d #1 (596-641)
-// and its leaky ReLU: each tap of the 3x3x3 window reads |fl - fr(x-d)|
-// (2.0 where x-d < 0), zero outside the volume (same padding).  One thread
-// per (voxel, OCG output channels); blockIdx.y is the channel group.
-template <int C, int OC, int OCG>
-__global__ void __launch_bounds__(128)
-    k_costvol_conv3d(const float *__restrict__ fl, const float *__restrict__ fr, int D, int h,
-                     int w, const float *__restrict__ wt, const float *__restrict__ b,
-                     float *__restrict__ y) {
-    const int og = blockIdx.y;
-    __shared__ float sw[OCG * C * 27];
-    __shared__ float sb[OCG];
-    for (int i = threadIdx.x; i < OCG * C * 27; i += blockDim.x) sw[i] = wt[og * OCG * C * 27 + i];
-    if (threadIdx.x < OCG) sb[threadIdx.x] = b[og * OCG + threadIdx.x];
-    __syncthreads();
-    const long hw = (long)h * w;
-    const long total = (long)D * hw;
-    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (idx >= total) return;
-    const int od = (int)(idx / hw);
-    const int rem = (int)(idx - od * hw);
-    const int oy = rem / w, ox = rem - (rem / w) * w;
-    float acc[OCG];
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
-    for (int c = 0; c < C; ++c) {
-        const float *flc = fl + c * hw, *frc = fr + c * hw;
-#pragma unroll
-        for (int kd = 0; kd < 3; ++kd) {
-            const int dd = od + kd - 1;
-            if (dd < 0 || dd >= D) continue;
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky) {
-                const int yy = oy + ky - 1;
-                if (yy < 0 || yy >= h) continue;
-#pragma unroll
-                for (int kx = 0; kx < 3; ++kx) {
-                    const int xx = ox + kx - 1;
-                    if (xx < 0 || xx >= w) continue;
-                    float v;
-                    if (xx - dd < 0) {
-                        v = 2.0f;
-                    } else {
-                        v = fabsf(__ldg(flc + yy * w + xx) - __ldg(frc + yy * w + xx - dd));
-                    }
-#pragma unroll
-                    for (int o = 0; o < OCG; ++o)
-                        acc[o] = fmaf(v, sw[(o * C + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) {
-        const float v = acc[o];
-        y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
-    }
-}
-
-// ---------------------------------------------------------- conv3d #2
-template <int IC, int OC, int OCG>
-__global__ void __launch_bounds__(128)
-    k_conv3d(const float *__restrict__ x, int D, int h, int w, const float *__restrict__ wt,
-             const float *__restrict__ b, float *__restrict__ y) {
-    const int og = blockIdx.y;
-    __shared__ float sw[OCG * IC * 27];
-    __shared__ float sb[OCG];
-    for (int i = threadIdx.x; i < OCG * IC * 27; i += blockDim.x) sw[i] = wt[og * OCG * IC * 27 + i];
-    if (threadIdx.x < OCG) sb[threadIdx.x] = b[og * OCG + threadIdx.x];
-    __syncthreads();
-    const long hw = (long)h * w;
-    const long total = (long)D * hw;
-    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
-    if (idx >= total) return;
-    const int od = (int)(idx / hw);
-    const int rem = (int)(idx - od * hw);
-    const int oy = rem / w, ox = rem - (rem / w) * w;
-    float acc[OCG];
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
-    for (int c = 0; c < IC; ++c) {
-        const float *xc = x + c * total;
-#pragma unroll
-        for (int kd = 0; kd < 3; ++kd) {
-            const int dd = od + kd - 1;
-            if (dd < 0 || dd >= D) continue;
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky) {
-                const int yy = oy + ky - 1;
-                if (yy < 0 || yy >= h) continue;
-#pragma unroll
-                for (int kx = 0; kx < 3; ++kx) {
-                    const int xx = ox + kx - 1;
-                    if (xx < 0 || xx >= w) continue;
-                    const float v = __ldg(xc + dd * hw + yy * w + xx);
-#pragma unroll
-                    for (int o = 0; o < OCG; ++o)
-                        acc[o] = fmaf(v, sw[(o * IC + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
-                }
-            }
-        }
-    }
 #pragma unroll
     for (int o = 0; o < OCG; ++o) {
         const float v = acc[o];
@@ -773,7 +613,7 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         constexpr int CG = CM % 2 == 0 ? 2 : CM;
         const dim3 vgrid((w + 31) / 32, h * ((D + CV_TD - 1) / CV_TD), CM / CG);
         count_launch();
-        k_costvol_conv3d_tiled<C, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(
+        k_costvol_conv3d_staged<C, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(
             b.fb[0], b.fb[1], D, h, w, n.cw[0], n.cb[0], b.v0);
         count_launch();
         k_conv3d_tiled<CM, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(b.v0, D, h, w, n.cw[1],

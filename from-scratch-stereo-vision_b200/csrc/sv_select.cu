@@ -9,7 +9,8 @@
 // (warp-aggregated), adds its non-zero bins into a global histogram, and the
 // last CTA to finish (a device-scope counter) scans that histogram, picks the
 // bin holding the rank and extends the prefix.  One launch per pass; after
-// pass 5 the prefix is the key.
+// pass 5 the prefix is the key.  Up to 16,384 values (the probe) the six
+// passes run in one CTA over keys kept in shared memory (k_sel_small).
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
@@ -123,11 +124,112 @@ __global__ void __launch_bounds__(1024)
     }
 }
 
+// Small inputs (the probe's few thousand values): one CTA keeps every key in
+// shared memory and runs the six passes there, one launch instead of seven.
+constexpr long SEL_SMALL_CAP = 16384;     // keys (128 KB of dynamic shared memory)
+
+__global__ void __launch_bounds__(1024)
+    k_sel_small(const double *__restrict__ x, long n, long long rank0, SelState *__restrict__ s) {
+    extern __shared__ __align__(16) unsigned long long keys[];
+    __shared__ unsigned hist[SEL_NB];
+    __shared__ unsigned wsum[32];
+    __shared__ unsigned long long s_prefix;
+    __shared__ long long s_rank;
+    __shared__ int owner;
+    __shared__ unsigned long long owner_excl;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
+    for (long i = t; i < n; i += nt) keys[i] = sel_key(x[i]);
+    if (t == 0) {
+        s_prefix = 0ull;
+        s_rank = rank0;
+    }
+    for (int pass = 0; pass < SEL_NPASS; ++pass) {
+        const int shift = kSelShift[pass], bits = kSelBits[pass], top = shift + bits;
+        const unsigned mask = (1u << bits) - 1u;
+        for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
+        __syncthreads();
+        const unsigned long long pre = s_prefix;
+        for (long i0 = 0; i0 < n; i0 += nt) {
+            const long i = i0 + t;
+            unsigned digit = 0xffffffffu;
+            if (i < n) {
+                const unsigned long long k = keys[i];
+                if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
+            }
+            const unsigned same = __match_any_sync(kFull, digit);
+            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
+                atomicAdd(&hist[digit], __popc(same));
+        }
+        __syncthreads();
+        const int per = SEL_NB / nt;
+        unsigned long long loc = 0;
+        for (int j = 0; j < per; ++j) loc += hist[t * per + j];
+        unsigned long long incl = loc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[wid] = (unsigned)incl;
+        __syncthreads();
+        if (wid == 0) {
+            const int nw = nt >> 5;
+            unsigned long long w = lane < nw ? wsum[lane] : 0ull, v = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(kFull, v, o);
+                if (lane >= o) v += y;
+            }
+            if (lane < nw) wsum[lane] = (unsigned)(v - w);
+        }
+        __syncthreads();
+        const long long rank = s_rank;
+        const long long excl = (long long)(wsum[wid] + incl - loc);
+        if (rank >= excl && rank < excl + (long long)loc) {
+            owner = t;
+            owner_excl = (unsigned long long)excl;
+        }
+        __syncthreads();
+        if (t == owner) {
+            long long rr = rank - (long long)owner_excl;
+            int b = t * per;
+            for (int j = 0; j < per; ++j) {
+                const long long c = hist[t * per + j];
+                if (rr < c) { b = t * per + j; break; }
+                rr -= c;
+            }
+            s_prefix = pre | ((unsigned long long)b << shift);
+            s_rank = rr;
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        s->prefix = s_prefix;
+        s->rank = s_rank;
+        s->value = sel_unkey(s_prefix);
+    }
+}
+
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st) {
     if (n < 1 || n >= (1l << 32) || rank < 0 || rank >= n) {
         set_error("select: n=%ld rank=%lld", n, rank);
         return SV_ERR_PARAM;
+    }
+    if (n <= SEL_SMALL_CAP) {
+        int dev = 0;
+        SV_CUDA_TRY(cudaGetDevice(&dev));
+        static bool ready[64] = {false};
+        if (dev >= 64 || !ready[dev]) {
+            SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
+            if (dev < 64) ready[dev] = true;
+        }
+        count_launch();
+        k_sel_small<<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(x, n, rank, state);
+        SV_LAUNCH_CHECK();
+        return SV_OK;
     }
     SV_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)SEL_NPASS * SEL_NB * sizeof(unsigned), st));
     count_launch();

@@ -27,6 +27,9 @@ struct SelState {
     long long rank;
     double value;
     unsigned done[SEL_NPASS];          // CTAs finished per pass
+    unsigned cdone;                    // CTAs finished in the compaction
+    unsigned count;                    // keys left after pass 1
+    unsigned finished;                 // the compaction's last CTA completed the select
 };
 
 __device__ __forceinline__ unsigned long long sel_key(double d) {
@@ -43,6 +46,9 @@ __global__ void k_sel_init(SelState *s, long long rank) {
     s->rank = rank;
     s->value = 0.0;
     for (int p = 0; p < SEL_NPASS; ++p) s->done[p] = 0u;
+    s->cdone = 0u;
+    s->count = 0u;
+    s->finished = 0u;
 }
 
 __global__ void __launch_bounds__(1024)
@@ -54,6 +60,7 @@ __global__ void __launch_bounds__(1024)
     __shared__ unsigned long long owner_excl;
     __shared__ bool last;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
+    if (*(volatile unsigned *)&s->finished) return;   // done from the compacted keys
     const int shift = kSelShift[pass], bits = kSelBits[pass];
     const int top = shift + bits;
     const unsigned mask = (1u << bits) - 1u;
@@ -121,6 +128,142 @@ __global__ void __launch_bounds__(1024)
         s->prefix |= (unsigned long long)b << shift;
         s->rank = r;
         if (pass == SEL_NPASS - 1) s->value = sel_unkey(s->prefix);
+    }
+}
+
+// After pass 1 the 22 top key bits are fixed and usually only a few hundred
+// keys still match.  k_sel_compact gathers them (warp-aggregated appends);
+// the last CTA to finish, when they fit in its shared memory, runs passes
+// 2..5 over them there and marks the select finished, so the four remaining
+// pass launches return at once.  Too many matches (a plateau of equal
+// values) leaves the select to those passes.
+constexpr int SEL_CAND_CAP = 4096;
+
+__device__ void sel_passes_smem(const unsigned long long *keys, long n, int pass0,
+                                unsigned long long &prefix, long long &rank, unsigned *hist,
+                                unsigned *wsum, int *owner, unsigned long long *owner_excl,
+                                unsigned long long *s_prefix, long long *s_rank) {
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
+    if (t == 0) {
+        *s_prefix = prefix;
+        *s_rank = rank;
+    }
+    __syncthreads();
+    for (int pass = pass0; pass < SEL_NPASS; ++pass) {
+        const int shift = kSelShift[pass], bits = kSelBits[pass], top = shift + bits;
+        const unsigned mask = (1u << bits) - 1u;
+        for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
+        __syncthreads();
+        const unsigned long long pre = *s_prefix;
+        for (long i0 = 0; i0 < n; i0 += nt) {
+            const long i = i0 + t;
+            unsigned digit = 0xffffffffu;
+            if (i < n) {
+                const unsigned long long k = keys[i];
+                if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
+            }
+            const unsigned same = __match_any_sync(kFull, digit);
+            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
+                atomicAdd(&hist[digit], __popc(same));
+        }
+        __syncthreads();
+        const int per = SEL_NB / nt;
+        unsigned long long loc = 0;
+        for (int j = 0; j < per; ++j) loc += hist[t * per + j];
+        unsigned long long incl = loc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[wid] = (unsigned)incl;
+        __syncthreads();
+        if (wid == 0) {
+            const int nw = nt >> 5;
+            unsigned long long w = lane < nw ? wsum[lane] : 0ull, v = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(kFull, v, o);
+                if (lane >= o) v += y;
+            }
+            if (lane < nw) wsum[lane] = (unsigned)(v - w);
+        }
+        __syncthreads();
+        const long long rk = *s_rank;
+        const long long excl = (long long)(wsum[wid] + incl - loc);
+        if (rk >= excl && rk < excl + (long long)loc) {
+            *owner = t;
+            *owner_excl = (unsigned long long)excl;
+        }
+        __syncthreads();
+        if (t == *owner) {
+            long long rr = rk - (long long)*owner_excl;
+            int b = t * per;
+            for (int j = 0; j < per; ++j) {
+                const long long c = hist[t * per + j];
+                if (rr < c) { b = t * per + j; break; }
+                rr -= c;
+            }
+            *s_prefix = pre | ((unsigned long long)b << shift);
+            *s_rank = rr;
+        }
+        __syncthreads();
+    }
+    prefix = *s_prefix;
+    rank = *s_rank;
+}
+
+__global__ void __launch_bounds__(1024)
+    k_sel_compact(const double *__restrict__ x, long n, SelState *__restrict__ s,
+                  unsigned long long *__restrict__ cand) {
+    __shared__ unsigned long long keys[SEL_CAND_CAP];
+    __shared__ unsigned hist[SEL_NB];
+    __shared__ unsigned wsum[32];
+    __shared__ int owner;
+    __shared__ unsigned long long owner_excl, s_prefix;
+    __shared__ long long s_rank;
+    __shared__ bool last;
+    const int t = threadIdx.x, lane = t & 31, nt = blockDim.x;
+    const int top = kSelShift[1];                    // bits above pass 2's digit are fixed
+    const unsigned long long pre = s->prefix;
+    const long stride = (long)gridDim.x * nt;
+    for (long i0 = blockIdx.x * (long)nt; i0 < n; i0 += stride) {
+        const long i = i0 + t;
+        unsigned long long k = 0;
+        bool hit = false;
+        if (i < n) {
+            k = sel_key(x[i]);
+            hit = (k >> top) == (pre >> top);
+        }
+        const unsigned m = __ballot_sync(kFull, hit);
+        if (m) {
+            unsigned base = 0;
+            if (lane == __ffs(m) - 1) base = atomicAdd(&s->count, __popc(m));
+            base = __shfl_sync(kFull, base, __ffs(m) - 1);
+            const unsigned pos = base + __popc(m & ((1u << lane) - 1u));
+            if (hit && pos < SEL_CAND_CAP) cand[pos] = k;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(&s->cdone, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const unsigned cnt = __ldcg(&s->count);
+    if (cnt > (unsigned)SEL_CAND_CAP) return;       // the pass launches finish the select
+    for (unsigned i = t; i < cnt; i += nt) keys[i] = __ldcg(cand + i);
+    __syncthreads();
+    unsigned long long prefix = s->prefix;
+    long long rank = s->rank;
+    sel_passes_smem(keys, cnt, 2, prefix, rank, hist, wsum, &owner, &owner_excl, &s_prefix,
+                    &s_rank);
+    if (t == 0) {
+        s->prefix = prefix;
+        s->rank = rank;
+        s->value = sel_unkey(prefix);
+        __threadfence();
+        s->finished = 1u;
     }
 }
 
@@ -235,7 +378,14 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
     count_launch();
     k_sel_init<<<1, 1, 0, st>>>(state, rank);
     const int blocks = grid_for(n, 1024 * 4, 148);
+    // the candidates follow the six histograms (8-byte aligned: 6 x 2048 words)
+    unsigned long long *cand =
+        reinterpret_cast<unsigned long long *>(hist + (size_t)SEL_NPASS * SEL_NB);
     for (int p = 0; p < SEL_NPASS; ++p) {
+        if (p == 2) {
+            count_launch();
+            k_sel_compact<<<blocks, 1024, 0, st>>>(x, n, state, cand);
+        }
         count_launch();
         k_sel_pass<<<blocks, 1024, 0, st>>>(x, n, p, state, hist + (size_t)p * SEL_NB);
     }
@@ -245,7 +395,7 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
 
 size_t select_state_bytes() { return sizeof(SelState); }
 size_t select_value_offset() { return offsetof(SelState, value); }
-size_t select_hist_words() { return (size_t)SEL_NPASS * SEL_NB; }
+size_t select_hist_words() { return (size_t)SEL_NPASS * SEL_NB + 2 * (size_t)SEL_CAND_CAP; }
 
 }  // namespace sv
 

@@ -39,3 +39,16 @@ def test_peak_matches_sorted(svb, n):
 def test_peak_rejects_bad_q(svb):
     with pytest.raises(ValueError):
         svb.network._peak(np.ones(10), 1.0)
+
+
+@pytest.mark.parametrize("plateau", [0, 3000, 5000, 40000])
+def test_peak_with_plateau_at_the_quantile(svb, plateau):
+    """Many equal values at the 95% quantile: up to 4096 matches after the
+    second pass finish in one CTA, more take the remaining passes."""
+    rng = np.random.default_rng(plateau + 1)
+    n = 168750
+    d = rng.uniform(0.0, 80.0, n)
+    if plateau:
+        d[rng.choice(n, size=plateau, replace=False)] = 60.0 + 1.0 / 3.0
+    for q in (0.95, 0.9):
+        assert svb.network._peak(d, q) == ref_peak(d, q), (plateau, q)

@@ -8,9 +8,11 @@
 // that match the prefix chosen so far into 2048 shared-memory bins
 // (warp-aggregated), adds its non-zero bins into a global histogram, and the
 // last CTA to finish (a device-scope counter) scans that histogram, picks the
-// bin holding the rank and extends the prefix.  One launch per pass; after
-// pass 5 the prefix is the key.  Up to 16,384 values (the probe) the six
-// passes run in one CTA over keys kept in shared memory (k_sel_small).
+// bin holding the rank and extends the prefix.  Passes 0 and 1 are one launch
+// each; passes 2..5 run in one CTA over the few keys that still match
+// (k_sel_compact); after pass 5 the prefix is the key.  Up to 16,384 values
+// (the probe) all six passes run in one CTA over keys kept in shared memory
+// (k_sel_small).
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
@@ -29,7 +31,6 @@ struct SelState {
     unsigned done[SEL_NPASS];          // CTAs finished per pass
     unsigned cdone;                    // CTAs finished in the compaction
     unsigned count;                    // keys left after pass 1
-    unsigned finished;                 // the compaction's last CTA completed the select
 };
 
 __device__ __forceinline__ unsigned long long sel_key(double d) {
@@ -48,7 +49,6 @@ __global__ void k_sel_init(SelState *s, long long rank) {
     for (int p = 0; p < SEL_NPASS; ++p) s->done[p] = 0u;
     s->cdone = 0u;
     s->count = 0u;
-    s->finished = 0u;
 }
 
 __global__ void __launch_bounds__(1024)
@@ -60,7 +60,6 @@ __global__ void __launch_bounds__(1024)
     __shared__ unsigned long long owner_excl;
     __shared__ bool last;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
-    if (*(volatile unsigned *)&s->finished) return;   // done from the compacted keys
     const int shift = kSelShift[pass], bits = kSelBits[pass];
     const int top = shift + bits;
     const unsigned mask = (1u << bits) - 1u;
@@ -133,16 +132,18 @@ __global__ void __launch_bounds__(1024)
 
 // After pass 1 the 22 top key bits are fixed and usually only a few hundred
 // keys still match.  k_sel_compact gathers them (warp-aggregated appends);
-// the last CTA to finish, when they fit in its shared memory, runs passes
-// 2..5 over them there and marks the select finished, so the four remaining
-// pass launches return at once.  Too many matches (a plateau of equal
-// values) leaves the select to those passes.
-constexpr int SEL_CAND_CAP = 4096;
+// the last CTA to finish runs passes 2..5 over them in its shared memory,
+// or, when more than SEL_CAND_CAP match (a plateau of equal values), over
+// all n values read again from global memory, filtered by the prefix.
+constexpr int SEL_CAND_CAP = 16384;      // keys (128 KB of dynamic shared memory)
 
-__device__ void sel_passes_smem(const unsigned long long *keys, long n, int pass0,
-                                unsigned long long &prefix, long long &rank, unsigned *hist,
-                                unsigned *wsum, int *owner, unsigned long long *owner_excl,
-                                unsigned long long *s_prefix, long long *s_rank) {
+// Passes pass0..5 in one CTA over `keys` (shared memory), or, when keys is
+// NULL, over sel_key(x[i]) for all n values read from global memory.
+__device__ void sel_passes_cta(const unsigned long long *keys, const double *__restrict__ x,
+                               long n, int pass0, unsigned long long &prefix, long long &rank,
+                               unsigned *hist, unsigned *wsum, int *owner,
+                               unsigned long long *owner_excl, unsigned long long *s_prefix,
+                               long long *s_rank) {
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
     if (t == 0) {
         *s_prefix = prefix;
@@ -159,7 +160,7 @@ __device__ void sel_passes_smem(const unsigned long long *keys, long n, int pass
             const long i = i0 + t;
             unsigned digit = 0xffffffffu;
             if (i < n) {
-                const unsigned long long k = keys[i];
+                const unsigned long long k = keys ? keys[i] : sel_key(x[i]);
                 if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
             }
             const unsigned same = __match_any_sync(kFull, digit);
@@ -216,7 +217,7 @@ __device__ void sel_passes_smem(const unsigned long long *keys, long n, int pass
 __global__ void __launch_bounds__(1024)
     k_sel_compact(const double *__restrict__ x, long n, SelState *__restrict__ s,
                   unsigned long long *__restrict__ cand) {
-    __shared__ unsigned long long keys[SEL_CAND_CAP];
+    extern __shared__ __align__(16) unsigned long long keys[];   // SEL_CAND_CAP
     __shared__ unsigned hist[SEL_NB];
     __shared__ unsigned wsum[32];
     __shared__ int owner;
@@ -251,19 +252,20 @@ __global__ void __launch_bounds__(1024)
     if (!last) return;
     __threadfence();
     const unsigned cnt = __ldcg(&s->count);
-    if (cnt > (unsigned)SEL_CAND_CAP) return;       // the pass launches finish the select
-    for (unsigned i = t; i < cnt; i += nt) keys[i] = __ldcg(cand + i);
+    const bool fits = cnt <= (unsigned)SEL_CAND_CAP;
+    if (fits)
+        for (unsigned i = t; i < cnt; i += nt) keys[i] = __ldcg(cand + i);
     __syncthreads();
     unsigned long long prefix = s->prefix;
     long long rank = s->rank;
-    sel_passes_smem(keys, cnt, 2, prefix, rank, hist, wsum, &owner, &owner_excl, &s_prefix,
-                    &s_rank);
+    // a bucket too large for shared memory (a plateau of equal values) is
+    // finished by this CTA from all n values, filtered by the prefix
+    sel_passes_cta(fits ? keys : nullptr, x, fits ? (long)cnt : n, 2, prefix, rank, hist, wsum,
+                   &owner, &owner_excl, &s_prefix, &s_rank);
     if (t == 0) {
         s->prefix = prefix;
         s->rank = rank;
         s->value = sel_unkey(prefix);
-        __threadfence();
-        s->finished = 1u;
     }
 }
 
@@ -276,80 +278,19 @@ __global__ void __launch_bounds__(1024)
     extern __shared__ __align__(16) unsigned long long keys[];
     __shared__ unsigned hist[SEL_NB];
     __shared__ unsigned wsum[32];
-    __shared__ unsigned long long s_prefix;
-    __shared__ long long s_rank;
     __shared__ int owner;
-    __shared__ unsigned long long owner_excl;
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
-    for (long i = t; i < n; i += nt) keys[i] = sel_key(x[i]);
-    if (t == 0) {
-        s_prefix = 0ull;
-        s_rank = rank0;
-    }
-    for (int pass = 0; pass < SEL_NPASS; ++pass) {
-        const int shift = kSelShift[pass], bits = kSelBits[pass], top = shift + bits;
-        const unsigned mask = (1u << bits) - 1u;
-        for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
-        __syncthreads();
-        const unsigned long long pre = s_prefix;
-        for (long i0 = 0; i0 < n; i0 += nt) {
-            const long i = i0 + t;
-            unsigned digit = 0xffffffffu;
-            if (i < n) {
-                const unsigned long long k = keys[i];
-                if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
-            }
-            const unsigned same = __match_any_sync(kFull, digit);
-            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
-                atomicAdd(&hist[digit], __popc(same));
-        }
-        __syncthreads();
-        const int per = SEL_NB / nt;
-        unsigned long long loc = 0;
-        for (int j = 0; j < per; ++j) loc += hist[t * per + j];
-        unsigned long long incl = loc;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long y = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) wsum[wid] = (unsigned)incl;
-        __syncthreads();
-        if (wid == 0) {
-            const int nw = nt >> 5;
-            unsigned long long w = lane < nw ? wsum[lane] : 0ull, v = w;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned long long y = __shfl_up_sync(kFull, v, o);
-                if (lane >= o) v += y;
-            }
-            if (lane < nw) wsum[lane] = (unsigned)(v - w);
-        }
-        __syncthreads();
-        const long long rank = s_rank;
-        const long long excl = (long long)(wsum[wid] + incl - loc);
-        if (rank >= excl && rank < excl + (long long)loc) {
-            owner = t;
-            owner_excl = (unsigned long long)excl;
-        }
-        __syncthreads();
-        if (t == owner) {
-            long long rr = rank - (long long)owner_excl;
-            int b = t * per;
-            for (int j = 0; j < per; ++j) {
-                const long long c = hist[t * per + j];
-                if (rr < c) { b = t * per + j; break; }
-                rr -= c;
-            }
-            s_prefix = pre | ((unsigned long long)b << shift);
-            s_rank = rr;
-        }
-        __syncthreads();
-    }
-    if (t == 0) {
-        s->prefix = s_prefix;
-        s->rank = s_rank;
-        s->value = sel_unkey(s_prefix);
+    __shared__ unsigned long long owner_excl, s_prefix;
+    __shared__ long long s_rank;
+    for (long i = threadIdx.x; i < n; i += blockDim.x) keys[i] = sel_key(x[i]);
+    __syncthreads();
+    unsigned long long prefix = 0ull;
+    long long rank = rank0;
+    sel_passes_cta(keys, nullptr, n, 0, prefix, rank, hist, wsum, &owner, &owner_excl, &s_prefix,
+                   &s_rank);
+    if (threadIdx.x == 0) {
+        s->prefix = prefix;
+        s->rank = rank;
+        s->value = sel_unkey(prefix);
     }
 }
 
@@ -359,7 +300,7 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
         set_error("select: n=%ld rank=%lld", n, rank);
         return SV_ERR_PARAM;
     }
-    if (n <= SEL_SMALL_CAP) {
+    {
         int dev = 0;
         SV_CUDA_TRY(cudaGetDevice(&dev));
         static bool ready[64] = {false};
@@ -367,35 +308,38 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
             SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
+            SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_compact,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(SEL_CAND_CAP * sizeof(unsigned long long))));
             if (dev < 64) ready[dev] = true;
         }
+    }
+    if (n <= SEL_SMALL_CAP) {
         count_launch();
         k_sel_small<<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(x, n, rank, state);
         SV_LAUNCH_CHECK();
         return SV_OK;
     }
-    SV_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)SEL_NPASS * SEL_NB * sizeof(unsigned), st));
+    SV_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)2 * SEL_NB * sizeof(unsigned), st));
     count_launch();
     k_sel_init<<<1, 1, 0, st>>>(state, rank);
     const int blocks = grid_for(n, 1024 * 4, 148);
-    // the candidates follow the six histograms (8-byte aligned: 6 x 2048 words)
-    unsigned long long *cand =
-        reinterpret_cast<unsigned long long *>(hist + (size_t)SEL_NPASS * SEL_NB);
-    for (int p = 0; p < SEL_NPASS; ++p) {
-        if (p == 2) {
-            count_launch();
-            k_sel_compact<<<blocks, 1024, 0, st>>>(x, n, state, cand);
-        }
+    // the candidates follow the two global histograms (8-byte aligned)
+    unsigned long long *cand = reinterpret_cast<unsigned long long *>(hist + 2 * SEL_NB);
+    for (int p = 0; p < 2; ++p) {
         count_launch();
         k_sel_pass<<<blocks, 1024, 0, st>>>(x, n, p, state, hist + (size_t)p * SEL_NB);
     }
+    count_launch();
+    k_sel_compact<<<blocks, 1024, (size_t)SEL_CAND_CAP * sizeof(unsigned long long), st>>>(
+        x, n, state, cand);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
 
 size_t select_state_bytes() { return sizeof(SelState); }
 size_t select_value_offset() { return offsetof(SelState, value); }
-size_t select_hist_words() { return (size_t)SEL_NPASS * SEL_NB + 2 * (size_t)SEL_CAND_CAP; }
+size_t select_hist_words() { return 2 * (size_t)SEL_NB + 2 * (size_t)SEL_CAND_CAP; }
 
 }  // namespace sv
 

@@ -42,7 +42,9 @@ __device__ __forceinline__ double sel_unkey(unsigned long long k) {
     return __longlong_as_double((long long)b);
 }
 
-__global__ void k_sel_init(SelState *s, long long rank) {
+__global__ void k_sel_init(SelState *s, long long rank, unsigned *hist) {
+    for (int i = threadIdx.x; i < 2 * SEL_NB; i += blockDim.x) hist[i] = 0u;
+    if (threadIdx.x) return;
     s->prefix = 0ull;
     s->rank = rank;
     s->value = 0.0;
@@ -320,9 +322,8 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
         SV_LAUNCH_CHECK();
         return SV_OK;
     }
-    SV_CUDA_TRY(cudaMemsetAsync(hist, 0, (size_t)2 * SEL_NB * sizeof(unsigned), st));
     count_launch();
-    k_sel_init<<<1, 1, 0, st>>>(state, rank);
+    k_sel_init<<<1, 1024, 0, st>>>(state, rank, hist);       // also clears the histograms
     const int blocks = grid_for(n, 1024 * 4, 148);
     // the candidates follow the two global histograms (8-byte aligned)
     unsigned long long *cand = reinterpret_cast<unsigned long long *>(hist + 2 * SEL_NB);

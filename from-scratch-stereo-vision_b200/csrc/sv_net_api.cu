@@ -238,12 +238,28 @@ static void work_dims(int W, int H, int work, int *Ww, int *Hw) {
     *Hw = hw < 8 ? 8 : hw;
 }
 
-// Read back the selected peak (the one host synchronisation of a stage).
+// Read back the selected peak (the one host synchronisation of a stage),
+// through a pinned 8-byte slot per host thread (a copy into pageable memory
+// is staged by the driver and returns later); the stack is the fallback if
+// the slot cannot be had.
 static int fetch_peak(const PredictWs &w, cudaStream_t st, double *peak) {
-    double v = 0.0;
-    SV_CUDA_TRY(cudaMemcpyAsync(&v, reinterpret_cast<const char *>(w.sel) + select_value_offset(),
+    struct Slot {
+        double *p = nullptr;
+        ~Slot() {
+            if (p) cudaFreeHost(p);
+        }
+    };
+    static thread_local Slot slot;
+    if (!slot.p && cudaMallocHost(reinterpret_cast<void **>(&slot.p), sizeof(double)) != cudaSuccess) {
+        slot.p = nullptr;
+        cudaGetLastError();
+    }
+    double local = 0.0;
+    double *dst = slot.p ? slot.p : &local;
+    SV_CUDA_TRY(cudaMemcpyAsync(dst, reinterpret_cast<const char *>(w.sel) + select_value_offset(),
                                 sizeof(double), cudaMemcpyDeviceToHost, st));
     SV_CUDA_TRY(cudaStreamSynchronize(st));
+    const double v = *dst;
     *peak = v > 0.5 ? v : 0.5;                      // _peak's floor
     return SV_OK;
 }

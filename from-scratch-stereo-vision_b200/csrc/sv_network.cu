@@ -199,6 +199,74 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH)
     }
 }
 
+// A Refinement level's first convolution (2 -> RC, stride 1, dilation dil,
+// leaky ReLU) with the level's input built while staging: channel 0 is
+// 2 * bilinear(prev) (BilinearUpsample.forward's half-pixel taps, FP64
+// weights, and StereoNet.forward's x2, stereonet.py:1224-1229) and channel 1
+// the guide, computed for every tile position (halo included), 0 outside the
+// image.  The CTAs of channel group 0 also store channel 0 of
+// their inner tile into rin0, the residual the level's last convolution adds.
+template <int RC, int OCG>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH)
+    k_conv2d_up(const float *__restrict__ prev, int ph, int pw, const float *__restrict__ guide,
+                int H, int W, int dil, const float *__restrict__ w, const float *__restrict__ b,
+                float *__restrict__ y, float *__restrict__ rin0) {
+    constexpr int IC = 2, NG = RC / OCG;
+    extern __shared__ __align__(16) float tile[];
+    __shared__ float sw[OCG * IC * 9];
+    __shared__ float sb[OCG];
+    const int og = blockIdx.z % NG;
+    const int tid = threadIdx.y * CT2_TW + threadIdx.x;
+    for (int i = tid; i < OCG * IC * 9; i += CT2_TW * CT2_TH) sw[i] = w[og * OCG * IC * 9 + i];
+    if (tid < OCG) sb[tid] = b[og * OCG + tid];
+    const int ox0 = blockIdx.x * CT2_TW, oy0 = blockIdx.y * CT2_TH;
+    const int ix0 = ox0 - dil, iy0 = oy0 - dil;
+    const int tw = CT2_TW + 2 * dil, th = CT2_TH + 2 * dil;
+    for (int i = tid; i < th * tw; i += CT2_TW * CT2_TH) {
+        const int ty = i / tw, tx = i - ty * tw;
+        const int gy = iy0 + ty, gx = ix0 + tx;
+        float v0 = 0.f, v1 = 0.f;
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W) {
+            const Taps t = bilinear_taps(gy, gx, ph, pw, H, W);
+            const float v = __ldg(prev + t.i00) * (float)t.w00 + __ldg(prev + t.i01) * (float)t.w01 +
+                            __ldg(prev + t.i10) * (float)t.w10 + __ldg(prev + t.i11) * (float)t.w11;
+            v0 = v * 2.0f;
+            v1 = __ldg(guide + (long)gy * W + gx);
+            if (og == 0 && ty >= dil && ty < dil + CT2_TH && tx >= dil && tx < dil + CT2_TW)
+                rin0[(long)gy * W + gx] = v0;
+        }
+        tile[i] = v0;
+        tile[th * tw + i] = v1;
+    }
+    __syncthreads();
+    const int ox = ox0 + threadIdx.x, oy = oy0 + threadIdx.y;
+    if (ox >= W || oy >= H) return;
+    float acc[OCG];
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
+#pragma unroll
+    for (int c = 0; c < IC; ++c) {
+        const float *tc = tile + c * th * tw;
+#pragma unroll
+        for (int ky = 0; ky < 3; ++ky) {
+            const float *row = tc + (threadIdx.y + ky * dil) * tw + threadIdx.x;
+#pragma unroll
+            for (int kx = 0; kx < 3; ++kx) {
+                const float v = row[kx * dil];
+#pragma unroll
+                for (int o = 0; o < OCG; ++o)
+                    acc[o] = fmaf(v, sw[(o * IC + c) * 9 + ky * 3 + kx], acc[o]);
+            }
+        }
+    }
+    const long HW = (long)H * W, oi = (long)oy * W + ox;
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) {
+        const float v = acc[o];
+        y[(og * OCG + o) * HW + oi] = v > 0.f ? v : v * 0.2f;
+    }
+}
+
 static size_t conv2d_tile_bytes(int IC, int stride, int dil) {
     return (size_t)IC * ((CT2_TH - 1) * stride + 2 * dil + 1) *
            ((CT2_TW - 1) * stride + 2 * dil + 1) * sizeof(float);
@@ -405,20 +473,6 @@ __global__ void __launch_bounds__(32 * SA_DMAX)
     disp[(long)oy * w + ox] = acc / total_e;
 }
 
-// ---------------------------------------------- refinement input: up x2
-// d_up = 2 * bilinear(d) at (H2, W2) into channel 0, guide into channel 1.
-__global__ void k_upsample_concat(const float *__restrict__ d, int h, int w, int H2, int W2,
-                                  const float *__restrict__ guide, float *__restrict__ out) {
-    int ox = blockIdx.x * blockDim.x + threadIdx.x;
-    int oy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ox >= W2 || oy >= H2) return;
-    Taps t = bilinear_taps(oy, ox, h, w, H2, W2);
-    float v = __ldg(d + t.i00) * (float)t.w00 + __ldg(d + t.i01) * (float)t.w01 +
-              __ldg(d + t.i10) * (float)t.w10 + __ldg(d + t.i11) * (float)t.w11;
-    long i = (long)oy * W2 + ox;
-    out[i] = v * 2.0f;
-    out[(long)H2 * W2 + i] = guide[i];
-}
 
 // ====================================================================
 // Host side
@@ -631,21 +685,17 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
     int ph = h, pw = w;
     for (int lv = 0; lv < 2; ++lv) {
         const int Hl = Hs[lv], Wl = Ws[lv];
-        count_launch();
-        k_upsample_concat<<<grid2d(Wl, Hl, blk), blk, 0, st>>>(prev, ph, pw, Hl, Wl, guides[lv],
-                                                              b.rin);
-        const float *cur = b.rin;
+        const float *cur = nullptr;
         float *bufs[2] = {b.ra, b.rb};
         constexpr int RG = RC % 4 == 0 ? 4 : RC;
         for (int i = 0; i < n.ndil; ++i) {
             float *dst = bufs[i & 1];
             const int dl = n.dil[i];
             count_launch();
-            if (i == 0)
-                k_conv2d_tiled<2, RC, RG, 1><<<tgrid(Wl, Hl, RC / RG), tb,
-                                               conv2d_tile_bytes(2, 1, dl), st>>>(
-                    cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
-                    nullptr);
+            if (i == 0)     // up-sample + concat built into the first convolution
+                k_conv2d_up<RC, RG><<<tgrid(Wl, Hl, RC / RG), tb, conv2d_tile_bytes(2, 1, dl),
+                                      st>>>(prev, ph, pw, guides[lv], Hl, Wl, dl, n.rw[lv][i],
+                                            n.rb[lv][i], dst, b.rin);
             else
                 k_conv2d_tiled<RC, RC, RG, 1><<<tgrid(Wl, Hl, RC / RG), tb,
                                                 conv2d_tile_bytes(RC, 1, dl), st>>>(

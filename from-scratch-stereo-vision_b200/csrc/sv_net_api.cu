@@ -181,12 +181,15 @@ static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictW
 }
 
 // predict (stereonet.py:5891-5897) on FP32 images already in lw/rw.
+// gh_ready: the resize already wrote the half-resolution guide
 static int predict_f32(const sv_net *net, const PredictWs &w, int W, int H, int precision,
-                       cudaStream_t st) {
+                       cudaStream_t st, bool gh_ready = false) {
     int rc = check_net_shape(net->view, H, W);
     if (rc) return rc;
-    rc = launch_avgpool2(w.lw, H, W, w.gh, st);
-    if (rc) return rc;
+    if (!gh_ready) {
+        rc = launch_avgpool2(w.lw, H, W, w.gh, st);
+        if (rc) return rc;
+    }
     return launch_forward(net->view, w.lw, w.rw, H, W, w.gh, w.lw, w.d0, w.d1, w.d2, w.fwd,
                           precision, st);
 }
@@ -211,10 +214,10 @@ static int predict_at_scale_impl(const sv_net *net, const PredictWs &w, const vo
     const int Ww = work;
     int Hw = (int)(H * scale + 0.5);
     if (Hw < 8) Hw = 8;
-    rc = launch_resize_pair(left, right, dtype, W, H, Ww, Hw, w.lw, w.rw, st);
-    if (!rc) rc = predict_f32(net, w, Ww, Hw, precision, st);
-    if (!rc) rc = launch_promote(w.d2, (long)Ww * Hw, disp_work, st);
-    if (!rc) rc = launch_upscale_disp(w.d2, Ww, Hw, W, H, 1.0 / scale, disp_full, st);
+    rc = check_net_shape(net->view, Hw, Ww);
+    if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, Ww, Hw, w.lw, w.rw, st, w.gh);
+    if (!rc) rc = predict_f32(net, w, Ww, Hw, precision, st, true);
+    if (!rc) rc = launch_work_outputs(w.d2, Ww, Hw, W, H, 1.0 / scale, disp_work, disp_full, st);
     *pWw = Ww;
     *pHw = Hw;
     return rc;
@@ -511,11 +514,16 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, precision, left, right, disp_full,
                      disp_work, workspace};
     SV_TRY(run_stage(mnet, key, st, [&]() -> int {
-        int rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st);
-        if (!rc) rc = predict_f32(net, w, pw, ph, precision, st);
-        if (!rc) rc = launch_promote(w.d2, (long)pw * ph, w.probe64, st);
-        if (!rc) rc = launch_select(w.probe64, (long)pw * ph, (long long)((long)pw * ph * 0.95),
-                                    w.sel, w.hist, st);
+        int rc = check_net_shape(net->view, ph, pw);
+        if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh);
+        if (!rc) rc = predict_f32(net, w, pw, ph, precision, st, true);
+        const long np = (long)pw * ph;
+        const long long rank = (long long)(np * 0.95);
+        if (!rc && np <= 16384) rc = launch_select_small_f32(w.d2, np, rank, w.sel, st);
+        else if (!rc) {
+            rc = launch_promote(w.d2, np, w.probe64, st);
+            if (!rc) rc = launch_select(w.probe64, np, rank, w.sel, w.hist, st);
+        }
         return rc;
     }));
     double pk;

@@ -56,14 +56,24 @@ __device__ __forceinline__ double blend64(const T *x, const Taps &t) {
 // second launch (k_avgpool2).
 template <typename T>
 __global__ void k_resize_pair(const T *__restrict__ l, const T *__restrict__ r, int W, int H,
-                              int W2, int H2, float *__restrict__ lo, float *__restrict__ ro) {
+                              int W2, int H2, float *__restrict__ lo, float *__restrict__ ro,
+                              float *__restrict__ gh) {
     const T *src = blockIdx.z ? r : l;
     float *dst = blockIdx.z ? ro : lo;
     int ox = blockIdx.x * blockDim.x + threadIdx.x;
     int oy = blockIdx.y * blockDim.y + threadIdx.y;
     if (ox >= W2 || oy >= H2) return;
-    Taps t = bilinear_taps(oy, ox, H, W, H2, W2);
-    dst[oy * W2 + ox] = (float)blend64<T>(src, t);
+    const float v = (float)blend64<T>(src, bilinear_taps(oy, ox, H, W, H2, W2));
+    dst[oy * W2 + ox] = v;
+    // the guide at half resolution, avgpool2 of the resized left view
+    // (stereonet.py:979-995): the top-left thread of each 2x2 block
+    // recomputes its three neighbours' values, which are the ones stored
+    if (gh && blockIdx.z == 0 && !(ox & 1) && !(oy & 1) && ox / 2 < W2 / 2 && oy / 2 < H2 / 2) {
+        const float v01 = (float)blend64<T>(src, bilinear_taps(oy, ox + 1, H, W, H2, W2));
+        const float v10 = (float)blend64<T>(src, bilinear_taps(oy + 1, ox, H, W, H2, W2));
+        const float v11 = (float)blend64<T>(src, bilinear_taps(oy + 1, ox + 1, H, W, H2, W2));
+        gh[(oy / 2) * (W2 / 2) + ox / 2] = 0.25f * (((v + v01) + v10) + v11);
+    }
 }
 
 // Copy (no resample) of a pair into FP32, for predict at native resolution.
@@ -88,6 +98,21 @@ __global__ void k_resize_scale(const T *__restrict__ x, int W, int H, int W2, in
     Taps t = bilinear_taps(oy, ox, H, W, H2, W2);
     double v = blend64<T>(x, t);
     out[(long)oy * W2 + ox] = scale ? __dmul_rn(v, inv) : v;
+}
+
+// predict_at_scale's two outputs from the FP32 work-resolution disparity in
+// one launch: the full-resolution map, bilinear and times inv
+// (stereonet.py:3957-3959), and the work map itself promoted to FP64 by the
+// threads that fall inside it (the work map is never larger).
+__global__ void k_work_outputs(const float *__restrict__ d, int Ww, int Hw, int W, int H,
+                               double inv, double *__restrict__ work64,
+                               double *__restrict__ full64) {
+    int ox = blockIdx.x * blockDim.x + threadIdx.x;
+    int oy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ox >= W || oy >= H) return;
+    Taps t = bilinear_taps(oy, ox, Hw, Ww, H, W);
+    full64[(long)oy * W + ox] = __dmul_rn(blend64<float>(d, t), inv);
+    if (ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
 }
 
 template <typename T>
@@ -483,16 +508,16 @@ static dim3 grid2d(int W, int H, dim3 blk, int z = 1) {
 }
 
 int launch_resize_pair(const void *l, const void *r, int dtype, int W, int H, int W2, int H2,
-                       float *lo, float *ro, cudaStream_t st) {
+                       float *lo, float *ro, cudaStream_t st, float *gh) {
     dim3 blk(32, 8);
     dim3 g = grid2d(W2, H2, blk, 2);
     if (W2 == W && H2 == H) {
         // a resample to the same size still runs the reference's arithmetic
     }
     switch (dtype) {
-    case SV_U8: count_launch(); k_resize_pair<uint8_t><<<g, blk, 0, st>>>((const uint8_t *)l, (const uint8_t *)r, W, H, W2, H2, lo, ro); break;
-    case SV_F32: count_launch(); k_resize_pair<float><<<g, blk, 0, st>>>((const float *)l, (const float *)r, W, H, W2, H2, lo, ro); break;
-    case SV_F64: count_launch(); k_resize_pair<double><<<g, blk, 0, st>>>((const double *)l, (const double *)r, W, H, W2, H2, lo, ro); break;
+    case SV_U8: count_launch(); k_resize_pair<uint8_t><<<g, blk, 0, st>>>((const uint8_t *)l, (const uint8_t *)r, W, H, W2, H2, lo, ro, gh); break;
+    case SV_F32: count_launch(); k_resize_pair<float><<<g, blk, 0, st>>>((const float *)l, (const float *)r, W, H, W2, H2, lo, ro, gh); break;
+    case SV_F64: count_launch(); k_resize_pair<double><<<g, blk, 0, st>>>((const double *)l, (const double *)r, W, H, W2, H2, lo, ro, gh); break;
     default: set_error("unknown dtype %d", dtype); return SV_ERR_PARAM;
     }
     SV_LAUNCH_CHECK();
@@ -524,6 +549,19 @@ int launch_upscale_disp(const float *dw, int Ww, int Hw, int W, int H, double in
                         double *out, cudaStream_t st) {
     dim3 blk(32, 8);
     count_launch(); k_resize_scale<float><<<grid2d(W, H, blk), blk, 0, st>>>(dw, Ww, Hw, W, H, inv, 1, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_work_outputs(const float *d, int Ww, int Hw, int W, int H, double inv,
+                        double *work64, double *full64, cudaStream_t st) {
+    if (Ww > W || Hw > H) {
+        set_error("work map %dx%d larger than %dx%d", Ww, Hw, W, H);
+        return SV_ERR_SHAPE;
+    }
+    dim3 blk(32, 8);
+    count_launch();
+    k_work_outputs<<<grid2d(W, H, blk), blk, 0, st>>>(d, Ww, Hw, W, H, inv, work64, full64);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

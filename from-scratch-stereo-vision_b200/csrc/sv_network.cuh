@@ -62,8 +62,11 @@ struct FwdBufs {
     int *flag;               // device error flag (the workspace's DevFlags)
 };
 
+// gh (optional): also avgpool2 of the resized left view, [H2/2][W2/2]
 int launch_resize_pair(const void *l, const void *r, int dtype, int W, int H, int W2, int H2,
-                       float *lo, float *ro, cudaStream_t st);
+                       float *lo, float *ro, cudaStream_t st, float *gh = nullptr);
+int launch_work_outputs(const float *d, int Ww, int Hw, int W, int H, double inv,
+                        double *work64, double *full64, cudaStream_t st);
 int launch_to_f32_pair(const void *l, const void *r, int dtype, long n, float *lo, float *ro,
                        cudaStream_t st);
 int launch_resize_f64(const double *x, int W, int H, int W2, int H2, double *out,
@@ -80,6 +83,9 @@ int launch_forward(const NetView &n, const float *left, const float *right, int 
 struct SelState;
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st);
+// the same over FP32 values (exactly their FP64 promotions), n <= 16384
+int launch_select_small_f32(const float *x, long n, long long rank, SelState *state,
+                            cudaStream_t st);
 size_t select_state_bytes();
 size_t select_value_offset();
 size_t select_hist_words();

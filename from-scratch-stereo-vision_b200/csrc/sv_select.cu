@@ -275,15 +275,16 @@ __global__ void __launch_bounds__(1024)
 // shared memory and runs the six passes there, one launch instead of seven.
 constexpr long SEL_SMALL_CAP = 16384;     // keys (128 KB of dynamic shared memory)
 
+template <typename T>
 __global__ void __launch_bounds__(1024)
-    k_sel_small(const double *__restrict__ x, long n, long long rank0, SelState *__restrict__ s) {
+    k_sel_small(const T *__restrict__ x, long n, long long rank0, SelState *__restrict__ s) {
     extern __shared__ __align__(16) unsigned long long keys[];
     __shared__ unsigned hist[SEL_NB];
     __shared__ unsigned wsum[32];
     __shared__ int owner;
     __shared__ unsigned long long owner_excl, s_prefix;
     __shared__ long long s_rank;
-    for (long i = threadIdx.x; i < n; i += blockDim.x) keys[i] = sel_key(x[i]);
+    for (long i = threadIdx.x; i < n; i += blockDim.x) keys[i] = sel_key((double)x[i]);
     __syncthreads();
     unsigned long long prefix = 0ull;
     long long rank = rank0;
@@ -296,6 +297,26 @@ __global__ void __launch_bounds__(1024)
     }
 }
 
+// The select kernels' dynamic shared-memory limits, once per device.
+static int select_setup() {
+    int dev = 0;
+    SV_CUDA_TRY(cudaGetDevice(&dev));
+    static bool ready[64] = {false};
+    if (dev >= 64 || !ready[dev]) {
+        SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small<double>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
+        SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small<float>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
+        SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_compact,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(SEL_CAND_CAP * sizeof(unsigned long long))));
+        if (dev < 64) ready[dev] = true;
+    }
+    return SV_OK;
+}
+
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st) {
     if (n < 1 || n >= (1l << 32) || rank < 0 || rank >= n) {
@@ -303,22 +324,13 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
         return SV_ERR_PARAM;
     }
     {
-        int dev = 0;
-        SV_CUDA_TRY(cudaGetDevice(&dev));
-        static bool ready[64] = {false};
-        if (dev >= 64 || !ready[dev]) {
-            SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
-            SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_compact,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(SEL_CAND_CAP * sizeof(unsigned long long))));
-            if (dev < 64) ready[dev] = true;
-        }
+        const int rc = select_setup();
+        if (rc) return rc;
     }
     if (n <= SEL_SMALL_CAP) {
         count_launch();
-        k_sel_small<<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(x, n, rank, state);
+        k_sel_small<double><<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(x, n, rank,
+                                                                                    state);
         SV_LAUNCH_CHECK();
         return SV_OK;
     }
@@ -334,6 +346,21 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
     count_launch();
     k_sel_compact<<<blocks, 1024, (size_t)SEL_CAND_CAP * sizeof(unsigned long long), st>>>(
         x, n, state, cand);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_select_small_f32(const float *x, long n, long long rank, SelState *state,
+                            cudaStream_t st) {
+    if (n < 1 || n > SEL_SMALL_CAP || rank < 0 || rank >= n) {
+        set_error("select: n=%ld rank=%lld", n, rank);
+        return SV_ERR_PARAM;
+    }
+    const int rc = select_setup();
+    if (rc) return rc;
+    count_launch();
+    k_sel_small<float><<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(x, n, rank,
+                                                                                 state);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

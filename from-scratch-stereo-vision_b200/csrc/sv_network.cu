@@ -297,144 +297,146 @@ static size_t conv2d_tile_bytes(int IC, int stride, int dil) {
            ((CT2_TW - 1) * stride + 2 * dil + 1) * sizeof(float);
 }
 
-constexpr int CV_TD = 4;    // disparities per CTA of the 3-D convolutions
+// ------------------------------------------------------------ conv 3d
+// The 3-D convolutions run on volumes of a few thousand voxels (w x h x D at
+// 1/4 resolution, D <= 16), so their cost is the latency of one thread's
+// chain of taps, not bandwidth or FLOPs.  A CTA stages its input tile --
+// 8 columns x TD disparities x 1 row plus the 3x3x3 halo, every input
+// channel -- in shared memory, zeros outside the volume (a zero tap adds
+// exactly what the reference's skipped tap adds: nothing), and each output
+// voxel's channel sum is split over CS lanes (C / CS channels each) that a
+// butterfly of shuffles adds up.  Plane and disparity strides of the tile
+// are padded so that the 32 lanes of a warp read 32 distinct banks.
+constexpr int C3_TX = 8;                 // columns per CTA
+constexpr int C3_RS = C3_TX + 2;         // tile row stride (halo included)
 
-// Cost volume + conv3d #1, staged: the CTA (32 columns x CV_TD disparities
-// of one row, OCG of the OC output channels) first writes the cost-volume tile it
-// reads -- |fl - fr(x - d)|, 2.0 where x - d < 0, 0 outside the volume --
-// into shared memory once, then every tap is one shared load and OCG FMAs.
-// CostVolume.forward (stereonet.py:771-799) fused into Conv3d #1 (596-641)
-// and its leaky ReLU; taps outside the volume are skipped, as in the
-// reference's loops.
-template <int C, int OC, int OCG>
-__global__ void __launch_bounds__(32 * CV_TD)
-    k_costvol_conv3d_staged(const float *__restrict__ fl, const float *__restrict__ fr, int D,
-                            int h, int w, const float *__restrict__ wt,
-                            const float *__restrict__ b, float *__restrict__ y) {
-    // the weights join the tile in shared memory when both fit the static
-    // 48 KB; otherwise every lane reads the same weight through the
-    // read-only cache (one broadcast transaction)
-    constexpr bool kWs = (C * (CV_TD + 2) * 102 + OCG * C * 27 + OCG) * 4 <= 48 * 1024;
-    __shared__ float sv[C][CV_TD + 2][3][34];
-    __shared__ float sw[kWs ? OCG * C * 27 : 1];
-    __shared__ float sb[OCG];
-    const int og = blockIdx.z;                     // output channels og*OCG ..
-    const int nd = (D + CV_TD - 1) / CV_TD;
-    const int x0 = blockIdx.x * 32, oy = blockIdx.y / nd, d0 = (blockIdx.y - oy * nd) * CV_TD;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    const float *wg = wt + og * OCG * C * 27;
-    if (kWs)
-        for (int i = tid; i < OCG * C * 27; i += 32 * CV_TD) sw[i] = wg[i];
-    if (tid < OCG) sb[tid] = b[og * OCG + tid];
+// True when the lanes of a warp (lane = position * CS + split, positions
+// 8 columns wide) hit distinct shared-memory banks for plane stride P and
+// disparity stride DS.
+__host__ __device__ constexpr bool c3_banks_ok(int CS, int CPS, int DS, int P) {
+    bool used[32] = {};
+    for (int lane = 0; lane < 32; ++lane) {
+        const int cs = lane % CS, pl = lane / CS;
+        const int bank = (cs * CPS * P + (pl / C3_TX) * DS + pl % C3_TX) % 32;
+        if (used[bank]) return false;
+        used[bank] = true;
+    }
+    return true;
+}
+
+// The smallest conflict-free (DS, P): which = 0 gives DS, 1 gives P, -1 if
+// none exists within 32 of the unpadded strides.
+__host__ __device__ constexpr int c3_layout(int CS, int CPS, int TD, int which) {
+    for (int ds = 3 * C3_RS; ds < 3 * C3_RS + 32; ++ds)
+        for (int pl = (TD + 2) * ds; pl < (TD + 2) * ds + 32; ++pl)
+            if (c3_banks_ok(CS, CPS, ds, pl)) return which == 0 ? ds : pl;
+    return -1;
+}
+
+// Stages rows d0-1 .. d0+TD, y-1 .. y+1, x0-1 .. x0+8 of every channel.
+// CV: the cost volume of CostVolume.forward (stereonet.py:771-799) built on
+// the fly -- |fl(x) - fr(x - d)|, 2.0 where x - d < 0; else x is a C x D x h
+// x w volume.
+template <int C, int TD, int DS, int P, int NT, bool CV>
+__device__ __forceinline__ void c3_stage(float *tile, const float *__restrict__ a,
+                                         const float *__restrict__ bsrc, int D, int h, int w,
+                                         int x0, int oy, int d0) {
+    constexpr int PER_C = (TD + 2) * 3 * C3_RS;
     const long hw = (long)h * w;
-    constexpr int PLANE = (CV_TD + 2) * 3 * 34;
-    for (int i = tid; i < C * PLANE; i += 32 * CV_TD) {
-        const int c = i / PLANE, rem = i - c * PLANE;
-        const int dz = rem / 102, rem2 = rem - dz * 102, r = rem2 / 34, j = rem2 - r * 34;
-        const int dd = d0 - 1 + dz, yy = oy - 1 + r, xx = x0 - 1 + j;
+    for (int i = threadIdx.x; i < C * PER_C; i += NT) {
+        const int c = i / PER_C;
+        int r = i - c * PER_C;
+        const int dz = r / (3 * C3_RS);
+        r -= dz * 3 * C3_RS;
+        const int ry = r / C3_RS, rx = r - ry * C3_RS;
+        const int dd = d0 - 1 + dz, yy = oy - 1 + ry, xx = x0 - 1 + rx;
         float v = 0.f;
         if (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w) {
-            if (xx - dd < 0) {
-                v = 2.0f;
-            } else {
-                const long row = c * hw + (long)yy * w;
-                v = fabsf(__ldg(fl + row + xx) - __ldg(fr + row + xx - dd));
-            }
-        }
-        sv[c][dz][r][j] = v;
-    }
-    __syncthreads();
-    const int ox = x0 + threadIdx.x, od = d0 + threadIdx.y;
-    if (ox >= w || od >= D) return;
-    float acc[OCG];
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
-    for (int c = 0; c < C; ++c) {
-#pragma unroll
-        for (int kd = 0; kd < 3; ++kd) {
-            const int dd = od + kd - 1;
-            if (dd < 0 || dd >= D) continue;
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky) {
-                const int yy = oy + ky - 1;
-                if (yy < 0 || yy >= h) continue;
-                const float *row = &sv[c][threadIdx.y + kd][ky][threadIdx.x];
-#pragma unroll
-                for (int kx = 0; kx < 3; ++kx) {
-                    const int xx = ox + kx - 1;
-                    if (xx < 0 || xx >= w) continue;
-                    const float v = row[kx];
-#pragma unroll
-                    for (int o = 0; o < OCG; ++o) {
-                        const int wi = (o * C + c) * 27 + kd * 9 + ky * 3 + kx;
-                        acc[o] = fmaf(v, kWs ? sw[wi] : __ldg(wg + wi), acc[o]);
-                    }
+            if (CV) {
+                if (xx - dd < 0) {
+                    v = 2.0f;
+                } else {
+                    const long row = c * hw + (long)yy * w;
+                    v = fabsf(__ldg(a + row + xx) - __ldg(bsrc + row + xx - dd));
                 }
+            } else {
+                v = __ldg(a + (c * (long)D + dd) * hw + (long)yy * w + xx);
             }
         }
-    }
-    const long total = (long)D * hw;
-    const long idx = (long)od * hw + (long)oy * w + ox;
-#pragma unroll
-    for (int o = 0; o < OCG; ++o) {
-        const float v = acc[o];
-        y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
+        tile[c * P + dz * DS + ry * C3_RS + rx] = v;
     }
 }
 
-// Tiled conv3d #2 (same CTA shape): stages x[c][d0-1..d0+CV_TD][y-1..y+1]
-// [x0-1..x0+32], zeros outside the volume.
-template <int IC, int OC, int OCG>
-__global__ void __launch_bounds__(32 * CV_TD)
-    k_conv3d_tiled(const float *__restrict__ x, int D, int h, int w, const float *__restrict__ wt,
-                   const float *__restrict__ b, float *__restrict__ y) {
-    __shared__ float sx[IC][CV_TD + 2][3][34];
-    __shared__ float sw[OCG * IC * 27];
-    __shared__ float sb[OCG];
-    const int og = blockIdx.z;
-    const int nd = (D + CV_TD - 1) / CV_TD;
-    const int x0 = blockIdx.x * 32, oy = blockIdx.y / nd;
-    const int d0 = (blockIdx.y - oy * nd) * CV_TD;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int i = tid; i < OCG * IC * 27; i += 32 * CV_TD) sw[i] = wt[og * OCG * IC * 27 + i];
-    if (tid < OCG) sb[tid] = b[og * OCG + tid];
-    const long hw = (long)h * w, total = (long)D * hw;
-    constexpr int PLANE = (CV_TD + 2) * 3 * 34;
-    for (int i = tid; i < IC * PLANE; i += 32 * CV_TD) {
-        const int c = i / PLANE, rem = i - c * PLANE;
-        const int dz = rem / (3 * 34), rem2 = rem - dz * 3 * 34, r = rem2 / 34, j = rem2 - r * 34;
-        const int dd = d0 - 1 + dz, yy = oy - 1 + r, xx = x0 - 1 + j;
-        sx[c][dz][r][j] = (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w)
-                              ? __ldg(x + c * total + dd * hw + yy * w + xx)
-                              : 0.f;
-    }
-    __syncthreads();
-    const int ox = x0 + threadIdx.x, od = d0 + threadIdx.y;
-    if (ox >= w || od >= D) return;
-    float acc[OCG];
+// One lane's share of a voxel: channels cs*CPS .. +CPS of the 27 taps, for
+// OCG output channels (weights [c][tap][o] in shared memory).
+template <int CPS, int OCG, int DS, int P>
+__device__ __forceinline__ void c3_taps(const float *tb, const float *wb, float (&acc)[OCG]) {
 #pragma unroll
-    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
+    for (int j = 0; j < CPS; ++j)
 #pragma unroll
-    for (int c = 0; c < IC; ++c) {
+        for (int kd = 0; kd < 3; ++kd)
 #pragma unroll
-        for (int kd = 0; kd < 3; ++kd) {
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky) {
-                const float *row = &sx[c][threadIdx.y + kd][ky][threadIdx.x];
+            for (int ky = 0; ky < 3; ++ky)
 #pragma unroll
                 for (int kx = 0; kx < 3; ++kx) {
-                    const float v = row[kx];
+                    const float v = tb[j * P + kd * DS + ky * C3_RS + kx];
+                    const float *wt = wb + (j * 27 + kd * 9 + ky * 3 + kx) * OCG;
+                    if (OCG == 2) {
+                        const float2 ww = *reinterpret_cast<const float2 *>(wt);
+                        acc[0] = fmaf(v, ww.x, acc[0]);
+                        acc[1] = fmaf(v, ww.y, acc[1]);
+                    } else {
 #pragma unroll
-                    for (int o = 0; o < OCG; ++o)
-                        acc[o] = fmaf(v, sw[(o * IC + c) * 27 + kd * 9 + ky * 3 + kx], acc[o]);
+                        for (int o = 0; o < OCG; ++o) acc[o] = fmaf(v, wt[o], acc[o]);
+                    }
                 }
-            }
-        }
+}
+
+template <int OCG, int CS>
+__device__ __forceinline__ void c3_reduce(float (&acc)[OCG]) {
+#pragma unroll
+    for (int o = 0; o < OCG; ++o)
+#pragma unroll
+        for (int m = 1; m < CS; m <<= 1) acc[o] += __shfl_xor_sync(kFull, acc[o], m);
+}
+
+// Conv3d #1 (with the cost volume built while staging, CV) or #2 of
+// CostFilter (stereonet.py:596-641, leaky ReLU 0.2): C -> OC channels, OCG
+// per CTA (blockIdx.z), 128 threads = 8 columns x TD disparities x CS splits.
+template <int C, int OCG, int CS, bool CV>
+__global__ void __launch_bounds__(128)
+    k_conv3d_split(const float *__restrict__ a, const float *__restrict__ bsrc, int D, int h,
+                   int w, const float *__restrict__ wt, const float *__restrict__ bias,
+                   float *__restrict__ y) {
+    constexpr int CPS = C / CS, TD = 16 / CS;
+    constexpr int DS = c3_layout(CS, CPS, TD, 0), P = c3_layout(CS, CPS, TD, 1);
+    static_assert(C % CS == 0 && (CS == 2 || CS == 4) && DS > 0, "tile layout");
+    __shared__ float tile[C * P];
+    __shared__ __align__(16) float sw[C * 27 * OCG];
+    __shared__ float sb[OCG];
+    const int og = blockIdx.z, nd = (D + TD - 1) / TD;
+    const int x0 = blockIdx.x * C3_TX, oy = blockIdx.y / nd, d0 = (blockIdx.y - oy * nd) * TD;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < C * 27 * OCG; i += 128) {
+        const int o = i % OCG, ct = i / OCG;       // ct = c * 27 + tap
+        sw[i] = __ldg(wt + (og * OCG + o) * C * 27 + ct);
     }
-    const long idx = (long)od * hw + (long)oy * w + ox;
+    if (tid < OCG) sb[tid] = __ldg(bias + og * OCG + tid);
+    c3_stage<C, TD, DS, P, 128, CV>(tile, a, bsrc, D, h, w, x0, oy, d0);
+    __syncthreads();
+    const int lane = tid & 31, cs = lane % CS, pos = (tid >> 5) * (32 / CS) + lane / CS;
+    const int px = pos % C3_TX, pd = pos / C3_TX;
+    float acc[OCG];
+#pragma unroll
+    for (int o = 0; o < OCG; ++o) acc[o] = 0.f;
+    c3_taps<CPS, OCG, DS, P>(tile + cs * CPS * P + pd * DS + px, sw + cs * CPS * 27 * OCG, acc);
+    c3_reduce<OCG, CS>(acc);
+    const int ox = x0 + px, od = d0 + pd;
+    if (cs != 0 || ox >= w || od >= D) return;
+    const long hw = (long)h * w, total = (long)D * hw, idx = (long)od * hw + (long)oy * w + ox;
 #pragma unroll
     for (int o = 0; o < OCG; ++o) {
-        const float v = acc[o];
+        const float v = acc[o] + sb[o];
         y[(og * OCG + o) * total + idx] = v > 0.f ? v : v * 0.2f;
     }
 }
@@ -443,59 +445,56 @@ __global__ void __launch_bounds__(32 * CV_TD)
 // Conv3d #3 (Cm -> 1), CostVolume.invalid_mask (+8 where x < d, d >= 1,
 // stereonet.py:827-840) and SoftArgmin.forward (858-885) in FP32 with
 // max-subtraction: disp = sum_d d * exp(-c_d - max(-c)) / sum_d exp(...).
-// A CTA is 32 columns x 16 disparities of one row: thread (x, d) computes
-// cost d, the first warp reduces over d.
+// A CTA is 8 columns x all D (<= 16) disparities of one row, each voxel's
+// channel sum split over CS lanes as above; then 16 lanes per column reduce
+// the soft-argmin over d with shuffles.
 constexpr int SA_DMAX = 16;
 
-template <int IC>
-__global__ void __launch_bounds__(32 * SA_DMAX)
+template <int IC, int CS>
+__global__ void __launch_bounds__(128 * CS)
     k_conv3d_softargmin(const float *__restrict__ x, int D, int h, int w,
                         const float *__restrict__ wt, const float *__restrict__ b,
                         float *__restrict__ disp) {
+    constexpr int CPS = IC / CS, TD = SA_DMAX, NT = 128 * CS;
+    constexpr int DS = c3_layout(CS, CPS, TD, 0), P = c3_layout(CS, CPS, TD, 1);
+    static_assert(IC % CS == 0 && DS > 0, "tile layout");
+    __shared__ float tile[IC * P];
     __shared__ float sw[IC * 27];
-    __shared__ float cost[SA_DMAX][33];
-    const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int i = tid; i < IC * 27; i += blockDim.x * blockDim.y) sw[i] = wt[i];
+    __shared__ float cost[SA_DMAX][C3_TX + 1];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < IC * 27; i += NT) sw[i] = __ldg(wt + i);
+    const int x0 = blockIdx.x * C3_TX, oy = blockIdx.y;
+    c3_stage<IC, TD, DS, P, NT, false>(tile, x, nullptr, D, h, w, x0, oy, 0);
     __syncthreads();
-    const long hw = (long)h * w;
-    const long total = (long)D * hw;
-    const int ox = blockIdx.x * 32 + threadIdx.x, oy = blockIdx.y, od = threadIdx.y;
-    if (ox < w && od < D) {
-        float acc = __ldg(b);
-        for (int c = 0; c < IC; ++c) {
-            const float *xc = x + c * total;
-#pragma unroll
-            for (int kd = 0; kd < 3; ++kd) {
-                const int dd = od + kd - 1;
-                if (dd < 0 || dd >= D) continue;
-#pragma unroll
-                for (int ky = 0; ky < 3; ++ky) {
-                    const int yy = oy + ky - 1;
-                    if (yy < 0 || yy >= h) continue;
-#pragma unroll
-                    for (int kx = 0; kx < 3; ++kx) {
-                        const int xx = ox + kx - 1;
-                        if (xx < 0 || xx >= w) continue;
-                        acc = fmaf(__ldg(xc + dd * hw + yy * w + xx),
-                                   sw[c * 27 + kd * 9 + ky * 3 + kx], acc);
-                    }
-                }
-            }
+    {
+        const int lane = tid & 31, cs = lane % CS, pos = (tid >> 5) * (32 / CS) + lane / CS;
+        const int px = pos % C3_TX, pd = pos / C3_TX;
+        float acc[1] = {0.f};
+        c3_taps<CPS, 1, DS, P>(tile + cs * CPS * P + pd * DS + px, sw + cs * CPS * 27, acc);
+        c3_reduce<1, CS>(acc);
+        if (cs == 0) {
+            float v = acc[0] + __ldg(b);
+            if (pd >= 1 && x0 + px < pd) v += 8.0f;
+            cost[pd][px] = v;
         }
-        if (od >= 1 && ox < od) acc += 8.0f;
-        cost[od][threadIdx.x] = acc;
     }
     __syncthreads();
-    if (threadIdx.y != 0 || ox >= w) return;
-    float best = -cost[0][threadIdx.x];
-    for (int d = 1; d < D; ++d) best = fmaxf(best, -cost[d][threadIdx.x]);
-    float total_e = 0.f, acc = 0.f;
-    for (int d = 0; d < D; ++d) {
-        const float e = expf(-cost[d][threadIdx.x] - best);
-        total_e += e;
-        acc = fmaf((float)d, e, acc);
+    if (tid >= C3_TX * SA_DMAX) return;
+    // 16 lanes per column: lane d holds -cost_d
+    const int px = tid / SA_DMAX, d = tid % SA_DMAX, ox = x0 + px;
+    const bool live = d < D;
+    const float nc = live ? -cost[d][px] : -INFINITY;
+    float best = nc;
+#pragma unroll
+    for (int m = 1; m < SA_DMAX; m <<= 1) best = fmaxf(best, __shfl_xor_sync(kFull, best, m));
+    const float e = live ? expf(nc - best) : 0.f;
+    float te = e, td = (float)d * e;
+#pragma unroll
+    for (int m = 1; m < SA_DMAX; m <<= 1) {
+        te += __shfl_xor_sync(kFull, te, m);
+        td += __shfl_xor_sync(kFull, td, m);
     }
-    disp[(long)oy * w + ox] = acc / total_e;
+    if (d == 0 && ox < w) disp[(long)oy * w + ox] = td / te;
 }
 
 
@@ -701,18 +700,21 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         k_conv2d_tiled<C, C, FG, 0><<<fg, tb, conv2d_tile_bytes(C, 1, 1), st>>>(
             b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
         SV_LAUNCH_CHECK();
-        // cost volume + CostFilter c1, c2 (2 output channels per thread)
+        // cost volume + CostFilter c1, c2 (2 output channels per CTA)
         constexpr int CG = CM % 2 == 0 ? 2 : CM;
-        const dim3 vgrid((w + 31) / 32, h * ((D + CV_TD - 1) / CV_TD), CM / CG);
+        constexpr int S1 = C % 4 == 0 ? 4 : 2, S2 = CM % 4 == 0 && CM > 4 ? 4 : 2;
+        const dim3 vg1((w + C3_TX - 1) / C3_TX, h * ((D + 16 / S1 - 1) / (16 / S1)), CM / CG);
+        const dim3 vg2((w + C3_TX - 1) / C3_TX, h * ((D + 16 / S2 - 1) / (16 / S2)), CM / CG);
         count_launch();
-        k_costvol_conv3d_staged<C, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(
-            b.fb[0], b.fb[1], D, h, w, n.cw[0], n.cb[0], b.v0);
+        k_conv3d_split<C, CG, S1, true><<<vg1, 128, 0, st>>>(b.fb[0], b.fb[1], D, h, w, n.cw[0],
+                                                             n.cb[0], b.v0);
         count_launch();
-        k_conv3d_tiled<CM, CM, CG><<<vgrid, dim3(32, CV_TD), 0, st>>>(b.v0, D, h, w, n.cw[1],
-                                                                      n.cb[1], b.v1);
+        k_conv3d_split<CM, CG, S2, false><<<vg2, 128, 0, st>>>(b.v0, nullptr, D, h, w, n.cw[1],
+                                                               n.cb[1], b.v1);
     }
+    constexpr int S3 = CM % 2 == 0 ? 2 : 1;
     count_launch();
-    k_conv3d_softargmin<CM><<<dim3((w + 31) / 32, h), dim3(32, SA_DMAX), 0, st>>>(
+    k_conv3d_softargmin<CM, S3><<<dim3((w + C3_TX - 1) / C3_TX, h), 128 * S3, 0, st>>>(
         b.v1, D, h, w, n.cw[2], n.cb[2], d0);
     SV_LAUNCH_CHECK();
     // Refinement levels

@@ -151,28 +151,46 @@ __global__ void k_avgpool2_f64(const double *__restrict__ img, int C, int H, int
 }
 
 // ------------------------------------------------------------- conv 2d
-// Shared-memory tiled 3x3 conv2d: a CTA of CT_TW x CT_TH threads computes a
-// CT_TW x CT_TH output tile for OCG output channels (blockIdx.z = image *
-// OC/OCG + group).  The input tile with its halo, for every input channel,
-// is staged once in shared memory (zeros outside the image, which adds
-// exactly what the reference's skipped taps add: nothing); weights are read
-// by broadcast.  act: 0 none, 1 leaky 0.2, 2 residual + relu0 (the
-// Refinement output, v > 0 ? v : v * 0).
+// Shared-memory tiled 3x3 conv2d: a CTA computes a CT2_TW x CT2_TH output
+// tile for OCG output channels (blockIdx.z = image * OC/OCG + group).  The
+// input tile with its halo, for every input channel, is staged once in
+// shared memory (zeros outside the image, which adds exactly what the
+// reference's skipped taps add: nothing); weights sit as [c][tap][o] so one
+// vector load feeds OCG FMAs.  With CS > 1 each output's channel sum is
+// split over CS lanes (IC / CS channels each, CT2_TW x CT2_TH x CS threads)
+// and a butterfly of shuffles adds the parts: a shorter dependent chain per
+// thread on these small, latency-bound images.  act: 0 none, 1 leaky 0.2,
+// 2 residual + relu0 (the Refinement output, v > 0 ? v : v * 0).
 constexpr int CT2_TW = 32, CT2_TH = 4;
 
-template <int IC, int OC, int OCG, int ACT>
-__global__ void __launch_bounds__(CT2_TW *CT2_TH)
+// Channel plane stride of a staged tile: th * tw, padded for CS > 1 so that
+// the CS lane groups of a warp (channels CPS planes apart, 32 / CS
+// consecutive columns each) start 32 / CS banks apart.
+__host__ __device__ inline int conv2d_plane(int th, int tw, int CPS, int CS) {
+    const int p = th * tw;
+    if (CS > 1)
+        for (int k = 0; k < 64; ++k)
+            if ((CPS * (p + k)) % 32 == 32 / CS) return p + k;
+    return p;
+}
+
+template <int IC, int OC, int OCG, int ACT, int CS>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
     k_conv2d_tiled(const float *__restrict__ x0, const float *__restrict__ x1, int H, int W,
                    int OH, int OW, int stride, int pad, int dil, const float *__restrict__ w,
                    const float *__restrict__ b, float *y0, float *y1,
                    const float *__restrict__ resid) {
-    constexpr int NG = OC / OCG;
+    constexpr int NG = OC / OCG, NT = CT2_TW * CT2_TH * CS, CPS = IC / CS;
+    static_assert(IC % CS == 0 && (CS == 1 || CS == 2 || CS == 4), "channel split");
     extern __shared__ __align__(16) float tile[];
-    __shared__ float sw[OCG * IC * 9];
+    __shared__ __align__(16) float sw[IC * 9 * OCG];
     __shared__ float sb[OCG];
     const int img = blockIdx.z / NG, og = blockIdx.z - img * NG;
-    const int tid = threadIdx.y * CT2_TW + threadIdx.x;
-    for (int i = tid; i < OCG * IC * 9; i += CT2_TW * CT2_TH) sw[i] = w[og * OCG * IC * 9 + i];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < IC * 9 * OCG; i += NT) {
+        const int o = i % OCG, ct = i / OCG;          // ct = c * 9 + tap
+        sw[i] = w[(og * OCG + o) * IC * 9 + ct];
+    }
     if (tid < OCG) sb[tid] = b[og * OCG + tid];
     const float *x = img ? x1 : x0;
     float *y = img ? y1 : y0;
@@ -180,41 +198,62 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH)
     const int ix0 = ox0 * stride - pad, iy0 = oy0 * stride - pad;
     const int tw = (CT2_TW - 1) * stride + 2 * dil + 1;
     const int th = (CT2_TH - 1) * stride + 2 * dil + 1;
+    const int plane = conv2d_plane(th, tw, CPS, CS);
     const long HW = (long)H * W;
-    for (int i = tid; i < IC * th * tw; i += CT2_TW * CT2_TH) {
+    for (int i = tid; i < IC * th * tw; i += NT) {
         const int c = i / (th * tw);
         const int rem = i - c * th * tw;
-        const int ty = rem / tw, tx = rem - (rem / tw) * tw;
+        const int ty = rem / tw, tx = rem - ty * tw;
         const int gy = iy0 + ty, gx = ix0 + tx;
-        tile[i] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(x + c * HW + (long)gy * W + gx)
-                                                            : 0.0f;
+        tile[c * plane + rem] = (gy >= 0 && gy < H && gx >= 0 && gx < W)
+                                    ? __ldg(x + c * HW + (long)gy * W + gx)
+                                    : 0.0f;
     }
     __syncthreads();
-    const int ox = ox0 + threadIdx.x, oy = oy0 + threadIdx.y;
-    if (ox >= OW || oy >= OH) return;
+    const int lane = tid & 31, cs = lane / (32 / CS);
+    const int pos = (tid >> 5) * (32 / CS) + lane % (32 / CS);
+    const int lx = pos % CT2_TW, ly = pos / CT2_TW;
     float acc[OCG];
 #pragma unroll
-    for (int o = 0; o < OCG; ++o) acc[o] = sb[o];
-    const int by = threadIdx.y * stride, bx = threadIdx.x * stride;
+    for (int o = 0; o < OCG; ++o) acc[o] = 0.f;
+    const int by = ly * stride, bx = lx * stride;
 #pragma unroll
-    for (int c = 0; c < IC; ++c) {
-        const float *tc = tile + c * th * tw;
+    for (int j = 0; j < CPS; ++j) {
+        const int c = cs * CPS + j;
+        const float *tc = tile + c * plane;
 #pragma unroll
         for (int ky = 0; ky < 3; ++ky) {
             const float *row = tc + (by + ky * dil) * tw + bx;
 #pragma unroll
             for (int kx = 0; kx < 3; ++kx) {
                 const float v = row[kx * dil];
+                const float *wt = sw + (c * 9 + ky * 3 + kx) * OCG;
+                if (OCG % 4 == 0) {
 #pragma unroll
-                for (int o = 0; o < OCG; ++o)
-                    acc[o] = fmaf(v, sw[(o * IC + c) * 9 + ky * 3 + kx], acc[o]);
+                    for (int o = 0; o < OCG; o += 4) {
+                        const float4 w4 = *reinterpret_cast<const float4 *>(wt + o);
+                        acc[o] = fmaf(v, w4.x, acc[o]);
+                        acc[o + 1] = fmaf(v, w4.y, acc[o + 1]);
+                        acc[o + 2] = fmaf(v, w4.z, acc[o + 2]);
+                        acc[o + 3] = fmaf(v, w4.w, acc[o + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int o = 0; o < OCG; ++o) acc[o] = fmaf(v, wt[o], acc[o]);
+                }
             }
         }
     }
+#pragma unroll
+    for (int o = 0; o < OCG; ++o)
+#pragma unroll
+        for (int m = 32 / CS; m < 32; m <<= 1) acc[o] += __shfl_xor_sync(kFull, acc[o], m);
+    const int ox = ox0 + lx, oy = oy0 + ly;
+    if (cs != 0 || ox >= OW || oy >= OH) return;
     const long OHW = (long)OH * OW, oi = (long)oy * OW + ox;
 #pragma unroll
     for (int o = 0; o < OCG; ++o) {
-        float v = acc[o];
+        float v = acc[o] + sb[o];
         if (ACT == 1) v = v > 0.f ? v : v * 0.2f;
         if (ACT == 2) {
             v = resid[oi] + v;
@@ -292,9 +331,9 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH)
     }
 }
 
-static size_t conv2d_tile_bytes(int IC, int stride, int dil) {
-    return (size_t)IC * ((CT2_TH - 1) * stride + 2 * dil + 1) *
-           ((CT2_TW - 1) * stride + 2 * dil + 1) * sizeof(float);
+static size_t conv2d_tile_bytes(int IC, int stride, int dil, int CS = 1) {
+    const int th = (CT2_TH - 1) * stride + 2 * dil + 1, tw = (CT2_TW - 1) * stride + 2 * dil + 1;
+    return (size_t)IC * conv2d_plane(th, tw, IC / CS, CS) * sizeof(float);
 }
 
 // ------------------------------------------------------------ conv 3d
@@ -677,6 +716,7 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
     const int D = n.D;
     dim3 blk(32, 8);
     const dim3 tb(CT2_TW, CT2_TH);
+    const int tb1 = CT2_TW * CT2_TH, tb2 = 2 * tb1, tb4 = 4 * tb1;   // k_conv2d_tiled, CS = 1/2/4
     auto tgrid = [&](int OW, int OH, int z) {
         return dim3((OW + CT2_TW - 1) / CT2_TW, (OH + CT2_TH - 1) / CT2_TH, z);
     };
@@ -688,16 +728,16 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         constexpr int FG = C % 4 == 0 ? 4 : C;
         const dim3 fg1 = tgrid(w1, h1, 2 * (C / FG)), fg = tgrid(w, h, 2 * (C / FG));
         count_launch();
-        k_conv2d_tiled<1, C, FG, 1><<<fg1, tb, conv2d_tile_bytes(1, 2, 1), st>>>(
+        k_conv2d_tiled<1, C, FG, 1, 1><<<fg1, tb1, conv2d_tile_bytes(1, 2, 1), st>>>(
             left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
         count_launch();
-        k_conv2d_tiled<C, C, FG, 1><<<fg, tb, conv2d_tile_bytes(C, 2, 1), st>>>(
+        k_conv2d_tiled<C, C, FG, 1, 1><<<fg, tb1, conv2d_tile_bytes(C, 2, 1), st>>>(
             b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
         count_launch();
-        k_conv2d_tiled<C, C, FG, 1><<<fg, tb, conv2d_tile_bytes(C, 1, 1), st>>>(
+        k_conv2d_tiled<C, C, FG, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
             b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1], nullptr);
         count_launch();
-        k_conv2d_tiled<C, C, FG, 0><<<fg, tb, conv2d_tile_bytes(C, 1, 1), st>>>(
+        k_conv2d_tiled<C, C, FG, 0, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
             b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
         SV_LAUNCH_CHECK();
         // cost volume + CostFilter c1, c2 (2 output channels per CTA)
@@ -737,14 +777,15 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
                                       st>>>(prev, ph, pw, guides[lv], Hl, Wl, dl, n.rw[lv][i],
                                             n.rb[lv][i], dst, b.rin);
             else
-                k_conv2d_tiled<RC, RC, RG, 1><<<tgrid(Wl, Hl, RC / RG), tb,
-                                                conv2d_tile_bytes(RC, 1, dl), st>>>(
+                k_conv2d_tiled<RC, RC, RG, 1, 2><<<tgrid(Wl, Hl, RC / RG), tb2,
+                                                   conv2d_tile_bytes(RC, 1, dl, 2), st>>>(
                     cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
                     nullptr);
             cur = dst;
         }
         count_launch();
-        k_conv2d_tiled<RC, 1, 1, 2><<<tgrid(Wl, Hl, 1), tb, conv2d_tile_bytes(RC, 1, 1), st>>>(
+        k_conv2d_tiled<RC, 1, 1, 2, 4><<<tgrid(Wl, Hl, 1), tb4, conv2d_tile_bytes(RC, 1, 1, 4),
+                                         st>>>(
             cur, cur, Hl, Wl, Hl, Wl, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
             outs[lv], b.rin);
         SV_LAUNCH_CHECK();

@@ -11,8 +11,9 @@
 // bin holding the rank and extends the prefix.  Passes 0 and 1 are one launch
 // each; passes 2..5 run in one CTA over the few keys that still match
 // (k_sel_compact); after pass 5 the prefix is the key.  Up to 16,384 values
-// (the probe) all six passes run in one CTA over keys kept in shared memory
-// (k_sel_small).
+// all six passes run in one CTA over keys kept in shared memory
+// (k_sel_small); the probe's FP32 map takes four 8-bit passes over 32-bit
+// keys instead (k_sel_small_f32).
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
@@ -20,6 +21,7 @@
 namespace sv {
 
 constexpr int SEL_NPASS = 6;
+constexpr int SEL_LB = 4;              // values a thread loads before it histograms them
 constexpr int SEL_NB = 2048;
 __constant__ int kSelBits[SEL_NPASS] = {11, 11, 11, 11, 10, 10};
 __constant__ int kSelShift[SEL_NPASS] = {53, 42, 31, 20, 10, 0};
@@ -65,19 +67,30 @@ __global__ void __launch_bounds__(1024)
     const int shift = kSelShift[pass], bits = kSelBits[pass];
     const int top = shift + bits;
     const unsigned mask = (1u << bits) - 1u;
+    const unsigned long long pre = pass ? s->prefix : 0ull;
     for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
     __syncthreads();
-    const unsigned long long pre = s->prefix;
     const long stride = (long)gridDim.x * nt;
-    for (long i0 = blockIdx.x * (long)nt; i0 < n; i0 += stride) {
-        const long i = i0 + t;
-        unsigned digit = 0xffffffffu;
-        if (i < n) {
-            const unsigned long long k = sel_key(x[i]);
-            if (top >= 64 || (k >> top) == (pre >> top)) digit = (unsigned)(k >> shift) & mask;
+    for (long b0 = blockIdx.x * (long)nt; b0 < n; b0 += SEL_LB * stride) {
+        double v[SEL_LB];                  // this thread's loads, all in flight at once
+#pragma unroll
+        for (int u = 0; u < SEL_LB; ++u) {
+            const long i = b0 + u * stride + t;
+            v[u] = i < n ? x[i] : 0.0;
         }
-        const unsigned same = __match_any_sync(kFull, digit);
-        if (digit != 0xffffffffu && lane == __ffs(same) - 1) atomicAdd(&hist[digit], __popc(same));
+#pragma unroll
+        for (int u = 0; u < SEL_LB; ++u) {
+            const long i = b0 + u * stride + t;
+            unsigned digit = 0xffffffffu;
+            if (i < n) {
+                const unsigned long long k = sel_key(v[u]);
+                if (top >= 64 || (k >> top) == (pre >> top))
+                    digit = (unsigned)(k >> shift) & mask;
+            }
+            const unsigned same = __match_any_sync(kFull, digit);
+            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
+                atomicAdd(&hist[digit], __popc(same));
+        }
     }
     __syncthreads();
     for (int i = t; i < SEL_NB; i += nt)
@@ -230,21 +243,30 @@ __global__ void __launch_bounds__(1024)
     const int top = kSelShift[1];                    // bits above pass 2's digit are fixed
     const unsigned long long pre = s->prefix;
     const long stride = (long)gridDim.x * nt;
-    for (long i0 = blockIdx.x * (long)nt; i0 < n; i0 += stride) {
-        const long i = i0 + t;
-        unsigned long long k = 0;
-        bool hit = false;
-        if (i < n) {
-            k = sel_key(x[i]);
-            hit = (k >> top) == (pre >> top);
+    for (long b0 = blockIdx.x * (long)nt; b0 < n; b0 += SEL_LB * stride) {
+        double v[SEL_LB];
+#pragma unroll
+        for (int u = 0; u < SEL_LB; ++u) {
+            const long i = b0 + u * stride + t;
+            v[u] = i < n ? x[i] : 0.0;
         }
-        const unsigned m = __ballot_sync(kFull, hit);
-        if (m) {
-            unsigned base = 0;
-            if (lane == __ffs(m) - 1) base = atomicAdd(&s->count, __popc(m));
-            base = __shfl_sync(kFull, base, __ffs(m) - 1);
-            const unsigned pos = base + __popc(m & ((1u << lane) - 1u));
-            if (hit && pos < SEL_CAND_CAP) cand[pos] = k;
+#pragma unroll
+        for (int u = 0; u < SEL_LB; ++u) {
+            const long i = b0 + u * stride + t;
+            unsigned long long k = 0;
+            bool hit = false;
+            if (i < n) {
+                k = sel_key(v[u]);
+                hit = (k >> top) == (pre >> top);
+            }
+            const unsigned m = __ballot_sync(kFull, hit);
+            if (m) {
+                unsigned base = 0;
+                if (lane == __ffs(m) - 1) base = atomicAdd(&s->count, __popc(m));
+                base = __shfl_sync(kFull, base, __ffs(m) - 1);
+                const unsigned pos = base + __popc(m & ((1u << lane) - 1u));
+                if (hit && pos < SEL_CAND_CAP) cand[pos] = k;
+            }
         }
     }
     __threadfence();
@@ -297,6 +319,81 @@ __global__ void __launch_bounds__(1024)
     }
 }
 
+// The probe's FP32 map: 32-bit order keys (the order of the floats is the
+// order of the FP64 values they convert to exactly; signed zeros share a
+// key), four 8-bit passes in one CTA of 256 threads -- one bin per thread,
+// so each pass's scan is one shuffle scan and an 8-term prefix -- with the
+// keys in shared memory.  Same result as the FP64 passes, a tenth of the
+// instructions at probe sizes.
+constexpr int SEL32_T = 256;
+
+__device__ __forceinline__ unsigned sel_key32(float f) {
+    const unsigned b = __float_as_uint(f == 0.0f ? 0.0f : f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ float sel_unkey32(unsigned k) {
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__global__ void __launch_bounds__(SEL32_T)
+    k_sel_small_f32(const float *__restrict__ x, int n, unsigned rank0,
+                    SelState *__restrict__ s) {
+    extern __shared__ unsigned keys32[];
+    __shared__ unsigned hist[SEL32_T];
+    __shared__ unsigned wsum[SEL32_T / 32];
+    __shared__ unsigned s_prefix, s_rank;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    for (int i = t; i < n; i += SEL32_T) keys32[i] = sel_key32(__ldg(x + i));
+    if (t == 0) {
+        s_prefix = 0u;
+        s_rank = rank0;
+    }
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 24 - 8 * pass;
+        hist[t] = 0u;
+        __syncthreads();                    // keys, bins and the prefix are ready
+        const unsigned pre = s_prefix;
+        for (int i0 = 0; i0 < n; i0 += SEL32_T) {
+            const int i = i0 + t;
+            unsigned digit = 0xffffffffu;
+            if (i < n) {
+                const unsigned k = keys32[i];
+                if (pass == 0 || (k >> (shift + 8)) == (pre >> (shift + 8)))
+                    digit = (k >> shift) & 255u;
+            }
+            const unsigned same = __match_any_sync(kFull, digit);
+            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
+                atomicAdd(&hist[digit], __popc(same));
+        }
+        __syncthreads();
+        const unsigned c = hist[t];
+        unsigned incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[wid] = incl;
+        __syncthreads();
+        unsigned excl = incl - c;
+        for (int w = 0; w < wid; ++w) excl += wsum[w];
+        const unsigned r = s_rank;
+        __syncthreads();                    // every thread has read the rank
+        if (r >= excl && r < excl + c) {    // exactly one bin holds the rank
+            s_prefix = pre | ((unsigned)t << shift);
+            s_rank = r - excl;
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        const double v = (double)sel_unkey32(s_prefix);
+        s->prefix = sel_key(v);
+        s->rank = s_rank;
+        s->value = v;
+    }
+}
+
 // The select kernels' dynamic shared-memory limits, once per device.
 static int select_setup() {
     int dev = 0;
@@ -306,9 +403,9 @@ static int select_setup() {
         SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small<double>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
-        SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small<float>,
+        SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small_f32,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
+                                         (int)(SEL_SMALL_CAP * sizeof(unsigned))));
         SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_compact,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(SEL_CAND_CAP * sizeof(unsigned long long))));
@@ -359,8 +456,8 @@ int launch_select_small_f32(const float *x, long n, long long rank, SelState *st
     const int rc = select_setup();
     if (rc) return rc;
     count_launch();
-    k_sel_small<float><<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(x, n, rank,
-                                                                                 state);
+    k_sel_small_f32<<<1, SEL32_T, (size_t)n * sizeof(unsigned), st>>>(x, (int)n, (unsigned)rank,
+                                                                       state);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

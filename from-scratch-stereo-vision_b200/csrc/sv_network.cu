@@ -51,29 +51,33 @@ __device__ __forceinline__ double blend64(const T *x, const Taps &t) {
 }
 
 // resize_gray of a left/right pair (blockIdx.z) from full resolution to the
-// work resolution, FP64 blend, FP32 output for the network.  Also writes
-// avgpool2 of the left result when guide_half != nullptr is requested by a
-// second launch (k_avgpool2).
+// work resolution, FP64 blend, FP32 output for the network; with gh, also
+// the guide at half resolution, avgpool2 of the resized left view
+// (stereonet.py:979-995), from the 2x2 blocks a 32 x 8 CTA holds in shared
+// memory.
 template <typename T>
-__global__ void k_resize_pair(const T *__restrict__ l, const T *__restrict__ r, int W, int H,
-                              int W2, int H2, float *__restrict__ lo, float *__restrict__ ro,
-                              float *__restrict__ gh) {
+__global__ void __launch_bounds__(256)
+    k_resize_pair(const T *__restrict__ l, const T *__restrict__ r, int W, int H, int W2, int H2,
+                  float *__restrict__ lo, float *__restrict__ ro, float *__restrict__ gh) {
+    __shared__ float sv[8][33];
     const T *src = blockIdx.z ? r : l;
     float *dst = blockIdx.z ? ro : lo;
-    int ox = blockIdx.x * blockDim.x + threadIdx.x;
-    int oy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ox >= W2 || oy >= H2) return;
-    const float v = (float)blend64<T>(src, bilinear_taps(oy, ox, H, W, H2, W2));
-    dst[oy * W2 + ox] = v;
-    // the guide at half resolution, avgpool2 of the resized left view
-    // (stereonet.py:979-995): the top-left thread of each 2x2 block
-    // recomputes its three neighbours' values, which are the ones stored
-    if (gh && blockIdx.z == 0 && !(ox & 1) && !(oy & 1) && ox / 2 < W2 / 2 && oy / 2 < H2 / 2) {
-        const float v01 = (float)blend64<T>(src, bilinear_taps(oy, ox + 1, H, W, H2, W2));
-        const float v10 = (float)blend64<T>(src, bilinear_taps(oy + 1, ox, H, W, H2, W2));
-        const float v11 = (float)blend64<T>(src, bilinear_taps(oy + 1, ox + 1, H, W, H2, W2));
-        gh[(oy / 2) * (W2 / 2) + ox / 2] = 0.25f * (((v + v01) + v10) + v11);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int ox = blockIdx.x * 32 + tx, oy = blockIdx.y * 8 + ty;
+    const bool in = ox < W2 && oy < H2;
+    float v = 0.f;
+    if (in) {
+        v = (float)blend64<T>(src, bilinear_taps(oy, ox, H, W, H2, W2));
+        dst[oy * W2 + ox] = v;
     }
+    if (!gh || blockIdx.z != 0) return;            // the same for the whole CTA
+    sv[ty][tx] = v;
+    __syncthreads();
+    // a 2x2 block inside the half-resolution image lies inside the image
+    // and inside this CTA (its origin is even, the CTA 32 x 8)
+    if (in && !(tx & 1) && !(ty & 1) && ox / 2 < W2 / 2 && oy / 2 < H2 / 2)
+        gh[(oy / 2) * (W2 / 2) + ox / 2] =
+            0.25f * (((v + sv[ty][tx + 1]) + sv[ty + 1][tx]) + sv[ty + 1][tx + 1]);
 }
 
 // Copy (no resample) of a pair into FP32, for predict at native resolution.
@@ -731,7 +735,7 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         k_conv2d_tiled<1, C, FG, 1, 1><<<fg1, tb1, conv2d_tile_bytes(1, 2, 1), st>>>(
             left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
         count_launch();
-        k_conv2d_tiled<C, C, FG, 1, 1><<<fg, tb1, conv2d_tile_bytes(C, 2, 1), st>>>(
+        k_conv2d_tiled<C, C, FG, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 2, 1, 2), st>>>(
             b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
         count_launch();
         k_conv2d_tiled<C, C, FG, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(

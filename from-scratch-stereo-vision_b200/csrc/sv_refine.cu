@@ -51,6 +51,27 @@ __global__ void k_base(const double *__restrict__ disp0, long N,
 // the top bit, exactly as the reference builds its Python int.
 constexpr int CT_W = 32, CT_H = 8;
 
+// The census word of the pixel at ctr (in a tile of CT_W + 2 RX columns)
+// with the window fixed at compile time: every offset's bit position is a
+// constant, so each neighbour costs a compare and an OR.
+template <typename T, int RX, int RY>
+__device__ __forceinline__ uint64_t census_bits(const T *ctr) {
+    constexpr int SW = CT_W + 2 * RX, WX = 2 * RX + 1;
+    constexpr int CENTRE = RY * WX + RX, NB = (2 * RY + 1) * WX - 1;
+    const T c = *ctr;
+    unsigned half[2] = {0u, 0u};
+#pragma unroll
+    for (int dy = -RY; dy <= RY; ++dy)
+#pragma unroll
+        for (int dx = -RX; dx <= RX; ++dx) {
+            const int lin = (dy + RY) * WX + dx + RX;
+            if (lin == CENTRE) continue;
+            const int bit = NB - 1 - (lin > CENTRE ? lin - 1 : lin);
+            half[bit >> 5] |= (unsigned)(ctr[dy * SW + dx] < c) << (bit & 31);
+        }
+    return ((uint64_t)half[1] << 32) | half[0];
+}
+
 // One CT_W x CT_H tile starting at (tx0, ty0), called by a whole CTA.
 template <typename T>
 __device__ __forceinline__ void census_tile(const T *__restrict__ img, int W, int H, int rx,
@@ -68,6 +89,10 @@ __device__ __forceinline__ void census_tile(const T *__restrict__ img, int W, in
     const int x = tx0 + threadIdx.x, y = ty0 + threadIdx.y;
     if (x >= W || y >= H) return;
     const T *ctr = tile + (threadIdx.y + ry) * sw + threadIdx.x + rx;
+    if (rx == 4 && ry == 3) {       // the 9 x 7 window of refine_disparity
+        out[(long)y * W + x] = census_bits<T, 4, 3>(ctr);
+        return;
+    }
     const T c = *ctr;
     uint64_t s = 0;
     for (int dy = -ry; dy <= ry; ++dy) {

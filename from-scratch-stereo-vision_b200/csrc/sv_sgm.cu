@@ -41,23 +41,28 @@ __device__ __forceinline__ void dir_of(int d, int &dx, int &dy) {
 }
 
 // ----------------------------------------------------------- band costs
-// The Kp slots of pixel p (slot 0 and padding are 0).
+// The Kp slots of pixel p (slot 0 and padding are 0).  KPC / KC > 0 fix Kp
+// and K at compile time (the loops unroll, the band tests fold).
+template <int KPC = 0, int KC = 0>
 __device__ __forceinline__ void cost_pixel_slot(const uint64_t *__restrict__ ref,
                                                 const uint64_t *__restrict__ oth,
                                                 const int32_t *__restrict__ base, int W, long p,
                                                 int R, int K, int Kp, int invalid, int view,
                                                 uint8_t *__restrict__ C, int rk) {
-    const int x = (int)(p % W);
+    const int kp = KPC > 0 ? KPC : Kp;
+    const int kk = KC > 0 ? KC : K;
+    const int x = p <= 0x7fffffffL ? (int)p % W : (int)(p % W);
     const uint64_t a = ref[p];
     const int b = base[p] - R;
-    uint64_t *dst = reinterpret_cast<uint64_t *>(C + p * Kp);
-    for (int c = 0; c < Kp; c += 8) {
-        uint64_t word = 0;
+    uint64_t *dst = reinterpret_cast<uint64_t *>(C + p * kp);
+#pragma unroll
+    for (int c = 0; c < kp; c += 8) {
+        unsigned half[2] = {0u, 0u};
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const int k = c + u - 1;
-            uint64_t v = 0;
-            if (k >= 0 && k < K) {
+            unsigned v = 0;
+            if (k >= 0 && k < kk) {
                 const int d = b + k;
                 int cost = invalid;
                 if (abs(k - R) > rk) {
@@ -66,15 +71,16 @@ __device__ __forceinline__ void cost_pixel_slot(const uint64_t *__restrict__ ref
                 } else {
                     if (d >= 0 && x + d <= W - 1) cost = __popcll(a ^ oth[p + d]);
                 }
-                v = (uint64_t)cost;
+                v = (unsigned)cost;
             }
-            word |= v << (8 * u);
+            half[u >> 2] |= v << (8 * (u & 3));
         }
-        dst[c >> 3] = word;
+        dst[c >> 3] = ((uint64_t)half[1] << 32) | half[0];
     }
 }
 
 // One thread per pixel writes its Kp slots.
+template <int KPC, int KC>
 __global__ void __launch_bounds__(256)
     k_band_costs_slot(const uint64_t *__restrict__ cl, const uint64_t *__restrict__ cr,
                       const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
@@ -87,8 +93,8 @@ __global__ void __launch_bounds__(256)
     uint8_t *C = view ? C1 : C0;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < N;
          p += (long)gridDim.x * blockDim.x)
-        cost_pixel_slot(ref, oth, base, W, p, R, K, Kp, invalid, view, C,
-                        view == 0 && rad0 ? (int)rad0[p] : R);
+        cost_pixel_slot<KPC, KC>(ref, oth, base, W, p, R, K, Kp, invalid, view, C,
+                                 view == 0 && rad0 ? (int)rad0[p] : R);
 }
 
 // ------------------------------------------------------------------ SGM
@@ -340,7 +346,9 @@ __device__ __forceinline__ void scanline_of(int W, int H, int dx, int dy, int j0
 
 // One scanline swept by one thread.  Cimg / base / Lo are the costs, band
 // centres and path-cost array of one view (and one direction for Lo).
-template <int NR, typename LT>
+// KC > 0 fixes K at compile time: the band masks of the slot registers
+// become constants and their selects fold away.
+template <int NR, typename LT, int KC = 0>
 __device__ __forceinline__ void sgm_line_thread(const uint8_t *__restrict__ Cimg,
                                                 const int32_t *__restrict__ base_img,
                                                 LT *__restrict__ Lo_img, int W, int K, int P1,
@@ -356,11 +364,12 @@ __device__ __forceinline__ void sgm_line_thread(const uint8_t *__restrict__ Cimg
     LT *__restrict__ Lo = Lo_img + p0 * Kp;
     const long lstep = step * Kp;
 
+    const int Kb = KC > 0 ? KC : K;
     unsigned vm[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) {
         const int sa = 2 * r, sb = sa + 1;
-        vm[r] = ((sa >= 1 && sa <= K) ? 0x0000FFFFu : 0u) | ((sb >= 1 && sb <= K) ? 0xFFFF0000u : 0u);
+        vm[r] = ((sa >= 1 && sa <= Kb) ? 0x0000FFFFu : 0u) | ((sb >= 1 && sb <= Kb) ? 0xFFFF0000u : 0u);
     }
     const unsigned P1P1 = (unsigned)P1 * 0x10001u;
 
@@ -459,7 +468,7 @@ __device__ __forceinline__ void sgm_line_thread(const uint8_t *__restrict__ Cimg
     }
 }
 
-template <int NR, typename LT>
+template <int NR, typename LT, int KC>
 __global__ void __launch_bounds__(128)
     k_sgm_thread(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
                  const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
@@ -476,9 +485,9 @@ __global__ void __launch_bounds__(128)
     dir_of(dir, dx, dy);
     scanline_of(W, H, dx, dy, j0, x0, y0, n);
     const long N = (long)W * H;
-    sgm_line_thread<NR, LT>(view ? C1 : C0, view ? base1 : base0,
-                            Lout + (long)(view * npaths + dir) * N * Kp, W, K, P1, P2, dx, dy,
-                            x0, y0, n);
+    sgm_line_thread<NR, LT, KC>(view ? C1 : C0, view ? base1 : base0,
+                                Lout + (long)(view * npaths + dir) * N * Kp, W, K, P1, P2, dx,
+                                dy, x0, y0, n);
 }
 
 // ------------------------------------------------------------------ WTA
@@ -490,14 +499,16 @@ __device__ __forceinline__ int path_sum_slot(const LT *__restrict__ L, long stri
     return acc;
 }
 
-template <typename LT>
+template <typename LT, int KPC = 0, int NPC = 0>
 __device__ __forceinline__ void wta_pixel(const LT *__restrict__ Lp, long stride, int npaths,
                                           int K, int Kp, int R, int32_t base_p,
                                           const double *__restrict__ d0p, double uniq,
                                           bool want_conf, double *__restrict__ outp,
                                           double *__restrict__ confp);
 
-template <typename LT>
+// nviews <= 2; KPC / NPC > 0 fix Kp and the path count at compile time, so
+// a pixel's loads all issue before its first sum.
+template <typename LT, int KPC, int NPC>
 __global__ void __launch_bounds__(256)
     k_wta_slot(const LT *__restrict__ Lall, int npaths, int nviews, long N, int K, int Kp, int R,
                const int32_t *__restrict__ base0, const int32_t *__restrict__ base1,
@@ -507,9 +518,9 @@ __global__ void __launch_bounds__(256)
     const long stride = N * Kp;                            // between path arrays
     for (long w = blockIdx.x * (long)blockDim.x + threadIdx.x; w < nviews * N;
          w += (long)gridDim.x * blockDim.x) {
-        const int view = (int)(w / N);
+        const int view = w >= N ? 1 : 0;
         const long p = w - view * N;
-        wta_pixel<LT>(Lall + (long)view * npaths * stride + p * Kp, stride, npaths, K, Kp, R,
+        wta_pixel<LT, KPC, NPC>(Lall + (long)view * npaths * stride + p * Kp, stride, npaths, K, Kp, R,
                       (view ? base1 : base0)[p], (view ? d01 : d00) + p, uniq,
                       want_conf && view == 0, (view ? out1 : out0) + p,
                       conf0 ? conf0 + p : nullptr);
@@ -518,18 +529,21 @@ __global__ void __launch_bounds__(256)
 
 // S = sum of the path costs at one pixel (Lp: its row in path array 0),
 // first minimum, FP64 parabola (stereonet.py:5271-5303).
-template <typename LT>
+template <typename LT, int KPC, int NPC>
 __device__ __forceinline__ void wta_pixel(const LT *__restrict__ Lp, long stride, int npaths,
                                           int K, int Kp, int R, int32_t base_p,
                                           const double *__restrict__ d0p, double uniq,
                                           bool want_conf, double *__restrict__ outp,
                                           double *__restrict__ confp) {
     constexpr int PER64 = 8 / sizeof(LT);                  // slots per 64-bit load
+    const int kp = KPC > 0 ? KPC : Kp, np = NPC > 0 ? NPC : npaths;
     {
         int bv = 0x7FFFFFFF, bs = -1;                      // best value, its slot
-        for (int c = 0; c < Kp; c += 8) {
+#pragma unroll
+        for (int c = 0; c < kp; c += 8) {
             unsigned acc[4] = {0u, 0u, 0u, 0u};            // 8 slots as u16x2
-            for (int d = 0; d < npaths; ++d) {
+#pragma unroll
+            for (int d = 0; d < np; ++d) {
                 if (PER64 == 8) {
                     const uint2 v = __ldg(reinterpret_cast<const uint2 *>(Lp + d * stride + c));
                     acc[0] += __byte_perm(v.x, 0, 0x4140);
@@ -560,14 +574,14 @@ __device__ __forceinline__ void wta_pixel(const LT *__restrict__ Lp, long stride
             if (want_conf) *confp = 0.0;
             return;
         }
-        const int va = path_sum_slot(Lp, stride, npaths, bs - 1);
-        const int vb = path_sum_slot(Lp, stride, npaths, bs + 1);
+        const int va = path_sum_slot(Lp, stride, np, bs - 1);
+        const int vb = path_sum_slot(Lp, stride, np, bs + 1);
         bool use_d0 = false;
         if (uniq > 0.0 || want_conf) {
             // second best away from the winner's neighbours (stereonet.py:5286-5290)
             int sv = 0x7FFFFFFF;
             for (int k = 0; k < K; ++k)
-                if (k < bk - 1 || k > bk + 1) sv = min(sv, path_sum_slot(Lp, stride, npaths, k + 1));
+                if (k < bk - 1 || k > bk + 1) sv = min(sv, path_sum_slot(Lp, stride, np, k + 1));
             double conf = 1.0;
             if (sv != 0x7FFFFFFF) {
                 const double dsv = (double)sv, dbv = (double)bv;
@@ -615,8 +629,12 @@ int launch_band_costs_slot(const uint64_t *cl, const uint64_t *cr, const int32_t
     const int K = 2 * R + 1;
     dim3 grd(grid_for(N, 256, 148 * 8), nviews);
     count_launch();
-    k_band_costs_slot<<<grd, 256, 0, st>>>(cl, cr, base0, base1, W, N, R, K, slot_width(K),
-                                           invalid, C0, C1, rad0);
+    if (K == 21)    // R = 10, the refine_disparity default: 24 slots
+        k_band_costs_slot<24, 21><<<grd, 256, 0, st>>>(cl, cr, base0, base1, W, N, R, K, 24,
+                                                       invalid, C0, C1, rad0);
+    else
+        k_band_costs_slot<0, 0><<<grd, 256, 0, st>>>(cl, cr, base0, base1, W, N, R, K,
+                                                     slot_width(K), invalid, C0, C1, rad0);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -636,15 +654,15 @@ static int sgm_packed_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0
     return SV_OK;
 }
 
-template <int NR, typename LT>
+template <int NR, typename LT, int KC = 0>
 static int sgm_thread_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
                          const int32_t *b1, int W, int H, int K, int P1, int P2, void *Lout,
                          int npaths, const SgmTasks &t, cudaStream_t st) {
     const long threads = t.start[t.nseg];
     const int blocks = (int)((threads + 127) / 128);
     count_launch();
-    k_sgm_thread<NR, LT><<<blocks, 128, 0, st>>>(C0, C1, b0, b1, W, H, K, P1, P2, (LT *)Lout,
-                                                  npaths, t);
+    k_sgm_thread<NR, LT, KC><<<blocks, 128, 0, st>>>(C0, C1, b0, b1, W, H, K, P1, P2,
+                                                      (LT *)Lout, npaths, t);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -658,7 +676,10 @@ static int sgm_packed_dispatch(const uint8_t *C0, const uint8_t *C1, const int32
     switch (g.Kp) {
     case 8: return sgm_thread_go<4, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
     case 16: return sgm_thread_go<8, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
-    case 24: return sgm_thread_go<12, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+    case 24:
+        if (K == 21)    // R = 10, the refine_disparity default
+            return sgm_thread_go<12, LT, 21>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        return sgm_thread_go<12, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
     case 32: return sgm_thread_go<16, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
     default: break;
     }
@@ -698,14 +719,22 @@ int launch_wta_slot(const void *L, bool l16, int npaths, int nviews, int W, int 
     const int Kp = slot_width(K);
     const int blocks = grid_for(nviews * N, 256, 148 * 16);
     count_launch();
+    if (nviews < 1 || nviews > 2) {
+        set_error("wta: nviews=%d", nviews);
+        return SV_ERR_PARAM;
+    }
     if (l16)
-        k_wta_slot<uint16_t><<<blocks, 256, 0, st>>>((const uint16_t *)L, npaths, nviews, N, K, Kp,
-                                                     R, b0, b1, d00, d01, uniq, conf0 != nullptr,
-                                                     out0, out1, conf0);
+        k_wta_slot<uint16_t, 0, 0><<<blocks, 256, 0, st>>>(
+            (const uint16_t *)L, npaths, nviews, N, K, Kp, R, b0, b1, d00, d01, uniq,
+            conf0 != nullptr, out0, out1, conf0);
+    else if (Kp == 24 && npaths == 8)    // R = 10 over the 8 paths
+        k_wta_slot<uint8_t, 24, 8><<<blocks, 256, 0, st>>>(
+            (const uint8_t *)L, npaths, nviews, N, K, Kp, R, b0, b1, d00, d01, uniq,
+            conf0 != nullptr, out0, out1, conf0);
     else
-        k_wta_slot<uint8_t><<<blocks, 256, 0, st>>>((const uint8_t *)L, npaths, nviews, N, K, Kp,
-                                                    R, b0, b1, d00, d01, uniq, conf0 != nullptr,
-                                                    out0, out1, conf0);
+        k_wta_slot<uint8_t, 0, 0><<<blocks, 256, 0, st>>>(
+            (const uint8_t *)L, npaths, nviews, N, K, Kp, R, b0, b1, d00, d01, uniq,
+            conf0 != nullptr, out0, out1, conf0);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

@@ -424,10 +424,13 @@ __device__ __forceinline__ void c3_taps(const float *tb, const float *wb, float 
                 for (int kx = 0; kx < 3; ++kx) {
                     const float v = tb[j * P + kd * DS + ky * C3_RS + kx];
                     const float *wt = wb + (j * 27 + kd * 9 + ky * 3 + kx) * OCG;
-                    if (OCG == 2) {
-                        const float2 ww = *reinterpret_cast<const float2 *>(wt);
-                        acc[0] = fmaf(v, ww.x, acc[0]);
-                        acc[1] = fmaf(v, ww.y, acc[1]);
+                    if (OCG % 2 == 0) {
+#pragma unroll
+                        for (int o = 0; o < OCG; o += 2) {
+                            const float2 ww = *reinterpret_cast<const float2 *>(wt + o);
+                            acc[o] = fmaf(v, ww.x, acc[o]);
+                            acc[o + 1] = fmaf(v, ww.y, acc[o + 1]);
+                        }
                     } else {
 #pragma unroll
                         for (int o = 0; o < OCG; ++o) acc[o] = fmaf(v, wt[o], acc[o]);
@@ -744,8 +747,9 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         k_conv2d_tiled<C, C, FG, 0, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
             b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
         SV_LAUNCH_CHECK();
-        // cost volume + CostFilter c1, c2 (2 output channels per CTA)
-        constexpr int CG = CM % 2 == 0 ? 2 : CM;
+        // cost volume + CostFilter c1, c2 (every output channel in each CTA,
+        // so the tile is staged once)
+        constexpr int CG = CM;
         constexpr int S1 = C % 4 == 0 ? 4 : 2, S2 = CM % 4 == 0 && CM > 4 ? 4 : 2;
         const dim3 vg1((w + C3_TX - 1) / C3_TX, h * ((D + 16 / S1 - 1) / (16 / S1)), CM / CG);
         const dim3 vg2((w + C3_TX - 1) / C3_TX, h * ((D + 16 / S2 - 1) / (16 / S2)), CM / CG);
@@ -772,6 +776,7 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         const float *cur = nullptr;
         float *bufs[2] = {b.ra, b.rb};
         constexpr int RG = RC % 4 == 0 ? 4 : RC;
+        constexpr int RS = RC % 4 == 0 ? 4 : 2;     // lanes per output of the dilated convs
         for (int i = 0; i < n.ndil; ++i) {
             float *dst = bufs[i & 1];
             const int dl = n.dil[i];
@@ -781,8 +786,8 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
                                       st>>>(prev, ph, pw, guides[lv], Hl, Wl, dl, n.rw[lv][i],
                                             n.rb[lv][i], dst, b.rin);
             else
-                k_conv2d_tiled<RC, RC, RG, 1, 2><<<tgrid(Wl, Hl, RC / RG), tb2,
-                                                   conv2d_tile_bytes(RC, 1, dl, 2), st>>>(
+                k_conv2d_tiled<RC, RC, RG, 1, RS><<<tgrid(Wl, Hl, RC / RG), RS * tb1,
+                                                    conv2d_tile_bytes(RC, 1, dl, RS), st>>>(
                     cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
                     nullptr);
             cur = dst;

@@ -2,7 +2,9 @@
 // checkpoint upload, StereoNet.forward, resize, predict_at_scale and the
 // host-side control flow of predict_auto (stereonet.py:3872-3960).
 
+#include <chrono>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -31,6 +33,7 @@ struct sv_graph_entry {
     cudaGraphExec_t exec;
     unsigned long long kernels;
     int device;
+    double *slot;             // mapped pinned slot the stage's peak lands in, or NULL
 };
 
 struct sv_net {
@@ -245,81 +248,177 @@ static void work_dims(int W, int H, int work, int *Ww, int *Hw) {
 // through a pinned 8-byte slot per host thread (a copy into pageable memory
 // is staged by the driver and returns later); the stack is the fallback if
 // the slot cannot be had.
-static int fetch_peak(const PredictWs &w, cudaStream_t st, double *peak) {
-    struct Slot {
-        double *p = nullptr;
-        ~Slot() {
-            if (p) cudaFreeHost(p);
+static int wait_slot(double *slot, cudaStream_t st, double *out);
+
+// The peak of the stage just queued on st (floored like _peak): from its
+// mapped slot when it published one, else copied out of the workspace.
+static int fetch_peak(const PredictWs &w, cudaStream_t st, double *slot, double *peak) {
+    double v = 0.0;
+    if (slot) {
+        SV_TRY(wait_slot(slot, st, &v));
+    } else {
+        struct Slot {
+            double *p = nullptr;
+            ~Slot() {
+                if (p) cudaFreeHost(p);
+            }
+        };
+        static thread_local Slot pinned;
+        if (!pinned.p &&
+            cudaMallocHost(reinterpret_cast<void **>(&pinned.p), sizeof(double)) != cudaSuccess) {
+            pinned.p = nullptr;
+            cudaGetLastError();
         }
-    };
-    static thread_local Slot slot;
-    if (!slot.p && cudaMallocHost(reinterpret_cast<void **>(&slot.p), sizeof(double)) != cudaSuccess) {
-        slot.p = nullptr;
-        cudaGetLastError();
+        double local = 0.0;
+        double *dst = pinned.p ? pinned.p : &local;
+        SV_CUDA_TRY(cudaMemcpyAsync(dst,
+                                    reinterpret_cast<const char *>(w.sel) + select_value_offset(),
+                                    sizeof(double), cudaMemcpyDeviceToHost, st));
+        SV_CUDA_TRY(cudaStreamSynchronize(st));
+        v = *dst;
     }
-    double local = 0.0;
-    double *dst = slot.p ? slot.p : &local;
-    SV_CUDA_TRY(cudaMemcpyAsync(dst, reinterpret_cast<const char *>(w.sel) + select_value_offset(),
-                                sizeof(double), cudaMemcpyDeviceToHost, st));
-    SV_CUDA_TRY(cudaStreamSynchronize(st));
-    const double v = *dst;
     *peak = v > 0.5 ? v : 0.5;                      // _peak's floor
     return SV_OK;
+}
+
+// A stage that ends with a peak selection publishes the value into a small
+// mapped pinned host slot owned by its graph: the host polls the slot
+// instead of queueing a device-to-host copy and synchronising the stream.
+// Before each launch the slot holds kSlotEmpty, a NaN no selection returns.
+constexpr uint64_t kSlotEmpty = 0x7ff4a5a5a5a5a5a5ull;
+
+static void arm_slot(double *slot) {
+    *reinterpret_cast<volatile uint64_t *>(slot) = kSlotEmpty;
+}
+
+// Wait for the stage launched on st to fill slot.  Bounded: a stream that
+// drains (or fails) without filling it, or a minute without a value, is an
+// error.
+static int wait_slot(double *slot, cudaStream_t st, double *out) {
+    const volatile uint64_t *p = reinterpret_cast<const volatile uint64_t *>(slot);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned long i = 1;; ++i) {
+        uint64_t b = *p;
+        if (b != kSlotEmpty) {
+            memcpy(out, &b, sizeof(b));
+            return SV_OK;
+        }
+        if ((i & 1023) == 0) {
+            const cudaError_t q = cudaStreamQuery(st);
+            if (q == cudaSuccess) {             // the stage is done: its store is visible
+                b = *p;
+                if (b != kSlotEmpty) {
+                    memcpy(out, &b, sizeof(b));
+                    return SV_OK;
+                }
+                set_error("peak slot not written by the finished stage");
+                return SV_ERR_CUDA;
+            }
+            if (q != cudaErrorNotReady) {
+                set_error("stage failed: %s", cudaGetErrorString(q));
+                return SV_ERR_CUDA;
+            }
+            if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60)) {
+                set_error("peak selection did not finish within 60 s");
+                return SV_ERR_CUDA;
+            }
+        }
+    }
 }
 
 // Run one predict_auto stage.  On a capturable stream the stage is recorded
 // into a CUDA graph the first time (per shape, buffers and device) and
 // replayed afterwards, so a network pass costs one launch on the host.  On
 // the legacy default stream, or inside the caller's own capture, the
-// kernels are enqueued directly.
+// kernels are enqueued directly.  enqueue(mirror) queues the stage; with
+// publish, a graphed stage gets a mapped slot as mirror and *slot points at
+// its host side (NULL otherwise: read the peak from the workspace).
 constexpr size_t kMaxGraphs = 48;
 
 template <typename F>
-static int run_stage(sv_net *net, const sv_graph_key &key, cudaStream_t st, F &&enqueue) {
-    if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread) return enqueue();
+static int run_stage(sv_net *net, const sv_graph_key &key, cudaStream_t st, bool publish,
+                     double **slot, F &&enqueue) {
+    *slot = nullptr;
+    if (st == nullptr || st == cudaStreamLegacy || st == cudaStreamPerThread)
+        return enqueue(nullptr);
     cudaStreamCaptureStatus cs;
     SV_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
-    if (cs != cudaStreamCaptureStatusNone) return enqueue();
+    if (cs != cudaStreamCaptureStatusNone) return enqueue(nullptr);
     int dev = 0;
     SV_CUDA_TRY(cudaGetDevice(&dev));
     {
         std::lock_guard<std::mutex> lock(net->graph_mu);
         for (auto &g : net->graphs) {
             if (g.device == dev && g.key == key) {
+                if (publish && g.slot) arm_slot(g.slot);
                 SV_CUDA_TRY(cudaGraphLaunch(g.exec, st));
                 count_launches(g.kernels);
+                if (publish) *slot = g.slot;
                 return SV_OK;
             }
         }
     }
+    double *host = nullptr, *mirror = nullptr;
+    if (publish) {
+        void *h = nullptr, *d = nullptr;
+        SV_CUDA_TRY(cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable));
+        const cudaError_t e = cudaHostGetDevicePointer(&d, h, 0);
+        if (e != cudaSuccess) {
+            cudaFreeHost(h);
+            set_error("mapped slot: %s", cudaGetErrorString(e));
+            return SV_ERR_CUDA;
+        }
+        host = static_cast<double *>(h);
+        mirror = static_cast<double *>(d);
+    }
     const unsigned long long before = launch_count_now();
-    SV_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    const int rc = enqueue();
+    {
+        const cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            if (host) cudaFreeHost(host);
+            set_error("stream capture failed: %s", cudaGetErrorString(e));
+            return SV_ERR_CUDA;
+        }
+    }
+    const int rc = enqueue(mirror);
     cudaGraph_t graph = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &graph);
     const unsigned long long kernels = launch_count_now() - before;
     uncount_launches(kernels);                       // they run at the launch below
-    if (rc || e != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
-        if (rc) return rc;
-        set_error("stream capture failed: %s", cudaGetErrorString(e));
-        return SV_ERR_CUDA;
-    }
     cudaGraphExec_t exec = nullptr;
-    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ei != cudaSuccess) {
-        set_error("graph instantiation failed: %s", cudaGetErrorString(ei));
+    cudaError_t ei = cudaSuccess;
+    if (!rc && e == cudaSuccess) ei = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc || e != cudaSuccess || ei != cudaSuccess) {
+        if (host) cudaFreeHost(host);
+        if (rc) return rc;
+        set_error("%s failed: %s", e != cudaSuccess ? "stream capture" : "graph instantiation",
+                  cudaGetErrorString(e != cudaSuccess ? e : ei));
         return SV_ERR_CUDA;
     }
-    SV_CUDA_TRY(cudaGraphLaunch(exec, st));
+    if (host) arm_slot(host);
+    {
+        const cudaError_t el = cudaGraphLaunch(exec, st);
+        if (el != cudaSuccess) {
+            cudaGraphExecDestroy(exec);
+            if (host) cudaFreeHost(host);
+            set_error("graph launch failed: %s", cudaGetErrorString(el));
+            return SV_ERR_CUDA;
+        }
+    }
     count_launches(kernels);
+    *slot = host;
     std::lock_guard<std::mutex> lock(net->graph_mu);
     if (net->graphs.size() >= kMaxGraphs) {
-        cudaGraphExecDestroy(net->graphs.front().exec);
+        sv_graph_entry &old = net->graphs.front();
+        cudaGraphExecDestroy(old.exec);
+        if (old.slot) {
+            cudaDeviceSynchronize();                 // its last launch may still write the slot
+            cudaFreeHost(old.slot);
+        }
         net->graphs.erase(net->graphs.begin());
     }
-    net->graphs.push_back({key, exec, kernels, dev});
+    net->graphs.push_back({key, exec, kernels, dev, host});
     return SV_OK;
 }
 
@@ -394,7 +493,10 @@ int sv_net_create(const int *arch, int n_arch, const double *params, long n_para
 
 void sv_net_destroy(sv_net *net) {
     if (!net) return;
-    for (auto &g : net->graphs) cudaGraphExecDestroy(g.exec);
+    for (auto &g : net->graphs) {
+        cudaGraphExecDestroy(g.exec);
+        if (g.slot) cudaFreeHost(g.slot);
+    }
     if (net->dev) cudaFree(net->dev);
     if (net->tc) cudaFree(net->tc);
     delete net;
@@ -513,21 +615,22 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     if (ph < 8) ph = 8;
     sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, precision, left, right, disp_full,
                      disp_work, workspace};
-    SV_TRY(run_stage(mnet, key, st, [&]() -> int {
+    double *slot = nullptr;
+    SV_TRY(run_stage(mnet, key, st, true, &slot, [&](double *mirror) -> int {
         int rc = check_net_shape(net->view, ph, pw);
         if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh);
         if (!rc) rc = predict_f32(net, w, pw, ph, precision, st, true);
         const long np = (long)pw * ph;
         const long long rank = (long long)(np * 0.95);
-        if (!rc && np <= 16384) rc = launch_select_small_f32(w.d2, np, rank, w.sel, st);
+        if (!rc && np <= 16384) rc = launch_select_small_f32(w.d2, np, rank, w.sel, st, mirror);
         else if (!rc) {
             rc = launch_promote(w.d2, np, w.probe64, st);
-            if (!rc) rc = launch_select(w.probe64, np, rank, w.sel, w.hist, st);
+            if (!rc) rc = launch_select(w.probe64, np, rank, w.sel, w.hist, st, mirror);
         }
         return rc;
     }));
     double pk;
-    SV_TRY(fetch_peak(w, st, &pk));
+    SV_TRY(fetch_peak(w, st, slot, &pk));
     const double peak = pk * (W / (double)pw);
     int work = width_for(W, target_peak, max_width, peak);
     int nt = 0;
@@ -539,12 +642,12 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
         sv_graph_key k{1, W, H, dtype, work, with_sel ? 1 : 0, precision, left, right, disp_full,
                        disp_work, workspace};
         int Ww, Hw;
-        SV_TRY(run_stage(mnet, k, st, [&]() -> int {
+        SV_TRY(run_stage(mnet, k, st, with_sel, &slot, [&](double *mirror) -> int {
             int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, precision,
                                            disp_full, disp_work, &Ww, &Hw, st);
             if (!rc && with_sel)
                 rc = launch_select(disp_full, (long)W * H, (long long)((long)W * H * 0.95), w.sel,
-                                   w.hist, st);
+                                   w.hist, st, mirror);
             return rc;
         }));
         work_dims(W, H, work, &Ww, &Hw);
@@ -552,7 +655,7 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
         *pHw = Hw;
         if (!with_sel) break;
         double np_;
-        SV_TRY(fetch_peak(w, st, &np_));
+        SV_TRY(fetch_peak(w, st, slot, &np_));
         const int nw = width_for(W, target_peak, max_width, np_);
         if (std::abs(nw - work) <= 0.08 * work) break;
         work = nw;

@@ -81,11 +81,14 @@ int launch_forward(const NetView &n, const float *left, const float *right, int 
                    const FwdBufs &b, int precision, cudaStream_t st);
 
 struct SelState;
+// The rank-th smallest of x into state's value; with mirror (a device
+// pointer, e.g. to mapped pinned host memory) the last kernel also stores
+// the value there.
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
-                  cudaStream_t st);
+                  cudaStream_t st, double *mirror = nullptr);
 // the same over FP32 values (exactly their FP64 promotions), n <= 16384
 int launch_select_small_f32(const float *x, long n, long long rank, SelState *state,
-                            cudaStream_t st);
+                            cudaStream_t st, double *mirror = nullptr);
 size_t select_state_bytes();
 size_t select_value_offset();
 size_t select_hist_words();

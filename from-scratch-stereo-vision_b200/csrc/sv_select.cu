@@ -231,7 +231,7 @@ __device__ void sel_passes_cta(const unsigned long long *keys, const double *__r
 
 __global__ void __launch_bounds__(1024)
     k_sel_compact(const double *__restrict__ x, long n, SelState *__restrict__ s,
-                  unsigned long long *__restrict__ cand) {
+                  unsigned long long *__restrict__ cand, double *mirror) {
     extern __shared__ __align__(16) unsigned long long keys[];   // SEL_CAND_CAP
     __shared__ unsigned hist[SEL_NB];
     __shared__ unsigned wsum[32];
@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(1024)
         s->prefix = prefix;
         s->rank = rank;
         s->value = sel_unkey(prefix);
+        if (mirror) *reinterpret_cast<volatile double *>(mirror) = s->value;
     }
 }
 
@@ -299,7 +300,8 @@ constexpr long SEL_SMALL_CAP = 16384;     // keys (128 KB of dynamic shared memo
 
 template <typename T>
 __global__ void __launch_bounds__(1024)
-    k_sel_small(const T *__restrict__ x, long n, long long rank0, SelState *__restrict__ s) {
+    k_sel_small(const T *__restrict__ x, long n, long long rank0, SelState *__restrict__ s,
+                double *mirror) {
     extern __shared__ __align__(16) unsigned long long keys[];
     __shared__ unsigned hist[SEL_NB];
     __shared__ unsigned wsum[32];
@@ -316,6 +318,7 @@ __global__ void __launch_bounds__(1024)
         s->prefix = prefix;
         s->rank = rank;
         s->value = sel_unkey(prefix);
+        if (mirror) *reinterpret_cast<volatile double *>(mirror) = s->value;
     }
 }
 
@@ -338,7 +341,7 @@ __device__ __forceinline__ float sel_unkey32(unsigned k) {
 
 __global__ void __launch_bounds__(SEL32_T)
     k_sel_small_f32(const float *__restrict__ x, int n, unsigned rank0,
-                    SelState *__restrict__ s) {
+                    SelState *__restrict__ s, double *mirror) {
     extern __shared__ unsigned keys32[];
     __shared__ unsigned hist[SEL32_T];
     __shared__ unsigned wsum[SEL32_T / 32];
@@ -391,6 +394,7 @@ __global__ void __launch_bounds__(SEL32_T)
         s->prefix = sel_key(v);
         s->rank = s_rank;
         s->value = v;
+        if (mirror) *reinterpret_cast<volatile double *>(mirror) = v;
     }
 }
 
@@ -415,7 +419,7 @@ static int select_setup() {
 }
 
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
-                  cudaStream_t st) {
+                  cudaStream_t st, double *mirror) {
     if (n < 1 || n >= (1l << 32) || rank < 0 || rank >= n) {
         set_error("select: n=%ld rank=%lld", n, rank);
         return SV_ERR_PARAM;
@@ -426,8 +430,8 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
     }
     if (n <= SEL_SMALL_CAP) {
         count_launch();
-        k_sel_small<double><<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(x, n, rank,
-                                                                                    state);
+        k_sel_small<double><<<1, 1024, (size_t)n * sizeof(unsigned long long), st>>>(
+            x, n, rank, state, mirror);
         SV_LAUNCH_CHECK();
         return SV_OK;
     }
@@ -442,13 +446,13 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
     }
     count_launch();
     k_sel_compact<<<blocks, 1024, (size_t)SEL_CAND_CAP * sizeof(unsigned long long), st>>>(
-        x, n, state, cand);
+        x, n, state, cand, mirror);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
 
 int launch_select_small_f32(const float *x, long n, long long rank, SelState *state,
-                            cudaStream_t st) {
+                            cudaStream_t st, double *mirror) {
     if (n < 1 || n > SEL_SMALL_CAP || rank < 0 || rank >= n) {
         set_error("select: n=%ld rank=%lld", n, rank);
         return SV_ERR_PARAM;
@@ -457,7 +461,7 @@ int launch_select_small_f32(const float *x, long n, long long rank, SelState *st
     if (rc) return rc;
     count_launch();
     k_sel_small_f32<<<1, SEL32_T, (size_t)n * sizeof(unsigned), st>>>(x, (int)n, (unsigned)rank,
-                                                                       state);
+                                                                       state, mirror);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

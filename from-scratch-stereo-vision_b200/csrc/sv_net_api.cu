@@ -200,9 +200,13 @@ static int predict_f32(const sv_net *net, const PredictWs &w, int W, int H, int 
 static int predict_at_scale_impl(const sv_net *net, const PredictWs &w, const void *left,
                                  const void *right, int dtype, int W, int H, int work,
                                  int precision, double *disp_full, double *disp_work, int *pWw,
-                                 int *pHw, cudaStream_t st) {
+                                 int *pHw, cudaStream_t st, const SelFuse *fuse = nullptr) {
     int rc;
     if (work >= W) {
+        if (fuse) {
+            set_error("a select fused into a native-resolution pass");
+            return SV_ERR_PARAM;
+        }
         rc = launch_to_f32_pair(left, right, dtype, (long)W * H, w.lw, w.rw, st);
         if (!rc) rc = predict_f32(net, w, W, H, precision, st);
         if (!rc) rc = launch_promote(w.d2, (long)W * H, disp_full, st);
@@ -218,9 +222,12 @@ static int predict_at_scale_impl(const sv_net *net, const PredictWs &w, const vo
     int Hw = (int)(H * scale + 0.5);
     if (Hw < 8) Hw = 8;
     rc = check_net_shape(net->view, Hw, Ww);
-    if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, Ww, Hw, w.lw, w.rw, st, w.gh);
+    if (!rc)
+        rc = launch_resize_pair(left, right, dtype, W, H, Ww, Hw, w.lw, w.rw, st, w.gh, fuse);
     if (!rc) rc = predict_f32(net, w, Ww, Hw, precision, st, true);
-    if (!rc) rc = launch_work_outputs(w.d2, Ww, Hw, W, H, 1.0 / scale, disp_work, disp_full, st);
+    if (!rc)
+        rc = launch_work_outputs(w.d2, Ww, Hw, W, H, 1.0 / scale, disp_work, disp_full, st,
+                                 fuse);
     *pWw = Ww;
     *pHw = Hw;
     return rc;
@@ -643,11 +650,18 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
                        disp_work, workspace};
         int Ww, Hw;
         SV_TRY(run_stage(mnet, k, st, with_sel, &slot, [&](double *mirror) -> int {
+            // the select's pass 0 runs inside the pass when it resamples
+            const long nf = (long)W * H;
+            const long long rank = (long long)((long)W * H * 0.95);
+            const bool fuse = with_sel && work < W && nf > select_small_cap();
+            const SelFuse sf{w.sel, w.hist, rank};
             int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, precision,
-                                           disp_full, disp_work, &Ww, &Hw, st);
-            if (!rc && with_sel)
-                rc = launch_select(disp_full, (long)W * H, (long long)((long)W * H * 0.95), w.sel,
-                                   w.hist, st, mirror);
+                                           disp_full, disp_work, &Ww, &Hw, st,
+                                           fuse ? &sf : nullptr);
+            if (!rc && fuse)
+                rc = launch_select_after_pass0(disp_full, nf, w.sel, w.hist, st, mirror);
+            else if (!rc && with_sel)
+                rc = launch_select(disp_full, nf, rank, w.sel, w.hist, st, mirror);
             return rc;
         }));
         work_dims(W, H, work, &Ww, &Hw);

@@ -20,6 +20,7 @@
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
+#include "sv_select.cuh"
 #include "sv_tc.cuh"
 
 namespace sv {
@@ -58,8 +59,11 @@ __device__ __forceinline__ double blend64(const T *x, const Taps &t) {
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_resize_pair(const T *__restrict__ l, const T *__restrict__ r, int W, int H, int W2, int H2,
-                  float *__restrict__ lo, float *__restrict__ ro, float *__restrict__ gh) {
+                  float *__restrict__ lo, float *__restrict__ ro, float *__restrict__ gh,
+                  SelState *sel, unsigned *sel_hist, long long sel_rank) {
     __shared__ float sv[8][33];
+    if (sel && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
+        sel_init_block(sel, sel_rank, sel_hist);      // the stage's select starts here
     const T *src = blockIdx.z ? r : l;
     float *dst = blockIdx.z ? ro : lo;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -108,15 +112,29 @@ __global__ void k_resize_scale(const T *__restrict__ x, int W, int H, int W2, in
 // one launch: the full-resolution map, bilinear and times inv
 // (stereonet.py:3957-3959), and the work map itself promoted to FP64 by the
 // threads that fall inside it (the work map is never larger).
-__global__ void k_work_outputs(const float *__restrict__ d, int Ww, int Hw, int W, int H,
-                               double inv, double *__restrict__ work64,
-                               double *__restrict__ full64) {
-    int ox = blockIdx.x * blockDim.x + threadIdx.x;
-    int oy = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ox >= W || oy >= H) return;
-    Taps t = bilinear_taps(oy, ox, Hw, Ww, H, W);
-    full64[(long)oy * W + ox] = __dmul_rn(blend64<float>(d, t), inv);
-    if (ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
+// With sel, also pass 0 of the stage's full-resolution select over the
+// values it writes (the select's first histogram: ghist).
+__global__ void __launch_bounds__(256)
+    k_work_outputs(const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
+                   double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
+                   unsigned *ghist) {
+    __shared__ unsigned hist[SEL_NB];
+    const int ox = blockIdx.x * blockDim.x + threadIdx.x;
+    const int oy = blockIdx.y * blockDim.y + threadIdx.y;
+    const bool in = ox < W && oy < H;
+    double v = 0.0;
+    if (in) {
+        const Taps t = bilinear_taps(oy, ox, Hw, Ww, H, W);
+        v = __dmul_rn(blend64<float>(d, t), inv);
+        full64[(long)oy * W + ox] = v;
+        if (ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
+    }
+    if (!sel) return;                              // the same for every CTA
+    for (int i = sel_tid(); i < SEL_NB; i += sel_nt()) hist[i] = 0u;
+    __syncthreads();
+    sel_count(hist, sel_key(v), in, 0ull, 0);
+    __syncthreads();
+    sel_pass_finish(0, sel, ghist, hist);
 }
 
 template <typename T>
@@ -553,16 +571,19 @@ static dim3 grid2d(int W, int H, dim3 blk, int z = 1) {
 }
 
 int launch_resize_pair(const void *l, const void *r, int dtype, int W, int H, int W2, int H2,
-                       float *lo, float *ro, cudaStream_t st, float *gh) {
+                       float *lo, float *ro, cudaStream_t st, float *gh, const SelFuse *fuse) {
+    SelState *ss = fuse ? fuse->state : nullptr;
+    unsigned *sh = fuse ? fuse->hist : nullptr;
+    const long long sr = fuse ? fuse->rank : 0;
     dim3 blk(32, 8);
     dim3 g = grid2d(W2, H2, blk, 2);
     if (W2 == W && H2 == H) {
         // a resample to the same size still runs the reference's arithmetic
     }
     switch (dtype) {
-    case SV_U8: count_launch(); k_resize_pair<uint8_t><<<g, blk, 0, st>>>((const uint8_t *)l, (const uint8_t *)r, W, H, W2, H2, lo, ro, gh); break;
-    case SV_F32: count_launch(); k_resize_pair<float><<<g, blk, 0, st>>>((const float *)l, (const float *)r, W, H, W2, H2, lo, ro, gh); break;
-    case SV_F64: count_launch(); k_resize_pair<double><<<g, blk, 0, st>>>((const double *)l, (const double *)r, W, H, W2, H2, lo, ro, gh); break;
+    case SV_U8: count_launch(); k_resize_pair<uint8_t><<<g, blk, 0, st>>>((const uint8_t *)l, (const uint8_t *)r, W, H, W2, H2, lo, ro, gh, ss, sh, sr); break;
+    case SV_F32: count_launch(); k_resize_pair<float><<<g, blk, 0, st>>>((const float *)l, (const float *)r, W, H, W2, H2, lo, ro, gh, ss, sh, sr); break;
+    case SV_F64: count_launch(); k_resize_pair<double><<<g, blk, 0, st>>>((const double *)l, (const double *)r, W, H, W2, H2, lo, ro, gh, ss, sh, sr); break;
     default: set_error("unknown dtype %d", dtype); return SV_ERR_PARAM;
     }
     SV_LAUNCH_CHECK();
@@ -599,14 +620,16 @@ int launch_upscale_disp(const float *dw, int Ww, int Hw, int W, int H, double in
 }
 
 int launch_work_outputs(const float *d, int Ww, int Hw, int W, int H, double inv,
-                        double *work64, double *full64, cudaStream_t st) {
+                        double *work64, double *full64, cudaStream_t st, const SelFuse *fuse) {
     if (Ww > W || Hw > H) {
         set_error("work map %dx%d larger than %dx%d", Ww, Hw, W, H);
         return SV_ERR_SHAPE;
     }
     dim3 blk(32, 8);
     count_launch();
-    k_work_outputs<<<grid2d(W, H, blk), blk, 0, st>>>(d, Ww, Hw, W, H, inv, work64, full64);
+    k_work_outputs<<<grid2d(W, H, blk), blk, 0, st>>>(d, Ww, Hw, W, H, inv, work64, full64,
+                                                       fuse ? fuse->state : nullptr,
+                                                       fuse ? fuse->hist : nullptr);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

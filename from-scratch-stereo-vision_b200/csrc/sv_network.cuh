@@ -62,11 +62,25 @@ struct FwdBufs {
     int *flag;               // device error flag (the workspace's DevFlags)
 };
 
+struct SelState;
+
+// A full-resolution select whose pass 0 runs inside a network stage: the
+// stage's resize starts the selection of `rank` (state and histograms
+// cleared), the kernel writing the FP64 map histograms its values, and
+// launch_select_after_pass0 finishes it.
+struct SelFuse {
+    SelState *state;
+    unsigned *hist;         // the select's histogram words (select_hist_words)
+    long long rank;
+};
+
 // gh (optional): also avgpool2 of the resized left view, [H2/2][W2/2]
 int launch_resize_pair(const void *l, const void *r, int dtype, int W, int H, int W2, int H2,
-                       float *lo, float *ro, cudaStream_t st, float *gh = nullptr);
+                       float *lo, float *ro, cudaStream_t st, float *gh = nullptr,
+                       const SelFuse *fuse = nullptr);
 int launch_work_outputs(const float *d, int Ww, int Hw, int W, int H, double inv,
-                        double *work64, double *full64, cudaStream_t st);
+                        double *work64, double *full64, cudaStream_t st,
+                        const SelFuse *fuse = nullptr);
 int launch_to_f32_pair(const void *l, const void *r, int dtype, long n, float *lo, float *ro,
                        cudaStream_t st);
 int launch_resize_f64(const double *x, int W, int H, int W2, int H2, double *out,
@@ -80,7 +94,11 @@ int launch_forward(const NetView &n, const float *left, const float *right, int 
                    const float *gh, const float *gf, float *d0, float *d1, float *d2,
                    const FwdBufs &b, int precision, cudaStream_t st);
 
-struct SelState;
+// Passes 1.. of a select whose pass 0 a network stage ran (SelFuse), n >
+// select_small_cap().
+int launch_select_after_pass0(const double *x, long n, SelState *state, unsigned *hist,
+                              cudaStream_t st, double *mirror = nullptr);
+long select_small_cap();
 // The rank-th smallest of x into state's value; with mirror (a device
 // pointer, e.g. to mapped pinned host memory) the last kernel also stores
 // the value there.

@@ -17,56 +17,21 @@
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
+#include "sv_select.cuh"
 
 namespace sv {
 
-constexpr int SEL_NPASS = 6;
 constexpr int SEL_LB = 4;              // values a thread loads before it histograms them
-constexpr int SEL_NB = 2048;
-__constant__ int kSelBits[SEL_NPASS] = {11, 11, 11, 11, 10, 10};
-__constant__ int kSelShift[SEL_NPASS] = {53, 42, 31, 20, 10, 0};
-
-struct SelState {
-    unsigned long long prefix;
-    long long rank;
-    double value;
-    unsigned done[SEL_NPASS];          // CTAs finished per pass
-    unsigned cdone;                    // CTAs finished in the compaction
-    unsigned count;                    // keys left after pass 1
-};
-
-__device__ __forceinline__ unsigned long long sel_key(double d) {
-    return ordkey(d == 0.0 ? 0.0 : d);
-}
-
-__device__ __forceinline__ double sel_unkey(unsigned long long k) {
-    const unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
-    return __longlong_as_double((long long)b);
-}
 
 __global__ void k_sel_init(SelState *s, long long rank, unsigned *hist) {
-    for (int i = threadIdx.x; i < 2 * SEL_NB; i += blockDim.x) hist[i] = 0u;
-    if (threadIdx.x) return;
-    s->prefix = 0ull;
-    s->rank = rank;
-    s->value = 0.0;
-    for (int p = 0; p < SEL_NPASS; ++p) s->done[p] = 0u;
-    s->cdone = 0u;
-    s->count = 0u;
+    sel_init_block(s, rank, hist);
 }
 
 __global__ void __launch_bounds__(1024)
     k_sel_pass(const double *__restrict__ x, long n, int pass, SelState *__restrict__ s,
                unsigned *__restrict__ ghist) {
     __shared__ unsigned hist[SEL_NB];
-    __shared__ unsigned wsum[32];
-    __shared__ int owner;
-    __shared__ unsigned long long owner_excl;
-    __shared__ bool last;
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5, nt = blockDim.x;
-    const int shift = kSelShift[pass], bits = kSelBits[pass];
-    const int top = shift + bits;
-    const unsigned mask = (1u << bits) - 1u;
+    const int t = threadIdx.x, nt = blockDim.x;
     const unsigned long long pre = pass ? s->prefix : 0ull;
     for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
     __syncthreads();
@@ -81,68 +46,11 @@ __global__ void __launch_bounds__(1024)
 #pragma unroll
         for (int u = 0; u < SEL_LB; ++u) {
             const long i = b0 + u * stride + t;
-            unsigned digit = 0xffffffffu;
-            if (i < n) {
-                const unsigned long long k = sel_key(v[u]);
-                if (top >= 64 || (k >> top) == (pre >> top))
-                    digit = (unsigned)(k >> shift) & mask;
-            }
-            const unsigned same = __match_any_sync(kFull, digit);
-            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
-                atomicAdd(&hist[digit], __popc(same));
+            sel_count(hist, sel_key(v[u]), i < n, pre, pass);
         }
     }
     __syncthreads();
-    for (int i = t; i < SEL_NB; i += nt)
-        if (hist[i]) atomicAdd(&ghist[i], hist[i]);
-    __threadfence();
-    __syncthreads();
-    if (t == 0) last = atomicAdd(&s->done[pass], 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    // ---- last CTA: find the bin holding s->rank (2 bins per thread at 1024)
-    const int per = SEL_NB / nt;
-    unsigned long long loc = 0;
-    for (int j = 0; j < per; ++j) loc += __ldcg(ghist + t * per + j);
-    unsigned long long incl = loc;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) wsum[wid] = (unsigned)incl;    // at most n < 2^32 keys
-    __syncthreads();
-    if (wid == 0) {
-        const int nw = nt >> 5;
-        unsigned long long w = lane < nw ? wsum[lane] : 0ull, v = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long y = __shfl_up_sync(kFull, v, o);
-            if (lane >= o) v += y;
-        }
-        if (lane < nw) wsum[lane] = (unsigned)(v - w);
-    }
-    __syncthreads();
-    const long long rank = s->rank;
-    const long long excl = (long long)(wsum[wid] + incl - loc);
-    if (rank >= excl && rank < excl + (long long)loc) {
-        owner = t;
-        owner_excl = (unsigned long long)excl;
-    }
-    __syncthreads();
-    if (t == owner) {
-        long long r = rank - (long long)owner_excl;
-        int b = t * per;
-        for (int j = 0; j < per; ++j) {
-            const long long c = __ldcg(ghist + t * per + j);
-            if (r < c) { b = t * per + j; break; }
-            r -= c;
-        }
-        s->prefix |= (unsigned long long)b << shift;
-        s->rank = r;
-        if (pass == SEL_NPASS - 1) s->value = sel_unkey(s->prefix);
-    }
+    sel_pass_finish(pass, s, ghist, hist);
 }
 
 // After pass 1 the 22 top key bits are fixed and usually only a few hundred
@@ -166,7 +74,7 @@ __device__ void sel_passes_cta(const unsigned long long *keys, const double *__r
     }
     __syncthreads();
     for (int pass = pass0; pass < SEL_NPASS; ++pass) {
-        const int shift = kSelShift[pass], bits = kSelBits[pass], top = shift + bits;
+        const int shift = sel_shift(pass), bits = sel_bits(pass), top = shift + bits;
         const unsigned mask = (1u << bits) - 1u;
         for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
         __syncthreads();
@@ -240,7 +148,7 @@ __global__ void __launch_bounds__(1024)
     __shared__ long long s_rank;
     __shared__ bool last;
     const int t = threadIdx.x, lane = t & 31, nt = blockDim.x;
-    const int top = kSelShift[1];                    // bits above pass 2's digit are fixed
+    const int top = sel_shift(1);                    // bits above pass 2's digit are fixed
     const unsigned long long pre = s->prefix;
     const long stride = (long)gridDim.x * nt;
     for (long b0 = blockIdx.x * (long)nt; b0 < n; b0 += SEL_LB * stride) {
@@ -450,6 +358,29 @@ int launch_select(const double *x, long n, long long rank, SelState *state, unsi
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
+
+int launch_select_after_pass0(const double *x, long n, SelState *state, unsigned *hist,
+                              cudaStream_t st, double *mirror) {
+    if (n <= SEL_SMALL_CAP || n >= (1l << 32)) {
+        set_error("select after pass 0: n=%ld", n);
+        return SV_ERR_PARAM;
+    }
+    {
+        const int rc = select_setup();
+        if (rc) return rc;
+    }
+    const int blocks = grid_for(n, 1024 * 4, 148);
+    unsigned long long *cand = reinterpret_cast<unsigned long long *>(hist + 2 * SEL_NB);
+    count_launch();
+    k_sel_pass<<<blocks, 1024, 0, st>>>(x, n, 1, state, hist + SEL_NB);
+    count_launch();
+    k_sel_compact<<<blocks, 1024, (size_t)SEL_CAND_CAP * sizeof(unsigned long long), st>>>(
+        x, n, state, cand, mirror);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+long select_small_cap() { return SEL_SMALL_CAP; }
 
 int launch_select_small_f32(const float *x, long n, long long rank, SelState *state,
                             cudaStream_t st, double *mirror) {

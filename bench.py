@@ -201,10 +201,10 @@ def run_ours(args, rank, world, local):
     def step(i=None):
         """One pair through predict_auto + lr_refine; with i, lr_refine also
         records its stage events (used outside the timed region only)."""
-        pipe.predict()
         if i is None:
-            pipe.refine()
+            pipe.run_device()
         else:
+            pipe.predict()
             pipe.refiner.run_timed(pipe.left, pipe.right, pipe.disp0, pipe.out, pipe.status, ev[i])
 
     # everything runs on the pipeline's own stream (captured passes replay as

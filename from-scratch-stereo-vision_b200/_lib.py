@@ -132,6 +132,8 @@ SIGNATURES = {
                              _IP, _IP, _VP, _SZ, _VP]),
     "sv_predict_at_scale": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _I, _VP, _VP, _IP, _IP,
                                  _VP, _SZ, _VP]),
+    "sv_predict_refine": (_I, [_VP, _VP, _VP, _I, _I, _I, _D, _I, _I, _I, _I, _VP, _VP, _IP,
+                               _IP, _IP, _VP, _SZ, _D, _PRM, _VP, _VP, _VP, _SZ, _VP]),
 }
 
 _lib = None

@@ -595,6 +595,20 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right, 
                                  disp_full, disp_work, Ww, Hw, (cudaStream_t)stream);
 }
 
+int sv_predict_refine(const sv_net *net, const void *left, const void *right, int dtype, int W,
+                      int H, double target_peak, int probe_width, int max_width, int passes,
+                      int precision, double *disp_full, double *disp_work, int *pWw, int *pHw,
+                      int *work_trace, void *pworkspace, size_t pworkspace_bytes, double tol,
+                      const sv_refine_params *p, double *out, uint8_t *status,
+                      void *rworkspace, size_t rworkspace_bytes, void *stream) {
+    const int rc = sv_predict_auto(net, left, right, dtype, W, H, target_peak, probe_width,
+                                   max_width, passes, precision, disp_full, disp_work, pWw, pHw,
+                                   work_trace, pworkspace, pworkspace_bytes, stream);
+    if (rc) return rc;
+    return sv_lr_refine(left, right, dtype, disp_full, W, H, tol, p, out, status, rworkspace,
+                        rworkspace_bytes, stream);
+}
+
 int sv_predict_auto(const sv_net *net, const void *left, const void *right, int dtype, int W,
                     int H, double target_peak, int probe_width, int max_width, int passes,
                     int precision, double *disp_full, double *disp_work, int *pWw, int *pHw,

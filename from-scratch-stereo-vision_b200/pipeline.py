@@ -70,9 +70,17 @@ class PairPipeline:
 
     def run_device(self, stream=None) -> None:
         """predict_auto + lr_refine on the images already in self.left/right
-        (on self.stream unless a stream handle is given)."""
-        self.predict(stream)
-        self.refine(stream)
+        (on self.stream unless a stream handle is given), one library call:
+        the refinement launches follow the last work-width read directly."""
+        s = self.stream.cuda_stream if stream is None else stream
+        r = self.refiner
+        _lib.check(self.lib.sv_predict_refine(
+            self.net.handle, _ptr(self.left), _ptr(self.right), self.code, self.W, self.H,
+            self.tp, self.probe_width, self.max_width, self.passes, self.precision,
+            _ptr(self.disp0), _ptr(self.disp_work), ctypes.byref(self._Ww),
+            ctypes.byref(self._Hw), self._trace, _ptr(self.pws), self.pneed, r.tol,
+            ctypes.byref(r.p), _ptr(self.out), _ptr(self.status), _ptr(r.ws), r.need, s),
+            "predict_refine")
 
     def run_host(self, left: torch.Tensor, right: torch.Tensor):
         """End to end from pinned host images: H2D, the path, D2H of the

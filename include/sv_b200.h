@@ -234,6 +234,21 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right,
                     double *disp_work, int *Ww, int *Hw, int *work_trace,
                     void *workspace, size_t workspace_bytes, void *stream);
 
+/* predict_auto followed by lr_refine on its full-resolution disparity: one
+ * pair's disparity hot path in one call (the callers' predict_auto then
+ * refine_disparity's lr_refine, stereonet.py:3872-3929 and 5865-5872), with
+ * no host work between the last work-width read and the refinement's
+ * launches.  disp_full receives predict_auto's disparity, out / status
+ * lr_refine's; pworkspace is predict_auto's workspace, rworkspace
+ * lr_refine's (sv_lr_refine_workspace_size). */
+int sv_predict_refine(const sv_net *net, const void *left, const void *right, int dtype,
+                      int W, int H, double target_peak, int probe_width, int max_width,
+                      int passes, int precision, double *disp_full, double *disp_work,
+                      int *Ww, int *Hw, int *work_trace, void *pworkspace,
+                      size_t pworkspace_bytes, double tol, const sv_refine_params *p,
+                      double *out, uint8_t *status, void *rworkspace,
+                      size_t rworkspace_bytes, void *stream);
+
 /* predict_at_scale, stereonet.py:3932-3960. */
 int sv_predict_at_scale(const sv_net *net, const void *left, const void *right,
                         int dtype, int W, int H, int work_width, int precision,

@@ -500,6 +500,8 @@ int sv_net_create(const int *arch, int n_arch, const double *params, long n_para
 
 void sv_net_destroy(sv_net *net) {
     if (!net) return;
+    // a replayed pass may still be writing its slot
+    if (!net->graphs.empty()) cudaDeviceSynchronize();
     for (auto &g : net->graphs) {
         cudaGraphExecDestroy(g.exec);
         if (g.slot) cudaFreeHost(g.slot);

@@ -748,6 +748,9 @@ int launch_wta_slot(const void *L, bool l16, int npaths, int nviews, int W, int 
 // so all pairs' scanlines share one launch and finish together.
 // ====================================================================
 
+// KPC / KC / NPC > 0: the band geometry fixed at compile time, as in the
+// single-pair kernels (the whole batch shares K).
+template <int KPC, int KC>
 __global__ void __launch_bounds__(256) k_b_costs(BatchTables t) {
     const int i = batch_find(t.px_blk, t.n, blockIdx.x);
     const BatchPair &P = t.pairs[i];
@@ -758,11 +761,11 @@ __global__ void __launch_bounds__(256) k_b_costs(BatchTables t) {
     const uint64_t *ref = view ? P.cen1 : P.cen0;
     const uint64_t *oth = view ? P.cen0 : P.cen1;
     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
-        cost_pixel_slot(ref, oth, view ? P.base1 : P.base0, P.W, p, t.R, t.K, t.Kp, t.invalid,
-                        view, view ? P.C1 : P.C0, t.R);
+        cost_pixel_slot<KPC, KC>(ref, oth, view ? P.base1 : P.base0, P.W, p, t.R, t.K, t.Kp,
+                                 t.invalid, view, view ? P.C1 : P.C0, t.R);
 }
 
-template <int NR, typename LT>
+template <int NR, typename LT, int KC>
 __global__ void __launch_bounds__(256) k_b_sgm(BatchTables t, long long total) {
     constexpr int Kp = 2 * NR;
     const int lane = threadIdx.x & 31;
@@ -782,14 +785,14 @@ __global__ void __launch_bounds__(256) k_b_sgm(BatchTables t, long long total) {
             dir_of(dir, dx, dy);
             scanline_of(P.W, P.H, dx, dy, (int)(task - t.seg_start[s]), x0, y0, n);
             const long N = (long)P.W * P.H;
-            sgm_line_thread<NR, LT>(view ? P.C1 : P.C0, view ? P.base1 : P.base0,
+            sgm_line_thread<NR, LT, KC>(view ? P.C1 : P.C0, view ? P.base1 : P.base0,
                                     reinterpret_cast<LT *>(P.L) + (long)(view * t.npaths + dir) * N * Kp,
                                     P.W, t.K, t.P1, t.P2, dx, dy, x0, y0, n);
         }
     }
 }
 
-template <typename LT>
+template <typename LT, int KPC, int NPC>
 __global__ void __launch_bounds__(256) k_b_wta(BatchTables t) {
     const int i = batch_find(t.px_blk, t.n, blockIdx.x);
     const BatchPair &P = t.pairs[i];
@@ -800,7 +803,7 @@ __global__ void __launch_bounds__(256) k_b_wta(BatchTables t) {
     const long p1 = min(N, p0 + (long)t.px_per_block);
     const LT *Lv = reinterpret_cast<const LT *>(P.L) + (long)view * t.npaths * stride;
     for (long p = p0 + threadIdx.x; p < p1; p += blockDim.x)
-        wta_pixel<LT>(Lv + p * t.Kp, stride, t.npaths, t.K, t.Kp, t.R,
+        wta_pixel<LT, KPC, NPC>(Lv + p * t.Kp, stride, t.npaths, t.K, t.Kp, t.R,
                       (view ? P.base1 : P.base0)[p], (view ? P.d0r : P.disp0) + p, t.uniq, false,
                       (view ? P.dr : P.dl) + p, nullptr);
 }
@@ -809,7 +812,7 @@ int launch_batch_front(const BatchTables &t, long long px_blocks, long long rows
                        long long tiles, cudaStream_t st);
 int launch_batch_back(const BatchTables &t, long long rows, cudaStream_t st);
 
-template <int NR, typename LT>
+template <int NR, typename LT, int KC = 0>
 static int batch_sgm_go(const BatchTables &t, long long tasks, int threads, int ctas_per_sm,
                         cudaStream_t st) {
     int dev = 0, sms = 148;
@@ -819,7 +822,7 @@ static int batch_sgm_go(const BatchTables &t, long long tasks, int threads, int 
     const long long cap = (long long)sms * ctas_per_sm;    // persistent: a few CTAs per SM
     const unsigned blocks = (unsigned)(want < cap ? (want < 1 ? 1 : want) : cap);
     count_launch();
-    k_b_sgm<NR, LT><<<blocks, threads, 0, st>>>(t, tasks);
+    k_b_sgm<NR, LT, KC><<<blocks, threads, 0, st>>>(t, tasks);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -829,10 +832,16 @@ int launch_batch_refine(const BatchTables &t, long long px_blocks, long long row
                         int sgm_ctas_per_sm, cudaStream_t st) {
     int rc = launch_batch_front(t, px_blocks, rows, tiles, st);
     if (rc) return rc;
+    const bool k21 = t.K == 21 && t.Kp == 24;       // R = 10, the refine_disparity default
     count_launch();
-    k_b_costs<<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+    if (k21)
+        k_b_costs<24, 21><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+    else
+        k_b_costs<0, 0><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
     SV_LAUNCH_CHECK();
-    switch (t.Kp) {
+    if (k21 && !l16)
+        rc = batch_sgm_go<12, uint8_t, 21>(t, tasks, sgm_threads, sgm_ctas_per_sm, st);
+    else switch (t.Kp) {
 #define SV_BGO(KP)                                                                      \
     case KP:                                                                            \
         rc = l16 ? batch_sgm_go<KP / 2, uint16_t>(t, tasks, sgm_threads, sgm_ctas_per_sm, st) \
@@ -850,9 +859,11 @@ int launch_batch_refine(const BatchTables &t, long long px_blocks, long long row
     if (rc) return rc;
     count_launch();
     if (l16)
-        k_b_wta<uint16_t><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+        k_b_wta<uint16_t, 0, 0><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+    else if (k21 && t.npaths == 8)
+        k_b_wta<uint8_t, 24, 8><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
     else
-        k_b_wta<uint8_t><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
+        k_b_wta<uint8_t, 0, 0><<<dim3((unsigned)px_blocks, 2), 256, 0, st>>>(t);
     SV_LAUNCH_CHECK();
     return launch_batch_back(t, rows, st);
 }

@@ -320,29 +320,32 @@ bool inflate_raw(const uint8_t *p, size_t n, Out &out) {
 // distances |b - c|, |a - c| and |a + b - 2c| so it compiles to selects.
 inline int paeth(int a, int b, int c) {
     const int pa = abs(b - c), pb = abs(a - c), pc = abs(a + b - 2 * c);
-    const int bc = pb <= pc ? b : c;
-    return ((pa <= pb) & (pa <= pc)) ? a : bc;      // no branch on pixel data
+    // selects as masks: a branch here would follow the pixel data
+    const int m1 = -(int)(pb <= pc), m2 = -(int)((pa <= pb) & (pa <= pc));
+    const int bc = (b & m1) | (c & ~m1);
+    return (a & m2) | (bc & ~m2);
 }
 
 // The sequential filters (Sub, Average, Paeth) for BPP bytes per pixel:
 // the left pixel (a) and the upper-left one (c) ride in registers, so the
-// dependency along the row does not go through memory.  i < BPP is done by
-// the caller.
-template <int BPP>
-void unfilter_seq(int ft, const uint8_t *__restrict__ row, const uint8_t *__restrict__ up,
-                  uint8_t *__restrict__ o, int stride) {
+// dependency along the row does not go through memory; the filter type and
+// whether a row lies above are template arguments, so the per-byte loop
+// carries no branch.  i < BPP is done by the caller.
+template <int BPP, int FT, bool UP>
+void unfilter_seq_t(const uint8_t *__restrict__ row, const uint8_t *__restrict__ up,
+                    uint8_t *__restrict__ o, int stride) {
     int a[BPP], c[BPP];
     for (int k = 0; k < BPP; ++k) {
         a[k] = o[k];
-        c[k] = up ? up[k] : 0;
+        c[k] = UP ? up[k] : 0;
     }
     int i = BPP;
     for (; i + BPP <= stride; i += BPP) {
         for (int k = 0; k < BPP; ++k) {
-            const int b = up ? up[i + k] : 0;
+            const int b = UP ? up[i + k] : 0;
             int v;
-            if (ft == 1) v = row[i + k] + a[k];
-            else if (ft == 3) v = row[i + k] + ((a[k] + b) >> 1);
+            if (FT == 1) v = row[i + k] + a[k];
+            else if (FT == 3) v = row[i + k] + ((a[k] + b) >> 1);
             else v = row[i + k] + paeth(a[k], b, c[k]);
             a[k] = v & 0xFF;
             c[k] = b;
@@ -350,12 +353,26 @@ void unfilter_seq(int ft, const uint8_t *__restrict__ row, const uint8_t *__rest
         }
     }
     for (int k = 0; i + k < stride; ++k) {      // a partial pixel (sub-byte rows)
-        const int b = up ? up[i + k] : 0;
-        const int v = ft == 1 ? row[i + k] + a[k]
-                    : ft == 3 ? row[i + k] + ((a[k] + b) >> 1)
+        const int b = UP ? up[i + k] : 0;
+        const int v = FT == 1 ? row[i + k] + a[k]
+                    : FT == 3 ? row[i + k] + ((a[k] + b) >> 1)
                               : row[i + k] + paeth(a[k], b, c[k]);
         o[i + k] = (uint8_t)v;
     }
+}
+
+template <int BPP>
+void unfilter_seq(int ft, const uint8_t *__restrict__ row, const uint8_t *__restrict__ up,
+                  uint8_t *__restrict__ o, int stride) {
+    if (ft == 1)
+        up ? unfilter_seq_t<BPP, 1, true>(row, up, o, stride)
+           : unfilter_seq_t<BPP, 1, false>(row, up, o, stride);
+    else if (ft == 3)
+        up ? unfilter_seq_t<BPP, 3, true>(row, up, o, stride)
+           : unfilter_seq_t<BPP, 3, false>(row, up, o, stride);
+    else
+        up ? unfilter_seq_t<BPP, 4, true>(row, up, o, stride)
+           : unfilter_seq_t<BPP, 4, false>(row, up, o, stride);
 }
 
 // One row of _unfilter (stereonet.py:3456-3496); `up` is NULL on row 0,

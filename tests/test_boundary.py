@@ -90,6 +90,13 @@ def test_null_and_workspace_checks(svb):
     assert rc == svb._lib.SV_ERR_WORKSPACE     # misaligned
     assert lib.sv_aggregate_path(ctypes.c_void_p(256), ctypes.c_void_p(256), 8, 8, 21, 1, 2, 2,
                                  0, ctypes.c_void_p(256), None) == svb._lib.SV_ERR_PARAM
+    # predict_auto + lr_refine in one call: argument errors surface before any device work
+    v = ctypes.c_void_p(256)
+    Ww, Hw = ctypes.c_int(), ctypes.c_int()
+    rc = lib.sv_predict_refine(None, v, v, 0, 64, 48, 2.0, 64, 320, 3, 0, v, v,
+                               ctypes.byref(Ww), ctypes.byref(Hw), None, v, 1 << 20, 2.0,
+                               ctypes.byref(p), v, v, v, 1 << 20, None)
+    assert rc == svb._lib.SV_ERR_NULL
 
 
 def test_batch_schedule_defaults_and_validation(svb):

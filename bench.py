@@ -297,6 +297,8 @@ def run_ours(args, rank, world, local):
                        "parallelism": "replicas x%d" % world},
             "stages_ms": {"predict_auto": round(pred_ms, 4),
                           **{s: round(v, 4) for s, v in zip(stages, stage_ms)}},
+            # lr_refine alone (its stage events), both views + LR check per pair
+            "refine_only_mpix_s": round(N / (sum(stage_ms) / 1e3) / 1e6, 3),
             "roofline": {"kernel": "k_sgm_thread (8 paths x 2 views)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),

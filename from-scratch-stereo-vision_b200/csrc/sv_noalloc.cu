@@ -5,20 +5,31 @@
 // forbids allocations afterwards, a plugin host that gives its plugins no
 // allocator, or code on a path where a cudaMalloc would stall or fail.
 // sv_refine_fullres_noalloc serves them: it runs the same kernels as
-// sv_refine_fullres, but its scratch (band centres, census words, band costs,
-// the eight path-cost arrays and the data-error flag) lives in one
-// file-scope __device__ array of SV_NOALLOC_SCRATCH_BYTES.  The caller still
-// passes the images, the disparity and the output; nothing is allocated.
+// sv_refine_fullres, but its scratch (band centres, census words, band costs
+// and the path-cost arrays) lives in one file-scope __device__ array of
+// SV_NOALLOC_SCRATCH_BYTES.  The caller still passes the images, the
+// disparity, the output and a device int for the data-error status; nothing
+// is allocated.
+//
+// Capacity.  The scratch holds, each rounded up to 256 bytes, a 256-byte
+// header, 4N bytes of band centres, 2 x 8N of census words, N*Kp of band
+// costs and npaths*N*Kp*(1 or 2) of path costs (N = W*H, Kp = K+2 rounded up
+// to 8, 16, 24, 32, 48, ...; 2 bytes per path cost when 4+bits+P2 > 255).
+// For refine_disparity's parameters (K = 21 -> Kp = 24, 8 paths, 1 byte) that
+// is 236 bytes per pixel, so up to about 71,000 pixels (300x236 fits, 320x240
+// does not); with paths = 4 it is 140 bytes per pixel.  Larger inputs are
+// rejected with SV_ERR_SHAPE before anything runs.
 //
 // Rules that come with a shared static array:
 //  * every GPU that loads this library holds the array until the process
 //    exits;
-//  * the first call on a device resolves the array's device address with
-//    cudaGetSymbolAddress (once per device, with that device current); make
-//    that first call before any stream capture;
+//  * the array's device address is resolved with cudaGetSymbolAddress on the
+//    first call on a device (with that device current) and cached per CUDA
+//    context, so a new context on the device (after cudaDeviceReset, or a
+//    driver-API context) resolves it again; make the first call on a device
+//    before any stream capture;
 //  * all calls share the one array and it keeps the last call's contents:
-//    the data-error flag is cleared at the start of every call and every
-//    other byte a call reads is written by the same call first;
+//    every byte a call reads is written by the same call first;
 //  * calls whose work overlaps on the GPU (two streams, or two host threads
 //    without ordering) race on the array and corrupt each other's results;
 //    serialise them.
@@ -39,9 +50,39 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-void *g_scratch_ptr[kMaxDevices] = {};
+struct ScratchSlot {
+    unsigned long long ctx_id;   // the CUDA context the address belongs to
+    void *ptr;
+};
+ScratchSlot g_scratch[kMaxDevices] = {};
 
-// Device address of the scratch on the current device (resolved once).
+// Unique id of the current CUDA context (never reused within a process), or
+// 0 when the driver offers no such query or no context is current yet.
+typedef int (*CtxGetCurrentFn)(void **);
+typedef int (*CtxGetIdFn)(void *, unsigned long long *);
+unsigned long long current_ctx_id() {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_cur = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    if (!get_cur || !get_id) return 0;
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the scratch in the current device's current context.
 int scratch_address(void **out) {
     int dev = 0;
     SV_CUDA_TRY(cudaGetDevice(&dev));
@@ -50,7 +91,9 @@ int scratch_address(void **out) {
         return SV_ERR_PARAM;
     }
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
+    ScratchSlot &slot = g_scratch[dev];
+    const unsigned long long id = current_ctx_id();
+    if (!slot.ptr || id == 0 || id != slot.ctx_id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -58,9 +101,10 @@ int scratch_address(void **out) {
                       cudaGetErrorString(e));
             return SV_ERR_CUDA;
         }
-        g_scratch_ptr[dev] = p;
+        slot.ptr = p;
+        slot.ctx_id = id ? id : current_ctx_id();   // the lookup made a context current
     }
-    *out = g_scratch_ptr[dev];
+    *out = slot.ptr;
     return SV_OK;
 }
 
@@ -75,8 +119,9 @@ extern "C" int sv_refine_fullres_noalloc(const void *left, const void *right, in
                                          const double *disp0, int W, int H,
                                          const sv_refine_params *p, double *out,
                                          int *data_status, void *stream) {
-    if (!left || !right || !disp0 || !out || !p) {
-        set_error("NULL argument");
+    if (!left || !right || !disp0 || !out || !p || !data_status) {
+        set_error("NULL argument (data_status is required: it is the only report of a "
+                  "NaN, infinite or out-of-range disparity)");
         return SV_ERR_NULL;
     }
     if (W < 1 || H < 1) { set_error("W=%d H=%d must be positive", W, H); return SV_ERR_SHAPE; }
@@ -107,7 +152,7 @@ extern "C" int sv_refine_fullres_noalloc(const void *left, const void *right, in
     const int npaths = p->paths == 8 ? 8 : 4;
     const bool l16 = invalid + P2 > 255;
     const size_t N = (size_t)W * H, NK = N * slot_width(K);
-    // layout: flag | base | census left | census right | costs | path costs
+    // layout: header | base | census left | census right | costs | path costs
     const size_t o_base = 256;
     const size_t o_cl = o_base + up256(N * 4);
     const size_t o_cr = o_cl + up256(N * 8);
@@ -124,7 +169,7 @@ extern "C" int sv_refine_fullres_noalloc(const void *left, const void *right, in
     int rc = scratch_address(reinterpret_cast<void **>(&s));
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    int *flag = data_status ? data_status : reinterpret_cast<int *>(s);
+    int *flag = data_status;
     int32_t *base = reinterpret_cast<int32_t *>(s + o_base);
     uint64_t *cl = reinterpret_cast<uint64_t *>(s + o_cl);
     uint64_t *cr = reinterpret_cast<uint64_t *>(s + o_cr);

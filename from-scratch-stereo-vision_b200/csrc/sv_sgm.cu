@@ -27,6 +27,9 @@
 // minimum (strict <, ascending k) and re-reads the two neighbours of the
 // winner for the FP64 parabola.
 
+#include <cstdlib>
+#include <cstring>
+
 #include "sv_common.cuh"
 #include "sv_refine.cuh"
 
@@ -490,6 +493,204 @@ __global__ void __launch_bounds__(128)
                                 dy, x0, y0, n);
 }
 
+// ------------------------------------------- SGM, lane group per scanline
+// GL lanes share one scanline; lane gl owns the SL consecutive slots
+// [SL*gl, SL*gl + SL) of every pixel as SL/2 u16x2 registers (Kp = SL*GL).
+// The predecessor's path costs reach the next pixel through a per-group
+// shared-memory row of u16 slots: INF padding on both sides of the Kp slots,
+// two buffers alternating by pixel parity, so a step is one vector store,
+// one __syncwarp and SL/2 + 2 word loads at the re-centred offset.  Any
+// re-centring jump (stereonet.py:5218) is then the same few instructions --
+// the window simply starts s slots further along, and a jump past the band
+// reads only padding -- so groups of one warp never diverge on it.  From the
+// aligned window B (B[r] = slots b+2r, b+2r+1 of the predecessor with
+// b = SL*gl + s - 1) the re-centred candidate minimum of slot pair r is
+//   min(centre, minus + P1, plus + P1) = vimin3(prmt(B[r], B[r+1]), B[r] + P1, B[r+1] + P1).
+// The path minimum is an in-lane vminu2 tree and GL - 1 independent shuffles.
+// Same recurrence, INF conventions and output layout as k_sgm_thread.
+template <int SL, int GL>
+struct SgmGroupGeom {
+    static constexpr int Kp = SL * GL;
+    static constexpr int NR = SL / 2;                            // u16x2 registers per lane
+    static constexpr int PADL = ((Kp + 4 + 7) / 8) * 8;          // INF slots before slot 0
+    // last word a window can touch (s <= Kp + 2), rounded to 16-byte rows
+    static constexpr int LASTW = ((PADL + SL * (GL - 1) + Kp + 1) >> 1) + NR + 1;
+    static constexpr int ROWW = ((LASTW + 1 + 3) / 4) * 4;       // words per row
+    static constexpr int GPW = 32 / GL;                          // groups per warp
+};
+constexpr int SGMG_WARPS = 4;    // warps per CTA of k_sgm_group
+constexpr int SGMG_PF = 8;       // prefetch distance in pixels (even: buffer parity is static)
+
+template <int SL>
+struct SgmCostWord;
+template <>
+struct SgmCostWord<8> { using T = uint2; };
+template <>
+struct SgmCostWord<4> { using T = unsigned; };
+
+template <int SL, int GL, typename LT, int KC>
+__device__ __forceinline__ void sgm_line_group(const uint8_t *__restrict__ Cimg,
+                                               const int32_t *__restrict__ base_img,
+                                               LT *__restrict__ Lo_img, int W, int K, int P1,
+                                               int P2, int dx, int dy, int x0, int y0, int n,
+                                               int gl, unsigned gmask, int glane0,
+                                               unsigned *__restrict__ row0,
+                                               unsigned *__restrict__ row1) {
+    using G = SgmGroupGeom<SL, GL>;
+    using CW = typename SgmCostWord<SL>::T;
+    constexpr int NR = G::NR, Kp = G::Kp;
+    const long step = (long)dy * W + dx;
+    const long p0 = (long)y0 * W + x0;
+    const uint8_t *__restrict__ Cl = Cimg + p0 * Kp + SL * gl;
+    const long cstep = step * Kp;
+    const int32_t *__restrict__ base = base_img + p0;
+    LT *__restrict__ Lo = Lo_img + p0 * Kp + SL * gl;
+
+    const int Kb = KC > 0 ? KC : K;
+    unsigned vm[NR], ninf[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int sa = SL * gl + 2 * r, sb = sa + 1;
+        vm[r] = ((sa >= 1 && sa <= Kb) ? 0x0000FFFFu : 0u) | ((sb >= 1 && sb <= Kb) ? 0xFFFF0000u : 0u);
+        ninf[r] = kInf2 & ~vm[r];
+    }
+    const unsigned P1P1 = (unsigned)P1 * 0x10001u;
+    int nb[GL > 1 ? GL - 1 : 1];                   // the other lanes of the group
+#pragma unroll
+    for (int j = 1; j < GL; ++j) nb[j - 1] = glane0 + (gl + j) % GL;
+
+    for (int w = gl; w < G::ROWW; w += GL) {
+        row0[w] = kInf2;
+        row1[w] = kInf2;
+    }
+    __syncwarp(gmask);
+
+    CW cring[SGMG_PF];
+    int bring[SGMG_PF];
+#pragma unroll
+    for (int u = 0; u < SGMG_PF; ++u) {
+        if (u < n) {
+            bring[u] = __ldg(base + u * step);
+            cring[u] = __ldg(reinterpret_cast<const CW *>(Cl + u * cstep));
+        }
+    }
+    int mq = 0, bprev = 0;
+    for (int tt = 0; tt < n; tt += SGMG_PF) {
+#pragma unroll
+        for (int u = 0; u < SGMG_PF; ++u) {
+            const int t = tt + u;
+            if (t >= n) break;                         // group-uniform
+            unsigned c[NR];
+            if constexpr (SL == 8) {
+                c[0] = __byte_perm(cring[u].x, 0, 0x4140);
+                c[1] = __byte_perm(cring[u].x, 0, 0x4342);
+                c[2] = __byte_perm(cring[u].y, 0, 0x4140);
+                c[3] = __byte_perm(cring[u].y, 0, 0x4342);
+            } else {
+                c[0] = __byte_perm(cring[u], 0, 0x4140);
+                c[1] = __byte_perm(cring[u], 0, 0x4342);
+            }
+            const int bcur = bring[u];
+            if (t + SGMG_PF < n) {
+                bring[u] = __ldg(base + (t + SGMG_PF) * step);
+                cring[u] = __ldg(reinterpret_cast<const CW *>(Cl + (t + SGMG_PF) * cstep));
+            }
+            unsigned Ls[NR], L[NR];
+            if (t == 0) {
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    Ls[r] = c[r] & vm[r];
+                    L[r] = Ls[r] | ninf[r];
+                }
+            } else {
+                // the predecessor's row, written at step t - 1 (tt is even)
+                const unsigned *__restrict__ rw = (u & 1) ? row0 : row1;
+                const int s = max(-Kp - 2, min(Kp + 2, bcur - bprev));
+                const int b = G::PADL + SL * gl + s - 1;
+                const unsigned *a = rw + (b >> 1);
+                unsigned A[NR + 2];
+#pragma unroll
+                for (int i = 0; i < NR + 2; ++i) A[i] = a[i];
+                const unsigned sel = (b & 1) ? 0x5432u : 0x3210u;
+                unsigned B[NR + 1];
+#pragma unroll
+                for (int i = 0; i < NR + 1; ++i) B[i] = __byte_perm(A[i], A[i + 1], sel);
+                const unsigned cap = (unsigned)(mq + P2) * 0x10001u;
+                const unsigned mm = (unsigned)mq * 0x10001u;
+#pragma unroll
+                for (int r = 0; r < NR; ++r) {
+                    const unsigned tr = __vimin3_u16x2(__byte_perm(B[r], B[r + 1], 0x5432),
+                                                       B[r] + P1P1, B[r + 1] + P1P1);
+                    const unsigned v = c[r] + __vminu2(tr, cap) - mm;
+                    Ls[r] = v & vm[r];
+                    L[r] = Ls[r] | ninf[r];
+                }
+            }
+            bprev = bcur;
+            {   // this pixel's path costs for the successor
+                unsigned *__restrict__ ww = ((u & 1) ? row1 : row0) + (G::PADL >> 1) + NR * gl;
+                if constexpr (NR == 4)
+                    *reinterpret_cast<uint4 *>(ww) = make_uint4(L[0], L[1], L[2], L[3]);
+                else
+                    *reinterpret_cast<uint2 *>(ww) = make_uint2(L[0], L[1]);
+            }
+            // path minimum over the group
+            unsigned m2 = L[0];
+#pragma unroll
+            for (int r = 1; r < NR; ++r) m2 = __vminu2(m2, L[r]);
+            const int m0 = (int)min(m2 & 0xFFFFu, m2 >> 16);
+            int m = m0;
+#pragma unroll
+            for (int j = 0; j < GL - 1; ++j) m = min(m, __shfl_sync(gmask, m0, nb[j]));
+            mq = m;
+            // store the pixel's path costs, padding slots as 0
+            LT *dst = Lo + t * cstep;
+            if constexpr (sizeof(LT) == 1) {
+                if constexpr (NR == 4)
+                    *reinterpret_cast<uint2 *>(dst) =
+                        make_uint2(__byte_perm(Ls[0], Ls[1], 0x6420), __byte_perm(Ls[2], Ls[3], 0x6420));
+                else
+                    *reinterpret_cast<unsigned *>(dst) = __byte_perm(Ls[0], Ls[1], 0x6420);
+            } else {
+                if constexpr (NR == 4)
+                    *reinterpret_cast<uint4 *>(dst) = make_uint4(Ls[0], Ls[1], Ls[2], Ls[3]);
+                else
+                    *reinterpret_cast<uint2 *>(dst) = make_uint2(Ls[0], Ls[1]);
+            }
+            __syncwarp(gmask);
+        }
+    }
+}
+
+template <int SL, int GL, typename LT, int KC>
+__global__ void __launch_bounds__(SGMG_WARPS * 32)
+    k_sgm_group(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
+                const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
+                int H, int K, int P1, int P2, LT *__restrict__ Lout, int npaths,
+                SgmTasks tasks) {
+    using G = SgmGroupGeom<SL, GL>;
+    constexpr int Kp = G::Kp, GPW = G::GPW;
+    __shared__ __align__(16) unsigned rows[SGMG_WARPS][2][GPW][G::ROWW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane / GL, gl = lane - g * GL;
+    if (g >= GPW) return;                                  // lanes past the last whole group
+    const long gid = ((long)blockIdx.x * SGMG_WARPS + warp) * GPW + g;
+    if (gid >= tasks.start[tasks.nseg]) return;            // whole groups leave together
+    const unsigned gmask = ((1u << GL) - 1u) << (g * GL);
+    int sg = 0;
+    while (gid >= tasks.start[sg + 1]) ++sg;
+    const int j0 = (int)(gid - tasks.start[sg]);
+    const int view = tasks.view[sg], dir = tasks.dir[sg];
+    int dx, dy, x0, y0, n;
+    dir_of(dir, dx, dy);
+    scanline_of(W, H, dx, dy, j0, x0, y0, n);
+    const long N = (long)W * H;
+    sgm_line_group<SL, GL, LT, KC>(view ? C1 : C0, view ? base1 : base0,
+                                   Lout + (long)(view * npaths + dir) * N * Kp, W, K, P1, P2,
+                                   dx, dy, x0, y0, n, gl, gmask, g * GL, rows[warp][0][g],
+                                   rows[warp][1][g]);
+}
+
 // ------------------------------------------------------------------ WTA
 template <typename LT>
 __device__ __forceinline__ int path_sum_slot(const LT *__restrict__ L, long stride, int npaths,
@@ -667,11 +868,63 @@ static int sgm_thread_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0
     return SV_OK;
 }
 
+template <int SL, int GL, typename LT, int KC = 0>
+static int sgm_group_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
+                        const int32_t *b1, int W, int H, int K, int P1, int P2, void *Lout,
+                        int npaths, const SgmTasks &t, cudaStream_t st) {
+    constexpr int GPW = SgmGroupGeom<SL, GL>::GPW;
+    const long groups = t.start[t.nseg];
+    const long warps = (groups + GPW - 1) / GPW;
+    const int blocks = (int)((warps + SGMG_WARPS - 1) / SGMG_WARPS);
+    count_launch();
+    k_sgm_group<SL, GL, LT, KC><<<blocks, SGMG_WARPS * 32, 0, st>>>(C0, C1, b0, b1, W, H, K, P1,
+                                                                     P2, (LT *)Lout, npaths, t);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+// Single-pair SGM kernel for bands up to K = 30: 0 = lane groups of 8 slots
+// per lane (default), 1 = lane groups of 4 slots per lane, 2 = one thread per
+// scanline.  SV_SGM_KERNEL=group8|group4|thread overrides it (all three are
+// complete and bit-identical; the choice only moves time).
+static int sgm_variant() {
+    static const int v = [] {
+        const char *e = getenv("SV_SGM_KERNEL");
+        if (e && !strcmp(e, "group4")) return 1;
+        if (e && !strcmp(e, "thread")) return 2;
+        return 0;
+    }();
+    return v;
+}
+
 template <typename LT>
 static int sgm_packed_dispatch(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
                                const int32_t *b1, int W, int H, int K, int P1, int P2,
                                void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
     const SgmGeom g = geom_for(K);
+    const int var = sgm_variant();
+    if (var == 0 && g.Kp <= 32) {
+        switch (g.Kp) {
+        case 8: return sgm_group_go<8, 1, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        case 16: return sgm_group_go<8, 2, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        case 24:
+            if (K == 21)
+                return sgm_group_go<8, 3, LT, 21>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+            return sgm_group_go<8, 3, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        default: return sgm_group_go<8, 4, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        }
+    }
+    if (var == 1 && g.Kp <= 32) {
+        switch (g.Kp) {
+        case 8: return sgm_group_go<4, 2, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        case 16: return sgm_group_go<4, 4, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        case 24:
+            if (K == 21)
+                return sgm_group_go<4, 6, LT, 21>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+            return sgm_group_go<4, 6, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        default: return sgm_group_go<4, 8, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);
+        }
+    }
     // bands up to K = 30: one thread per scanline
     switch (g.Kp) {
     case 8: return sgm_thread_go<4, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);

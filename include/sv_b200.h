@@ -174,16 +174,22 @@ int sv_batch_lr_refine_ex(const sv_pair_desc *pairs, int n, int dtype, double to
  * inside this library, held on every GPU that loads it until exit.  No
  * counterpart in the reference (it is an allocation-free variant of this
  * library's own sv_refine_fullres).
- *  - Images up to the scratch size: W*H*(20 + 9K) bytes plus alignment
- *    (uint8 path costs; 20 + 17K when 4 + nbits + P2 > 255), e.g. 320x240 at
- *    K=21.  Larger sizes return SV_ERR_SHAPE and allocate nothing.
- *  - The first call on a device resolves the array's address
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - Capacity: with N = W*H and Kp = K+2 rounded up to 8, 16, 24, 32, 48,
+ *    64, 96, 128, 192 or 256, the scratch needs 256 + 4N + 2*8N + N*Kp +
+ *    npaths*N*Kp*b bytes (b = 1, or 2 when 4 + nbits + P2 > 255), each term
+ *    rounded up to 256.  At refine_disparity's parameters (K = 21, Kp = 24,
+ *    8 paths, b = 1) that is 236 bytes per pixel: up to about 71,000 pixels
+ *    (300x236 fits, 320x240 does not); paths = 4 needs 140 bytes per pixel.
+ *    Larger sizes return SV_ERR_SHAPE and run nothing.
+ *  - The array's device address is resolved (cudaGetSymbolAddress) on the
+ *    first call on a device and again in each new CUDA context on it; make
+ *    the first call on a device before any stream capture.
  *  - All calls share the array, which keeps the last call's contents; each
- *    call clears what must start at zero.  Calls that overlap on the GPU
+ *    call writes every scratch byte it reads.  Calls that overlap on the GPU
  *    race on it: serialise them.
- *  - data_status (optional): a device int that receives SV_ERR_DISP if a
- *    disparity is NaN, infinite or out of range (cleared by the call). */
+ *  - data_status (required): a device int, cleared by the call, that
+ *    receives SV_ERR_DISP if a disparity is NaN, infinite or out of range;
+ *    a NULL data_status returns SV_ERR_NULL. */
 #define SV_NOALLOC_SCRATCH_BYTES (16u << 20)
 int sv_refine_fullres_noalloc(const void *left, const void *right, int dtype,
                               const double *disp0, int W, int H,

@@ -56,6 +56,11 @@ def parse():
                              "train"])
     ap.add_argument("--pairs", type=int, default=256, help="pairs of the batched workload")
     ap.add_argument("--batch", type=int, default=64, help="crops per step of the train workload")
+    ap.add_argument("--cpu-leg", default=None, choices=["pair", "refpy"],
+                    help=argparse.SUPPRESS)          # child process: one CPU baseline leg
+    ap.add_argument("--clock-sampler", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--pci", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--threads", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound on the CPU-baseline sample")
     return ap.parse_args()
@@ -68,6 +73,13 @@ def make_pair(pkg, workload):
             "450x375 u8 pair, 8-15 slanted planes, 0-80 px, ~10% occluded, ~20% low texture")
 
 
+def pair_config(desc, world):
+    """The `config` of the single-pair workloads: identical in both arms."""
+    return {"workload": "%s: predict_auto + lr_refine (R=10, 9x7 census, P1=12, P2=150, "
+                        "tol=2)" % desc,
+            "pairs_per_step_per_gpu": 1, "parallelism": "replicas x%d" % world}
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -76,9 +88,12 @@ def dist_env():
 
 
 # ------------------------------------------------------------------ CPU
+# The CPU legs run in child processes, so the measured process maps only the
+# product library (the oracle's shared object never loads beside it).
 def cpu_port_run(pair, net, seconds, threads):
     """Time the FP64 C port (oracle/) of predict_auto + lr_refine on the host
-    cores: whole pairs until `seconds` have passed (at least one)."""
+    cores: whole pairs until `seconds` have passed (at least one).  Runs in
+    the calling process (the reference arm and the child leg use it)."""
     import __graft_entry__
     orc = __graft_entry__.load_oracle()
     orc.set_threads(threads)
@@ -94,10 +109,123 @@ def cpu_port_run(pair, net, seconds, threads):
     return n, el
 
 
-# --------------------------------------------------------------- clocks
-class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+def _child(argv, timeout):
+    """Run bench.py in a child process and return its last JSON line."""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__)] + argv, capture_output=True,
+                       text=True, timeout=timeout, cwd=REPO)
+    lines = [ln for ln in r.stdout.strip().splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        raise RuntimeError("CPU leg %s failed (rc %d): %s" % (argv, r.returncode,
+                                                             r.stderr.strip()[-400:]))
+    return json.loads(lines[-1])
 
+
+def cpu_port_leg(workload, seconds, threads):
+    """cpu_port_run of the workload's pair in a child process."""
+    d = _child(["--cpu-leg", "pair", "--workload", workload, "--cpu-seconds", str(seconds),
+                "--threads", str(threads)], timeout=600 + 4 * seconds)
+    return d["pairs"], d["seconds"]
+
+
+REF_SRC_ENV = "SV_REFERENCE_SRC"
+
+
+def reference_source():
+    """Path of the reference's own stereonet.py if this machine has one:
+    $SV_REFERENCE_SRC, or baseline/_ref/stereonet.py.  None otherwise."""
+    for c in (os.environ.get(REF_SRC_ENV), os.path.join(REPO, "baseline", "_ref", "stereonet.py")):
+        if c and os.path.isfile(c):
+            return c
+    return None
+
+
+def reference_cpython_leg():
+    """The reference's own lr_refine under this interpreter, one call on the
+    160x120 pair (about 3.4 s under CPython 3.12), in a child process; or why
+    it could not run."""
+    src = reference_source()
+    if src is None:
+        return {"available": False,
+                "why": "reference source not on box (stereonet.py is not pip-installable: no "
+                       "setup.py or pyproject.toml; set %s to a copy)" % REF_SRC_ENV}
+    try:
+        d = _child(["--cpu-leg", "refpy"], timeout=900)
+    except (RuntimeError, subprocess.TimeoutExpired) as e:
+        return {"available": False, "why": str(e)[:300]}
+    d["available"] = True
+    return d
+
+
+def cpu_leg_main(args):
+    """Child-process body of the CPU legs (prints one JSON line)."""
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    if args.cpu_leg == "pair":
+        pair, _ = make_pair(pkg, args.workload)
+        net = pkg.weights.load_model()
+        n, el = cpu_port_run(pair, net, args.cpu_seconds, args.threads or (os.cpu_count() or 1))
+        print(json.dumps({"pairs": n, "seconds": el}))
+        return
+    # refpy: exec the reference (as its own test harness does) and time lr_refine
+    import platform
+    src = reference_source()
+    code = open(src).read().replace("if __name__ == '__main__':", "if False:").replace(
+        'if __name__ == "__main__":', "if False:")
+    SN = {"__name__": "stereonet_ref"}
+    exec(compile(code, src, "exec"), SN)
+    pair = pkg.synth.config_small()
+    W, H = pair.W, pair.H
+    L = [float(v) for v in pair.gray("left").ravel()]
+    R = [float(v) for v in pair.gray("right").ravel()]
+    d0 = [float(v) for v in pair.disp.ravel()]
+    t0 = time.perf_counter()
+    SN["lr_refine"](L, R, d0, W, H, tol=TOL, **PARAMS)
+    el = time.perf_counter() - t0
+    print(json.dumps({"value": round(W * H / el / 1e6, 6), "unit": UNIT, "cores": 1,
+                      "interpreter": "%s %s" % (platform.python_implementation(),
+                                                platform.python_version()),
+                      "sample": "the reference's own lr_refine (R=10, 9x7, P1=12, P2=150, tol=2) "
+                                "once on the 160x120 pair, ground-truth disp0, %.2f s" % el,
+                      "pypy": "unavailable (no pypy3 on this machine)"}))
+
+
+# --------------------------------------------------------------- clocks
+# Read-only NVML sampling of the SM clock and the clock-event reasons at
+# about 1 ms, in a child process so the launching thread shares no GIL time
+# with it.  nvidia-smi (100 ms) is the fallback when NVML is unavailable.
+_REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
+
+
+def clock_sampler_main(args):
+    """Child body: append 't_ms,sm_mhz,reason_bits' lines to args.clock_sampler
+    until terminated; the first line is '#max,<max sm MHz>'."""
+    import signal
+    import pynvml
+    pynvml.nvmlInit()
+    h = None
+    if args.pci:
+        try:
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(args.pci)
+        except pynvml.NVMLError:
+            h = None
+    if h is None:
+        h = pynvml.nvmlDeviceGetHandleByIndex(0)
+    get_r = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+        pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+    stop = []
+    signal.signal(signal.SIGTERM, lambda *a: stop.append(1))
+    with open(args.clock_sampler, "w", buffering=1) as f:
+        f.write("#max,%d\n" % pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        t0 = time.perf_counter()
+        while not stop:
+            sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+            f.write("%.3f,%d,%d\n" % (1e3 * (time.perf_counter() - t0), sm, get_r(h)))
+            time.sleep(0.001)
+
+
+class ClockSampler:
+    """SM clock / clock-event reasons during the timed region (see above)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -106,16 +234,46 @@ class ClockSampler:
         self.index = index
         self.path = tempfile.mktemp(suffix=".csv")
         self.proc = None
+        self.kind = None
+
+    def _pci(self):
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.index)
+            return "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+        except Exception:
+            return None
 
     def __enter__(self):
         try:
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
-                stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml  # noqa: F401
+            argv = [sys.executable, os.path.abspath(__file__), "--clock-sampler", self.path]
+            pci = self._pci()
+            if pci:
+                argv += ["--pci", pci]
+            self.proc = subprocess.Popen(argv, stdout=subprocess.DEVNULL,
+                                         stderr=subprocess.DEVNULL)
+            self.kind = "nvml"
+            t0 = time.time()
+            while time.time() - t0 < 20:                  # until the first sample lands
+                if os.path.exists(self.path) and open(self.path).read().count("\n") >= 2:
+                    break
+                if self.proc.poll() is not None:
+                    raise OSError("NVML sampler exited")
+                time.sleep(0.01)
+        except (ImportError, OSError):
+            if self.proc is not None and self.proc.poll() is None:
+                self.proc.kill()
+            try:
+                self.f = open(self.path, "w")
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                     "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                    stderr=subprocess.DEVNULL)
+                self.kind = "nvidia-smi"
+            except OSError:
+                self.proc = None
+        self.t_enter = time.perf_counter()
         return self
 
     def __exit__(self, *a):
@@ -125,28 +283,42 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-            self.f.close()
+            if self.kind == "nvidia-smi":
+                self.f.close()
 
     def summary(self):
         if self.proc is None or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock source"]}
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            p = [s.strip() for s in line.split(",")]
-            if len(p) < 9:
-                continue
-            try:
+        if self.kind == "nvml":
+            for line in open(self.path):
+                p = line.strip().split(",")
+                if p[0] == "#max":
+                    mx = float(p[1])
+                    continue
+                if len(p) != 3:
+                    continue
                 sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
+                for nm, bit in _REASON_BITS.items():
+                    if int(p[2]) & bit:
+                        reasons.add(nm)
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx = float(p[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
         os.unlink(self.path)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "source": self.kind, "reasons": sorted(reasons)}
 
 
 def hbm_peak():
@@ -277,11 +449,14 @@ def run_ours(args, rank, world, local):
         cpu = None
         if world == 1:
             threads = os.cpu_count() or 1
-            n, el = cpu_port_run(pair, net, args.cpu_seconds, threads)
+            n, el = cpu_port_leg(args.workload, args.cpu_seconds, threads)
             cpu = {"value": round(n * N / el / 1e6, 6), "unit": UNIT, "cores": threads,
                    "kind": "port",
                    "sample": "%d whole pairs (%s) through the FP64 C port of predict_auto + "
-                             "lr_refine, %.1f s, OpenMP over %d threads" % (n, desc, el, threads)}
+                             "lr_refine, %.1f s, OpenMP over %d threads (child process)"
+                             % (n, desc, el, threads),
+                   "reference_cpython": reference_cpython_leg()}
+        dram_gbs = None if traffic is None else traffic / (sgm_ms / 1e3) / 1e9
         result = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -289,23 +464,26 @@ def run_ours(args, rank, world, local):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "u8/u64/int32 integer refinement, f64 subpixel+LR, f32 network",
             "data": "synthetic (seeded generator; reference weights stereonet_weights.txt)",
-            "config": {"workload": "%s: predict_auto + lr_refine (R=10, 9x7 census, P1=12, "
-                                   "P2=150, tol=2)" % desc,
-                       "pairs_per_step_per_gpu": 1, "work_size": list(pipe.work_size),
-                       "work_trace": pipe.work_trace,
-                       "l2": "flushed before every step (256 MB write, untimed)",
-                       "parallelism": "replicas x%d" % world},
+            "config": pair_config(desc, world),
+            "l2": "flushed before every step (256 MB write, untimed)",
+            "work": {"work_size": list(pipe.work_size), "work_trace": pipe.work_trace},
             "stages_ms": {"predict_auto": round(pred_ms, 4),
                           **{s: round(v, 4) for s, v in zip(stages, stage_ms)}},
             # lr_refine alone (its stage events), both views + LR check per pair
             "refine_only_mpix_s": round(N / (sum(stage_ms) / 1e3) / 1e6, 3),
-            "roofline": {"kernel": "k_sgm_thread (8 paths x 2 views)", "bound": "hbm",
+            # achieved = the survey's algorithmic SGM bytes (48*K per pixel per
+            # view) / the SGM stage time; a pair's working set is L2-resident,
+            # so the DRAM bytes ncu measures are far fewer (dram_frac)
+            "roofline": {"kernel": "%s (8 paths x 2 views)" % pkg.refine.sgm_kernel_name(),
+                         "bound": "hbm",
+                         "basis": "algorithmic bytes (working set L2-resident)",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind
                          if peak_kind == "measured" else "fallback",
                          "algorithmic_bytes_per_launch": alg,
-                         "traffic": traffic},
+                         "traffic": traffic,
+                         "dram_frac": None if dram_gbs is None else round(dram_gbs / peak, 4)},
             "cpu_baseline": cpu,
             "e2e": {"value": round(evalue, 3), "unit": UNIT,
                     "h2d_bytes_per_step": pipe.h2d_bytes(),
@@ -345,8 +523,7 @@ def run_reference(args, rank, world):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * t_tot / n_tot, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "%s: predict_auto + lr_refine (R=10, 9x7 census, P1=12, "
-                                   "P2=150, tol=2)" % desc, "pairs_per_step": 1},
+            "config": pair_config(desc, world),
             "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": threads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -861,6 +1038,10 @@ def run_train(args, rank, world, local):
 
 def main():
     args = parse()
+    if args.clock_sampler:
+        return clock_sampler_main(args)
+    if args.cpu_leg:
+        return cpu_leg_main(args)
     rank, world, local = dist_env()
     if args.impl == "reference":
         res = run_reference(args, rank, world)

@@ -36,6 +36,20 @@ _NP_CODE = {np.dtype(np.uint8): _lib.SV_U8, np.dtype(np.float32): _lib.SV_F32,
             np.dtype(np.float64): _lib.SV_F64}
 
 
+def sgm_kernel_name(K: int = 21) -> str:
+    """Name of the single-pair SGM kernel the library runs for a band of K
+    (the library reads SV_SGM_KERNEL = group8 | group4 | thread once)."""
+    import os
+    Kp = next((k for k in (8, 16, 24, 32) if k >= K + 2), None)
+    if Kp is None:
+        return "k_sgm_packed"
+    v = os.environ.get("SV_SGM_KERNEL", "group8")
+    if v == "thread":
+        return "k_sgm_thread"
+    sl = 4 if v == "group4" else 8
+    return "k_sgm_group<%d slots x %d lanes>" % (sl, Kp // sl)
+
+
 def _device() -> torch.device:
     if not torch.cuda.is_available():
         raise RuntimeError("the refinement runs on a CUDA device; none is available")

@@ -691,6 +691,113 @@ __global__ void __launch_bounds__(SGMG_WARPS * 32)
                                    rows[warp][1][g]);
 }
 
+// ------------------------------------------------- SGM, warp per scanline
+// For bands up to K = 30 one warp sweeps one scanline and lane k owns slot k
+// (band index k - 1) as a 32-bit value; lane 0 and lanes K+1..31 hold INF.
+// Per pixel, with s the band re-centring (warp-uniform, stereonet.py:5218):
+//   a, bm, bp = L_{q}(k+s), L_q(k+s-1), L_q(k+s+1)      -- three shuffles
+//   L_p(k)    = C(k) + min(a, min(bm, bp) + P1, mq + P2) - mq
+//   mq        = min over the warp of L_p                  -- one REDUX
+// A shuffle source past either end wraps around the warp; for |s| <= 31 - K
+// every wrapped source of an in-band lane lands on an INF lane, so the
+// common case needs no range test.  Larger jumps (depth edges) take a
+// warp-uniform branch that tests each source.  The costs come through an
+// 8-pixel prefetch ring (one byte per lane); the band centres arrive 32
+// pixels at a time, one per lane, and are broadcast by a shuffle.  Same
+// recurrence, INF conventions and output layout as the other SGM kernels.
+constexpr int SGMW_WARPS = 4;    // warps per CTA of k_sgm_warp
+constexpr int SGMW_PF = 8;       // cost prefetch distance in pixels (divides 32)
+constexpr int kInfW = 0x3FFFFFFF;
+
+template <typename LT, int KC>
+__device__ __forceinline__ void sgm_line_warp(const uint8_t *__restrict__ Cimg,
+                                              const int32_t *__restrict__ base_img,
+                                              LT *__restrict__ Lo_img, int W, int K, int Kp,
+                                              int P1, int P2, int dx, int dy, int x0, int y0,
+                                              int n, int lane) {
+    const int Kb = KC > 0 ? KC : K;
+    const long step = (long)dy * W + dx;
+    const long p0 = (long)y0 * W + x0;
+    const long cstep = step * Kp;
+    const bool inband = lane >= 1 && lane <= Kb;
+    const bool has_slot = lane < Kp;
+    const int fast = 31 - Kb;                       // |s| up to this: wrapped sources are INF
+    const uint8_t *__restrict__ cnext = Cimg + p0 * Kp + (has_slot ? lane : 0);
+    LT *__restrict__ lout = Lo_img + p0 * Kp + lane;
+    const int32_t *__restrict__ base = base_img + p0;
+
+    unsigned cring[SGMW_PF];
+#pragma unroll
+    for (int u = 0; u < SGMW_PF; ++u) {
+        cring[u] = u < n ? (unsigned)__ldg(cnext) : 0u;
+        cnext += cstep;
+    }
+    // band centres of pixels [32j, 32j + 32): bcv now, bnv the next block
+    int bcv = lane < n ? __ldg(base + lane * step) : 0;
+    int bnv = 32 + lane < n ? __ldg(base + (32 + lane) * step) : 0;
+    int L = kInfW, mq = 0, bprev = 0;
+    for (int tt = 0; tt < n; tt += SGMW_PF) {
+        if (tt > 0 && (tt & 31) == 0) {             // next block of centres
+            bcv = bnv;
+            const int t2 = tt + 32 + lane;
+            bnv = t2 < n ? __ldg(base + t2 * step) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < SGMW_PF; ++u) {
+            const int t = tt + u;
+            if (t >= n) break;                          // warp-uniform
+            const int c = (int)cring[u];
+            if (t + SGMW_PF < n) cring[u] = (unsigned)__ldg(cnext);
+            cnext += cstep;
+            const int bcur = __shfl_sync(kFull, bcv, t & 31);
+            int Lnew;
+            if (t == 0) {
+                Lnew = inband ? c : kInfW;
+            } else {
+                const int s = bcur - bprev;
+                const int src = lane + s;
+                int a = __shfl_sync(kFull, L, src & 31);
+                int bm = __shfl_sync(kFull, L, (src - 1) & 31);
+                int bp = __shfl_sync(kFull, L, (src + 1) & 31);
+                if (s < -fast || s > fast) {            // warp-uniform: test every source
+                    if ((unsigned)src >= 32u) a = kInfW;
+                    if ((unsigned)(src - 1) >= 32u) bm = kInfW;
+                    if ((unsigned)(src + 1) >= 32u) bp = kInfW;
+                }
+                const int best = min(min(a, min(bm, bp) + P1), mq + P2);
+                Lnew = inband ? c + best - mq : kInfW;
+            }
+            bprev = bcur;
+            L = Lnew;
+            mq = (int)__reduce_min_sync(kFull, (unsigned)L);
+            if (has_slot) *lout = (LT)(inband ? L : 0);
+            lout += cstep;
+        }
+    }
+}
+
+template <typename LT, int KC>
+__global__ void __launch_bounds__(SGMW_WARPS * 32)
+    k_sgm_warp(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
+               const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
+               int H, int K, int Kp, int P1, int P2, LT *__restrict__ Lout, int npaths,
+               SgmTasks tasks) {
+    const int lane = threadIdx.x & 31;
+    const long gid = (long)blockIdx.x * SGMW_WARPS + (threadIdx.x >> 5);
+    if (gid >= tasks.start[tasks.nseg]) return;            // whole warps leave together
+    int sg = 0;
+    while (gid >= tasks.start[sg + 1]) ++sg;
+    const int j0 = (int)(gid - tasks.start[sg]);
+    const int view = tasks.view[sg], dir = tasks.dir[sg];
+    int dx, dy, x0, y0, n;
+    dir_of(dir, dx, dy);
+    scanline_of(W, H, dx, dy, j0, x0, y0, n);
+    const long N = (long)W * H;
+    sgm_line_warp<LT, KC>(view ? C1 : C0, view ? base1 : base0,
+                          Lout + (long)(view * npaths + dir) * N * Kp, W, K, Kp, P1, P2, dx, dy,
+                          x0, y0, n, lane);
+}
+
 // ------------------------------------------------------------------ WTA
 template <typename LT>
 __device__ __forceinline__ int path_sum_slot(const LT *__restrict__ L, long stride, int npaths,
@@ -883,16 +990,31 @@ static int sgm_group_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
     return SV_OK;
 }
 
-// Single-pair SGM kernel for bands up to K = 30: 0 = lane groups of 8 slots
-// per lane (default), 1 = lane groups of 4 slots per lane, 2 = one thread per
-// scanline.  SV_SGM_KERNEL=group8|group4|thread overrides it (all three are
-// complete and bit-identical; the choice only moves time).
+template <typename LT, int KC = 0>
+static int sgm_warp_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
+                       const int32_t *b1, int W, int H, int K, int Kp, int P1, int P2,
+                       void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
+    const long warps = t.start[t.nseg];
+    const int blocks = (int)((warps + SGMW_WARPS - 1) / SGMW_WARPS);
+    count_launch();
+    k_sgm_warp<LT, KC><<<blocks, SGMW_WARPS * 32, 0, st>>>(C0, C1, b0, b1, W, H, K, Kp, P1, P2,
+                                                            (LT *)Lout, npaths, t);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+// Single-pair SGM kernel for bands up to K = 30: 3 = one warp per scanline
+// (default), 0 = lane groups of 8 slots per lane, 1 = lane groups of 4 slots
+// per lane, 2 = one thread per scanline.  SV_SGM_KERNEL = warp | group8 |
+// group4 | thread overrides it (all four are complete and bit-identical; the
+// choice only moves time).
 static int sgm_variant() {
     static const int v = [] {
         const char *e = getenv("SV_SGM_KERNEL");
+        if (e && !strcmp(e, "group8")) return 0;
         if (e && !strcmp(e, "group4")) return 1;
         if (e && !strcmp(e, "thread")) return 2;
-        return 0;
+        return 3;
     }();
     return v;
 }
@@ -903,6 +1025,11 @@ static int sgm_packed_dispatch(const uint8_t *C0, const uint8_t *C1, const int32
                                void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
     const SgmGeom g = geom_for(K);
     const int var = sgm_variant();
+    if (var == 3 && g.Kp <= 32) {
+        if (K == 21)
+            return sgm_warp_go<LT, 21>(C0, C1, b0, b1, W, H, K, g.Kp, P1, P2, Lout, npaths, t, st);
+        return sgm_warp_go<LT>(C0, C1, b0, b1, W, H, K, g.Kp, P1, P2, Lout, npaths, t, st);
+    }
     if (var == 0 && g.Kp <= 32) {
         switch (g.Kp) {
         case 8: return sgm_group_go<8, 1, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);

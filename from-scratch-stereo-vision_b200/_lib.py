@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsv_b200.so")
 
 SV_OK, SV_ERR_SHAPE, SV_ERR_PARAM, SV_ERR_DISP, SV_ERR_WORKSPACE, SV_ERR_CUDA, \
-    SV_ERR_NULL, SV_ERR_NET = range(8)
+    SV_ERR_NULL, SV_ERR_NET, SV_ERR_TIMEOUT = range(9)
 SV_U8, SV_F32, SV_F64 = 0, 1, 2
 SV_FP32, SV_BF16 = 0, 1
 
@@ -67,6 +67,8 @@ SIGNATURES = {
     "sv_lr_refine_timed": (_I, [_VP, _VP, _I, _VP, _I, _I, _D, _PRM, _VP, _VP, _VP, _SZ, _VP,
                                 ctypes.POINTER(_VP), _I]),
     "sv_refine_fullres_noalloc": (_I, [_VP, _VP, _I, _VP, _I, _I, _PRM, _VP, _VP, _VP]),
+    "sv_selftest_wait_timeout": (_I, [ctypes.c_uint, _VP, _VP]),
+    "sv_selftest_slot_wait": (_I, [_VP]),
     "sv_batch_lr_refine_workspace_size": (_SZ, [_VP, _I, _PRM]),
     "sv_batch_lr_refine": (_I, [_VP, _I, _I, _D, _PRM, _VP, _SZ, _VP]),
     "sv_batch_config_default": (None, [_VP]),
@@ -169,7 +171,7 @@ def check(rc: int, what: str) -> None:
     lib = load()
     detail = lib.sv_last_error().decode(errors="replace")
     msg = "%s: %s (%s)" % (what, lib.sv_status_string(rc).decode(), detail)
-    if rc == SV_ERR_CUDA:
+    if rc in (SV_ERR_CUDA, SV_ERR_TIMEOUT):
         raise RuntimeError(msg)
     raise ValueError(msg)
 

@@ -136,6 +136,7 @@ const char *sv_status_string(int s) {
     case SV_ERR_CUDA: return "CUDA error";
     case SV_ERR_NULL: return "NULL pointer";
     case SV_ERR_NET: return "weights do not match the architecture";
+    case SV_ERR_TIMEOUT: return "a bounded device wait or host poll gave up";
     default: return "unknown status";
     }
 }

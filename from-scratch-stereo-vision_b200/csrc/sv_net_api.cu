@@ -319,7 +319,7 @@ static int wait_slot(double *slot, cudaStream_t st, double *out) {
                     return SV_OK;
                 }
                 set_error("peak slot not written by the finished stage");
-                return SV_ERR_CUDA;
+                return SV_ERR_TIMEOUT;
             }
             if (q != cudaErrorNotReady) {
                 set_error("stage failed: %s", cudaGetErrorString(q));
@@ -327,7 +327,7 @@ static int wait_slot(double *slot, cudaStream_t st, double *out) {
             }
             if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60)) {
                 set_error("peak selection did not finish within 60 s");
-                return SV_ERR_CUDA;
+                return SV_ERR_TIMEOUT;
             }
         }
     }
@@ -693,6 +693,27 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     }
     if (work_trace) work_trace[nt] = 0;
     return SV_OK;
+}
+
+// Self-test of the host side of a stage's peak hand-off: arm a mapped slot
+// that no kernel will write, and poll it while the stream has nothing queued.
+// The poll must give up with SV_ERR_TIMEOUT instead of waiting forever.
+int sv_selftest_slot_wait(void *stream) {
+    void *h = nullptr;
+    SV_CUDA_TRY(cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable));
+    double *slot = static_cast<double *>(h);
+    arm_slot(slot);
+    double v = 0.0;
+    const int rc = wait_slot(slot, (cudaStream_t)stream, &v);
+    cudaFreeHost(h);
+    return rc;
+}
+
+// Self-test of the device side: one CTA holding tensor memory waits, at most
+// `limit` polls, on an mbarrier nothing arrives at (launch_selftest_wait).
+int sv_selftest_wait_timeout(unsigned limit, int *flag_done, void *stream) {
+    if (!flag_done) { set_error("NULL argument"); return SV_ERR_NULL; }
+    return launch_selftest_wait(limit, flag_done, flag_done + 1, (cudaStream_t)stream);
 }
 
 }  // extern "C"

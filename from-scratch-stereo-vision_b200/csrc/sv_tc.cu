@@ -63,9 +63,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
 }
 
 // Bounded wait for phase `parity` of the barrier; true when it completed.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity,
+                                          unsigned limit = kWaitLimit) {
     const uint32_t a = smem_u32(bar);
-    for (unsigned it = 0; it < kWaitLimit; ++it) {
+    for (unsigned it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(kTcM) k_conv_tc(TcConv a) {
         // ---- wait for the accumulator (bounded), then the epilogue
         if (!failed && !mbar_wait(&mbar, phase)) {
             failed = 1;
-            flag_error(a.err, SV_ERR_CUDA);
+            flag_error(a.err, SV_ERR_TIMEOUT);
         }
         phase ^= 1u;
         __syncthreads();
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(kTcM) k_conv2d_tc(TcConv a, int PH, int PW) {
         }
         if (!failed && !mbar_wait(&mbar, phase)) {
             failed = 1;
-            flag_error(a.err, SV_ERR_CUDA);
+            flag_error(a.err, SV_ERR_TIMEOUT);
         }
         phase ^= 1u;
         __syncthreads();
@@ -474,6 +475,51 @@ static int launch_conv2d_tc(const TcConv &a, cudaStream_t st) {
     return SV_OK;
 }
 
+// Self-test of the failure path every tensor-core kernel here shares: a CTA
+// allocates its tensor memory, arms an mbarrier that nothing will arrive at
+// (no MMA is issued), and waits with a bounded poll count.  The wait must
+// give up, record SV_ERR_TIMEOUT in the flag, free the tensor memory and
+// return, leaving the context usable.  done receives 1 once the CTA has
+// passed its dealloc.
+__global__ void __launch_bounds__(kTcM) k_selftest_wait(unsigned limit, int *flag, int *done) {
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    const int warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+    if (threadIdx.x == 0 && !mbar_wait(&mbar, 0, limit)) {
+        failed = 1;
+        flag_error(flag, SV_ERR_TIMEOUT);
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(kTmemCols));
+    __syncthreads();
+    if (threadIdx.x == 0) *done = failed ? 1 : 2;
+}
+
+int launch_selftest_wait(unsigned limit, int *flag, int *done, cudaStream_t st) {
+    count_launch();
+    k_selftest_wait<<<1, kTcM, 0, st>>>(limit, flag, done);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
 int launch_conv_tc(const TcConv &a, cudaStream_t st) {
     if (a.OC < 1 || a.OC > kTcN || a.K < 1 || a.K > kTcMaxK || a.Kpad != tc_kpad(a.K) ||
         (a.mode == 0 && (a.nimg < 1 || a.nimg > 2)) || (a.mode == 1 && a.nd != 3) ||
@@ -564,7 +610,7 @@ __global__ void __launch_bounds__(kTcM) k_wgrad_tc(TcWgrad a, int mtiles) {
         unsigned char *sB = sA + (size_t)mtiles * a_tile;
         if (it >= 2 && !failed && !mbar_wait(&mbar[s], ((it - 2) >> 1) & 1)) {
             failed = 1;
-            flag_error(a.err, SV_ERR_CUDA);
+            flag_error(a.err, SV_ERR_TIMEOUT);
         }
         __syncthreads();
         if (failed) break;
@@ -648,7 +694,7 @@ __global__ void __launch_bounds__(kTcM) k_wgrad_tc(TcWgrad a, int mtiles) {
     // the last commit covers every MMA this CTA issued
     if (it > 0 && !failed && !mbar_wait(&mbar[(it - 1) & 1], ((it - 1) >> 1) & 1)) {
         failed = 1;
-        flag_error(a.err, SV_ERR_CUDA);
+        flag_error(a.err, SV_ERR_TIMEOUT);
     }
     __syncthreads();
     if (it > 0 && !failed) {

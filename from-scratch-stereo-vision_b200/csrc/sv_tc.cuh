@@ -59,5 +59,9 @@ inline size_t tc_weight_elems(int K) { return (size_t)tc_kpad(K) * 16; }
 // Host: FP64 weights [OC][K] (OC <= 16) -> packed BF16 operand B.
 void tc_pack_weights(const double *w, int OC, int K, uint16_t *out);
 int launch_conv_tc(const TcConv &a, cudaStream_t st);
+// One CTA that holds tensor memory and waits at most `limit` polls on an
+// mbarrier nothing arrives at; *flag gets SV_ERR_TIMEOUT, *done 1 (gave up)
+// or 2 (the barrier completed).
+int launch_selftest_wait(unsigned limit, int *flag, int *done, cudaStream_t st);
 
 }  // namespace sv

@@ -37,7 +37,8 @@ enum sv_status {
     SV_ERR_WORKSPACE = 4, /* workspace NULL, misaligned or smaller than required     */
     SV_ERR_CUDA = 5,      /* a CUDA runtime call failed (detail in sv_last_error)    */
     SV_ERR_NULL = 6,      /* a required pointer is NULL                               */
-    SV_ERR_NET = 7        /* weights do not match the architecture                    */
+    SV_ERR_NET = 7,       /* weights do not match the architecture                    */
+    SV_ERR_TIMEOUT = 8    /* a bounded device wait or host poll gave up               */
 };
 
 enum sv_dtype { SV_U8 = 0, SV_F32 = 1, SV_F64 = 2 };
@@ -195,6 +196,20 @@ int sv_refine_fullres_noalloc(const void *left, const void *right, int dtype,
                               const double *disp0, int W, int H,
                               const sv_refine_params *p, double *out,
                               int *data_status, void *stream);
+
+/* Failure-path self-tests (no reference counterpart: the reference only
+ * raises Python exceptions, serve.py:72-84).  They exercise the bounded waits
+ * every long-running path here relies on, without faulting the GPU.
+ *  - sv_selftest_wait_timeout: one CTA allocates tensor memory and waits at
+ *    most `limit` polls on an mbarrier that nothing arrives at -- the wait of
+ *    the tcgen05 convolutions.  flag_done is two device ints: [0] receives
+ *    SV_ERR_TIMEOUT (clear it first), [1] becomes 1 once the CTA gave up and
+ *    freed its tensor memory (2 if the barrier had completed).
+ *  - sv_selftest_slot_wait: polls a mapped host slot that no kernel writes,
+ *    on an idle stream -- the host side of predict_auto's peak hand-off --
+ *    and returns SV_ERR_TIMEOUT. */
+int sv_selftest_wait_timeout(unsigned limit, int *flag_done, void *stream);
+int sv_selftest_slot_wait(void *stream);
 
 /* ------------------------------------------------------------ network */
 typedef struct sv_net sv_net;

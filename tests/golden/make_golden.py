@@ -1,8 +1,9 @@
 """Generate the golden fixtures by running the reference itself.
 
-Run in a container that has the reference checkout (read-only is fine):
+Run where the reference checkout is available (read-only is fine), giving
+its directory as the argument or in SV_REFERENCE_DIR:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 It executes ``stereonet.py`` into a namespace exactly the way the reference's
 own test suite does (test_stereonet.py:18-22: strip the ``run_demo()`` guard,
@@ -476,7 +477,10 @@ def signatures(ref_dir):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--")]
-    ref = args[0] if args else "/root/reference"
+    ref = args[0] if args else os.environ.get("SV_REFERENCE_DIR")
+    if not ref or not os.path.isfile(os.path.join(ref, "stereonet.py")):
+        sys.exit("usage: make_golden.py <reference checkout> [--...-only] "
+                 "(or set SV_REFERENCE_DIR)")
     if "--postproc-only" in sys.argv:
         postproc(ref)
     elif "--images-only" in sys.argv:

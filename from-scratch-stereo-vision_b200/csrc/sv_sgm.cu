@@ -498,8 +498,8 @@ __global__ void __launch_bounds__(128)
 // [SL*gl, SL*gl + SL) of every pixel as SL/2 u16x2 registers (Kp = SL*GL).
 // The predecessor's path costs reach the next pixel through a per-group
 // shared-memory row of u16 slots: INF padding on both sides of the Kp slots,
-// two buffers alternating by pixel parity, so a step is one vector store,
-// one __syncwarp and SL/2 + 2 word loads at the re-centred offset.  Any
+// two buffers alternating by pixel parity, so a step is one store, one
+// __syncwarp and SL/2 + 2 word loads at the re-centred offset.  Any
 // re-centring jump (stereonet.py:5218) is then the same few instructions --
 // the window simply starts s slots further along, and a jump past the band
 // reads only padding -- so groups of one warp never diverge on it.  From the
@@ -507,7 +507,15 @@ __global__ void __launch_bounds__(128)
 // b = SL*gl + s - 1) the re-centred candidate minimum of slot pair r is
 //   min(centre, minus + P1, plus + P1) = vimin3(prmt(B[r], B[r+1]), B[r] + P1, B[r+1] + P1).
 // The path minimum is an in-lane vminu2 tree and GL - 1 independent shuffles.
-// Same recurrence, INF conventions and output layout as k_sgm_thread.
+//
+// A pixel's costs and band centre arrive through cp.async into a per-lane
+// shared ring of 2 * SGMG_PF slots (laid out [slot][lane]), issued SGMG_PF
+// pixels ahead and read one pixel ahead.  Register prefetch rings of loads
+// in flight stalled every step: loads share a warp's few scoreboards, so a
+// use waited for later loads as well; async copies are tracked by commit
+// groups instead.  Same recurrence, INF conventions and output layout as
+// k_sgm_thread, except that uint8 path costs keep the padding slots' INF
+// byte (0xFF): the WTA reads slots 1..K only, and 8 x 255 cannot carry.
 template <int SL, int GL>
 struct SgmGroupGeom {
     static constexpr int Kp = SL * GL;
@@ -519,7 +527,7 @@ struct SgmGroupGeom {
     static constexpr int GPW = 32 / GL;                          // groups per warp
 };
 constexpr int SGMG_WARPS = 4;    // warps per CTA of k_sgm_group
-constexpr int SGMG_PF = 8;       // prefetch distance in pixels (even: buffer parity is static)
+constexpr int SGMG_PF = 8;       // copy distance in pixels (even: buffer parity is static)
 
 template <int SL>
 struct SgmCostWord;
@@ -528,23 +536,40 @@ struct SgmCostWord<8> { using T = uint2; };
 template <>
 struct SgmCostWord<4> { using T = unsigned; };
 
+template <int BYTES>
+__device__ __forceinline__ void cp_async_bytes(void *smem_dst, const void *gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gsrc), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 template <int SL, int GL, typename LT, int KC>
 __device__ __forceinline__ void sgm_line_group(const uint8_t *__restrict__ Cimg,
                                                const int32_t *__restrict__ base_img,
                                                LT *__restrict__ Lo_img, int W, int K, int P1,
                                                int P2, int dx, int dy, int x0, int y0, int n,
-                                               int gl, unsigned gmask, int glane0,
+                                               int gl, unsigned gmask, int glane0, int lane,
                                                unsigned *__restrict__ row0,
-                                               unsigned *__restrict__ row1) {
+                                               unsigned *__restrict__ row1,
+                                               typename SgmCostWord<SL>::T *__restrict__ cst,
+                                               int *__restrict__ bst) {
     using G = SgmGroupGeom<SL, GL>;
     using CW = typename SgmCostWord<SL>::T;
-    constexpr int NR = G::NR, Kp = G::Kp;
+    constexpr int NR = G::NR, Kp = G::Kp, PF = SGMG_PF;
     const long step = (long)dy * W + dx;
     const long p0 = (long)y0 * W + x0;
-    const uint8_t *__restrict__ Cl = Cimg + p0 * Kp + SL * gl;
     const long cstep = step * Kp;
-    const int32_t *__restrict__ base = base_img + p0;
-    LT *__restrict__ Lo = Lo_img + p0 * Kp + SL * gl;
+    const uint8_t *cnx = Cimg + p0 * Kp + SL * gl;     // next pixel to copy
+    const int32_t *bnx = base_img + p0;
+    LT *__restrict__ lpx = Lo_img + p0 * Kp + SL * gl;
 
     const int Kb = KC > 0 ? KC : K;
     unsigned vm[NR], ninf[NR];
@@ -563,45 +588,58 @@ __device__ __forceinline__ void sgm_line_group(const uint8_t *__restrict__ Cimg,
         row0[w] = kInf2;
         row1[w] = kInf2;
     }
-    __syncwarp(gmask);
-
-    CW cring[SGMG_PF];
-    int bring[SGMG_PF];
+    // pixels 0 .. PF-1 into ring slots 0 .. PF-1, one commit group each
 #pragma unroll
-    for (int u = 0; u < SGMG_PF; ++u) {
+    for (int u = 0; u < PF; ++u) {
         if (u < n) {
-            bring[u] = __ldg(base + u * step);
-            cring[u] = __ldg(reinterpret_cast<const CW *>(Cl + u * cstep));
+            cp_async_bytes<SL>(cst + u * 32 + lane, cnx);
+            cp_async_bytes<4>(bst + u * 32 + lane, bnx);
         }
+        cp_async_commit();
+        cnx += cstep;
+        bnx += step;
     }
+    cp_async_wait<PF - 1>();
+    __syncwarp(gmask);
+    CW cw = cst[lane];                             // pixel 0
+    int bnext = bst[lane];
     int mq = 0, bprev = 0;
-    for (int tt = 0; tt < n; tt += SGMG_PF) {
+    for (int tt = 0; tt < n; tt += PF) {
+        const int h = (tt / PF & 1) * PF;          // ring half of pixels tt .. tt+PF-1
 #pragma unroll
-        for (int u = 0; u < SGMG_PF; ++u) {
+        for (int u = 0; u < PF; ++u) {
             const int t = tt + u;
-            if (t >= n) break;                         // group-uniform
+            if (t >= n) break;                     // group-uniform
             unsigned c[NR];
             if constexpr (SL == 8) {
-                c[0] = __byte_perm(cring[u].x, 0, 0x4140);
-                c[1] = __byte_perm(cring[u].x, 0, 0x4342);
-                c[2] = __byte_perm(cring[u].y, 0, 0x4140);
-                c[3] = __byte_perm(cring[u].y, 0, 0x4342);
+                c[0] = __byte_perm(cw.x, 0, 0x4140);
+                c[1] = __byte_perm(cw.x, 0, 0x4342);
+                c[2] = __byte_perm(cw.y, 0, 0x4140);
+                c[3] = __byte_perm(cw.y, 0, 0x4342);
             } else {
-                c[0] = __byte_perm(cring[u], 0, 0x4140);
-                c[1] = __byte_perm(cring[u], 0, 0x4342);
+                c[0] = __byte_perm(cw, 0, 0x4140);
+                c[1] = __byte_perm(cw, 0, 0x4342);
             }
-            const int bcur = bring[u];
-            if (t + SGMG_PF < n) {
-                bring[u] = __ldg(base + (t + SGMG_PF) * step);
-                cring[u] = __ldg(reinterpret_cast<const CW *>(Cl + (t + SGMG_PF) * cstep));
+            const int bcur = bnext;
+            // the next pixel's copy has landed (PF - 2 younger groups may not)
+            cp_async_wait<PF - 2>();
+            {
+                const int sn = u + 1 < PF ? h + u + 1 : PF - h;   // ring slot of pixel t+1
+                cw = cst[sn * 32 + lane];
+                bnext = bst[sn * 32 + lane];
             }
-            unsigned Ls[NR], L[NR];
+            if (t + PF < n) {                      // pixel t+PF into the other half
+                const int sp = PF - h + u;
+                cp_async_bytes<SL>(cst + sp * 32 + lane, cnx);
+                cp_async_bytes<4>(bst + sp * 32 + lane, bnx);
+            }
+            cp_async_commit();
+            cnx += cstep;
+            bnx += step;
+            unsigned L[NR];
             if (t == 0) {
 #pragma unroll
-                for (int r = 0; r < NR; ++r) {
-                    Ls[r] = c[r] & vm[r];
-                    L[r] = Ls[r] | ninf[r];
-                }
+                for (int r = 0; r < NR; ++r) L[r] = (c[r] & vm[r]) | ninf[r];
             } else {
                 // the predecessor's row, written at step t - 1 (tt is even)
                 const unsigned *__restrict__ rw = (u & 1) ? row0 : row1;
@@ -622,8 +660,7 @@ __device__ __forceinline__ void sgm_line_group(const uint8_t *__restrict__ Cimg,
                     const unsigned tr = __vimin3_u16x2(__byte_perm(B[r], B[r + 1], 0x5432),
                                                        B[r] + P1P1, B[r + 1] + P1P1);
                     const unsigned v = c[r] + __vminu2(tr, cap) - mm;
-                    Ls[r] = v & vm[r];
-                    L[r] = Ls[r] | ninf[r];
+                    L[r] = (v & vm[r]) | ninf[r];
                 }
             }
             bprev = bcur;
@@ -643,23 +680,27 @@ __device__ __forceinline__ void sgm_line_group(const uint8_t *__restrict__ Cimg,
 #pragma unroll
             for (int j = 0; j < GL - 1; ++j) m = min(m, __shfl_sync(gmask, m0, nb[j]));
             mq = m;
-            // store the pixel's path costs, padding slots as 0
-            LT *dst = Lo + t * cstep;
+            // store the pixel's path costs (uint8: padding keeps INF's low byte;
+            // uint16: padding 0, so the WTA's 16-bit sums never carry)
+            LT *dst = lpx;
+            lpx += cstep;
             if constexpr (sizeof(LT) == 1) {
                 if constexpr (NR == 4)
                     *reinterpret_cast<uint2 *>(dst) =
-                        make_uint2(__byte_perm(Ls[0], Ls[1], 0x6420), __byte_perm(Ls[2], Ls[3], 0x6420));
+                        make_uint2(__byte_perm(L[0], L[1], 0x6420), __byte_perm(L[2], L[3], 0x6420));
                 else
-                    *reinterpret_cast<unsigned *>(dst) = __byte_perm(Ls[0], Ls[1], 0x6420);
+                    *reinterpret_cast<unsigned *>(dst) = __byte_perm(L[0], L[1], 0x6420);
             } else {
                 if constexpr (NR == 4)
-                    *reinterpret_cast<uint4 *>(dst) = make_uint4(Ls[0], Ls[1], Ls[2], Ls[3]);
+                    *reinterpret_cast<uint4 *>(dst) =
+                        make_uint4(L[0] & vm[0], L[1] & vm[1], L[2] & vm[2], L[3] & vm[3]);
                 else
-                    *reinterpret_cast<uint2 *>(dst) = make_uint2(Ls[0], Ls[1]);
+                    *reinterpret_cast<uint2 *>(dst) = make_uint2(L[0] & vm[0], L[1] & vm[1]);
             }
             __syncwarp(gmask);
         }
     }
+    cp_async_wait<0>();
 }
 
 template <int SL, int GL, typename LT, int KC>
@@ -669,8 +710,11 @@ __global__ void __launch_bounds__(SGMG_WARPS * 32)
                 int H, int K, int P1, int P2, LT *__restrict__ Lout, int npaths,
                 SgmTasks tasks) {
     using G = SgmGroupGeom<SL, GL>;
+    using CW = typename SgmCostWord<SL>::T;
     constexpr int Kp = G::Kp, GPW = G::GPW;
     __shared__ __align__(16) unsigned rows[SGMG_WARPS][2][GPW][G::ROWW];
+    __shared__ __align__(16) CW cstage[SGMG_WARPS][2 * SGMG_PF][32];
+    __shared__ __align__(16) int bstage[SGMG_WARPS][2 * SGMG_PF][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane / GL, gl = lane - g * GL;
     if (g >= GPW) return;                                  // lanes past the last whole group
@@ -687,115 +731,8 @@ __global__ void __launch_bounds__(SGMG_WARPS * 32)
     const long N = (long)W * H;
     sgm_line_group<SL, GL, LT, KC>(view ? C1 : C0, view ? base1 : base0,
                                    Lout + (long)(view * npaths + dir) * N * Kp, W, K, P1, P2,
-                                   dx, dy, x0, y0, n, gl, gmask, g * GL, rows[warp][0][g],
-                                   rows[warp][1][g]);
-}
-
-// ------------------------------------------------- SGM, warp per scanline
-// For bands up to K = 30 one warp sweeps one scanline and lane k owns slot k
-// (band index k - 1) as a 32-bit value; lane 0 and lanes K+1..31 hold INF.
-// Per pixel, with s the band re-centring (warp-uniform, stereonet.py:5218):
-//   a, bm, bp = L_{q}(k+s), L_q(k+s-1), L_q(k+s+1)      -- three shuffles
-//   L_p(k)    = C(k) + min(a, min(bm, bp) + P1, mq + P2) - mq
-//   mq        = min over the warp of L_p                  -- one REDUX
-// A shuffle source past either end wraps around the warp; for |s| <= 31 - K
-// every wrapped source of an in-band lane lands on an INF lane, so the
-// common case needs no range test.  Larger jumps (depth edges) take a
-// warp-uniform branch that tests each source.  The costs come through an
-// 8-pixel prefetch ring (one byte per lane); the band centres arrive 32
-// pixels at a time, one per lane, and are broadcast by a shuffle.  Same
-// recurrence, INF conventions and output layout as the other SGM kernels.
-constexpr int SGMW_WARPS = 4;    // warps per CTA of k_sgm_warp
-constexpr int SGMW_PF = 8;       // cost prefetch distance in pixels (divides 32)
-constexpr int kInfW = 0x3FFFFFFF;
-
-template <typename LT, int KC>
-__device__ __forceinline__ void sgm_line_warp(const uint8_t *__restrict__ Cimg,
-                                              const int32_t *__restrict__ base_img,
-                                              LT *__restrict__ Lo_img, int W, int K, int Kp,
-                                              int P1, int P2, int dx, int dy, int x0, int y0,
-                                              int n, int lane) {
-    const int Kb = KC > 0 ? KC : K;
-    const long step = (long)dy * W + dx;
-    const long p0 = (long)y0 * W + x0;
-    const long cstep = step * Kp;
-    const bool inband = lane >= 1 && lane <= Kb;
-    const bool has_slot = lane < Kp;
-    const int fast = 31 - Kb;                       // |s| up to this: wrapped sources are INF
-    const uint8_t *__restrict__ cnext = Cimg + p0 * Kp + (has_slot ? lane : 0);
-    LT *__restrict__ lout = Lo_img + p0 * Kp + lane;
-    const int32_t *__restrict__ base = base_img + p0;
-
-    unsigned cring[SGMW_PF];
-#pragma unroll
-    for (int u = 0; u < SGMW_PF; ++u) {
-        cring[u] = u < n ? (unsigned)__ldg(cnext) : 0u;
-        cnext += cstep;
-    }
-    // band centres of pixels [32j, 32j + 32): bcv now, bnv the next block
-    int bcv = lane < n ? __ldg(base + lane * step) : 0;
-    int bnv = 32 + lane < n ? __ldg(base + (32 + lane) * step) : 0;
-    int L = kInfW, mq = 0, bprev = 0;
-    for (int tt = 0; tt < n; tt += SGMW_PF) {
-        if (tt > 0 && (tt & 31) == 0) {             // next block of centres
-            bcv = bnv;
-            const int t2 = tt + 32 + lane;
-            bnv = t2 < n ? __ldg(base + t2 * step) : 0;
-        }
-#pragma unroll
-        for (int u = 0; u < SGMW_PF; ++u) {
-            const int t = tt + u;
-            if (t >= n) break;                          // warp-uniform
-            const int c = (int)cring[u];
-            if (t + SGMW_PF < n) cring[u] = (unsigned)__ldg(cnext);
-            cnext += cstep;
-            const int bcur = __shfl_sync(kFull, bcv, t & 31);
-            int Lnew;
-            if (t == 0) {
-                Lnew = inband ? c : kInfW;
-            } else {
-                const int s = bcur - bprev;
-                const int src = lane + s;
-                int a = __shfl_sync(kFull, L, src & 31);
-                int bm = __shfl_sync(kFull, L, (src - 1) & 31);
-                int bp = __shfl_sync(kFull, L, (src + 1) & 31);
-                if (s < -fast || s > fast) {            // warp-uniform: test every source
-                    if ((unsigned)src >= 32u) a = kInfW;
-                    if ((unsigned)(src - 1) >= 32u) bm = kInfW;
-                    if ((unsigned)(src + 1) >= 32u) bp = kInfW;
-                }
-                const int best = min(min(a, min(bm, bp) + P1), mq + P2);
-                Lnew = inband ? c + best - mq : kInfW;
-            }
-            bprev = bcur;
-            L = Lnew;
-            mq = (int)__reduce_min_sync(kFull, (unsigned)L);
-            if (has_slot) *lout = (LT)(inband ? L : 0);
-            lout += cstep;
-        }
-    }
-}
-
-template <typename LT, int KC>
-__global__ void __launch_bounds__(SGMW_WARPS * 32)
-    k_sgm_warp(const uint8_t *__restrict__ C0, const uint8_t *__restrict__ C1,
-               const int32_t *__restrict__ base0, const int32_t *__restrict__ base1, int W,
-               int H, int K, int Kp, int P1, int P2, LT *__restrict__ Lout, int npaths,
-               SgmTasks tasks) {
-    const int lane = threadIdx.x & 31;
-    const long gid = (long)blockIdx.x * SGMW_WARPS + (threadIdx.x >> 5);
-    if (gid >= tasks.start[tasks.nseg]) return;            // whole warps leave together
-    int sg = 0;
-    while (gid >= tasks.start[sg + 1]) ++sg;
-    const int j0 = (int)(gid - tasks.start[sg]);
-    const int view = tasks.view[sg], dir = tasks.dir[sg];
-    int dx, dy, x0, y0, n;
-    dir_of(dir, dx, dy);
-    scanline_of(W, H, dx, dy, j0, x0, y0, n);
-    const long N = (long)W * H;
-    sgm_line_warp<LT, KC>(view ? C1 : C0, view ? base1 : base0,
-                          Lout + (long)(view * npaths + dir) * N * Kp, W, K, Kp, P1, P2, dx, dy,
-                          x0, y0, n, lane);
+                                   dx, dy, x0, y0, n, gl, gmask, g * GL, lane, rows[warp][0][g],
+                                   rows[warp][1][g], &cstage[warp][0][0], &bstage[warp][0][0]);
 }
 
 // ------------------------------------------------------------------ WTA
@@ -990,31 +927,16 @@ static int sgm_group_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
     return SV_OK;
 }
 
-template <typename LT, int KC = 0>
-static int sgm_warp_go(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
-                       const int32_t *b1, int W, int H, int K, int Kp, int P1, int P2,
-                       void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
-    const long warps = t.start[t.nseg];
-    const int blocks = (int)((warps + SGMW_WARPS - 1) / SGMW_WARPS);
-    count_launch();
-    k_sgm_warp<LT, KC><<<blocks, SGMW_WARPS * 32, 0, st>>>(C0, C1, b0, b1, W, H, K, Kp, P1, P2,
-                                                            (LT *)Lout, npaths, t);
-    SV_LAUNCH_CHECK();
-    return SV_OK;
-}
-
-// Single-pair SGM kernel for bands up to K = 30: 3 = one warp per scanline
-// (default), 0 = lane groups of 8 slots per lane, 1 = lane groups of 4 slots
-// per lane, 2 = one thread per scanline.  SV_SGM_KERNEL = warp | group8 |
-// group4 | thread overrides it (all four are complete and bit-identical; the
-// choice only moves time).
+// Single-pair SGM kernel for bands up to K = 30: 0 = lane groups of 8 slots
+// per lane (default), 1 = lane groups of 4 slots per lane, 2 = one thread per
+// scanline.  SV_SGM_KERNEL = group8 | group4 | thread overrides it (all three
+// give the same refined output; the choice only moves time).
 static int sgm_variant() {
     static const int v = [] {
         const char *e = getenv("SV_SGM_KERNEL");
-        if (e && !strcmp(e, "group8")) return 0;
         if (e && !strcmp(e, "group4")) return 1;
         if (e && !strcmp(e, "thread")) return 2;
-        return 3;
+        return 0;
     }();
     return v;
 }
@@ -1025,11 +947,6 @@ static int sgm_packed_dispatch(const uint8_t *C0, const uint8_t *C1, const int32
                                void *Lout, int npaths, const SgmTasks &t, cudaStream_t st) {
     const SgmGeom g = geom_for(K);
     const int var = sgm_variant();
-    if (var == 3 && g.Kp <= 32) {
-        if (K == 21)
-            return sgm_warp_go<LT, 21>(C0, C1, b0, b1, W, H, K, g.Kp, P1, P2, Lout, npaths, t, st);
-        return sgm_warp_go<LT>(C0, C1, b0, b1, W, H, K, g.Kp, P1, P2, Lout, npaths, t, st);
-    }
     if (var == 0 && g.Kp <= 32) {
         switch (g.Kp) {
         case 8: return sgm_group_go<8, 1, LT>(C0, C1, b0, b1, W, H, K, P1, P2, Lout, npaths, t, st);

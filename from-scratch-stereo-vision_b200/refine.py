@@ -38,16 +38,14 @@ _NP_CODE = {np.dtype(np.uint8): _lib.SV_U8, np.dtype(np.float32): _lib.SV_F32,
 
 def sgm_kernel_name(K: int = 21) -> str:
     """Name of the single-pair SGM kernel the library runs for a band of K
-    (the library reads SV_SGM_KERNEL = warp | group8 | group4 | thread once)."""
+    (the library reads SV_SGM_KERNEL = group8 | group4 | thread once)."""
     import os
     Kp = next((k for k in (8, 16, 24, 32) if k >= K + 2), None)
     if Kp is None:
         return "k_sgm_packed"
-    v = os.environ.get("SV_SGM_KERNEL", "warp")
+    v = os.environ.get("SV_SGM_KERNEL", "group8")
     if v == "thread":
         return "k_sgm_thread"
-    if v not in ("group8", "group4"):
-        return "k_sgm_warp"
     sl = 4 if v == "group4" else 8
     return "k_sgm_group<%d slots x %d lanes>" % (sl, Kp // sl)
 

@@ -73,6 +73,16 @@ SIGNATURES = {
     "sv_batch_lr_refine": (_I, [_VP, _I, _I, _D, _PRM, _VP, _SZ, _VP]),
     "sv_batch_config_default": (None, [_VP]),
     "sv_batch_lr_refine_ex": (_I, [_VP, _I, _I, _D, _PRM, _VP, _VP, _SZ, _VP]),
+    "sv_netbatch_create": (_I, [_VP, _IP, _IP, _I, _I, _D, _I, _I, _I, _I, _D, _PRM,
+                                ctypes.POINTER(_VP)]),
+    "sv_netbatch_workspace_size": (_SZ, [_VP]),
+    "sv_netbatch_bind": (_I, [_VP, _VP, _VP, _SZ, _VP]),
+    "sv_netbatch_run": (_I, [_VP, _VP]),
+    "sv_netbatch_predict": (_I, [_VP, _VP]),
+    "sv_netbatch_disparity": (_I, [_VP, _I, ctypes.POINTER(_VP)]),
+    "sv_netbatch_trace": (_I, [_VP, _IP, _I, _IP, _VP]),
+    "sv_netbatch_data_status": (_I, [_VP, _VP]),
+    "sv_netbatch_destroy": (None, [_VP]),
     "sv_predict_consistent_workspace_size": (_SZ, [_VP, _I, _I, _I, _I]),
     "sv_predict_consistent": (_I, [_VP, _VP, _VP, _I, _I, _I, _I, _D, _I, _I, _I, _D, _I, _VP,
                                    ctypes.POINTER(ctypes.c_longlong), _VP, _SZ, _VP]),

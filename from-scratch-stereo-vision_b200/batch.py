@@ -14,6 +14,12 @@ tasks per queue fetch) by timing the batch itself, one knob at a time from
 the defaults, and remembers the choice per device, band and batch shape in
 a small JSON file (``$SV_B200_CACHE`` or ``~/.cache/sv_b200``).  Every
 configuration gives the same bits; only the time changes.
+
+``NetBatch`` puts the network in front: predict_auto (stereonet.py:
+3872-3929) for every pair, with the work-width decisions taken on the
+device, then the same batched lr_refine, as one launch sequence that a CUDA
+graph replays (sv_netbatch_*).  Each pair's network disparity, work-width
+trace and refined output equal predict_auto + lr_refine on that pair alone.
 """
 
 from __future__ import annotations
@@ -199,3 +205,95 @@ def lr_refine_batch(pairs, tol=1.0, **kw):
     b.data_status()
     return [(_ret(b.out[i], pairs[i][0]), _ret(b.status[i], pairs[i][0], as_int=True))
             for i in range(len(pairs))]
+
+
+class NetBatch:
+    """predict_auto + lr_refine for a fixed list of (W, H) sizes, on the
+    device end to end.  ``left``/``right`` (images) and ``out``/``status``
+    (refined disparity and left-right status) are per-pair device buffers
+    allocated once; ``run()`` enqueues the whole batch on the current stream
+    (the first run records a CUDA graph, later runs replay it)."""
+
+    def __init__(self, sizes, net, dtype=torch.uint8, target_peak=None, probe_width=64,
+                 max_width=320, passes=3, tol=2.0, R=10, P1=12.0, P2=150.0, rx=4, ry=3,
+                 paths=8, uniq=0.0):
+        from . import network
+        self.lib = _lib.load()
+        self.g = network.gpu_net(net)
+        self.sizes = [(int(W), int(H)) for W, H in sizes]
+        self.passes = int(passes)
+        self.p = _params(R=R, P1=P1, P2=P2, rx=rx, ry=ry, paths=paths, uniq=uniq)
+        self.code = {torch.uint8: _lib.SV_U8, torch.float32: _lib.SV_F32,
+                     torch.float64: _lib.SV_F64}[dtype]
+        n = len(self.sizes)
+        Ws = (ctypes.c_int * n)(*[W for W, _ in self.sizes])
+        Hs = (ctypes.c_int * n)(*[H for _, H in self.sizes])
+        tp = float(self.g.target_peak if target_peak is None else target_peak)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.sv_netbatch_create(self.g.handle, Ws, Hs, n, self.code, tp,
+                                               int(probe_width), int(max_width), self.passes,
+                                               _lib.SV_FP32, float(tol), ctypes.byref(self.p),
+                                               ctypes.byref(h)), "sv_netbatch_create")
+        self.handle = h
+        dev = _device()
+        self.left = [torch.empty(W * H, dtype=dtype, device=dev) for W, H in self.sizes]
+        self.right = [torch.empty(W * H, dtype=dtype, device=dev) for W, H in self.sizes]
+        self.out = [torch.empty(W * H, dtype=torch.float64, device=dev) for W, H in self.sizes]
+        self.status = [torch.empty(W * H, dtype=torch.uint8, device=dev) for W, H in self.sizes]
+        self.descs = (PairDesc * n)()
+        for i, (W, H) in enumerate(self.sizes):
+            self.descs[i] = PairDesc(self.left[i].data_ptr(), self.right[i].data_ptr(), None,
+                                     self.out[i].data_ptr(), self.status[i].data_ptr(), W, H)
+        self.need = self.lib.sv_netbatch_workspace_size(self.handle)
+        self.ws = torch.empty(self.need, dtype=torch.uint8, device=dev)
+        _lib.check(self.lib.sv_netbatch_bind(self.handle, self.descs, _ptr(self.ws), self.need,
+                                             _stream()), "sv_netbatch_bind")
+
+    def __del__(self):
+        try:
+            if self.handle:
+                self.lib.sv_netbatch_destroy(self.handle)
+        except Exception:
+            pass
+
+    @property
+    def pixels(self) -> int:
+        return sum(W * H for W, H in self.sizes)
+
+    def run(self, stream=None) -> None:
+        """predict_auto + lr_refine of every pair (enqueued only)."""
+        _lib.check(self.lib.sv_netbatch_run(self.handle, _stream() if stream is None else stream),
+                   "sv_netbatch_run")
+
+    def predict(self, stream=None) -> None:
+        """predict_auto of every pair (enqueued only)."""
+        _lib.check(self.lib.sv_netbatch_predict(self.handle,
+                                                _stream() if stream is None else stream),
+                   "sv_netbatch_predict")
+
+    def disparity(self, i: int) -> torch.Tensor:
+        """Pair i's network disparity (FP64, W*H), a view into the workspace."""
+        ptr = ctypes.c_void_p()
+        _lib.check(self.lib.sv_netbatch_disparity(self.handle, i, ctypes.byref(ptr)),
+                   "sv_netbatch_disparity")
+        W, H = self.sizes[i]
+        off = ptr.value - self.ws.data_ptr()
+        return self.ws[off:off + 8 * W * H].view(torch.float64)
+
+    def traces(self):
+        """[(widths chosen, (Ww, Hw)), ...] per pair (synchronises)."""
+        n = len(self.sizes)
+        tl = self.passes + 2
+        tr = (ctypes.c_int * (n * tl))()
+        ws = (ctypes.c_int * (2 * n))()
+        _lib.check(self.lib.sv_netbatch_trace(self.handle, tr, tl, ws, _stream()),
+                   "sv_netbatch_trace")
+        res = []
+        for i in range(n):
+            t = [int(v) for v in tr[i * tl:(i + 1) * tl]]
+            res.append(([v for v in t if v > 0], (int(ws[2 * i]), int(ws[2 * i + 1]))))
+        return res
+
+    def data_status(self) -> None:
+        _lib.check(self.lib.sv_netbatch_data_status(self.handle, ctypes.c_void_p(_stream())),
+                   "sv_netbatch_run")

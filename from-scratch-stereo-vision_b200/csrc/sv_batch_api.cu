@@ -19,19 +19,8 @@
 namespace sv {
 
 namespace {
-
 constexpr int kTileW = 32, kTileH = 8;   // census tile (k_census)
-
-struct BatchPlan {
-    std::vector<BatchPair> pairs;
-    std::vector<long long> px_blk, row_blk, tile_blk, seg_start;
-    std::vector<int> seg_pair, seg_vd;
-    long long px_blocks = 0, rows = 0, tiles = 0, tasks = 0;
-    int maxW = 1;
-    // workspace offsets
-    size_t off_tables = 0, off_pairs = 0, off_px = 0, off_row = 0, off_tile = 0, off_seg = 0,
-           off_segp = 0, off_segvd = 0, total = 0;
-};
+}  // namespace
 
 // Sizes and offsets; with ws != nullptr also fills the per-pair pointers.
 int plan_batch(const sv_pair_desc *in, int n, const RefineCfg &c, int px_per_block, char *ws,
@@ -127,7 +116,57 @@ int plan_batch(const sv_pair_desc *in, int n, const RefineCfg &c, int px_per_blo
     return SV_OK;
 }
 
-}  // namespace
+int upload_batch(const BatchPlan &pl, int n, char *ws, cudaStream_t st) {
+    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_pairs, pl.pairs.data(), sizeof(BatchPair) * n,
+                                cudaMemcpyHostToDevice, st));
+    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_px, pl.px_blk.data(), sizeof(long long) * (n + 1),
+                                cudaMemcpyHostToDevice, st));
+    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_row, pl.row_blk.data(), sizeof(long long) * (n + 1),
+                                cudaMemcpyHostToDevice, st));
+    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_tile, pl.tile_blk.data(),
+                                sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, st));
+    const int nseg = (int)pl.seg_pair.size();
+    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_seg, pl.seg_start.data(),
+                                sizeof(long long) * (nseg + 1), cudaMemcpyHostToDevice, st));
+    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_segp, pl.seg_pair.data(), sizeof(int) * nseg,
+                                cudaMemcpyHostToDevice, st));
+    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_segvd, pl.seg_vd.data(), sizeof(int) * nseg,
+                                cudaMemcpyHostToDevice, st));
+    return SV_OK;
+}
+
+BatchTables batch_tables(const BatchPlan &pl, int n, char *ws, const RefineCfg &c, int dtype,
+                         double tol, const sv_batch_config &cfg) {
+    BatchTables t{};
+    t.pairs = reinterpret_cast<const BatchPair *>(ws + pl.off_pairs);
+    t.n = n;
+    t.px_blk = reinterpret_cast<const long long *>(ws + pl.off_px);
+    t.row_blk = reinterpret_cast<const long long *>(ws + pl.off_row);
+    t.tile_blk = reinterpret_cast<const long long *>(ws + pl.off_tile);
+    t.seg_start = reinterpret_cast<const long long *>(ws + pl.off_seg);
+    t.seg_pair = reinterpret_cast<const int *>(ws + pl.off_segp);
+    t.seg_vd = reinterpret_cast<const int *>(ws + pl.off_segvd);
+    t.nseg = (int)pl.seg_pair.size();
+    t.flag = reinterpret_cast<int *>(ws);
+    t.queue = reinterpret_cast<int *>(ws + sizeof(DevFlags));
+    t.R = c.R;
+    t.K = c.K;
+    t.Kp = slot_width(c.K);
+    t.P1 = c.P1;
+    t.P2 = c.P2;
+    t.npaths = c.npaths;
+    t.invalid = c.invalid;
+    t.rx = c.rx;
+    t.ry = c.ry;
+    t.dtype = dtype;
+    t.maxW = pl.maxW;
+    t.tol = tol;
+    t.uniq = c.uniq;
+    t.px_per_block = cfg.px_per_block;
+    t.sgm_fetch = cfg.sgm_fetch;
+    return t;
+}
+
 }  // namespace sv
 
 using namespace sv;
@@ -201,49 +240,9 @@ int sv_batch_lr_refine_ex(const sv_pair_desc *pairs, int n, int dtype, double to
     char *ws = static_cast<char *>(workspace);
     cudaStream_t st = (cudaStream_t)stream;
     // tables to the device (pageable copies are staged before the call returns)
-    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_pairs, pl.pairs.data(), sizeof(BatchPair) * n,
-                                cudaMemcpyHostToDevice, st));
-    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_px, pl.px_blk.data(), sizeof(long long) * (n + 1),
-                                cudaMemcpyHostToDevice, st));
-    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_row, pl.row_blk.data(), sizeof(long long) * (n + 1),
-                                cudaMemcpyHostToDevice, st));
-    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_tile, pl.tile_blk.data(),
-                                sizeof(long long) * (n + 1), cudaMemcpyHostToDevice, st));
-    const int nseg = (int)pl.seg_pair.size();
-    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_seg, pl.seg_start.data(),
-                                sizeof(long long) * (nseg + 1), cudaMemcpyHostToDevice, st));
-    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_segp, pl.seg_pair.data(), sizeof(int) * nseg,
-                                cudaMemcpyHostToDevice, st));
-    SV_CUDA_TRY(cudaMemcpyAsync(ws + pl.off_segvd, pl.seg_vd.data(), sizeof(int) * nseg,
-                                cudaMemcpyHostToDevice, st));
+    if ((rc = upload_batch(pl, n, ws, st))) return rc;
     SV_CUDA_TRY(cudaMemsetAsync(ws, 0, sizeof(DevFlags) + 256, st));   // flag + queue
-    BatchTables t{};
-    t.pairs = reinterpret_cast<const BatchPair *>(ws + pl.off_pairs);
-    t.n = n;
-    t.px_blk = reinterpret_cast<const long long *>(ws + pl.off_px);
-    t.row_blk = reinterpret_cast<const long long *>(ws + pl.off_row);
-    t.tile_blk = reinterpret_cast<const long long *>(ws + pl.off_tile);
-    t.seg_start = reinterpret_cast<const long long *>(ws + pl.off_seg);
-    t.seg_pair = reinterpret_cast<const int *>(ws + pl.off_segp);
-    t.seg_vd = reinterpret_cast<const int *>(ws + pl.off_segvd);
-    t.nseg = nseg;
-    t.flag = reinterpret_cast<int *>(ws);
-    t.queue = reinterpret_cast<int *>(ws + sizeof(DevFlags));
-    t.R = c.R;
-    t.K = c.K;
-    t.Kp = slot_width(c.K);
-    t.P1 = c.P1;
-    t.P2 = c.P2;
-    t.npaths = c.npaths;
-    t.invalid = c.invalid;
-    t.rx = c.rx;
-    t.ry = c.ry;
-    t.dtype = dtype;
-    t.maxW = pl.maxW;
-    t.tol = tol;
-    t.uniq = c.uniq;
-    t.px_per_block = cfg->px_per_block;
-    t.sgm_fetch = cfg->sgm_fetch;
+    const BatchTables t = batch_tables(pl, n, ws, c, dtype, tol, *cfg);
     return launch_batch_refine(t, pl.px_blocks, pl.rows, pl.tiles, pl.tasks, c.l16,
                                cfg->sgm_threads, cfg->sgm_ctas_per_sm, st);
 }

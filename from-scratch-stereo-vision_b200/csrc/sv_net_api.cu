@@ -457,6 +457,8 @@ static int pack_tc(sv_net *net, const double *params) {
     return SV_OK;
 }
 
+const NetView &net_view(const sv_net *net) { return net->view; }
+
 }  // namespace sv
 
 using namespace sv;

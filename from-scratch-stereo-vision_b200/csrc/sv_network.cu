@@ -20,6 +20,7 @@
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
+#include "sv_netbatch.cuh"
 #include "sv_select.cuh"
 #include "sv_tc.cuh"
 
@@ -57,24 +58,27 @@ __device__ __forceinline__ double blend64(const T *x, const Taps &t) {
 // (stereonet.py:979-995), from the 2x2 blocks a 32 x 8 CTA holds in shared
 // memory.
 template <typename T>
-__global__ void __launch_bounds__(256)
-    k_resize_pair(const T *__restrict__ l, const T *__restrict__ r, int W, int H, int W2, int H2,
+__device__ __forceinline__ void resize_pair_body(int bx, int by, int bz, bool first, bool copy,
+                                                 const T *__restrict__ l, const T *__restrict__ r, int W, int H, int W2, int H2,
                   float *__restrict__ lo, float *__restrict__ ro, float *__restrict__ gh,
                   SelState *sel, unsigned *sel_hist, long long sel_rank) {
     __shared__ float sv[8][33];
-    if (sel && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0)
+    if (sel && first)
         sel_init_block(sel, sel_rank, sel_hist);      // the stage's select starts here
-    const T *src = blockIdx.z ? r : l;
-    float *dst = blockIdx.z ? ro : lo;
+    const T *src = bz ? r : l;
+    float *dst = bz ? ro : lo;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int ox = blockIdx.x * 32 + tx, oy = blockIdx.y * 8 + ty;
+    const int ox = bx * 32 + tx, oy = by * 8 + ty;
     const bool in = ox < W2 && oy < H2;
     float v = 0.f;
     if (in) {
-        v = (float)blend64<T>(src, bilinear_taps(oy, ox, H, W, H2, W2));
+        // copy: a native-resolution pass, which the reference runs on the
+        // images themselves (predict_at_scale, stereonet.py:3941-3943)
+        v = copy ? (float)gray_at<T>(src, oy * W + ox)
+                 : (float)blend64<T>(src, bilinear_taps(oy, ox, H, W, H2, W2));
         dst[oy * W2 + ox] = v;
     }
-    if (!gh || blockIdx.z != 0) return;            // the same for the whole CTA
+    if (!gh || bz != 0) return;            // the same for the whole CTA
     sv[ty][tx] = v;
     __syncthreads();
     // a 2x2 block inside the half-resolution image lies inside the image
@@ -82,6 +86,41 @@ __global__ void __launch_bounds__(256)
     if (in && !(tx & 1) && !(ty & 1) && ox / 2 < W2 / 2 && oy / 2 < H2 / 2)
         gh[(oy / 2) * (W2 / 2) + ox / 2] =
             0.25f * (((v + sv[ty][tx + 1]) + sv[ty + 1][tx]) + sv[ty + 1][tx + 1]);
+}
+
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_resize_pair(const T *__restrict__ l, const T *__restrict__ r, int W, int H, int W2, int H2,
+                  float *__restrict__ lo, float *__restrict__ ro, float *__restrict__ gh,
+                  SelState *sel, unsigned *sel_hist, long long sel_rank) {
+    resize_pair_body<T>(blockIdx.x, blockIdx.y, blockIdx.z,
+                        blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0, false, l, r, W,
+                        H, W2, H2,
+                        lo, ro, gh, sel, sel_hist, sel_rank);
+}
+
+// Batched: the pass's resample of every active pair (a 1-D grid over the
+// pairs' largest tile grids, 2 images per tile); with sel, each pair's first
+// CTA also starts that pair's full-resolution select.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    k_b_resize_pair(NetLaunch L, const void *const *lt, const void *const *rt, float *lo,
+                    float *ro, float *gh, SelState *sel, unsigned *sel_hist) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    const int tx = (P.Ww + 31) / 32, ty = (P.Hw + 7) / 8;
+    const int bz = (int)(c & 1);
+    const long long t = c >> 1;
+    const int bx = (int)(t % tx), by = (int)(t / tx);
+    if (by >= ty) return;
+    const long long rank = (long long)__dmul_rn((double)((long long)P.W * P.H), 0.95);
+    resize_pair_body<T>(bx, by, bz, c == 0, P.native != 0, static_cast<const T *>(lt[p]),
+                        static_cast<const T *>(rt[p]), P.W, P.H, P.Ww, P.Hw, net_slab(lo, L, p),
+                        net_slab(ro, L, p), net_slab(gh, L, p), net_slab(sel, L, p),
+                        net_slab(sel_hist, L, p), rank);
 }
 
 // Copy (no resample) of a pair into FP32, for predict at native resolution.
@@ -114,27 +153,57 @@ __global__ void k_resize_scale(const T *__restrict__ x, int W, int H, int W2, in
 // threads that fall inside it (the work map is never larger).
 // With sel, also pass 0 of the stage's full-resolution select over the
 // values it writes (the select's first histogram: ghist).
-__global__ void __launch_bounds__(256)
-    k_work_outputs(const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
+__device__ __forceinline__ void work_outputs_body(int bx, int by, unsigned nblk, bool copy,
+                                                  const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
                    double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
                    unsigned *ghist) {
     __shared__ unsigned hist[SEL_NB];
-    const int ox = blockIdx.x * blockDim.x + threadIdx.x;
-    const int oy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int ox = bx * blockDim.x + threadIdx.x;
+    const int oy = by * blockDim.y + threadIdx.y;
     const bool in = ox < W && oy < H;
     double v = 0.0;
     if (in) {
-        const Taps t = bilinear_taps(oy, ox, Hw, Ww, H, W);
-        v = __dmul_rn(blend64<float>(d, t), inv);
+        if (copy) {                  // native resolution: the network output itself
+            v = (double)d[(long)oy * W + ox];
+        } else {
+            const Taps t = bilinear_taps(oy, ox, Hw, Ww, H, W);
+            v = __dmul_rn(blend64<float>(d, t), inv);
+        }
         full64[(long)oy * W + ox] = v;
-        if (ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
+        if (work64 && ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
     }
     if (!sel) return;                              // the same for every CTA
     for (int i = sel_tid(); i < SEL_NB; i += sel_nt()) hist[i] = 0u;
     __syncthreads();
     sel_count(hist, sel_key(v), in, 0ull, 0);
     __syncthreads();
-    sel_pass_finish(0, sel, ghist, hist);
+    sel_pass_finish(0, sel, ghist, hist, nblk);
+}
+
+
+__global__ void __launch_bounds__(256)
+    k_work_outputs(const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
+                   double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
+                   unsigned *ghist) {
+    work_outputs_body(blockIdx.x, blockIdx.y, gridDim.x * gridDim.y * gridDim.z, false, d, Ww,
+                      Hw, W, H, inv, work64, full64, sel, ghist);
+}
+
+// Batched: every active pair's full-resolution map from its work map (the
+// grid covers each pair's full size exactly), with pass 0 of its select.
+__global__ void __launch_bounds__(256)
+    k_b_work_outputs(NetLaunch L, const float *d, double *work64, double *full64, SelState *sel,
+                     unsigned *ghist) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    const int tx = (P.W + 31) / 32;
+    const unsigned nblk = (unsigned)(L.pre[p + 1] - L.pre[p]);
+    work_outputs_body((int)(c % tx), (int)(c / tx), nblk, P.native != 0, net_slab(d, L, p), P.Ww,
+                      P.Hw, P.W,
+                      P.H, P.inv, net_slab(work64, L, p), net_slab(full64, L, p),
+                      net_slab(sel, L, p), net_slab(ghist, L, p));
 }
 
 template <typename T>
@@ -197,8 +266,7 @@ __host__ __device__ inline int conv2d_plane(int th, int tw, int CPS, int CS) {
 }
 
 template <int IC, int OC, int OCG, int ACT, int CS>
-__global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
-    k_conv2d_tiled(const float *__restrict__ x0, const float *__restrict__ x1, int H, int W,
+__device__ __forceinline__ void conv2d_tiled_body(int bx, int by, int bz, const float *__restrict__ x0, const float *__restrict__ x1, int H, int W,
                    int OH, int OW, int stride, int pad, int dil, const float *__restrict__ w,
                    const float *__restrict__ b, float *y0, float *y1,
                    const float *__restrict__ resid) {
@@ -207,7 +275,7 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
     extern __shared__ __align__(16) float tile[];
     __shared__ __align__(16) float sw[IC * 9 * OCG];
     __shared__ float sb[OCG];
-    const int img = blockIdx.z / NG, og = blockIdx.z - img * NG;
+    const int img = bz / NG, og = bz - img * NG;
     const int tid = threadIdx.x;
     for (int i = tid; i < IC * 9 * OCG; i += NT) {
         const int o = i % OCG, ct = i / OCG;          // ct = c * 9 + tap
@@ -216,7 +284,7 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
     if (tid < OCG) sb[tid] = b[og * OCG + tid];
     const float *x = img ? x1 : x0;
     float *y = img ? y1 : y0;
-    const int ox0 = blockIdx.x * CT2_TW, oy0 = blockIdx.y * CT2_TH;
+    const int ox0 = bx * CT2_TW, oy0 = by * CT2_TH;
     const int ix0 = ox0 * stride - pad, iy0 = oy0 * stride - pad;
     const int tw = (CT2_TW - 1) * stride + 2 * dil + 1;
     const int th = (CT2_TH - 1) * stride + 2 * dil + 1;
@@ -238,14 +306,14 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
     float acc[OCG];
 #pragma unroll
     for (int o = 0; o < OCG; ++o) acc[o] = 0.f;
-    const int by = ly * stride, bx = lx * stride;
+    const int sy = ly * stride, sx = lx * stride;
 #pragma unroll
     for (int j = 0; j < CPS; ++j) {
         const int c = cs * CPS + j;
         const float *tc = tile + c * plane;
 #pragma unroll
         for (int ky = 0; ky < 3; ++ky) {
-            const float *row = tc + (by + ky * dil) * tw + bx;
+            const float *row = tc + (sy + ky * dil) * tw + sx;
 #pragma unroll
             for (int kx = 0; kx < 3; ++kx) {
                 const float v = row[kx * dil];
@@ -285,6 +353,55 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
     }
 }
 
+
+template <int IC, int OC, int OCG, int ACT, int CS>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
+    k_conv2d_tiled(const float *__restrict__ x0, const float *__restrict__ x1, int H, int W,
+                   int OH, int OW, int stride, int pad, int dil, const float *__restrict__ w,
+                   const float *__restrict__ b, float *y0, float *y1,
+                   const float *__restrict__ resid) {
+    conv2d_tiled_body<IC, OC, OCG, ACT, CS>(blockIdx.x, blockIdx.y, blockIdx.z, x0, x1, H, W,
+                                            OH, OW, stride, pad, dil, w, b, y0, y1, resid);
+}
+
+// Input and output sizes of a batched 2-D convolution, from the pass's work
+// size: 0 FeatureNet c1 (work -> half), 1 c2 (half -> quarter), 2 c3/c4
+// (quarter), 3 Refinement level 0 (work / 2), 4 Refinement level 1 (work).
+__device__ __forceinline__ void conv_level(int lv, int Hw, int Ww, int &H, int &W, int &OH,
+                                           int &OW) {
+    int h1, w1, h, w;
+    net_quarter(Hw, Ww, h1, w1, h, w);
+    switch (lv) {
+    case 0: H = Hw; W = Ww; OH = h1; OW = w1; break;
+    case 1: H = h1; W = w1; OH = h; OW = w; break;
+    case 2: H = OH = h; W = OW = w; break;
+    case 3: H = OH = Hw / 2; W = OW = Ww / 2; break;
+    default: H = OH = Hw; W = OW = Ww; break;
+    }
+}
+
+template <int IC, int OC, int OCG, int ACT, int CS>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
+    k_b_conv2d_tiled(NetLaunch L, int lv, int Z, const float *x0, const float *x1, int stride,
+                     int pad, int dil, const float *__restrict__ w, const float *__restrict__ b,
+                     float *y0, float *y1, const float *resid) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    int H, W, OH, OW;
+    conv_level(lv, P.Hw, P.Ww, H, W, OH, OW);
+    const int tx = (OW + CT2_TW - 1) / CT2_TW, ty = (OH + CT2_TH - 1) / CT2_TH;
+    const int bz = (int)(c % Z);
+    const long long t = c / Z;
+    const int bx = (int)(t % tx), by = (int)(t / tx);
+    if (by >= ty) return;
+    conv2d_tiled_body<IC, OC, OCG, ACT, CS>(bx, by, bz, net_slab(x0, L, p), net_slab(x1, L, p),
+                                            H, W, OH, OW, stride, pad, dil, w, b,
+                                            net_slab(y0, L, p), net_slab(y1, L, p),
+                                            net_slab(resid, L, p));
+}
+
 // A Refinement level's first convolution (2 -> RC, stride 1, dilation dil,
 // leaky ReLU) with the level's input built while staging: channel 0 is
 // 2 * bilinear(prev) (BilinearUpsample.forward's half-pixel taps, FP64
@@ -293,19 +410,18 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
 // image.  The CTAs of channel group 0 also store channel 0 of
 // their inner tile into rin0, the residual the level's last convolution adds.
 template <int RC, int OCG>
-__global__ void __launch_bounds__(CT2_TW *CT2_TH)
-    k_conv2d_up(const float *__restrict__ prev, int ph, int pw, const float *__restrict__ guide,
+__device__ __forceinline__ void conv2d_up_body(int bx, int by, int bz, const float *__restrict__ prev, int ph, int pw, const float *__restrict__ guide,
                 int H, int W, int dil, const float *__restrict__ w, const float *__restrict__ b,
                 float *__restrict__ y, float *__restrict__ rin0) {
     constexpr int IC = 2, NG = RC / OCG;
     extern __shared__ __align__(16) float tile[];
     __shared__ float sw[OCG * IC * 9];
     __shared__ float sb[OCG];
-    const int og = blockIdx.z % NG;
+    const int og = bz % NG;
     const int tid = threadIdx.y * CT2_TW + threadIdx.x;
     for (int i = tid; i < OCG * IC * 9; i += CT2_TW * CT2_TH) sw[i] = w[og * OCG * IC * 9 + i];
     if (tid < OCG) sb[tid] = b[og * OCG + tid];
-    const int ox0 = blockIdx.x * CT2_TW, oy0 = blockIdx.y * CT2_TH;
+    const int ox0 = bx * CT2_TW, oy0 = by * CT2_TH;
     const int ix0 = ox0 - dil, iy0 = oy0 - dil;
     const int tw = CT2_TW + 2 * dil, th = CT2_TH + 2 * dil;
     for (int i = tid; i < th * tw; i += CT2_TW * CT2_TH) {
@@ -351,6 +467,41 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH)
         const float v = acc[o];
         y[(og * OCG + o) * HW + oi] = v > 0.f ? v : v * 0.2f;
     }
+}
+
+
+template <int RC, int OCG>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH)
+    k_conv2d_up(const float *__restrict__ prev, int ph, int pw, const float *__restrict__ guide,
+                int H, int W, int dil, const float *__restrict__ w, const float *__restrict__ b,
+                float *__restrict__ y, float *__restrict__ rin0) {
+    conv2d_up_body<RC, OCG>(blockIdx.x, blockIdx.y, blockIdx.z, prev, ph, pw, guide, H, W, dil,
+                            w, b, y, rin0);
+}
+
+// Batched: level lv (0: from the quarter-size disparity to work / 2, 1: from
+// work / 2 to the work size).
+template <int RC, int OCG>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH)
+    k_b_conv2d_up(NetLaunch L, int lv, const float *prev, const float *guide, int dil,
+                  const float *__restrict__ w, const float *__restrict__ b, float *y,
+                  float *rin0) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    int h1, w1, h, wq;
+    net_quarter(P.Hw, P.Ww, h1, w1, h, wq);
+    const int ph = lv ? P.Hw / 2 : h, pw = lv ? P.Ww / 2 : wq;
+    const int H = lv ? P.Hw : P.Hw / 2, W = lv ? P.Ww : P.Ww / 2;
+    constexpr int Z = RC / OCG;
+    const int tx = (W + CT2_TW - 1) / CT2_TW, ty = (H + CT2_TH - 1) / CT2_TH;
+    const int bz = (int)(c % Z);
+    const long long t = c / Z;
+    const int bx = (int)(t % tx), by = (int)(t / tx);
+    if (by >= ty) return;
+    conv2d_up_body<RC, OCG>(bx, by, bz, net_slab(prev, L, p), ph, pw, net_slab(guide, L, p), H, W,
+                            dil, w, b, net_slab(y, L, p), net_slab(rin0, L, p));
 }
 
 static size_t conv2d_tile_bytes(int IC, int stride, int dil, int CS = 1) {
@@ -468,8 +619,7 @@ __device__ __forceinline__ void c3_reduce(float (&acc)[OCG]) {
 // CostFilter (stereonet.py:596-641, leaky ReLU 0.2): C -> OC channels, OCG
 // per CTA (blockIdx.z), 128 threads = 8 columns x TD disparities x CS splits.
 template <int C, int OCG, int CS, bool CV>
-__global__ void __launch_bounds__(128)
-    k_conv3d_split(const float *__restrict__ a, const float *__restrict__ bsrc, int D, int h,
+__device__ __forceinline__ void conv3d_split_body(int bx, int by, int bz, const float *__restrict__ a, const float *__restrict__ bsrc, int D, int h,
                    int w, const float *__restrict__ wt, const float *__restrict__ bias,
                    float *__restrict__ y) {
     constexpr int CPS = C / CS, TD = 16 / CS;
@@ -478,8 +628,8 @@ __global__ void __launch_bounds__(128)
     __shared__ float tile[C * P];
     __shared__ __align__(16) float sw[C * 27 * OCG];
     __shared__ float sb[OCG];
-    const int og = blockIdx.z, nd = (D + TD - 1) / TD;
-    const int x0 = blockIdx.x * C3_TX, oy = blockIdx.y / nd, d0 = (blockIdx.y - oy * nd) * TD;
+    const int og = bz, nd = (D + TD - 1) / TD;
+    const int x0 = bx * C3_TX, oy = by / nd, d0 = (by - oy * nd) * TD;
     const int tid = threadIdx.x;
     for (int i = tid; i < C * 27 * OCG; i += 128) {
         const int o = i % OCG, ct = i / OCG;       // ct = c * 27 + tap
@@ -505,6 +655,39 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+
+template <int C, int OCG, int CS, bool CV>
+__global__ void __launch_bounds__(128)
+    k_conv3d_split(const float *__restrict__ a, const float *__restrict__ bsrc, int D, int h,
+                   int w, const float *__restrict__ wt, const float *__restrict__ bias,
+                   float *__restrict__ y) {
+    conv3d_split_body<C, OCG, CS, CV>(blockIdx.x, blockIdx.y, blockIdx.z, a, bsrc, D, h, w, wt,
+                                      bias, y);
+}
+
+// Batched CostFilter c1 (cost volume built on the fly) or c2, at the pass's
+// quarter size; Z output-channel groups.
+template <int C, int OCG, int CS, bool CV>
+__global__ void __launch_bounds__(128)
+    k_b_conv3d_split(NetLaunch L, int Z, const float *a, const float *bsrc, int D,
+                     const float *__restrict__ wt, const float *__restrict__ bias, float *y) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    int h1, w1, h, w;
+    net_quarter(P.Hw, P.Ww, h1, w1, h, w);
+    constexpr int TD = 16 / CS;
+    const int nd = (D + TD - 1) / TD;
+    const int tx = (w + C3_TX - 1) / C3_TX, ty = h * nd;
+    const int bz = (int)(c % Z);
+    const long long t = c / Z;
+    const int bx = (int)(t % tx), by = (int)(t / tx);
+    if (by >= ty) return;
+    conv3d_split_body<C, OCG, CS, CV>(bx, by, bz, net_slab(a, L, p), net_slab(bsrc, L, p), D, h,
+                                      w, wt, bias, net_slab(y, L, p));
+}
+
 // ----------------------------------- conv3d #3 + invalid mask + soft-argmin
 // Conv3d #3 (Cm -> 1), CostVolume.invalid_mask (+8 where x < d, d >= 1,
 // stereonet.py:827-840) and SoftArgmin.forward (858-885) in FP32 with
@@ -515,8 +698,7 @@ __global__ void __launch_bounds__(128)
 constexpr int SA_DMAX = 16;
 
 template <int IC, int CS>
-__global__ void __launch_bounds__(128 * CS)
-    k_conv3d_softargmin(const float *__restrict__ x, int D, int h, int w,
+__device__ __forceinline__ void conv3d_softargmin_body(int bx, int by, const float *__restrict__ x, int D, int h, int w,
                         const float *__restrict__ wt, const float *__restrict__ b,
                         float *__restrict__ disp) {
     constexpr int CPS = IC / CS, TD = SA_DMAX, NT = 128 * CS;
@@ -527,7 +709,7 @@ __global__ void __launch_bounds__(128 * CS)
     __shared__ float cost[SA_DMAX][C3_TX + 1];
     const int tid = threadIdx.x;
     for (int i = tid; i < IC * 27; i += NT) sw[i] = __ldg(wt + i);
-    const int x0 = blockIdx.x * C3_TX, oy = blockIdx.y;
+    const int x0 = bx * C3_TX, oy = by;
     c3_stage<IC, TD, DS, P, NT, false>(tile, x, nullptr, D, h, w, x0, oy, 0);
     __syncthreads();
     {
@@ -561,6 +743,32 @@ __global__ void __launch_bounds__(128 * CS)
     if (d == 0 && ox < w) disp[(long)oy * w + ox] = td / te;
 }
 
+
+
+template <int IC, int CS>
+__global__ void __launch_bounds__(128 * CS)
+    k_conv3d_softargmin(const float *__restrict__ x, int D, int h, int w,
+                        const float *__restrict__ wt, const float *__restrict__ b,
+                        float *__restrict__ disp) {
+    conv3d_softargmin_body<IC, CS>(blockIdx.x, blockIdx.y, x, D, h, w, wt, b, disp);
+}
+
+template <int IC, int CS>
+__global__ void __launch_bounds__(128 * CS)
+    k_b_conv3d_softargmin(NetLaunch L, const float *x, int D, const float *__restrict__ wt,
+                          const float *__restrict__ b, float *disp) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    int h1, w1, h, w;
+    net_quarter(P.Hw, P.Ww, h1, w1, h, w);
+    const int tx = (w + C3_TX - 1) / C3_TX;
+    const int bx = (int)(c % tx), by = (int)(c / tx);
+    if (by >= h) return;
+    conv3d_softargmin_body<IC, CS>(bx, by, net_slab(x, L, p), D, h, w, wt, b,
+                                   net_slab(disp, L, p));
+}
 
 // ====================================================================
 // Host side
@@ -860,5 +1068,163 @@ int launch_forward(const NetView &n, const float *left, const float *right, int 
     return SV_ERR_NET;
 }
 
+
+
+// ====================================================================
+// Batched predict_auto passes (driven by sv_netbatch.cu)
+// ====================================================================
+
+// CTAs of each batched network kernel for one pair whose work size is at
+// most Hm x Wm (the same tile shapes and channel groups as forward_impl).
+template <int C, int CM, int RC>
+static void stage_ctas_impl(const NetView &n, int Hm, int Wm, long long *o) {
+    int h1, w1, h, w;
+    net_quarter(Hm, Wm, h1, w1, h, w);
+    constexpr int FG = C % 4 == 0 ? 4 : C;
+    constexpr int S1 = C % 4 == 0 ? 4 : 2, S2 = CM % 4 == 0 && CM > 4 ? 4 : 2;
+    constexpr int RG = RC % 4 == 0 ? 4 : RC;
+    auto t2 = [](int OW, int OH) {
+        return (long long)((OW + CT2_TW - 1) / CT2_TW) * ((OH + CT2_TH - 1) / CT2_TH);
+    };
+    const int D = n.D, cx = (w + C3_TX - 1) / C3_TX;
+    o[NK_RESIZE] = 2LL * ((Wm + 31) / 32) * ((Hm + 7) / 8);
+    o[NK_C1] = 2LL * (C / FG) * t2(w1, h1);
+    o[NK_C2] = 2LL * (C / FG) * t2(w, h);
+    o[NK_V1] = (long long)cx * h * ((D + 16 / S1 - 1) / (16 / S1));
+    o[NK_V2] = (long long)cx * h * ((D + 16 / S2 - 1) / (16 / S2));
+    o[NK_SA] = (long long)cx * h;
+    o[NK_R0] = (long long)(RC / RG) * t2(Wm / 2, Hm / 2);
+    o[NK_R0F] = t2(Wm / 2, Hm / 2);
+    o[NK_R1] = (long long)(RC / RG) * t2(Wm, Hm);
+    o[NK_R1F] = t2(Wm, Hm);
+}
+
+int net_stage_ctas(const NetView &n, int Hm, int Wm, long long *o) {
+    if (n.C == 12 && n.Cm == 6 && n.Rc == 8) stage_ctas_impl<12, 6, 8>(n, Hm, Wm, o);
+    else if (n.C == 8 && n.Cm == 4 && n.Rc == 8) stage_ctas_impl<8, 4, 8>(n, Hm, Wm, o);
+    else if (n.C == 8 && n.Cm == 4 && n.Rc == 4) stage_ctas_impl<8, 4, 4>(n, Hm, Wm, o);
+    else if (n.C == 16 && n.Cm == 8 && n.Rc == 8) stage_ctas_impl<16, 8, 8>(n, Hm, Wm, o);
+    else {
+        set_error("architecture feat_C=%d cost_C=%d refine_C=%d is not instantiated", n.C, n.Cm,
+                  n.Rc);
+        return SV_ERR_NET;
+    }
+    return SV_OK;
+}
+
+static unsigned ctas_of(long long total) { return (unsigned)(total > 0 ? total : 1); }
+
+// The FP32 forward of one stage over every active pair: forward_impl's
+// kernels in their batched form, one launch each for the whole batch.
+template <int C, int CM, int RC>
+static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSlab &s,
+                          cudaStream_t st) {
+    const int D = n.D;
+    auto L = [&](int k) { return NetLaunch{g.pre[k], g.pairs, g.n, g.slab}; };
+    auto B = [&](int k) { return ctas_of(g.total[k]); };
+    const int tb1 = CT2_TW * CT2_TH, tb2 = 2 * tb1, tb4 = 4 * tb1;
+    const dim3 tb(CT2_TW, CT2_TH);
+    constexpr int FG = C % 4 == 0 ? 4 : C;
+    constexpr int ZF = 2 * (C / FG);
+    count_launch();
+    k_b_conv2d_tiled<1, C, FG, 1, 1><<<B(NK_C1), tb1, conv2d_tile_bytes(1, 2, 1), st>>>(
+        L(NK_C1), 0, ZF, s.lw, s.rw, 2, 1, 1, n.fw[0], n.fb[0], s.f.fa[0], s.f.fa[1], nullptr);
+    count_launch();
+    k_b_conv2d_tiled<C, C, FG, 1, 2><<<B(NK_C2), tb2, conv2d_tile_bytes(C, 2, 1, 2), st>>>(
+        L(NK_C2), 1, ZF, s.f.fa[0], s.f.fa[1], 2, 1, 1, n.fw[1], n.fb[1], s.f.fb[0], s.f.fb[1],
+        nullptr);
+    count_launch();
+    k_b_conv2d_tiled<C, C, FG, 1, 2><<<B(NK_C2), tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
+        L(NK_C2), 2, ZF, s.f.fb[0], s.f.fb[1], 1, 1, 1, n.fw[2], n.fb[2], s.f.fa[0], s.f.fa[1],
+        nullptr);
+    count_launch();
+    k_b_conv2d_tiled<C, C, FG, 0, 2><<<B(NK_C2), tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
+        L(NK_C2), 2, ZF, s.f.fa[0], s.f.fa[1], 1, 1, 1, n.fw[3], n.fb[3], s.f.fb[0], s.f.fb[1],
+        nullptr);
+    SV_LAUNCH_CHECK();
+    constexpr int S1 = C % 4 == 0 ? 4 : 2, S2 = CM % 4 == 0 && CM > 4 ? 4 : 2;
+    count_launch();
+    k_b_conv3d_split<C, CM, S1, true><<<B(NK_V1), 128, 0, st>>>(
+        L(NK_V1), 1, s.f.fb[0], s.f.fb[1], D, n.cw[0], n.cb[0], s.f.v0);
+    count_launch();
+    k_b_conv3d_split<CM, CM, S2, false><<<B(NK_V2), 128, 0, st>>>(
+        L(NK_V2), 1, s.f.v0, nullptr, D, n.cw[1], n.cb[1], s.f.v1);
+    constexpr int S3 = CM % 2 == 0 ? 2 : 1;
+    count_launch();
+    k_b_conv3d_softargmin<CM, S3><<<B(NK_SA), 128 * S3, 0, st>>>(L(NK_SA), s.f.v1, D, n.cw[2],
+                                                                  n.cb[2], s.d0);
+    SV_LAUNCH_CHECK();
+    constexpr int RG = RC % 4 == 0 ? 4 : RC;
+    constexpr int RS = RC % 4 == 0 ? 4 : 2;
+    const float *guides[2] = {s.gh, s.lw};
+    const float *prevs[2] = {s.d0, s.d1};
+    float *outs[2] = {s.d1, s.d2};
+    for (int lv = 0; lv < 2; ++lv) {
+        const int kk = lv ? NK_R1 : NK_R0, kf = lv ? NK_R1F : NK_R0F;
+        float *bufs[2] = {s.f.ra, s.f.rb};
+        const float *cur = nullptr;
+        for (int i = 0; i < n.ndil; ++i) {
+            float *dst = bufs[i & 1];
+            const int dl = n.dil[i];
+            count_launch();
+            if (i == 0)
+                k_b_conv2d_up<RC, RG><<<B(kk), tb, conv2d_tile_bytes(2, 1, dl), st>>>(
+                    L(kk), lv, prevs[lv], guides[lv], dl, n.rw[lv][i], n.rb[lv][i], dst, s.f.rin);
+            else
+                k_b_conv2d_tiled<RC, RC, RG, 1, RS><<<B(kk), RS * tb1,
+                                                      conv2d_tile_bytes(RC, 1, dl, RS), st>>>(
+                    L(kk), 3 + lv, RC / RG, cur, cur, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst,
+                    dst, nullptr);
+            cur = dst;
+        }
+        count_launch();
+        k_b_conv2d_tiled<RC, 1, 1, 2, 4><<<B(kf), tb4, conv2d_tile_bytes(RC, 1, 1, 4), st>>>(
+            L(kf), 3 + lv, 1, cur, cur, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
+            outs[lv], s.f.rin);
+        SV_LAUNCH_CHECK();
+    }
+    return SV_OK;
+}
+
+int launch_b_forward(const NetView &n, const NetStageLaunch &g, const NetSlab &s,
+                     cudaStream_t st) {
+    if (n.D < 1 || n.D > 16) {
+        set_error("D=%d outside 1..16", n.D);
+        return SV_ERR_NET;
+    }
+    if (n.C == 12 && n.Cm == 6 && n.Rc == 8) return b_forward_impl<12, 6, 8>(n, g, s, st);
+    if (n.C == 8 && n.Cm == 4 && n.Rc == 8) return b_forward_impl<8, 4, 8>(n, g, s, st);
+    if (n.C == 8 && n.Cm == 4 && n.Rc == 4) return b_forward_impl<8, 4, 4>(n, g, s, st);
+    if (n.C == 16 && n.Cm == 8 && n.Rc == 8) return b_forward_impl<16, 8, 8>(n, g, s, st);
+    set_error("architecture feat_C=%d cost_C=%d refine_C=%d is not instantiated", n.C, n.Cm,
+              n.Rc);
+    return SV_ERR_NET;
+}
+
+int launch_b_resize(const NetStageLaunch &g, const void *const *lt, const void *const *rt,
+                    int dtype, const NetSlab &s, bool with_sel, cudaStream_t st) {
+    const NetLaunch L{g.pre[NK_RESIZE], g.pairs, g.n, g.slab};
+    const unsigned B = ctas_of(g.total[NK_RESIZE]);
+    const dim3 blk(32, 8);
+    SelState *sel = with_sel ? s.sel : nullptr;
+    count_launch();
+    switch (dtype) {
+    case SV_U8: k_b_resize_pair<uint8_t><<<B, blk, 0, st>>>(L, lt, rt, s.lw, s.rw, s.gh, sel, s.hist); break;
+    case SV_F32: k_b_resize_pair<float><<<B, blk, 0, st>>>(L, lt, rt, s.lw, s.rw, s.gh, sel, s.hist); break;
+    case SV_F64: k_b_resize_pair<double><<<B, blk, 0, st>>>(L, lt, rt, s.lw, s.rw, s.gh, sel, s.hist); break;
+    default: set_error("unknown dtype %d", dtype); return SV_ERR_PARAM;
+    }
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_b_work_outputs(const NetLaunch &L, long long total, const NetSlab &s, bool with_sel,
+                          cudaStream_t st) {
+    count_launch();
+    k_b_work_outputs<<<ctas_of(total), dim3(32, 8), 0, st>>>(
+        L, s.d2, nullptr, s.full, with_sel ? s.sel : nullptr, with_sel ? s.hist : nullptr);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
 
 }  // namespace sv

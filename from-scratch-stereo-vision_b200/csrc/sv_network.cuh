@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "sv_b200.h"
+
 namespace sv {
 
 struct Taps {
@@ -93,6 +95,46 @@ int launch_avgpool2_f64(const double *img, int C, int H, int W, double *out, cud
 int launch_forward(const NetView &n, const float *left, const float *right, int H, int W,
                    const float *gh, const float *gf, float *d0, float *d1, float *d2,
                    const FwdBufs &b, int precision, cudaStream_t st);
+
+// ------------------------------------------------ batched predict_auto
+// (sv_netbatch.cuh describes the scheme.)  Kernels of one stage, in launch
+// order; a stage's CTA prefix tables are indexed by these.
+enum NetKind { NK_RESIZE, NK_C1, NK_C2, NK_V1, NK_V2, NK_SA, NK_R0, NK_R0F, NK_R1, NK_R1F,
+               NK_COUNT };
+struct NetPair;
+struct NetLaunch;
+
+// One stage (the probe, or a pass) of a batched predict_auto.
+struct NetStageLaunch {
+    const long long *pre[NK_COUNT];   // device CTA prefixes, [n+1] each
+    long long total[NK_COUNT];        // CTAs of each launch
+    const NetPair *pairs;
+    int n;
+    long long slab;
+};
+
+// Pair 0's network scratch (the other pairs' sit `slab` bytes apart).
+struct NetSlab {
+    float *lw, *rw, *gh, *d0, *d1, *d2;
+    FwdBufs f;
+    double *full;
+    SelState *sel;
+    unsigned *hist;
+};
+
+int net_stage_ctas(const NetView &n, int Hm, int Wm, long long *ctas);
+const NetView &net_view(const sv_net *net);
+int launch_b_resize(const NetStageLaunch &g, const void *const *lt, const void *const *rt,
+                    int dtype, const NetSlab &s, bool with_sel, cudaStream_t st);
+int launch_b_forward(const NetView &n, const NetStageLaunch &g, const NetSlab &s,
+                     cudaStream_t st);
+int launch_b_work_outputs(const NetLaunch &L, long long total, const NetSlab &s, bool with_sel,
+                          cudaStream_t st);
+// The probe's select (one CTA per pair) and passes 1..5 of the
+// full-resolution select after the pass's work outputs ran pass 0.
+int launch_b_sel_probe(const NetLaunch &L, const NetSlab &s, cudaStream_t st);
+int launch_b_sel_rest(const NetLaunch &L, long long total, const NetSlab &s, cudaStream_t st);
+long long select_ctas(long n);
 
 // Passes 1.. of a select whose pass 0 a network stage ran (SelFuse), n >
 // select_small_cap().

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace sv {
 
 // Scanline work table of the SGM kernels: segment i covers the scanlines of
@@ -104,6 +106,24 @@ __device__ __forceinline__ int batch_find(const long long *prefix, int n, long l
     }
     return lo;
 }
+
+// A batch's layout in its workspace: per-pair slices and the host copies of
+// the device tables (sv_batch_api.cu).
+struct BatchPlan {
+    std::vector<BatchPair> pairs;
+    std::vector<long long> px_blk, row_blk, tile_blk, seg_start;
+    std::vector<int> seg_pair, seg_vd;
+    long long px_blocks = 0, rows = 0, tiles = 0, tasks = 0;
+    int maxW = 1;
+    size_t off_tables = 0, off_pairs = 0, off_px = 0, off_row = 0, off_tile = 0, off_seg = 0,
+           off_segp = 0, off_segvd = 0, total = 0;
+};
+// Sizes and offsets; with ws != nullptr also fills the per-pair pointers.
+int plan_batch(const sv_pair_desc *in, int n, const RefineCfg &c, int px_per_block, char *ws,
+               BatchPlan *pl);
+int upload_batch(const BatchPlan &pl, int n, char *ws, cudaStream_t st);
+BatchTables batch_tables(const BatchPlan &pl, int n, char *ws, const RefineCfg &c, int dtype,
+                         double tol, const sv_batch_config &cfg);
 
 int launch_batch_refine(const BatchTables &t, long long px_blocks, long long rows,
                         long long tiles, long long tasks, bool l16, int sgm_threads,

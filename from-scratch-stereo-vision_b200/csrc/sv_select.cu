@@ -16,6 +16,7 @@
 // keys instead (k_sel_small_f32).
 
 #include "sv_common.cuh"
+#include "sv_netbatch.cuh"
 #include "sv_network.cuh"
 #include "sv_select.cuh"
 
@@ -27,16 +28,16 @@ __global__ void k_sel_init(SelState *s, long long rank, unsigned *hist) {
     sel_init_block(s, rank, hist);
 }
 
-__global__ void __launch_bounds__(1024)
-    k_sel_pass(const double *__restrict__ x, long n, int pass, SelState *__restrict__ s,
-               unsigned *__restrict__ ghist) {
+__device__ __forceinline__ void sel_pass_body(long blk, long nblk, const double *__restrict__ x,
+                                              long n, int pass, SelState *__restrict__ s,
+                                              unsigned *__restrict__ ghist) {
     __shared__ unsigned hist[SEL_NB];
     const int t = threadIdx.x, nt = blockDim.x;
     const unsigned long long pre = pass ? s->prefix : 0ull;
     for (int i = t; i < SEL_NB; i += nt) hist[i] = 0u;
     __syncthreads();
-    const long stride = (long)gridDim.x * nt;
-    for (long b0 = blockIdx.x * (long)nt; b0 < n; b0 += SEL_LB * stride) {
+    const long stride = nblk * nt;
+    for (long b0 = blk * (long)nt; b0 < n; b0 += SEL_LB * stride) {
         double v[SEL_LB];                  // this thread's loads, all in flight at once
 #pragma unroll
         for (int u = 0; u < SEL_LB; ++u) {
@@ -50,7 +51,25 @@ __global__ void __launch_bounds__(1024)
         }
     }
     __syncthreads();
-    sel_pass_finish(pass, s, ghist, hist);
+    sel_pass_finish(pass, s, ghist, hist, (unsigned)nblk);
+}
+
+__global__ void __launch_bounds__(1024)
+    k_sel_pass(const double *__restrict__ x, long n, int pass, SelState *__restrict__ s,
+               unsigned *__restrict__ ghist) {
+    sel_pass_body(blockIdx.x, gridDim.x, x, n, pass, s, ghist);
+}
+
+// Batched: pass `pass` of every active pair's full-resolution select (each
+// pair's CTAs cover its W x H map).
+__global__ void __launch_bounds__(1024)
+    k_b_sel_pass(NetLaunch L, const double *x, int pass, SelState *s, unsigned *ghist) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    sel_pass_body(c, L.pre[p + 1] - L.pre[p], net_slab(x, L, p), (long)P.W * P.H, pass,
+                  net_slab(s, L, p), net_slab(ghist, L, p));
 }
 
 // After pass 1 the 22 top key bits are fixed and usually only a few hundred
@@ -137,9 +156,10 @@ __device__ void sel_passes_cta(const unsigned long long *keys, const double *__r
     rank = *s_rank;
 }
 
-__global__ void __launch_bounds__(1024)
-    k_sel_compact(const double *__restrict__ x, long n, SelState *__restrict__ s,
-                  unsigned long long *__restrict__ cand, double *mirror) {
+__device__ __forceinline__ void sel_compact_body(long blk, long nblk, const double *__restrict__ x,
+                                                 long n, SelState *__restrict__ s,
+                                                 unsigned long long *__restrict__ cand,
+                                                 double *mirror) {
     extern __shared__ __align__(16) unsigned long long keys[];   // SEL_CAND_CAP
     __shared__ unsigned hist[SEL_NB];
     __shared__ unsigned wsum[32];
@@ -150,8 +170,8 @@ __global__ void __launch_bounds__(1024)
     const int t = threadIdx.x, lane = t & 31, nt = blockDim.x;
     const int top = sel_shift(1);                    // bits above pass 2's digit are fixed
     const unsigned long long pre = s->prefix;
-    const long stride = (long)gridDim.x * nt;
-    for (long b0 = blockIdx.x * (long)nt; b0 < n; b0 += SEL_LB * stride) {
+    const long stride = nblk * nt;
+    for (long b0 = blk * (long)nt; b0 < n; b0 += SEL_LB * stride) {
         double v[SEL_LB];
 #pragma unroll
         for (int u = 0; u < SEL_LB; ++u) {
@@ -179,7 +199,7 @@ __global__ void __launch_bounds__(1024)
     }
     __threadfence();
     __syncthreads();
-    if (t == 0) last = atomicAdd(&s->cdone, 1u) == gridDim.x - 1;
+    if (t == 0) last = atomicAdd(&s->cdone, 1u) == (unsigned)nblk - 1;
     __syncthreads();
     if (!last) return;
     __threadfence();
@@ -200,6 +220,27 @@ __global__ void __launch_bounds__(1024)
         s->value = sel_unkey(prefix);
         if (mirror) *reinterpret_cast<volatile double *>(mirror) = s->value;
     }
+}
+
+
+__global__ void __launch_bounds__(1024)
+    k_sel_compact(const double *__restrict__ x, long n, SelState *__restrict__ s,
+                  unsigned long long *__restrict__ cand, double *mirror) {
+    sel_compact_body(blockIdx.x, gridDim.x, x, n, s, cand, mirror);
+}
+
+// Batched: the compaction and passes 2..5 of every active pair's select.
+// The candidates follow the pair's two global histograms.
+__global__ void __launch_bounds__(1024)
+    k_b_sel_compact(NetLaunch L, const double *x, SelState *s, unsigned *hist) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    unsigned *h = net_slab(hist, L, p);
+    sel_compact_body(c, L.pre[p + 1] - L.pre[p], net_slab(x, L, p), (long)P.W * P.H,
+                     net_slab(s, L, p), reinterpret_cast<unsigned long long *>(h + 2 * SEL_NB),
+                     nullptr);
 }
 
 // Small inputs (the probe's few thousand values): one CTA keeps every key in
@@ -306,6 +347,72 @@ __global__ void __launch_bounds__(SEL32_T)
     }
 }
 
+// Batched probe select: one CTA per pair over the probe's FP32 map (the
+// pass's Ww x Hw values), the same four 8-bit passes over 32-bit keys as
+// k_sel_small_f32 but with the keys read from global memory each pass, so a
+// tall pair's probe (more than SEL_SMALL_CAP values) needs no other path.
+__global__ void __launch_bounds__(SEL32_T)
+    k_b_sel_probe(NetLaunch L, const float *x0, SelState *s0) {
+    __shared__ unsigned hist[SEL32_T];
+    __shared__ unsigned wsum[SEL32_T / 32];
+    __shared__ unsigned s_prefix, s_rank;
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    const float *__restrict__ x = net_slab(x0, L, p);
+    SelState *s = net_slab(s0, L, p);
+    const int n = P.Ww * P.Hw;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    if (t == 0) {
+        s_prefix = 0u;
+        s_rank = (unsigned)(long long)__dmul_rn((double)n, 0.95);
+    }
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 24 - 8 * pass;
+        hist[t] = 0u;
+        __syncthreads();
+        const unsigned pre = s_prefix;
+        for (int i0 = 0; i0 < n; i0 += SEL32_T) {
+            const int i = i0 + t;
+            unsigned digit = 0xffffffffu;
+            if (i < n) {
+                const unsigned k = sel_key32(__ldg(x + i));
+                if (pass == 0 || (k >> (shift + 8)) == (pre >> (shift + 8)))
+                    digit = (k >> shift) & 255u;
+            }
+            const unsigned same = __match_any_sync(kFull, digit);
+            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
+                atomicAdd(&hist[digit], __popc(same));
+        }
+        __syncthreads();
+        const unsigned cnt = hist[t];
+        unsigned incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[wid] = incl;
+        __syncthreads();
+        unsigned excl = incl - cnt;
+        for (int w = 0; w < wid; ++w) excl += wsum[w];
+        const unsigned r = s_rank;
+        __syncthreads();
+        if (r >= excl && r < excl + cnt) {
+            s_prefix = pre | ((unsigned)t << shift);
+            s_rank = r - excl;
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        const double v = (double)sel_unkey32(s_prefix);
+        s->prefix = sel_key(v);
+        s->rank = s_rank;
+        s->value = v;
+    }
+}
+
 // The select kernels' dynamic shared-memory limits, once per device.
 static int select_setup() {
     int dev = 0;
@@ -319,6 +426,9 @@ static int select_setup() {
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(SEL_SMALL_CAP * sizeof(unsigned))));
         SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_compact,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(SEL_CAND_CAP * sizeof(unsigned long long))));
+        SV_CUDA_TRY(cudaFuncSetAttribute(k_b_sel_compact,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(SEL_CAND_CAP * sizeof(unsigned long long))));
         if (dev < 64) ready[dev] = true;
@@ -379,6 +489,31 @@ int launch_select_after_pass0(const double *x, long n, SelState *state, unsigned
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
+
+int launch_b_sel_probe(const NetLaunch &L, const NetSlab &s, cudaStream_t st) {
+    count_launch();
+    k_b_sel_probe<<<(unsigned)L.n, SEL32_T, 0, st>>>(L, s.d2, s.sel);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_b_sel_rest(const NetLaunch &L, long long total, const NetSlab &s, cudaStream_t st) {
+    {
+        const int rc = select_setup();
+        if (rc) return rc;
+    }
+    const unsigned B = (unsigned)(total > 0 ? total : 1);
+    count_launch();
+    k_b_sel_pass<<<B, 1024, 0, st>>>(L, s.full, 1, s.sel, s.hist + SEL_NB);
+    count_launch();
+    k_b_sel_compact<<<B, 1024, (size_t)SEL_CAND_CAP * sizeof(unsigned long long), st>>>(
+        L, s.full, s.sel, s.hist);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+// CTAs of a pair's full-resolution select passes (the single-pair grid).
+long long select_ctas(long n) { return grid_for(n, 1024 * 4, 148); }
 
 long select_small_cap() { return SEL_SMALL_CAP; }
 

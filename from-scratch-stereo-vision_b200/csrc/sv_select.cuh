@@ -71,10 +71,11 @@ __device__ __forceinline__ void sel_count(unsigned *hist, unsigned long long k, 
 
 // The end of pass `pass`, called by every thread of every CTA once its
 // counts are in the shared `hist`: the non-zero bins go into ghist, and the
-// last CTA to finish (counted in s->done[pass]) finds the bin holding
-// s->rank and extends the prefix.  Block sizes that divide SEL_NB, >= 64.
+// last of the nblk CTAs working on this select to finish (counted in
+// s->done[pass]) finds the bin holding s->rank and extends the prefix.
+// Block sizes that divide SEL_NB, >= 64.
 __device__ __forceinline__ void sel_pass_finish(int pass, SelState *s, unsigned *ghist,
-                                                const unsigned *hist) {
+                                                const unsigned *hist, unsigned nblk) {
     __shared__ unsigned wsum[32];
     __shared__ int owner;
     __shared__ unsigned long long owner_excl;
@@ -85,10 +86,7 @@ __device__ __forceinline__ void sel_pass_finish(int pass, SelState *s, unsigned 
         if (hist[i]) atomicAdd(&ghist[i], hist[i]);
     __threadfence();
     __syncthreads();
-    if (t == 0) {
-        const unsigned nblk = gridDim.x * gridDim.y * gridDim.z;
-        last = atomicAdd(&s->done[pass], 1u) == nblk - 1;
-    }
+    if (t == 0) last = atomicAdd(&s->done[pass], 1u) == nblk - 1;
     __syncthreads();
     if (!last) return;
     __threadfence();

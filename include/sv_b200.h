@@ -276,6 +276,41 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right,
                         double *disp_full, double *disp_work, int *Ww, int *Hw,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* predict_auto followed by lr_refine for many pairs of uneven sizes
+ * (predict_auto, stereonet.py:3872-3929; lr_refine, 5343-5391), with the
+ * work-width decisions taken on the device: the probe, every pass and the
+ * peaks between them, and the batched refinement behind them, are one fixed
+ * launch sequence, recorded into a CUDA graph by the first run on a
+ * capturable stream and replayed afterwards.  Each pair's network
+ * disparity, work-width trace and refined output are those of predict_auto
+ * and lr_refine run on that pair alone.  FP32 network.
+ *  - create: plans the batch for the pairs' sizes (W[i], H[i]) and
+ *    predict_auto's / lr_refine's parameters; allocates host memory only.
+ *  - bind: the pairs' device buffers (left, right, out, status of each
+ *    sv_pair_desc; disp0 is ignored: the network writes it) and a workspace
+ *    of sv_netbatch_workspace_size bytes, 256-aligned; uploads the tables
+ *    and synchronises the stream.
+ *  - run: enqueues the whole batch (no host synchronisation); predict runs
+ *    the network part only.
+ *  - disparity: device pointer of pair i's network disparity (FP64, W x H).
+ *  - trace: each pair's chosen widths (0-terminated, trace_len per pair)
+ *    and final work size; synchronises the stream. */
+typedef struct sv_netbatch sv_netbatch;
+int sv_netbatch_create(const sv_net *net, const int *W, const int *H, int n, int dtype,
+                       double target_peak, int probe_width, int max_width, int passes,
+                       int precision, double tol, const sv_refine_params *p,
+                       sv_netbatch **out);
+size_t sv_netbatch_workspace_size(const sv_netbatch *nb);
+int sv_netbatch_bind(sv_netbatch *nb, const sv_pair_desc *pairs, void *workspace,
+                     size_t workspace_bytes, void *stream);
+int sv_netbatch_run(sv_netbatch *nb, void *stream);
+int sv_netbatch_predict(sv_netbatch *nb, void *stream);
+int sv_netbatch_disparity(const sv_netbatch *nb, int i, const double **disp_full);
+int sv_netbatch_trace(const sv_netbatch *nb, int *work_trace, int trace_len, int *work_size,
+                      void *stream);
+int sv_netbatch_data_status(const sv_netbatch *nb, void *stream);
+void sv_netbatch_destroy(sv_netbatch *nb);
+
 /* predict_consistent, stereonet.py:5048-5076 (with mirror_h 4974-4983,
  * lr_consistency 4986-5009, fill_invalid 5012-5045): the network on the pair
  * (predict_auto when work_width <= 0, else predict_at_scale) and on the

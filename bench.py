@@ -56,7 +56,7 @@ def parse():
                              "train"])
     ap.add_argument("--pairs", type=int, default=256, help="pairs of the batched workload")
     ap.add_argument("--batch", type=int, default=64, help="crops per step of the train workload")
-    ap.add_argument("--cpu-leg", default=None, choices=["pair", "refpy"],
+    ap.add_argument("--cpu-leg", default=None, choices=["pair", "refpy", "batch16"],
                     help=argparse.SUPPRESS)          # child process: one CPU baseline leg
     ap.add_argument("--clock-sampler", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--pci", default=None, help=argparse.SUPPRESS)
@@ -165,6 +165,23 @@ def cpu_leg_main(args):
         net = pkg.weights.load_model()
         n, el = cpu_port_run(pair, net, args.cpu_seconds, args.threads or (os.cpu_count() or 1))
         print(json.dumps({"pairs": n, "seconds": el}))
+        return
+    if args.cpu_leg == "batch16":
+        net = pkg.weights.load_model()
+        orc = __graft_entry__.load_oracle()
+        orc.set_threads(args.threads or (os.cpu_count() or 1))
+        pairs = pkg.synth.config_batched(n=16, seed=3)
+        t0 = time.perf_counter()
+        done, mpix = 0, 0.0
+        for p in pairs:
+            L, R = p.gray("left").ravel(), p.gray("right").ravel()
+            df, _, _, _ = orc.predict_auto(net, L, R, p.W, p.H)
+            orc.lr_refine(L, R, df, p.W, p.H, tol=TOL, **PARAMS)
+            done += 1
+            mpix += p.W * p.H / 1e6
+            if time.perf_counter() - t0 >= args.cpu_seconds and done >= 4:
+                break
+        print(json.dumps({"pairs": done, "mpix": mpix, "seconds": time.perf_counter() - t0}))
         return
     # refpy: exec the reference (as its own test harness does) and time lr_refine
     import platform
@@ -531,11 +548,12 @@ def run_reference(args, rank, world):
 
 
 def run_batched(args, rank, world, local):
-    """The batched refinement workload: 256 pairs of uneven sizes
-    (200x150..1400x1100, max disparity 10-200 px), sharded over ranks by
-    pixel count.  Network disparities are computed once per pair before
-    timing (predict_auto); a step is one batched lr_refine of every pair,
-    from device-resident images and disparities."""
+    """The batched workload: 256 pairs of uneven sizes (200x150..1400x1100,
+    max disparity 10-200 px), sharded over ranks by pixel count.  A step is
+    the whole path for every pair -- predict_auto with its work-width
+    decisions on the device, then lr_refine -- replayed from one CUDA graph
+    (batch.NetBatch), images already in HBM; e2e adds the H2D of every
+    image and the D2H of every refined disparity and status."""
     import torch
     import __graft_entry__
     pkg = __graft_entry__.load_package()
@@ -550,71 +568,107 @@ def run_batched(args, rank, world, local):
     pairs = pkg.synth.config_batched(n=args.pairs, seed=3)
     mine = pkg.shard.shard([p.W * p.H for p in pairs], rank, world)
     pairs = [pairs[i] for i in mine]
-    b = pkg.batch.BatchRefiner([(p.W, p.H) for p in pairs], **PARAMS, tol=TOL)
-    t_net = 0.0
-    for i, p in enumerate(pairs):
-        b.left[i].copy_(torch.from_numpy(p.left.ravel()))
-        b.right[i].copy_(torch.from_numpy(p.right.ravel()))
-        tn0 = time.perf_counter()
-        df, _, _, _ = pkg.network.predict_auto(net, b.left[i], b.right[i], p.W, p.H,
-                                               verbose=False)
-        torch.cuda.synchronize()
-        t_net += time.perf_counter() - tn0
-        b.disp0[i].copy_(df)
-    N = b.pixels
-    K = 2 * PARAMS["R"] + 1
+    nb = pkg.batch.NetBatch([(p.W, p.H) for p in pairs], net, **PARAMS, tol=TOL)
+    hl = [torch.from_numpy(p.left.ravel()).pin_memory() for p in pairs]
+    hr = [torch.from_numpy(p.right.ravel()).pin_memory() for p in pairs]
+    ho = [torch.empty(p.W * p.H, dtype=torch.float64).pin_memory() for p in pairs]
+    hs = [torch.empty(p.W * p.H, dtype=torch.uint8).pin_memory() for p in pairs]
+    for i in range(len(pairs)):
+        nb.left[i].copy_(hl[i])
+        nb.right[i].copy_(hr[i])
+    N = nb.pixels
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    for _ in range(args.warmup):
-        b.run()
-    b.data_status()
-    # scheduling picked by timing this batch (untimed; results do not change)
-    tune = b.autotune(reps=3, use_cache=False)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            nb.run()
+        nb.data_status()
     torch.cuda.synchronize()
-    t0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    t1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+
+    def timed(fn, steps):
+        t0 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        t1 = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for i in range(steps):
+                flush.zero_()
+                t0[i].record()
+                fn()
+                t1[i].record()
+        torch.cuda.synchronize()
+        return [t0[i].elapsed_time(t1[i]) for i in range(steps)]
+
     lib = pkg._lib.load()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     l0 = lib.sv_launch_count()
     with ClockSampler(local) as clk:
-        for i in range(args.steps):
-            flush.zero_()
-            t0[i].record()
-            b.run()
-            t1[i].record()
-        torch.cuda.synchronize()
+        times = timed(nb.run, args.steps)
     launches = lib.sv_launch_count() - l0
-    ms = sum(t0[i].elapsed_time(t1[i]) for i in range(args.steps))
-    ms = pkg.shard.max_over_ranks(ms, device="cuda")
+    ms = pkg.shard.max_over_ranks(sum(times), device="cuda")
     value = world * N * args.steps / (ms / 1e3) / 1e6
+    # the network alone (same graph without the refinement), for the stage split
+    pred_ms = statistics.median(timed(nb.predict, max(3, args.steps // 2)))
+
+    def e2e_step():
+        for i in range(len(pairs)):
+            nb.left[i].copy_(hl[i], non_blocking=True)
+            nb.right[i].copy_(hr[i], non_blocking=True)
+        nb.run()
+        for i in range(len(pairs)):
+            ho[i].copy_(nb.out[i], non_blocking=True)
+            hs[i].copy_(nb.status[i], non_blocking=True)
+
+    ems = pkg.shard.max_over_ranks(sum(timed(e2e_step, args.steps)), device="cuda")
+    evalue = world * N * args.steps / (ems / 1e3) / 1e6
+    traces = nb.traces()
     if rank != 0:
         if dist:
             dist.barrier()
             dist.destroy_process_group()
         return None
     peak, peak_kind = hbm_peak()
-    alg = 48 * K * N * 2
-    achieved = alg * args.steps / (ms / 1e3) / 1e9
+    K = 2 * PARAMS["R"] + 1
+    step_ms = ms / args.steps
+    ref_ms = step_ms - pred_ms
+    alg = 2350 * N                       # whole refinement, both views + LR, per left pixel
+    achieved = alg / (ref_ms / 1e3) / 1e9
+    cpu = None
+    if world == 1:
+        threads = os.cpu_count() or 1
+        d = _child(["--cpu-leg", "batch16", "--cpu-seconds", str(args.cpu_seconds),
+                    "--threads", str(threads)], timeout=3600)
+        cpu = {"value": round(d["mpix"] / d["seconds"], 6), "unit": UNIT, "cores": threads,
+               "kind": "port",
+               "sample": "the first %d pairs of the same seeded batch (%.2f Mpix) through the "
+                         "FP64 C port of predict_auto + lr_refine, %.1f s, OpenMP over %d threads "
+                         "(child process)" % (d["pairs"], d["mpix"], d["seconds"], threads)}
+    passes = [len(t[0]) for t in traces]
     res = {
-        "metric": "refined Mpix/s per B200, batched refinement (bit-exact)", "value": round(value, 3),
-        "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u8/u64/int32 integer refinement, f64 subpixel+LR",
-        "data": "synthetic (seeded generator)",
+        "metric": "refined Mpix/s per B200, batched predict_auto + lr_refine (bit-exact)",
+        "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8/u64/int32 integer refinement, f64 subpixel+LR, f32 network",
+        "data": "synthetic (seeded generator; reference weights stereonet_weights.txt)",
         "config": {"workload": "%d pairs of uneven sizes 200x150..1400x1100, max disparity "
-                               "10-200 px: batched lr_refine (R=10, 9x7 census, P1=12, P2=150, "
-                               "tol=2) of network disparities" % args.pairs,
-                   "pixels_per_step_per_gpu": N, "pairs_per_gpu": len(pairs),
-                   "network_s_per_pair_untimed": round(t_net / len(pairs), 5),
-                   "schedule": dict(tune["config"], autotuned=True,
-                                    default_ms=round(tune["default_ms"], 4),
-                                    tuned_ms=round(tune["ms"], 4)),
-                   "l2": "flushed before every step (256 MB write, untimed)"},
-        "roofline": {"kernel": "whole batched refinement (7 launches)", "bound": "hbm",
+                               "10-200 px: predict_auto + lr_refine (R=10, 9x7 census, P1=12, "
+                               "P2=150, tol=2), one CUDA graph per step" % args.pairs,
+                   "pairs_per_step_per_gpu": len(pairs), "parallelism": "replicas x%d" % world},
+        "l2": "flushed before every step (256 MB write, untimed); the batch is larger than L2",
+        "stages_ms": {"predict_auto": round(pred_ms, 3), "lr_refine": round(ref_ms, 3)},
+        "passes_per_pair": {str(k): passes.count(k) for k in sorted(set(passes))},
+        "pixels_per_step_per_gpu": N,
+        "roofline": {"kernel": "batched lr_refine (census, band costs, 8-path SGM, WTA, LR: 7 "
+                               "launches)", "bound": "hbm",
+                     "basis": "algorithmic bytes, 2350 B per left pixel at K = %d" % K,
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4),
-                     "peak_source": peak_kind, "algorithmic_bytes_per_step": alg},
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "algorithmic_bytes_per_step": alg, "traffic": None},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(evalue, 3), "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(2 * p.W * p.H for p in pairs)),
+                "d2h_bytes_per_step": int(sum(9 * p.W * p.H for p in pairs))},
         "gpu_launches": int(launches), "clocks": clk.summary(),
     }
     if dist:

@@ -417,11 +417,162 @@ __global__ void __launch_bounds__(kTcM) k_conv2d_tc(TcConv a, int PH, int PW) {
                      ::"r"(tmem), "r"(kTmemCols));
 }
 
+// Stride-1 2-D convolutions with at most 16 input channels, without an
+// im2col operand.  A tile is 128 consecutive output pixels of one row; the
+// three input rows its taps read (rows oy - pad + ky * dil) are staged in
+// shared memory as BF16 in the UMMA K-major layout directly: two planes of 8
+// channels each, every pixel 16 bytes, so 8 consecutive pixels form one
+// 128-byte core matrix.  The A operand of tap (ky, kx) is then the same
+// patch read from pixel ky * PWp + kx * dil on (start address shifted by a
+// multiple of 16 bytes; LBO = one channel plane, SBO = 128 bytes), and a
+// tile is 9 MMAs of K = 16 -- one per tap -- accumulating in tensor memory.
+// Operand B is re-ordered on the way into shared memory from the packed
+// channel-major K (k = c * 9 + t) to one 16-channel block per tap
+// (k = t * 16 + c, zero for c >= IC).  The bounded wait and the epilogue
+// are those of k_conv2d_tc.
+constexpr int kTapW = 128;              // output pixels per tile
+constexpr int kTapMaxDil = 8;
+
+__device__ __forceinline__ int tc_b_off(int n, int k) {    // BF16 index in a packed operand B
+    return (((k >> 3) * 2 + (n >> 3)) * 128 + (n & 7) * 16 + (k & 7) * 2) >> 1;
+}
+
+__global__ void __launch_bounds__(kTcM) k_conv2d_tc_tap(TcConv a, int PWp) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int failed;
+    unsigned char *sB = smem;                                    // 9 taps x 16 x 16 BF16
+    unsigned char *patch = smem + 9 * 512;                       // [2][3][PWp] x 16 bytes
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    {
+        uint16_t *wd = reinterpret_cast<uint16_t *>(sB);
+        for (int i = tid; i < 9 * 256; i += kTcM) {
+            const int t = i >> 8, n = (i >> 4) & 15, c = i & 15;
+            uint16_t v = 0;
+            if (c < a.IC) v = a.wB[tc_b_off(n, c * 9 + t)];
+            wd[tc_b_off(n, t * 16 + c)] = v;
+        }
+    }
+    if (tid == 0) {
+        mbar_init(&mbar, 1);
+        failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_slot;
+
+    const int tiles_x = (a.OW + kTapW - 1) / kTapW;
+    const long tiles_img = (long)tiles_x * a.OH;
+    const int nb = a.nb > 0 ? a.nb : 1;
+    const long tiles = tiles_img * a.nimg * nb;
+    const long plane = (long)a.H * a.W, M = (long)a.OH * a.OW;
+    const uint32_t lbo = 3u * (uint32_t)PWp * 16u;               // one 8-channel plane
+    unsigned phase = 0;
+    for (long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int item = (int)(tile / tiles_img);
+        const int img = item / nb, bi = item - img * nb;
+        const int t2 = (int)(tile - item * tiles_img);
+        const int oy = t2 / tiles_x, ox0 = (t2 - oy * tiles_x) * kTapW;
+        const float *x0 = (img ? a.x[1] : a.x[0]) + bi * a.xs;
+        // ---- stage rows oy - pad + ky * dil: consecutive threads take
+        // consecutive pixels, each 8 channels packed into one 16-byte store
+        for (int e = tid; e < 2 * 3 * PWp; e += kTcM) {
+            const int r = e / PWp, px = e - r * PWp;
+            const int ch = r / 3, ky = r - ch * 3;
+            const int iy = oy - a.pad + ky * a.dil, ix = ox0 - a.pad + px;
+            const bool ok = iy >= 0 && iy < a.H && ix >= 0 && ix < a.W;
+            const float *src = x0 + (long)iy * a.W + ix;
+            uint32_t q[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c0 = ch * 8 + 2 * j;
+                const float f0 = ok && c0 < a.IC ? __ldg(src + c0 * plane) : 0.f;
+                const float f1 = ok && c0 + 1 < a.IC ? __ldg(src + (c0 + 1) * plane) : 0.f;
+                const __nv_bfloat162 h2 = __floats2bfloat162_rn(f0, f1);
+                q[j] = *reinterpret_cast<const uint32_t *>(&h2);
+            }
+            *reinterpret_cast<uint4 *>(patch + (size_t)(r * PWp + px) * 16) =
+                make_uint4(q[0], q[1], q[2], q[3]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        if (tid == 0 && !failed) {
+            const uint32_t p0 = smem_u32(patch), b0 = smem_u32(sB);
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                const int ky = t / 3, kx = t - (t / 3) * 3;
+                const uint64_t da =
+                    umma_desc(p0 + (uint32_t)(ky * PWp + kx * a.dil) * 16u, lbo, 128);
+                const uint64_t db = umma_desc(b0 + t * 512, (kTcN / 8) * 128, 128);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(kIdescBf16), "r"(t));
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                ::"r"(smem_u32(&mbar))
+                : "memory");
+        }
+        if (!failed && !mbar_wait(&mbar, phase)) {
+            failed = 1;
+            flag_error(a.err, SV_ERR_TIMEOUT);
+        }
+        phase ^= 1u;
+        __syncthreads();
+        if (failed) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int ox = ox0 + tid;
+        if (ox < a.OW) {
+            const long mi = (long)oy * a.OW + ox;
+            float *y = (img ? a.y[1] : a.y[0]) + bi * a.ys;
+            const float *aux = a.aux ? a.aux + bi * a.ys : nullptr;
+#pragma unroll
+            for (int n = 0; n < kTcN; ++n) {
+                if (n < a.OC) {
+                    float v = __uint_as_float(r[n]);
+                    if (a.bias) v += __ldg(a.bias + n);
+                    if (a.act == 1) v = v > 0.f ? v : v * 0.2f;
+                    if (a.act == 2) v = __ldg(aux + (long)n * M + mi) > 0.f ? v : v * 0.2f;
+                    y[(long)n * M + mi] = v;
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(kTmemCols));
+}
+
 // Per-device launch set-up, done once: the SM count and each kernel's
 // dynamic shared-memory limit (raised to kTcSmemMax; every launch checks
 // its own size against it).  Launches stay free of attribute calls.
 constexpr size_t kTcSmemMax = 200 * 1024;
-enum { kKConv = 0, kKConv2d = 1, kKWgrad = 2, kKCount = 3 };
+enum { kKConv = 0, kKConv2d = 1, kKWgrad = 2, kKConv2dTap = 3, kKCount = 4 };
 
 static int tc_setup(int which, const void *fn, int *sms) {
     static std::mutex mu;
@@ -452,6 +603,23 @@ static long tc_ctas_per_sm(size_t smem) {
 }
 
 static int launch_conv2d_tc(const TcConv &a, cudaStream_t st) {
+    if (a.stride == 1 && a.IC <= 16 && a.dil <= kTapMaxDil && a.pad >= 0 &&
+        a.K == a.IC * 9) {
+        const int PWp = kTapW + 2 * a.dil;
+        const size_t smem = 9 * 512 + (size_t)2 * 3 * PWp * 16;
+        const long tiles = (long)((a.OW + kTapW - 1) / kTapW) * a.OH * a.nimg *
+                           (a.nb > 0 ? a.nb : 1);
+        if (tiles == 0) return SV_OK;
+        int sms = 148;
+        const int rc = tc_setup(kKConv2dTap, (const void *)k_conv2d_tc_tap, &sms);
+        if (rc) return rc;
+        const long cap = (long)sms * 8;               // 8 CTAs (32 TMEM columns each) per SM
+        const unsigned blocks = (unsigned)(tiles < cap ? tiles : cap);
+        count_launch();
+        k_conv2d_tc_tap<<<blocks, kTcM, smem, st>>>(a, PWp);
+        SV_LAUNCH_CHECK();
+        return SV_OK;
+    }
     const int PH = (kT2H - 1) * a.stride + 2 * a.dil + 1;
     const int PW = (kT2W - 1) * a.stride + 2 * a.dil + 1;
     const size_t patch = ((size_t)a.IC * PH * PW * 2 + 15) / 16 * 16;

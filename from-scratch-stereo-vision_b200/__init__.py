@@ -31,6 +31,6 @@ def __getattr__(name):
     # heavy modules (torch) load on first use
     import importlib
     if name in ("refine", "network", "pipeline", "shim", "shard", "batch", "band", "post",
-                "image", "train"):
+                "image", "train", "band_train"):
         return importlib.import_module("." + name, __name__)
     raise AttributeError(name)

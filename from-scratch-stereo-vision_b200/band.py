@@ -4,9 +4,11 @@ The reference refines the network disparity inside a fixed +-R band
 (lr_refine, stereonet.py:5343-5391 with refine_disparity's R=10).  Where the
 network is more than R px off -- thin foreground structures, boundaries --
 the true disparity is outside the band and cannot be recovered.  The band
-net (4 convolutions, 5810 parameters, BF16 tensor-core kernels) reads six
+net (4 convolutions, 6098 parameters, BF16 tensor-core kernels) reads eight
 per-pixel features (network disparity, a wide 9-row census search, costs at
-the network disparity and inside its band, gray level) and predicts a shift
+the network disparity and inside its band, gray level, and how sure the
+network was: the spread and peak probability of its soft-argmin
+distribution, stereonet.py:858-885) and predicts a shift
 of the band centre with a Laplace scale b.  Where b <= b_thr the band moves
 to disparity + shift and narrows to ceil(rad_k * b) (at least rad_min); the
 fixed band stays everywhere else.  It is trained on the method's own
@@ -32,11 +34,12 @@ from .refine import _data_status, _device, _finite_disp, _image, _params, _ptr, 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "band_weights.npz")
 
-N_FEATURES = 6
+N_FEATURES = 8
 N_OUTPUTS = 2
-LAYERS = ((6, 16, 1), (16, 16, 2), (16, 16, 4), (16, 2, 1))    # (in, out, dilation)
+LAYERS = ((8, 16, 1), (16, 16, 2), (16, 16, 4), (16, 2, 1))    # (in, out, dilation)
 # band application defaults (a trained checkpoint may carry its own)
-APPLY = dict(b_thr=3.0, rad_k=3.0, rad_min=3, R=10, shift_max=160.0)
+APPLY = dict(b_thr=3.0, rad_k=3.0, rad_min=3, R=10, shift_max=160.0,
+             rule_tau=0.1)           # rule_tau: the no-net ablation's threshold (band_train)
 
 
 def param_count() -> int:
@@ -61,8 +64,10 @@ def _f32_dev(x, n, name):
     return _to_dev(x, n, torch.float32, name=name)
 
 
-def features(left, right, disp0, W, H, dmax=255):
-    """[6][H][W] FP32 device tensor (see the module docstring)."""
+def features(left, right, disp0, W, H, dmax=255, spread=None, pmax=None):
+    """[8][H][W] FP32 device tensor (see the module docstring); spread and
+    pmax are the network's confidence maps of the pass that gave disp0
+    (network.confidence); without them planes 6 and 7 are 0."""
     lib = _lib.load()
     N = W * H
     _finite_disp(disp0)
@@ -77,6 +82,12 @@ def features(left, right, disp0, W, H, dmax=255):
     _lib.check(lib.sv_band_features(_ptr(tl), _ptr(tr), code, _ptr(td), W, H, int(dmax),
                                     _ptr(feat), _ptr(ws), need, _stream()), "band_features")
     _data_status(ws, "band_features")
+    sp = torch.zeros(N, dtype=torch.float64, device=td.device) if spread is None else \
+        _to_dev(spread, N, torch.float64, name="spread")
+    pm = torch.full((N,), 0.5, dtype=torch.float64, device=td.device) if pmax is None else \
+        _to_dev(pmax, N, torch.float64, name="pmax")
+    _lib.check(lib.sv_band_conf_features(_ptr(sp), _ptr(pm), W, H, _ptr(feat), _stream()),
+               "band_conf_features")
     return feat
 
 
@@ -254,11 +265,15 @@ class LearnedBandRefiner:
         self.rws = _workspace(self.rneed)
         self.bws, self.bneed = band._workspace(1, W, H)
 
-    def run(self, left, right, code, disp0, out, status, stream):
+    def run(self, left, right, code, disp0, out, status, stream, spread, pmax):
+        """spread / pmax: the network's confidence maps of the pass that gave
+        disp0 (PairPipeline.confidence)."""
         W, H, m = self.W, self.H, self.band.meta
         _lib.check(self.lib.sv_band_features(_ptr(left), _ptr(right), code, _ptr(disp0), W, H,
                                              self.dmax, _ptr(self.feat), _ptr(self.fws),
                                              self.fneed, stream), "band_features")
+        _lib.check(self.lib.sv_band_conf_features(_ptr(spread), _ptr(pmax), W, H,
+                                                  _ptr(self.feat), stream), "band_conf_features")
         _lib.check(self.lib.sv_band_forward(self.band.handle, _ptr(self.feat), 1, W, H,
                                             _ptr(self.out), _ptr(self.bws), self.bneed, stream),
                    "band_forward")

@@ -135,7 +135,7 @@ class Labeller:
         self.full = FullRange(svb, W, H)
         self.W, self.H = W, H
         N = W * H
-        self.feat = torch.empty(6 * N, dtype=torch.float32, device="cuda")
+        self.feat = torch.empty(svb.band.N_FEATURES * N, dtype=torch.float32, device="cuda")
         self.fneed = self.full.lib.sv_band_features_workspace_size(W, H)
         self.fws = torch.empty(self.fneed, dtype=torch.uint8, device="cuda")
         self.t = torch.empty(N, dtype=torch.float32, device="cuda")
@@ -150,10 +150,13 @@ class Labeller:
             pp.left.copy_(torch.from_numpy(left.ravel()), non_blocking=False)
             pp.right.copy_(torch.from_numpy(right.ravel()), non_blocking=False)
         pp.predict()
+        sp, pm = pp.confidence()
         lab, st = self.full.run(pp.left, pp.right, pp.code, full_range_R(disp), s)
         svb._lib.check(lib.sv_band_features(vp(pp.left), vp(pp.right), pp.code, vp(pp.disp0),
                                             W, H, DMAX, vp(self.feat), vp(self.fws), self.fneed,
                                             s), "band_features")
+        svb._lib.check(lib.sv_band_conf_features(vp(sp), vp(pm), W, H, vp(self.feat), s),
+                       "band_conf_features")
         svb._lib.check(lib.sv_band_targets(vp(lab), vp(st), vp(pp.disp0), W * H, 160.0,
                                            vp(self.t), vp(self.m), s), "band_targets")
         return self.feat, self.t, self.m
@@ -164,7 +167,7 @@ def make_dataset(svb, pool, n, W=256, H=192, seed0=TRAIN_SEED0, log=print):
     net = svb.weights.load_model()
     lab = Labeller(svb, net, W, H)
     N = W * H
-    feats = torch.empty(n, 6 * N, dtype=torch.float32, device="cuda")
+    feats = torch.empty(n, svb.band.N_FEATURES * N, dtype=torch.float32, device="cuda")
     tgt = torch.empty(n, N, dtype=torch.float32, device="cuda")
     msk = torch.empty(n, N, dtype=torch.uint8, device="cuda")
     t0 = time.time()
@@ -241,13 +244,45 @@ class Evaluator:
     def learned(self):
         pp = self.pp
         pp.predict()
+        sp, pm = pp.confidence()
         self.lb.run(pp.left, pp.right, pp.code, pp.disp0, self.out_l, self.st_l,
-                    pp.stream.cuda_stream)
+                    pp.stream.cuda_stream, sp, pm)
         return self.out_l
 
     def full_range(self, R):
         return self.full.run(self.pp.left, self.pp.right, self.pp.code, R,
                              self.pp.stream.cuda_stream)[0]
+
+    def rule(self, tau):
+        """The ablation without the net: the band centre moves to the wide
+        search's argmin (feature 1) wherever that argmin's 9-row cost
+        (feature 2) is below tau, keeping the full +-R width; the fixed band
+        elsewhere.  The same band application and masked lr_refine kernels as
+        the learned band, fed a hand-made 'net output' (moved: shift = argmin
+        - disparity, b = 1 px; elsewhere b = 128 px, above any threshold)."""
+        torch, pp, lb, W, H = self.torch, self.pp, self.lb, self.W, self.H
+        lib, N = lb.lib, W * H
+        vp = lambda t: ctypes.c_void_p(t.data_ptr())                     # noqa: E731
+        s = pp.stream.cuda_stream
+        pp.predict()
+        self.svb._lib.check(lib.sv_band_features(vp(pp.left), vp(pp.right), pp.code,
+                                                 vp(pp.disp0), W, H, DMAX, vp(lb.feat),
+                                                 vp(lb.fws), lb.fneed, s), "band_features")
+        with torch.cuda.stream(pp.stream):
+            f = lb.feat.view(-1, N)
+            moved = f[2] < tau
+            o = lb.out.view(2, N)
+            o[0] = torch.where(moved, 2.0 * f[1], torch.zeros_like(f[1]))
+            o[1] = torch.where(moved, torch.full_like(f[1], -1.0), torch.full_like(f[1], 10.0))
+        self.svb._lib.check(lib.sv_band_apply(vp(lb.out), vp(pp.disp0), W, H, 3.0, 100.0, 3,
+                                              10, 160.0, vp(lb.centre), vp(lb.rad), s),
+                            "band_apply")
+        self.svb._lib.check(lib.sv_lr_refine_band(vp(pp.left), vp(pp.right), pp.code,
+                                                  vp(lb.centre), vp(lb.rad), W, H, TOL,
+                                                  ctypes.byref(lb.p), vp(self.out_l),
+                                                  vp(self.st_l), vp(lb.rws), lb.rneed, s),
+                            "lr_refine_band")
+        return self.out_l
 
 
 def _timed(torch, stream, fn):
@@ -264,22 +299,30 @@ def _timed(torch, stream, fn):
     return r, e0.elapsed_time(e1)
 
 
-def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None, log=print):
-    """Scores of the three methods on n pairs; with apply_grid, every band
-    application setting is scored and the best (bad2, then EPE) kept."""
+def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None,
+             rule_taus=None, log=print):
+    """Scores of the methods on n pairs: the fixed band, full-range SGM, the
+    learned band and the no-net rule (Evaluator.rule).  With apply_grid
+    every band application setting is scored and the best (bad2, then EPE)
+    kept; with rule_taus every rule threshold likewise (else the band's
+    rule_tau).  The learned band's half-width histogram is reported."""
     import torch
     net = svb.weights.load_model()
     ev = Evaluator(svb, net, band, W, H)
     grid = apply_grid or [dict(band.meta)]
+    taus = rule_taus or [float(band.meta.get("rule_tau", 0.1))]
     acc = {"fixed": [], "full": []}
     acc_l = [[] for _ in grid]
-    times = {"fixed": 0.0, "learned": 0.0, "full": 0.0}
+    acc_r = [[] for _ in taus]
+    hist_l = [torch.zeros(11, dtype=torch.int64, device="cuda") for _ in grid]
+    times = {"fixed": 0.0, "learned": 0.0, "full": 0.0, "rule": 0.0}
     st = ev.pp.stream
     # warm-up: the first predict_auto per work width records its CUDA graphs
     for seed, L, R, D, V in generate(pool, range(seed0 - 2, seed0), W, H):
         ev.load(L, R)
         ev.fixed()
         ev.learned()
+        ev.rule(taus[0])
     for i, (seed, L, R, D, V) in enumerate(generate(pool, range(seed0, seed0 + n), W, H)):
         ev.load(L, R)
         out, dt = _timed(torch, st, ev.fixed)
@@ -295,6 +338,13 @@ def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None
             if j == 0:
                 times["learned"] += dt
             acc_l[j].append(_score(out.cpu().numpy(), D, V))
+            with torch.cuda.stream(st):
+                hist_l[j] += torch.bincount(ev.lb.rad.long(), minlength=11)[:11]
+        for j, tau in enumerate(taus):
+            out, dt = _timed(torch, st, lambda: ev.rule(tau))
+            if j == 0:
+                times["rule"] += dt
+            acc_r[j].append(_score(out.cpu().numpy(), D, V))
         if (i + 1) % 100 == 0:
             log("  %d / %d pairs" % (i + 1, n))
     mpix = n * W * H / 1e6
@@ -306,23 +356,38 @@ def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None
     scores = [np.array(a) for a in acc_l]
     best = min(range(len(grid)), key=lambda j: (scores[j][:, 1].mean(), scores[j][:, 0].mean()))
     band.meta.update(grid[best])
+    h = hist_l[best].cpu().numpy()
     res["learned"] = dict(epe=float(scores[best][:, 0].mean()),
                           bad2=float(scores[best][:, 1].mean()),
-                          mpix_s=mpix / (times["learned"] / 1e3), apply=dict(grid[best]))
+                          mpix_s=mpix / (times["learned"] / 1e3), apply=dict(grid[best]),
+                          half_width_hist={str(r): int(h[r]) for r in range(11) if h[r]})
+    rs = [np.array(a) for a in acc_r]
+    rb = min(range(len(taus)), key=lambda j: (rs[j][:, 1].mean(), rs[j][:, 0].mean()))
+    band.meta["rule_tau"] = float(taus[rb])
+    res["rule_no_net"] = dict(epe=float(rs[rb][:, 0].mean()), bad2=float(rs[rb][:, 1].mean()),
+                              mpix_s=mpix / (times["rule"] / 1e3), tau=float(taus[rb]))
     if apply_grid:
         res["grid"] = [dict(g, epe=float(s[:, 0].mean()), bad2=float(s[:, 1].mean()))
                        for g, s in zip(grid, scores)]
+    if rule_taus:
+        res["rule_grid"] = [dict(tau=float(t), epe=float(s[:, 0].mean()),
+                                 bad2=float(s[:, 1].mean())) for t, s in zip(taus, rs)]
     return res
 
 
 def apply_grid():
-    """Band application settings tried on the validation pairs (rad_k = 100
-    keeps the full +-10 width wherever the centre moves)."""
+    """Band application settings tried on the validation pairs: thresholds on
+    the predicted Laplace scale b, and half-widths ceil(rad_k * b) clamped
+    to [rad_min, 10] that vary with b (the full +-10 width around a moved
+    centre, rad_k = 100, is not among them)."""
     out = []
-    for b_thr in (2.5, 4.0, 6.0, 10.0, 16.0, 32.0, 128.0):
-        for rad_k in (2.0, 3.0, 100.0):
+    for b_thr in (2.5, 4.0, 6.0, 10.0, 16.0, 32.0):
+        for rad_k in (1.0, 1.5, 2.0, 3.0, 4.0):
             out.append(dict(b_thr=b_thr, rad_k=rad_k, rad_min=3, R=10, shift_max=160.0))
     return out
+
+
+RULE_TAUS = (0.05, 0.08, 0.12, 0.16, 0.22, 0.3)
 
 
 def main(argv=None):
@@ -356,7 +421,8 @@ def main(argv=None):
         del feats, tgt, msk
         torch.cuda.empty_cache()
         if a.val > 0:
-            val = evaluate(svb, pool, band, a.val, seed0=VAL_SEED0, apply_grid=apply_grid())
+            val = evaluate(svb, pool, band, a.val, seed0=VAL_SEED0, apply_grid=apply_grid(),
+                           rule_taus=list(RULE_TAUS))
             report["validation"] = val
             print("validation:", json.dumps(val["learned"]), flush=True)
         if a.out:

@@ -22,7 +22,9 @@
 
 namespace sv {
 
-constexpr int kBandF = 6, kBandC = 16, kBandO = 2, kBandL = 4;
+// input planes: the six search / image features of k_band_features and the
+// network's confidence (k_band_conf)
+constexpr int kBandF = 8, kBandC = 16, kBandO = 2, kBandL = 4;
 constexpr int kBandIC[kBandL] = {kBandF, kBandC, kBandC, kBandC};
 constexpr int kBandOC[kBandL] = {kBandC, kBandC, kBandC, kBandO};
 constexpr int kBandDil[kBandL] = {1, 2, 4, 1};
@@ -421,6 +423,21 @@ int check_band_ws(void *ws, size_t bytes, int nb, int W, int H) {
         if (rc_ != SV_OK) return rc_; \
     } while (0)
 
+namespace sv {
+
+// Feature planes 6 and 7: the network's spread (full-resolution px / 16)
+// and its peak probability - 0.5, per pixel of the last pass.
+__global__ void k_band_conf(const double *__restrict__ spread, const double *__restrict__ pmax,
+                            long N, float *__restrict__ feat) {
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < N;
+         p += (long)gridDim.x * blockDim.x) {
+        feat[6 * N + p] = (float)__ddiv_rn(spread[p], 16.0);
+        feat[7 * N + p] = (float)__dsub_rn(pmax[p], 0.5);
+    }
+}
+
+}  // namespace sv
+
 extern "C" {
 
 long sv_band_param_count(void) { return band_param_count(); }
@@ -499,6 +516,17 @@ size_t sv_band_features_workspace_size(int W, int H) {
     cv.take<uint64_t>((size_t)W * H);
     cv.take<uint64_t>((size_t)W * H);
     return cv.off;
+}
+
+int sv_band_conf_features(const double *spread, const double *pmax, int W, int H, float *feat,
+                          void *stream) {
+    if (!spread || !pmax || !feat) { set_error("NULL argument"); return SV_ERR_NULL; }
+    if (W < 1 || H < 1) { set_error("bad shape %dx%d", W, H); return SV_ERR_SHAPE; }
+    const long N = (long)W * H;
+    count_launch();
+    k_band_conf<<<grid_for(N, 256), 256, 0, (cudaStream_t)stream>>>(spread, pmax, N, feat);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
 }
 
 int sv_band_features(const void *left, const void *right, int dtype, const double *disp0,

@@ -179,6 +179,8 @@ static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictW
     p.sel = reinterpret_cast<SelState *>(cv.take<unsigned char>(select_state_bytes()));
     p.hist = cv.take<unsigned>(select_hist_words());
     carve_fwd(cv, n, Hm, Wm, flag, &p.fwd);
+    p.fwd.qspread = cv.take<float>((size_t)h * w);   // the last pass's confidence maps
+    p.fwd.qpmax = cv.take<float>((size_t)h * w);
     if (o) *o = p;
     return cv.off;
 }
@@ -597,6 +599,25 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right, 
     SV_TRY(predict_ws(net, W, H, mw, 64, workspace, workspace_bytes, &w));
     return predict_at_scale_impl(net, w, left, right, dtype, W, H, work_width, precision,
                                  disp_full, disp_work, Ww, Hw, (cudaStream_t)stream);
+}
+
+int sv_predict_confidence(const sv_net *net, int W, int H, int Ww, int Hw, int probe_width,
+                          int max_width, const void *workspace, size_t workspace_bytes,
+                          double *spread, double *pmax, void *stream) {
+    if (!net || !spread || !pmax) { set_error("NULL argument"); return SV_ERR_NULL; }
+    if (W < 1 || H < 1 || Ww < 2 || Hw < 2 || Ww > W || probe_width < 1 || max_width < 1) {
+        set_error("bad sizes");
+        return SV_ERR_SHAPE;
+    }
+    PredictWs w;
+    SV_TRY(predict_ws(net, W, H, max_width, probe_width, const_cast<void *>(workspace),
+                      workspace_bytes, &w));
+    int h1, w1, hq, wq;
+    conv_out(Hw, Ww, &h1, &w1, &hq, &wq);
+    cudaStream_t st = (cudaStream_t)stream;
+    // spread in full-resolution pixels: quarter -> work (x4) -> full (x W / Ww)
+    SV_TRY(launch_upscale_disp(w.fwd.qspread, wq, hq, W, H, 4.0 * W / (double)Ww, spread, st));
+    return launch_resize_f32(w.fwd.qpmax, wq, hq, W, H, pmax, st);
 }
 
 int sv_predict_refine(const sv_net *net, const void *left, const void *right, int dtype, int W,

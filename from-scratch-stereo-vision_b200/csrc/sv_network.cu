@@ -700,7 +700,7 @@ constexpr int SA_DMAX = 16;
 template <int IC, int CS>
 __device__ __forceinline__ void conv3d_softargmin_body(int bx, int by, const float *__restrict__ x, int D, int h, int w,
                         const float *__restrict__ wt, const float *__restrict__ b,
-                        float *__restrict__ disp) {
+                        float *__restrict__ disp, float *__restrict__ spread, float *__restrict__ pmax) {
     constexpr int CPS = IC / CS, TD = SA_DMAX, NT = 128 * CS;
     constexpr int DS = c3_layout(CS, CPS, TD, 0), P = c3_layout(CS, CPS, TD, 1);
     static_assert(IC % CS == 0 && DS > 0, "tile layout");
@@ -741,6 +741,17 @@ __device__ __forceinline__ void conv3d_softargmin_body(int bx, int by, const flo
         td += __shfl_xor_sync(kFull, td, m);
     }
     if (d == 0 && ox < w) disp[(long)oy * w + ox] = td / te;
+    if (!spread) return;                           // the same for the whole CTA
+    // the distribution's spread and its peak probability (the exponent of
+    // the best disparity is 1): how sure the network is of this disparity
+    float t2 = (float)d * (float)d * e;
+#pragma unroll
+    for (int m = 1; m < SA_DMAX; m <<= 1) t2 += __shfl_xor_sync(kFull, t2, m);
+    if (d == 0 && ox < w) {
+        const float mu = td / te;
+        spread[(long)oy * w + ox] = sqrtf(fmaxf(t2 / te - mu * mu, 0.f));
+        pmax[(long)oy * w + ox] = 1.f / te;
+    }
 }
 
 
@@ -749,8 +760,9 @@ template <int IC, int CS>
 __global__ void __launch_bounds__(128 * CS)
     k_conv3d_softargmin(const float *__restrict__ x, int D, int h, int w,
                         const float *__restrict__ wt, const float *__restrict__ b,
-                        float *__restrict__ disp) {
-    conv3d_softargmin_body<IC, CS>(blockIdx.x, blockIdx.y, x, D, h, w, wt, b, disp);
+                        float *__restrict__ disp, float *__restrict__ spread,
+                        float *__restrict__ pmax) {
+    conv3d_softargmin_body<IC, CS>(blockIdx.x, blockIdx.y, x, D, h, w, wt, b, disp, spread, pmax);
 }
 
 template <int IC, int CS>
@@ -767,7 +779,7 @@ __global__ void __launch_bounds__(128 * CS)
     const int bx = (int)(c % tx), by = (int)(c / tx);
     if (by >= h) return;
     conv3d_softargmin_body<IC, CS>(bx, by, net_slab(x, L, p), D, h, w, wt, b,
-                                   net_slab(disp, L, p));
+                                   net_slab(disp, L, p), nullptr, nullptr);
 }
 
 // ====================================================================
@@ -823,6 +835,14 @@ int launch_upscale_disp(const float *dw, int Ww, int Hw, int W, int H, double in
                         double *out, cudaStream_t st) {
     dim3 blk(32, 8);
     count_launch(); k_resize_scale<float><<<grid2d(W, H, blk), blk, 0, st>>>(dw, Ww, Hw, W, H, inv, 1, out);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
+int launch_resize_f32(const float *x, int W, int H, int W2, int H2, double *out,
+                      cudaStream_t st) {
+    dim3 blk(32, 8);
+    count_launch(); k_resize_scale<float><<<grid2d(W2, H2, blk), blk, 0, st>>>(x, W, H, W2, H2, 1.0, 0, out);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }
@@ -994,7 +1014,7 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
     constexpr int S3 = CM % 2 == 0 ? 2 : 1;
     count_launch();
     k_conv3d_softargmin<CM, S3><<<dim3((w + C3_TX - 1) / C3_TX, h), 128 * S3, 0, st>>>(
-        b.v1, D, h, w, n.cw[2], n.cb[2], d0);
+        b.v1, D, h, w, n.cw[2], n.cb[2], d0, b.qspread, b.qspread ? b.qpmax : nullptr);
     SV_LAUNCH_CHECK();
     // Refinement levels
     const int Hs[2] = {H / 2, H}, Ws[2] = {W / 2, W};

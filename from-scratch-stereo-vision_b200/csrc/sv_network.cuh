@@ -62,6 +62,9 @@ struct FwdBufs {
     float *v0, *v1;          // filtered cost volumes [Cm][D][h][w]
     float *rin, *ra, *rb;    // refinement input [2][H][W] and ping-pong [Rc][H][W]
     int *flag;               // device error flag (the workspace's DevFlags)
+    // optional, [h][w]: the soft-argmin distribution's spread (std, quarter
+    // px) and peak probability (both or neither)
+    float *qspread, *qpmax;
 };
 
 struct SelState;
@@ -90,6 +93,9 @@ int launch_resize_f64(const double *x, int W, int H, int W2, int H2, double *out
 int launch_upscale_disp(const float *dw, int Ww, int Hw, int W, int H, double inv, double *out,
                         cudaStream_t st);
 int launch_promote(const float *x, long n, double *out, cudaStream_t st);
+// bilinear resample of an FP32 map to FP64 (resize_gray's arithmetic), no scaling
+int launch_resize_f32(const float *x, int W, int H, int W2, int H2, double *out,
+                      cudaStream_t st);
 int launch_avgpool2(const float *img, int H, int W, float *out, cudaStream_t st);
 int launch_avgpool2_f64(const double *img, int C, int H, int W, double *out, cudaStream_t st);
 int launch_forward(const NetView &n, const float *left, const float *right, int H, int W,

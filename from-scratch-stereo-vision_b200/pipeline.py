@@ -64,6 +64,21 @@ class PairPipeline:
             _ptr(self.disp0), _ptr(self.disp_work), ctypes.byref(self._Ww),
             ctypes.byref(self._Hw), self._trace, _ptr(self.pws), self.pneed, s), "predict_auto")
 
+    def confidence(self, stream=None):
+        """The network's spread and peak probability of the last predict()'s
+        final pass, at W x H (FP64 device tensors self.spread, self.pmax)."""
+        if not hasattr(self, "spread"):
+            N = self.W * self.H
+            self.spread = torch.empty(N, dtype=torch.float64, device=self.dev)
+            self.pmax = torch.empty(N, dtype=torch.float64, device=self.dev)
+        Ww, Hw = self.work_size
+        s = self.stream.cuda_stream if stream is None else stream
+        _lib.check(self.lib.sv_predict_confidence(
+            self.net.handle, self.W, self.H, Ww, Hw, self.probe_width, self.max_width,
+            _ptr(self.pws), self.pneed, _ptr(self.spread), _ptr(self.pmax), s),
+            "predict_confidence")
+        return self.spread, self.pmax
+
     def refine(self, stream=None) -> None:
         self.refiner.run(self.left, self.right, self.disp0, self.out, self.status,
                          self.stream.cuda_stream if stream is None else stream)

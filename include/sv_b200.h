@@ -276,6 +276,18 @@ int sv_predict_at_scale(const sv_net *net, const void *left, const void *right,
                         double *disp_full, double *disp_work, int *Ww, int *Hw,
                         void *workspace, size_t workspace_bytes, void *stream);
 
+/* How sure the network was, per pixel, in the last pass of the
+ * sv_predict_auto (or sv_predict_refine) call that used this workspace:
+ * the spread (standard deviation, in full-resolution pixels) and the peak
+ * probability of its soft-argmin distribution (SoftArgmin.forward,
+ * stereonet.py:858-885), bilinearly resampled from the quarter-resolution
+ * volume to W x H (FP64).  Ww x Hw is that call's final work size;
+ * probe_width and max_width must be the call's.  No reference counterpart:
+ * they feed the learned band's net. */
+int sv_predict_confidence(const sv_net *net, int W, int H, int Ww, int Hw, int probe_width,
+                          int max_width, const void *workspace, size_t workspace_bytes,
+                          double *spread, double *pmax, void *stream);
+
 /* predict_auto followed by lr_refine for many pairs of uneven sizes
  * (predict_auto, stereonet.py:3872-3929; lr_refine, 5343-5391), with the
  * work-width decisions taken on the device: the probe, every pass and the
@@ -391,14 +403,19 @@ void sv_band_destroy(sv_band *band);
 /* copies the (FP32 master) parameters to host memory as doubles; syncs */
 int sv_band_get_params(const sv_band *band, double *out, long n_params);
 
-/* features [6][H][W] FP32 from the two views (9x7 census) and disp0 (FP64),
- * disparities searched over 0..dmax (dmax <= 255) */
+/* Band-net input planes [8][H][W] FP32.  sv_band_features writes planes
+ * 0-5 from the two views (9x7 census) and disp0 (FP64), disparities
+ * searched over 0..dmax (dmax <= 255); sv_band_conf_features writes planes
+ * 6-7 from the network's spread and peak probability of the same pass
+ * (sv_predict_confidence). */
 size_t sv_band_features_workspace_size(int W, int H);
 int sv_band_features(const void *left, const void *right, int dtype,
                      const double *disp0, int W, int H, int dmax, float *feat,
                      void *workspace, size_t workspace_bytes, void *stream);
+int sv_band_conf_features(const double *spread, const double *pmax, int W, int H, float *feat,
+                          void *stream);
 
-/* forward of nb items: feat [nb][6][H][W] -> out [nb][2][H][W] */
+/* forward of nb items: feat [nb][8][H][W] -> out [nb][2][H][W] */
 size_t sv_band_workspace_size(int nb, int W, int H);
 int sv_band_forward(const sv_band *band, const float *feat, int nb, int W, int H,
                     float *out, void *workspace, size_t workspace_bytes,

@@ -246,14 +246,21 @@ def band_param_count() -> int:
     return int(lib().orc_band_param_count())
 
 
-def band_features(left, right, disp0, W, H, dmax) -> np.ndarray:
-    """[6][H][W] features (census 9x7 of both views, disparity, gray)."""
+def band_features(left, right, disp0, W, H, dmax, spread=None, pmax=None) -> np.ndarray:
+    """[8][H][W] band-net inputs: six features (census 9x7 of both views,
+    disparity, gray) and the network's spread / 16 and peak probability - 0.5
+    (given; zero spread and 0.5 probability when absent)."""
     gl, gr = _f64(left), _f64(right)
     cl, cr = census(gl, W, H, 4, 3), census(gr, W, H, 4, 3)
     d0 = _f64(disp0)
-    out = np.zeros(6 * W * H)
+    N = W * H
+    out = np.zeros(8 * N)
     _check(lib().orc_band_features(_p(cl, _u64), _p(cr, _u64), _p(d0), _p(gl), W, H,
                                    int(dmax), _p(out)), "band_features")
+    if spread is not None:
+        out[6 * N:7 * N] = (_f64(spread) / 16.0).astype(np.float32)
+    if pmax is not None:
+        out[7 * N:] = (_f64(pmax) - 0.5).astype(np.float32)
     return out
 
 

@@ -26,7 +26,7 @@
 #define ORC_ENOMEM 2
 #define ORC_ERANGE 3
 
-#define BAND_F 6
+#define BAND_F 8               /* net inputs: the 6 features below + 2 given planes */
 #define BAND_C 16
 #define BAND_O 2
 #define BAND_L 4
@@ -58,7 +58,9 @@ long orc_band_param_count(void) {
  *   f3 = agg(r0) / 558           r0 = min(max(0, int(d0 + 0.5)), dmax)
  *   f4 = min of agg over [max(0, r0-10), min(dmax, r0+10)] / 558
  *   f5 = gray(left) - 0.5
- * feat is [6][H][W]. */
+ * feat is [6][H][W] here; the net reads BAND_F = 8 planes per item, the
+ * last two being the network's spread / 16 and peak probability - 0.5,
+ * which are inputs (copied, not computed). */
 int orc_band_features(const uint64_t *cl, const uint64_t *cr, const double *d0,
                       const double *gray, int W, int H, int dmax, double *feat) {
     if (W < 1 || H < 1 || dmax < 0) return ORC_EBADARG;

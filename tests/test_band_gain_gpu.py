@@ -1,13 +1,18 @@
-"""What the trained band net gains over the method without it.
+"""What the trained band net gains over the method without it, and over a
+rule that uses the same wide search without a net.
 
 Held-out 640x480 pairs of the learned-band workload (disparities 30-150 px,
 thin foreground bars, 30% low texture; seeds outside the training and
-validation ranges) are refined twice after the same FP32 predict_auto:
-with the fixed +-10 band (lr_refine, refine_disparity's parameters) and with
-the committed trained band net (weights/band_weights.npz).  Against the
-generator's ground truth on valid pixels the learned band must cut both the
-end-point error and the share of pixels off by more than 2 px at least in
-half, at no less than 0.7x the fixed band's throughput.
+validation ranges) are refined after the same FP32 predict_auto three ways:
+with the fixed +-10 band (lr_refine, refine_disparity's parameters), with
+the committed trained band net (weights/band_weights.npz, which reads the
+network's own confidence among its inputs), and with the no-net rule (the
+band centre moved to the wide search's argmin wherever its cost is below the
+threshold chosen on the validation pairs, band_train.Evaluator.rule).
+Against the generator's ground truth on valid pixels the learned band must
+cut both the end-point error and the share of pixels off by more than 2 px
+at least in half relative to the fixed band, at no less than 0.7x its
+throughput, and must beat the rule on both scores.
 """
 
 import numpy as np
@@ -25,34 +30,34 @@ def _score(d, gt, valid):
     return e.mean(), (e > 2.0).mean()
 
 
-def test_trained_band_beats_fixed_band(svb, net):
+def test_trained_band_beats_fixed_band_and_rule(svb, net):
     band = svb.band.BandNet.load()
-    pp = svb.pipeline.PairPipeline(W, H, net)
-    lb = svb.band.LearnedBandRefiner(W, H, band, dmax=160)
-    out = torch.empty(W * H, dtype=torch.float64, device="cuda")
-    st = torch.empty(W * H, dtype=torch.uint8, device="cuda")
-    fixed, learned, t_fixed, t_learned = [], [], 0.0, 0.0
+    ev = svb.band_train.Evaluator(svb, net, band, W, H)
+    tau = float(band.meta["rule_tau"])
+    fixed, learned, rule, t_fixed, t_learned = [], [], [], 0.0, 0.0
+    st = ev.pp.stream
     for seed in SEEDS:
         p = svb.synth.config_learned_crop(seed, W, H)
-        with torch.cuda.stream(pp.stream):
-            pp.left.copy_(torch.from_numpy(p.left.ravel()))
-            pp.right.copy_(torch.from_numpy(p.right.ravel()))
+        ev.load(p.left, p.right)
         for k in range(2):                       # the first round records CUDA graphs
             e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-            e[0].record(pp.stream)
-            pp.run_device()
-            e[1].record(pp.stream)
-            pp.predict()
-            lb.run(pp.left, pp.right, pp.code, pp.disp0, out, st, pp.stream.cuda_stream)
-            e[2].record(pp.stream)
+            e[0].record(st)
+            ev.fixed()
+            e[1].record(st)
+            ev.learned()
+            e[2].record(st)
             e[2].synchronize()
             if k:
                 t_fixed += e[0].elapsed_time(e[1])
                 t_learned += e[1].elapsed_time(e[2])
-        fixed.append(_score(pp.out.cpu().numpy(), p.disp, p.valid))
-        learned.append(_score(out.cpu().numpy(), p.disp, p.valid))
-    f, l = np.mean(fixed, axis=0), np.mean(learned, axis=0)
-    print("\nfixed +-10: EPE %.3f bad2 %.4f; learned: EPE %.3f bad2 %.4f; throughput ratio %.2f"
-          % (f[0], f[1], l[0], l[1], t_fixed / t_learned))
+        fixed.append(_score(ev.pp.out.cpu().numpy(), p.disp, p.valid))
+        learned.append(_score(ev.out_l.cpu().numpy(), p.disp, p.valid))
+        ev.rule(tau)
+        rule.append(_score(ev.out_l.cpu().numpy(), p.disp, p.valid))
+    f, l, r = (np.mean(x, axis=0) for x in (fixed, learned, rule))
+    print("\nfixed +-10: EPE %.3f bad2 %.4f; rule (tau %.2f): EPE %.3f bad2 %.4f; learned: "
+          "EPE %.3f bad2 %.4f; throughput ratio %.2f"
+          % (f[0], f[1], tau, r[0], r[1], l[0], l[1], t_fixed / t_learned))
     assert l[0] < 0.5 * f[0] and l[1] < 0.5 * f[1]
+    assert l[0] < r[0] and l[1] < r[1]
     assert t_fixed / t_learned >= 0.7

@@ -34,9 +34,12 @@ def test_features_bit_exact(svb, orc, W, H, dmax):
     p, d0 = _pair(svb, W, H, W + H)
     d0[::37] = -3.7
     d0[5] = 400.0
-    ref = orc.band_features(p.gray("left"), p.gray("right"), d0, W, H, dmax).astype(np.float32)
+    rng = np.random.default_rng(W)
+    sp, pm = rng.uniform(0, 9, W * H), rng.uniform(0, 1, W * H)
+    ref = orc.band_features(p.gray("left"), p.gray("right"), d0, W, H, dmax, sp,
+                            pm).astype(np.float32)
     for L, R in ((p.left, p.right), (p.gray("left"), p.gray("right"))):
-        got = svb.band.features(L, R, d0, W, H, dmax).cpu().numpy()
+        got = svb.band.features(L, R, d0, W, H, dmax, sp, pm).cpu().numpy()
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
@@ -130,7 +133,7 @@ def test_training_lowers_loss(svb, orc):
     nb, W, H = 4, 64, 48
     f, _, m = _batch(svb, orc, nb, W, H, 30)
     # a learnable target: the wide-search shift the features carry
-    t = np.clip(64.0 * f.reshape(nb, 6, -1)[:, 1], -160, 160).astype(np.float32).ravel()
+    t = np.clip(64.0 * f.reshape(nb, 8, -1)[:, 1], -160, 160).astype(np.float32).ravel()
     net = svb.band.BandNet(seed=1)
     ft, tt, mt = (torch.from_numpy(a).cuda() for a in (f, t, m))
     _, l0 = net.grads(f, t, m, nb, W, H)

@@ -11,14 +11,14 @@ def _case(orc, nb=2, W=9, H=7, seed=0):
     rng = np.random.default_rng(seed)
     n = orc.band_param_count()
     params = rng.normal(0, 0.3, n)
-    feat = rng.normal(0, 1, nb * 6 * W * H)
+    feat = rng.normal(0, 1, nb * 8 * W * H)
     target = rng.normal(0, 20, nb * W * H)
     mask = (rng.random(nb * W * H) < 0.8).astype(np.uint8)
     return params, feat, target, mask
 
 
 def test_param_count(orc):
-    assert orc.band_param_count() == 5810 <= 20000
+    assert orc.band_param_count() == 6098 <= 20000
 
 
 def test_band_gradients_central_differences(orc):
@@ -79,7 +79,7 @@ def test_band_features_numpy(orc):
     L = rng.integers(0, 256, (H, W)).astype(np.float64) / 255.0
     R = rng.integers(0, 256, (H, W)).astype(np.float64) / 255.0
     d0 = rng.uniform(-2, 12, W * H)
-    f = orc.band_features(L, R, d0, W, H, dmax).reshape(6, H, W)
+    f = orc.band_features(L, R, d0, W, H, dmax).reshape(8, H, W)
     cl = orc.census(L, W, H, 4, 3).reshape(H, W)
     cr = orc.census(R, W, H, 4, 3).reshape(H, W)
     pop = np.vectorize(lambda v: bin(int(v)).count("1"))
@@ -98,4 +98,10 @@ def test_band_features_numpy(orc):
         lo, hi = max(0, r - 10), min(dmax, r + 10)
         exp = [dd / 64, (dw - dd) / 64, agg[dw] / 558, agg[r] / 558, agg[lo:hi + 1].min() / 558,
                L[y, x] - 0.5]
-        assert np.allclose(f[:, y, x], exp, rtol=0, atol=1e-15), (y, x)
+        assert np.allclose(f[:6, y, x], exp, rtol=0, atol=1e-15), (y, x)
+    assert not f[6:].any()                       # no network confidence given: zero planes
+    sp, pm = rng.uniform(0, 9, W * H), rng.uniform(0, 1, W * H)
+    g = orc.band_features(L, R, d0, W, H, dmax, sp, pm).reshape(8, H, W)
+    assert np.array_equal(g[:6], f[:6])
+    assert np.array_equal(g[6].ravel(), (sp / 16).astype(np.float32).astype(np.float64))
+    assert np.array_equal(g[7].ravel(), (pm - 0.5).astype(np.float32).astype(np.float64))

@@ -115,6 +115,7 @@ SIGNATURES = {
     "sv_band_get_params": (_I, [_VP, _VP, ctypes.c_long]),
     "sv_band_features_workspace_size": (_SZ, [_I, _I]),
     "sv_band_conf_features": (_I, [_VP, _VP, _I, _I, _VP, _VP]),
+    "sv_band_rule_centre": (_I, [_VP, _VP, _I, _I, _D, _VP, _VP]),
     "sv_predict_confidence": (_I, [_VP, _I, _I, _I, _I, _I, _I, _VP, _SZ, _VP, _VP, _VP]),
     "sv_band_features": (_I, [_VP, _VP, _I, _VP, _I, _I, _I, _VP, _VP, _SZ, _VP]),
     "sv_band_workspace_size": (_SZ, [_I, _I, _I]),

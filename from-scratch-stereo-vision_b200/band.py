@@ -8,15 +8,19 @@ net (4 convolutions, 6098 parameters, BF16 tensor-core kernels) reads eight
 per-pixel features (network disparity, a wide 9-row census search, costs at
 the network disparity and inside its band, gray level, and how sure the
 network was: the spread and peak probability of its soft-argmin
-distribution, stereonet.py:858-885) and predicts a shift
-of the band centre with a Laplace scale b.  Where b <= b_thr the band moves
-to disparity + shift and narrows to ceil(rad_k * b) (at least rad_min); the
-fixed band stays everywhere else.  It is trained on the method's own
+distribution, stereonet.py:858-885).  The band is built around a rule
+centre -- the network disparity moved to the wide search's argmin wherever
+that argmin's cost is below rule_tau (chosen on validation pairs) -- and
+the net predicts a shift from that centre with a Laplace scale b.  Where
+b <= b_thr the band moves to centre + shift and narrows to ceil(rad_k * b)
+(at least rad_min); elsewhere it stays at the rule centre with the full
++-R width.  It is trained on the method's own
 full-range SGM disparities (refine_fullres with disp0 = R, R = (dmax+2)//2+1
 as in eval_real.py:143-146) with Adam (stereonet.py:1354-1387).
 
-Entry points: ``features``, ``BandNet`` (forward / grads / train_step),
-``targets``, ``apply``, ``lr_refine_band`` and ``LearnedBandRefiner``.
+Entry points: ``features``, ``rule_centre``, ``BandNet`` (forward / grads /
+train_step), ``targets``, ``apply``, ``lr_refine_band`` and
+``LearnedBandRefiner``.
 """
 
 from __future__ import annotations
@@ -89,6 +93,18 @@ def features(left, right, disp0, W, H, dmax=255, spread=None, pmax=None):
     _lib.check(lib.sv_band_conf_features(_ptr(sp), _ptr(pm), W, H, _ptr(feat), _stream()),
                "band_conf_features")
     return feat
+
+
+def rule_centre(feat, disp0, W, H, tau):
+    """The rule centre (FP64 device tensor) from the features and disp0."""
+    lib = _lib.load()
+    N = W * H
+    f = _f32_dev(feat, N_FEATURES * N, "feat")
+    td = _to_dev(disp0, N, torch.float64, name="disp0")
+    out = torch.empty(N, dtype=torch.float64, device=td.device)
+    _lib.check(lib.sv_band_rule_centre(_ptr(f), _ptr(td), W, H, float(tau), _ptr(out),
+                                       _stream()), "band_rule_centre")
+    return out
 
 
 class BandNet:
@@ -257,6 +273,7 @@ class LearnedBandRefiner:
         N = W * H
         self.feat = torch.empty(N_FEATURES * N, dtype=torch.float32, device=dev)
         self.out = torch.empty(N_OUTPUTS * N, dtype=torch.float32, device=dev)
+        self.base = torch.empty(N, dtype=torch.float64, device=dev)     # the rule centre
         self.centre = torch.empty(N, dtype=torch.float64, device=dev)
         self.rad = torch.empty(N, dtype=torch.uint8, device=dev)
         self.fneed = self.lib.sv_band_features_workspace_size(W, H)
@@ -274,10 +291,13 @@ class LearnedBandRefiner:
                                              self.fneed, stream), "band_features")
         _lib.check(self.lib.sv_band_conf_features(_ptr(spread), _ptr(pmax), W, H,
                                                   _ptr(self.feat), stream), "band_conf_features")
+        _lib.check(self.lib.sv_band_rule_centre(_ptr(self.feat), _ptr(disp0), W, H,
+                                                float(m["rule_tau"]), _ptr(self.base), stream),
+                   "band_rule_centre")
         _lib.check(self.lib.sv_band_forward(self.band.handle, _ptr(self.feat), 1, W, H,
                                             _ptr(self.out), _ptr(self.bws), self.bneed, stream),
                    "band_forward")
-        _lib.check(self.lib.sv_band_apply(_ptr(self.out), _ptr(disp0), W, H, float(m["b_thr"]),
+        _lib.check(self.lib.sv_band_apply(_ptr(self.out), _ptr(self.base), W, H, float(m["b_thr"]),
                                           float(m["rad_k"]), int(m["rad_min"]), int(m["R"]),
                                           float(m["shift_max"]), _ptr(self.centre),
                                           _ptr(self.rad), stream), "band_apply")

@@ -5,10 +5,14 @@
 
 Training data: seeded synthetic 256x192 crops (disparities 30-150 px, 1-3
 thin foreground bars 2-6 px wide, 30% low-texture area).  Per crop the GPU
-runs the network (predict_auto), the band features and the label: the
-plain method's full-range census + SGM disparity, lr_refine with
-disp0 = R and R = (max disparity + 2) // 2 + 1 (eval_real.py:143-146);
-pixels whose label fails the left-right check are unlabelled.  The band
+runs the network (predict_auto), the band features (with the network's own
+confidence), the rule centre and the label: the plain method's full-range
+census + SGM disparity, lr_refine with disp0 = R and
+R = (max disparity + 2) // 2 + 1 (eval_real.py:143-146); pixels whose label
+fails the left-right check are unlabelled; the target is the label's shift
+from the rule centre.  The rule's threshold (the wide search's cost below
+which its argmin replaces the network disparity) is chosen first, on the
+validation pairs, with no net.  The band
 net is trained with its own BF16 kernels and Adam (lr 5e-4).  The band
 application thresholds are then chosen on validation pairs, and the
 evaluation scores held-out 640x480 pairs against the generator's ground
@@ -128,10 +132,11 @@ class FullRange:
 class Labeller:
     """Network disparity, features and full-range labels of one crop size."""
 
-    def __init__(self, svb, net, W, H):
+    def __init__(self, svb, net, W, H, tau):
         import torch
-        self.svb, self.torch = svb, torch
+        self.svb, self.torch, self.tau = svb, torch, float(tau)
         self.pipe = svb.pipeline.PairPipeline(W, H, net)
+        self.base = torch.empty(W * H, dtype=torch.float64, device="cuda")
         self.full = FullRange(svb, W, H)
         self.W, self.H = W, H
         N = W * H
@@ -157,15 +162,18 @@ class Labeller:
                                             s), "band_features")
         svb._lib.check(lib.sv_band_conf_features(vp(sp), vp(pm), W, H, vp(self.feat), s),
                        "band_conf_features")
-        svb._lib.check(lib.sv_band_targets(vp(lab), vp(st), vp(pp.disp0), W * H, 160.0,
+        # the net learns the shift from the rule centre
+        svb._lib.check(lib.sv_band_rule_centre(vp(self.feat), vp(pp.disp0), W, H, self.tau,
+                                               vp(self.base), s), "band_rule_centre")
+        svb._lib.check(lib.sv_band_targets(vp(lab), vp(st), vp(self.base), W * H, 160.0,
                                            vp(self.t), vp(self.m), s), "band_targets")
         return self.feat, self.t, self.m
 
 
-def make_dataset(svb, pool, n, W=256, H=192, seed0=TRAIN_SEED0, log=print):
+def make_dataset(svb, pool, n, tau, W=256, H=192, seed0=TRAIN_SEED0, log=print):
     import torch
     net = svb.weights.load_model()
-    lab = Labeller(svb, net, W, H)
+    lab = Labeller(svb, net, W, H, tau)
     N = W * H
     feats = torch.empty(n, svb.band.N_FEATURES * N, dtype=torch.float32, device="cuda")
     tgt = torch.empty(n, N, dtype=torch.float32, device="cuda")
@@ -254,29 +262,23 @@ class Evaluator:
                              self.pp.stream.cuda_stream)[0]
 
     def rule(self, tau):
-        """The ablation without the net: the band centre moves to the wide
-        search's argmin (feature 1) wherever that argmin's 9-row cost
-        (feature 2) is below tau, keeping the full +-R width; the fixed band
-        elsewhere.  The same band application and masked lr_refine kernels as
-        the learned band, fed a hand-made 'net output' (moved: shift = argmin
-        - disparity, b = 1 px; elsewhere b = 128 px, above any threshold)."""
+        """The ablation without the net: lr_refine with the full +-R band
+        around the rule centre (the network disparity moved to the wide
+        search's argmin wherever that argmin's 9-row cost is below tau) --
+        the learned band's starting point, with no net on top."""
         torch, pp, lb, W, H = self.torch, self.pp, self.lb, self.W, self.H
-        lib, N = lb.lib, W * H
+        lib = lb.lib
         vp = lambda t: ctypes.c_void_p(t.data_ptr())                     # noqa: E731
         s = pp.stream.cuda_stream
         pp.predict()
         self.svb._lib.check(lib.sv_band_features(vp(pp.left), vp(pp.right), pp.code,
                                                  vp(pp.disp0), W, H, DMAX, vp(lb.feat),
                                                  vp(lb.fws), lb.fneed, s), "band_features")
+        self.svb._lib.check(lib.sv_band_rule_centre(vp(lb.feat), vp(pp.disp0), W, H,
+                                                    float(tau), vp(lb.centre), s),
+                            "band_rule_centre")
         with torch.cuda.stream(pp.stream):
-            f = lb.feat.view(-1, N)
-            moved = f[2] < tau
-            o = lb.out.view(2, N)
-            o[0] = torch.where(moved, 2.0 * f[1], torch.zeros_like(f[1]))
-            o[1] = torch.where(moved, torch.full_like(f[1], -1.0), torch.full_like(f[1], 10.0))
-        self.svb._lib.check(lib.sv_band_apply(vp(lb.out), vp(pp.disp0), W, H, 3.0, 100.0, 3,
-                                              10, 160.0, vp(lb.centre), vp(lb.rad), s),
-                            "band_apply")
+            lb.rad.fill_(REFINE["R"])
         self.svb._lib.check(lib.sv_lr_refine_band(vp(pp.left), vp(pp.right), pp.code,
                                                   vp(lb.centre), vp(lb.rad), W, H, TOL,
                                                   ctypes.byref(lb.p), vp(self.out_l),
@@ -300,7 +302,7 @@ def _timed(torch, stream, fn):
 
 
 def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None,
-             rule_taus=None, log=print):
+             rule_taus=None, learned=True, log=print):
     """Scores of the methods on n pairs: the fixed band, full-range SGM, the
     learned band and the no-net rule (Evaluator.rule).  With apply_grid
     every band application setting is scored and the best (bad2, then EPE)
@@ -309,7 +311,7 @@ def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None
     import torch
     net = svb.weights.load_model()
     ev = Evaluator(svb, net, band, W, H)
-    grid = apply_grid or [dict(band.meta)]
+    grid = (apply_grid or [dict(band.meta)]) if learned else []
     taus = rule_taus or [float(band.meta.get("rule_tau", 0.1))]
     acc = {"fixed": [], "full": []}
     acc_l = [[] for _ in grid]
@@ -321,7 +323,8 @@ def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None
     for seed, L, R, D, V in generate(pool, range(seed0 - 2, seed0), W, H):
         ev.load(L, R)
         ev.fixed()
-        ev.learned()
+        if learned:
+            ev.learned()
         ev.rule(taus[0])
     for i, (seed, L, R, D, V) in enumerate(generate(pool, range(seed0, seed0 + n), W, H)):
         ev.load(L, R)
@@ -354,16 +357,17 @@ def evaluate(svb, pool, band, n, W=640, H=480, seed0=TEST_SEED0, apply_grid=None
         res[name] = dict(epe=float(a[:, 0].mean()), bad2=float(a[:, 1].mean()),
                          mpix_s=mpix / (times[key] / 1e3))
     scores = [np.array(a) for a in acc_l]
-    best = min(range(len(grid)), key=lambda j: (scores[j][:, 1].mean(), scores[j][:, 0].mean()))
-    band.meta.update(grid[best])
-    h = hist_l[best].cpu().numpy()
-    res["learned"] = dict(epe=float(scores[best][:, 0].mean()),
-                          bad2=float(scores[best][:, 1].mean()),
-                          mpix_s=mpix / (times["learned"] / 1e3), apply=dict(grid[best]),
-                          half_width_hist={str(r): int(h[r]) for r in range(11) if h[r]})
+    if grid:
+        best = min(range(len(grid)),
+                   key=lambda j: (scores[j][:, 1].mean(), scores[j][:, 0].mean()))
+        band.meta.update(grid[best])
+        h = hist_l[best].cpu().numpy()
+        res["learned"] = dict(epe=float(scores[best][:, 0].mean()),
+                              bad2=float(scores[best][:, 1].mean()),
+                              mpix_s=mpix / (times["learned"] / 1e3), apply=dict(grid[best]),
+                              half_width_hist={str(r): int(h[r]) for r in range(11) if h[r]})
     rs = [np.array(a) for a in acc_r]
     rb = min(range(len(taus)), key=lambda j: (rs[j][:, 1].mean(), rs[j][:, 0].mean()))
-    band.meta["rule_tau"] = float(taus[rb])
     res["rule_no_net"] = dict(epe=float(rs[rb][:, 0].mean()), bad2=float(rs[rb][:, 1].mean()),
                               mpix_s=mpix / (times["rule"] / 1e3), tau=float(taus[rb]))
     if apply_grid:
@@ -387,7 +391,7 @@ def apply_grid():
     return out
 
 
-RULE_TAUS = (0.05, 0.08, 0.12, 0.16, 0.22, 0.3)
+RULE_TAUS = (0.15, 0.2, 0.3, 0.4, 0.5, 0.7, 1.1)   # 1.1: always the argmin
 
 
 def main(argv=None):
@@ -410,19 +414,30 @@ def main(argv=None):
     torch.cuda.init()
     report = {"host_cores": os.cpu_count()}
     if a.cmd == "train":
+        # the rule's threshold first: the net learns the shift from its centre
         t0 = time.time()
-        feats, tgt, msk = make_dataset(svb, pool, a.crops)
+        probe = svb.band.BandNet(seed=0)
+        rv = evaluate(svb, pool, probe, a.val, seed0=VAL_SEED0, rule_taus=list(RULE_TAUS),
+                      learned=False)
+        tau = rv["rule_no_net"]["tau"]
+        report["rule_validation"] = dict(rv["rule_no_net"], grid=rv["rule_grid"],
+                                         seconds=round(time.time() - t0, 1))
+        print("rule: tau %.2f, EPE %.3f bad2 %.4f on %d validation pairs"
+              % (tau, rv["rule_no_net"]["epe"], rv["rule_no_net"]["bad2"], a.val), flush=True)
+        del probe
+        t0 = time.time()
+        feats, tgt, msk = make_dataset(svb, pool, a.crops, tau)
         report["data"] = dict(crops=a.crops, size=[256, 192], seconds=round(time.time() - t0, 1),
                               labelled=float(msk.float().mean()))
         print("dataset: %d crops, %.1f%% labelled, %.1f s"
               % (a.crops, 100 * report["data"]["labelled"], time.time() - t0), flush=True)
         band, info = train(svb, feats, tgt, msk, 256, 192, epochs=a.epochs, nb=a.batch, lr=a.lr)
+        band.meta["rule_tau"] = tau
         report["train"] = info
         del feats, tgt, msk
         torch.cuda.empty_cache()
         if a.val > 0:
-            val = evaluate(svb, pool, band, a.val, seed0=VAL_SEED0, apply_grid=apply_grid(),
-                           rule_taus=list(RULE_TAUS))
+            val = evaluate(svb, pool, band, a.val, seed0=VAL_SEED0, apply_grid=apply_grid())
             report["validation"] = val
             print("validation:", json.dumps(val["learned"]), flush=True)
         if a.out:

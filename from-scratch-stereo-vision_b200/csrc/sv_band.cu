@@ -425,6 +425,18 @@ int check_band_ws(void *ws, size_t bytes, int nb, int W, int H) {
 
 namespace sv {
 
+// The rule centre: the network disparity moved to the wide search's first
+// argmin (d0 + 64 * feature 1) wherever that argmin's 9-row cost (feature 2)
+// is below tau.  The learned band refines around it.
+__global__ void k_band_rule(const float *__restrict__ feat, const double *__restrict__ d0,
+                            long N, double tau, double *__restrict__ centre) {
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < N;
+         p += (long)gridDim.x * blockDim.x) {
+        const double f1 = (double)feat[N + p], f2 = (double)feat[2 * N + p];
+        centre[p] = f2 < tau ? __dadd_rn(d0[p], __dmul_rn(64.0, f1)) : d0[p];
+    }
+}
+
 // Feature planes 6 and 7: the network's spread (full-resolution px / 16)
 // and its peak probability - 0.5, per pixel of the last pass.
 __global__ void k_band_conf(const double *__restrict__ spread, const double *__restrict__ pmax,
@@ -516,6 +528,18 @@ size_t sv_band_features_workspace_size(int W, int H) {
     cv.take<uint64_t>((size_t)W * H);
     cv.take<uint64_t>((size_t)W * H);
     return cv.off;
+}
+
+int sv_band_rule_centre(const float *feat, const double *disp0, int W, int H, double tau,
+                        double *centre, void *stream) {
+    if (!feat || !disp0 || !centre) { set_error("NULL argument"); return SV_ERR_NULL; }
+    if (W < 1 || H < 1) { set_error("bad shape %dx%d", W, H); return SV_ERR_SHAPE; }
+    if (!std::isfinite(tau)) { set_error("tau must be finite"); return SV_ERR_PARAM; }
+    const long N = (long)W * H;
+    count_launch();
+    k_band_rule<<<grid_for(N, 256), 256, 0, (cudaStream_t)stream>>>(feat, disp0, N, tau, centre);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
 }
 
 int sv_band_conf_features(const double *spread, const double *pmax, int W, int H, float *feat,

@@ -414,6 +414,11 @@ int sv_band_features(const void *left, const void *right, int dtype,
                      void *workspace, size_t workspace_bytes, void *stream);
 int sv_band_conf_features(const double *spread, const double *pmax, int W, int H, float *feat,
                           void *stream);
+/* The rule centre the learned band refines around: disp0 + 64 * feat[1]
+ * (the wide search's first argmin) where feat[2] (its 9-row census cost /
+ * 558) < tau, else disp0 (FP64). */
+int sv_band_rule_centre(const float *feat, const double *disp0, int W, int H, double tau,
+                        double *centre, void *stream);
 
 /* forward of nb items: feat [nb][8][H][W] -> out [nb][2][H][W] */
 size_t sv_band_workspace_size(int nb, int W, int H);

@@ -264,6 +264,14 @@ def band_features(left, right, disp0, W, H, dmax, spread=None, pmax=None) -> np.
     return out
 
 
+def band_rule_centre(feat, disp0, W, H, tau) -> np.ndarray:
+    """disp0 + 64 * f1 where f2 < tau, else disp0 (the learned band's base)."""
+    N = W * H
+    f = np.asarray(feat, dtype=np.float32).astype(np.float64).reshape(-1, N)
+    d0 = _f64(disp0)
+    return np.where(f[2] < tau, d0 + 64.0 * f[1], d0)
+
+
 def band_forward(params, feat, nb, W, H) -> np.ndarray:
     params, feat = _f64(params), _f64(feat)
     out = np.zeros(nb * 2 * W * H)

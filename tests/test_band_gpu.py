@@ -142,3 +142,13 @@ def test_training_lowers_loss(svb, orc):
         net.train_step(ft, tt, mt, nb, W, H, lr=2e-3)
     _, l1 = net.grads(f, t, m, nb, W, H)
     assert l1.item() < 0.8 * l0, (l0, l1.item())
+
+
+def test_rule_centre_vs_oracle(svb, orc):
+    W, H = 64, 48
+    p, d0 = _pair(svb, W, H, 77)
+    f = orc.band_features(p.gray("left"), p.gray("right"), d0, W, H, 80)
+    for tau in (0.1, 0.3, 1.1):
+        got = svb.band.rule_centre(f.astype(np.float32), d0, W, H, tau).cpu().numpy()
+        ref = orc.band_rule_centre(f, d0, W, H, tau)
+        assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))

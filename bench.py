@@ -53,9 +53,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="full",
                     choices=["full", "small", "batched", "refine_disparity", "read_image",
-                             "train"])
+                             "train", "band"])
     ap.add_argument("--pairs", type=int, default=256, help="pairs of the batched workload")
     ap.add_argument("--batch", type=int, default=64, help="crops per step of the train workload")
+    ap.add_argument("--band-pairs", type=int, default=48,
+                    help="held-out 640x480 pairs of the band workload")
     ap.add_argument("--cpu-leg", default=None, choices=["pair", "refpy", "batch16"],
                     help=argparse.SUPPRESS)          # child process: one CPU baseline leg
     ap.add_argument("--clock-sampler", default=None, help=argparse.SUPPRESS)
@@ -677,6 +679,44 @@ def run_batched(args, rank, world, local):
     return res
 
 
+def run_band(args, rank, world, local):
+    """The learned-band workload on held-out 640x480 pairs (disparities
+    30-150 px, thin bars, 30% low texture): every method after the same FP32
+    predict_auto -- the fixed +-10 band, the no-net rule, the learned band
+    (weights/band_weights.npz) and full-range SGM -- scored against the
+    generator's ground truth (EPE, bad2 = share of valid pixels off by more
+    than 2 px) and timed per pair with CUDA events.  One rank."""
+    if rank != 0:
+        return None
+    import __graft_entry__
+    pkg = __graft_entry__.load_package()
+    bt = pkg.band_train
+    pool = bt.make_pool()                        # before any CUDA call
+    import torch
+    torch.cuda.set_device(local)
+    band = pkg.band.BandNet.load()
+    with ClockSampler(local) as clk:
+        res = bt.evaluate(pkg, pool, band, args.band_pairs)
+    pool.close()
+    acc = {k: {m: round(v, 6) if isinstance(v, float) else v for m, v in res[k].items()}
+           for k in ("fixed_pm10", "rule_no_net", "learned", "full_range")}
+    return {
+        "metric": "learned-band refined Mpix/s per B200 (640x480, incl. predict_auto)",
+        "value": round(res["learned"]["mpix_s"], 3), "unit": "Mpix/s", "n_gpus": 1,
+        "steps": args.band_pairs, "warmup": 2,
+        "ms_per_step": round(640 * 480 / res["learned"]["mpix_s"] / 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 network, bf16 band net (tensor cores), integer refinement",
+        "data": "synthetic (seeded held-out pairs, seeds from %d)" % bt.TEST_SEED0,
+        "config": {"workload": "%d held-out 640x480 pairs, disparities 30-150 px, 1-3 bars "
+                               "2-6 px, 30%% low texture; band search 0..%d" % (args.band_pairs,
+                                                                              bt.DMAX),
+                   "pairs_per_step_per_gpu": 1, "parallelism": "replicas x1"},
+        "accuracy": acc,
+        "cpu_baseline": None, "e2e": None, "clocks": clk.summary(),
+    }
+
+
 def pseudo_rgb(pair):
     """An RGB image for plane_snap's SLIC: the left gray level and two smooth
     transforms of it, interleaved, in [0, 1] (as read_image returns)."""
@@ -1107,6 +1147,8 @@ def main():
         res = run_image(args, rank, world, local)
     elif args.workload == "train":
         res = run_train(args, rank, world, local)
+    elif args.workload == "band":
+        res = run_band(args, rank, world, local)
     else:
         res = run_ours(args, rank, world, local)
     if res is not None and rank == 0:

@@ -688,16 +688,19 @@ def run_band(args, rank, world, local):
     than 2 px) and timed per pair with CUDA events.  One rank."""
     if rank != 0:
         return None
-    import __graft_entry__
-    pkg = __graft_entry__.load_package()
-    bt = pkg.band_train
-    pool = bt.make_pool()                        # before any CUDA call
-    import torch
-    torch.cuda.set_device(local)
-    band = pkg.band.BandNet.load()
+    # the harness's own eval command in a child process (its generator pool
+    # spawns workers that import the harness as a script)
+    rep = tempfile.mktemp(suffix=".json")
+    harness = os.path.join(REPO, "from-scratch-stereo-vision_b200", "band_train.py")
     with ClockSampler(local) as clk:
-        res = bt.evaluate(pkg, pool, band, args.band_pairs)
-    pool.close()
+        r = subprocess.run([sys.executable, harness, "eval", "--pairs", str(args.band_pairs),
+                            "--report", rep], capture_output=True, text=True, timeout=3600,
+                           cwd=REPO)
+    if r.returncode != 0:
+        raise RuntimeError("band evaluation failed: %s" % r.stderr.strip()[-600:])
+    res = json.load(open(rep))["test"]
+    os.unlink(rep)
+    TEST_SEED0, DMAX = 3_000_000, 160
     acc = {k: {m: round(v, 6) if isinstance(v, float) else v for m, v in res[k].items()}
            for k in ("fixed_pm10", "rule_no_net", "learned", "full_range")}
     return {
@@ -707,10 +710,10 @@ def run_band(args, rank, world, local):
         "ms_per_step": round(640 * 480 / res["learned"]["mpix_s"] / 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 network, bf16 band net (tensor cores), integer refinement",
-        "data": "synthetic (seeded held-out pairs, seeds from %d)" % bt.TEST_SEED0,
+        "data": "synthetic (seeded held-out pairs, seeds from %d)" % TEST_SEED0,
         "config": {"workload": "%d held-out 640x480 pairs, disparities 30-150 px, 1-3 bars "
                                "2-6 px, 30%% low texture; band search 0..%d" % (args.band_pairs,
-                                                                              bt.DMAX),
+                                                                              DMAX),
                    "pairs_per_step_per_gpu": 1, "parallelism": "replicas x1"},
         "accuracy": acc,
         "cpu_baseline": None, "e2e": None, "clocks": clk.summary(),

@@ -350,7 +350,7 @@ def hbm_peak():
 def sgm_traffic(K, N):
     """DRAM bytes per SGM launch from the committed ncu summary, scaled to
     this launch's pixel count (traffic grows with the pixels swept)."""
-    p = os.path.join(REPO, "profiles", "ncu_sgm_thread_450x375.md")
+    p = os.path.join(REPO, "profiles", "ncu_sgm_group_450x375.md")
     if not os.path.exists(p):
         return None
     per_px = None

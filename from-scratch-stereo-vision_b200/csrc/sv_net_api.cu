@@ -659,13 +659,17 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     const int pw = probe_width < W ? probe_width : W;
     int ph = (int)(H * pw / (double)W + 0.5);
     if (ph < 8) ph = 8;
-    sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, precision, left, right, disp_full,
+    // BF16 runs only where no work-width decision follows: the probe and the
+    // passes whose 95% quantile picks the next width stay FP32, so the widths
+    // are FP32's; the last permitted pass (no select after it) runs at the
+    // requested precision.
+    sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, SV_FP32, left, right, disp_full,
                      disp_work, workspace};
     double *slot = nullptr;
     SV_TRY(run_stage(mnet, key, st, true, &slot, [&](double *mirror) -> int {
         int rc = check_net_shape(net->view, ph, pw);
         if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh);
-        if (!rc) rc = predict_f32(net, w, pw, ph, precision, st, true);
+        if (!rc) rc = predict_f32(net, w, pw, ph, SV_FP32, st, true);
         const long np = (long)pw * ph;
         const long long rank = (long long)(np * 0.95);
         if (!rc && np <= 16384) rc = launch_select_small_f32(w.d2, np, rank, w.sel, st, mirror);
@@ -685,7 +689,8 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     // when another pass may follow
     for (int pass = 1;; ++pass) {
         const bool with_sel = pass < passes;
-        sv_graph_key k{1, W, H, dtype, work, with_sel ? 1 : 0, precision, left, right, disp_full,
+        const int prec = with_sel ? SV_FP32 : precision;
+        sv_graph_key k{1, W, H, dtype, work, with_sel ? 1 : 0, prec, left, right, disp_full,
                        disp_work, workspace};
         int Ww, Hw;
         SV_TRY(run_stage(mnet, k, st, with_sel, &slot, [&](double *mirror) -> int {
@@ -694,7 +699,7 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
             const long long rank = (long long)((long)W * H * 0.95);
             const bool fuse = with_sel && work < W && nf > select_small_cap();
             const SelFuse sf{w.sel, w.hist, rank};
-            int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, precision,
+            int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, prec,
                                            disp_full, disp_work, &Ww, &Hw, st,
                                            fuse ? &sf : nullptr);
             if (!rc && fuse)

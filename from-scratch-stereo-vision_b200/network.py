@@ -114,7 +114,8 @@ def _f32(x, n, name):
 def _precision(precision) -> int:
     """"fp32" (default) or "bf16": FeatureNet and CostFilter c1/c2 as BF16
     tensor-core GEMMs with FP32 accumulation (soft-argmin and Refinement stay
-    FP32)."""
+    FP32).  In predict_auto BF16 applies to the last permitted pass only --
+    the one no work-width decision follows -- so the widths are FP32's."""
     codes = {"fp32": _lib.SV_FP32, "bf16": _lib.SV_BF16, _lib.SV_FP32: _lib.SV_FP32,
              _lib.SV_BF16: _lib.SV_BF16}
     if precision not in codes:

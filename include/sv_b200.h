@@ -247,7 +247,10 @@ int sv_stereonet_forward(const sv_net *net, const float *left, const float *righ
  * `dtype`.  disp_full: FP64 [H][W]; disp_work: FP64, at least W*H elements.
  * The work-width choice needs the peak of each pass on the host, so this
  * call synchronises the stream once per pass.  *work_trace (optional, at
- * least passes+1 ints) receives the work widths tried, 0-terminated. */
+ * least passes+1 ints) receives the work widths tried, 0-terminated.
+ * precision = SV_BF16 applies to the last permitted pass only (the one no
+ * work-width decision follows); the probe and the passes whose 95%
+ * quantile picks the next width run FP32, so the widths chosen are FP32's. */
 size_t sv_predict_workspace_size(const sv_net *net, int W, int H, int max_width);
 int sv_predict_auto(const sv_net *net, const void *left, const void *right,
                     int dtype, int W, int H, double target_peak, int probe_width,

@@ -402,6 +402,122 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
                                             net_slab(resid, L, p));
 }
 
+// Batched stride-1 convolutions with every output channel in one thread
+// (OC <= 8), two pixels 16 columns apart per thread: the throughput form of
+// k_conv2d_tiled<IC, OC, *, ACT, CS> for the batch.  It keeps that kernel's
+// arithmetic exactly -- each of the CS channel groups' partial sums is its
+// own fmaf chain over (channel, ky, kx) in the same order, combined as the
+// butterfly combines them ((s0 + s1) + (s2 + s3) for CS = 4, s0 + s1 for
+// CS = 2), then the bias and the activation -- so a pair's result is
+// bit-identical to its single-pair run, with one staged input tile for all
+// output channels and half the shared-memory loads per FMA.
+constexpr int CTB_TW = 32, CTB_TH = 4;          // output tile (threads: 16 x 4)
+
+template <int IC, int OC, int ACT, int CS>
+__device__ __forceinline__ void conv2d_wide_body(int bx, int by, const float *__restrict__ x,
+                                                 int H, int W, int dil,
+                                                 const float *__restrict__ w,
+                                                 const float *__restrict__ b, float *y,
+                                                 const float *__restrict__ resid) {
+    constexpr int CPS = IC / CS, NT = (CTB_TW / 2) * CTB_TH;
+    static_assert(IC % CS == 0 && (CS == 1 || CS == 2 || CS == 4) && OC <= 8, "shape");
+    extern __shared__ __align__(16) float tile[];
+    __shared__ __align__(16) float sw[IC * 9 * 8];
+    __shared__ float sb[8];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < IC * 9 * 8; i += NT) {
+        const int o = i & 7, ct = i >> 3;             // ct = c * 9 + tap
+        sw[i] = o < OC ? w[o * IC * 9 + ct] : 0.f;
+    }
+    if (tid < 8) sb[tid] = tid < OC ? b[tid] : 0.f;
+    const int ox0 = bx * CTB_TW, oy0 = by * CTB_TH;
+    const int ix0 = ox0 - dil, iy0 = oy0 - dil;
+    const int tw = CTB_TW + 2 * dil, th = CTB_TH + 2 * dil;
+    const long HW = (long)H * W;
+    for (int i = tid; i < IC * th * tw; i += NT) {
+        const int c = i / (th * tw);
+        const int rem = i - c * th * tw;
+        const int ty = rem / tw, tx = rem - ty * tw;
+        const int gy = iy0 + ty, gx = ix0 + tx;
+        tile[i] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? __ldg(x + c * HW + (long)gy * W + gx)
+                                                           : 0.0f;
+    }
+    __syncthreads();
+    const int lx = tid % (CTB_TW / 2), ly = tid / (CTB_TW / 2);
+    float acc[CS][2][OC];
+#pragma unroll
+    for (int g = 0; g < CS; ++g)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int o = 0; o < OC; ++o) acc[g][q][o] = 0.f;
+#pragma unroll
+    for (int g = 0; g < CS; ++g)
+#pragma unroll
+        for (int j = 0; j < CPS; ++j) {
+            const int c = g * CPS + j;
+            const float *tc = tile + c * th * tw;
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                const float *row = tc + (ly + ky * dil) * tw + lx;
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) {
+                    const float v0 = row[kx * dil], v1 = row[kx * dil + CTB_TW / 2];
+                    const float *wt = sw + (c * 9 + ky * 3 + kx) * 8;
+                    const float4 wa = *reinterpret_cast<const float4 *>(wt);
+                    const float4 wb = *reinterpret_cast<const float4 *>(wt + 4);
+                    const float wv[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+                    for (int o = 0; o < OC; ++o) {
+                        acc[g][0][o] = fmaf(v0, wv[o], acc[g][0][o]);
+                        acc[g][1][o] = fmaf(v1, wv[o], acc[g][1][o]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int ox = ox0 + lx + q * (CTB_TW / 2), oy = oy0 + ly;
+        if (ox >= W || oy >= H) continue;
+        const long oi = (long)oy * W + ox;
+#pragma unroll
+        for (int o = 0; o < OC; ++o) {
+            float s;
+            if (CS == 4) s = (acc[0][q][o] + acc[1][q][o]) + (acc[2][q][o] + acc[3][q][o]);
+            else if (CS == 2) s = acc[0][q][o] + acc[1][q][o];
+            else s = acc[0][q][o];
+            float v = s + sb[o];
+            if (ACT == 1) v = v > 0.f ? v : v * 0.2f;
+            if (ACT == 2) {
+                v = resid[oi] + v;
+                v = v > 0.f ? v : v * 0.f;
+            }
+            y[o * HW + oi] = v;
+        }
+    }
+}
+
+// Batched Refinement convolution at level lv (0: work / 2, 1: work size).
+template <int IC, int OC, int ACT, int CS>
+__global__ void __launch_bounds__((CTB_TW / 2) * CTB_TH)
+    k_b_conv2d_wide(NetLaunch L, int lv, const float *x, int dil, const float *__restrict__ w,
+                    const float *__restrict__ b, float *y, const float *resid) {
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    const int H = lv ? P.Hw : P.Hw / 2, W = lv ? P.Ww : P.Ww / 2;
+    const int tx = (W + CTB_TW - 1) / CTB_TW, ty = (H + CTB_TH - 1) / CTB_TH;
+    const int bx = (int)(c % tx), by = (int)(c / tx);
+    if (by >= ty) return;
+    conv2d_wide_body<IC, OC, ACT, CS>(bx, by, net_slab(x, L, p), H, W, dil, w, b,
+                                      net_slab(y, L, p), net_slab(resid, L, p));
+}
+
+static size_t conv2d_wide_bytes(int IC, int dil) {
+    return (size_t)IC * (CTB_TW + 2 * dil) * (CTB_TH + 2 * dil) * sizeof(float);
+}
+
 // A Refinement level's first convolution (2 -> RC, stride 1, dilation dil,
 // leaky ReLU) with the level's input built while staging: channel 0 is
 // 2 * bilinear(prev) (BilinearUpsample.forward's half-pixel taps, FP64
@@ -1142,7 +1258,7 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
     const int D = n.D;
     auto L = [&](int k) { return NetLaunch{g.pre[k], g.pairs, g.n, g.slab}; };
     auto B = [&](int k) { return ctas_of(g.total[k]); };
-    const int tb1 = CT2_TW * CT2_TH, tb2 = 2 * tb1, tb4 = 4 * tb1;
+    const int tb1 = CT2_TW * CT2_TH, tb2 = 2 * tb1;
     const dim3 tb(CT2_TW, CT2_TH);
     constexpr int FG = C % 4 == 0 ? 4 : C;
     constexpr int ZF = 2 * (C / FG);
@@ -1190,7 +1306,15 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
             if (i == 0)
                 k_b_conv2d_up<RC, RG><<<B(kk), tb, conv2d_tile_bytes(2, 1, dl), st>>>(
                     L(kk), lv, prevs[lv], guides[lv], dl, n.rw[lv][i], n.rb[lv][i], dst, s.f.rin);
-            else
+            else if (RC <= 8) {     // every output channel per thread (same arithmetic)
+                if (conv2d_wide_bytes(RC, dl) > 48 * 1024)
+                    cudaFuncSetAttribute(k_b_conv2d_wide<RC, RC, 1, RS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)conv2d_wide_bytes(RC, dl));
+                k_b_conv2d_wide<RC, RC, 1, RS><<<B(kf), (CTB_TW / 2) * CTB_TH,
+                                                 conv2d_wide_bytes(RC, dl), st>>>(
+                    L(kf), lv, cur, dl, n.rw[lv][i], n.rb[lv][i], dst, nullptr);
+            } else
                 k_b_conv2d_tiled<RC, RC, RG, 1, RS><<<B(kk), RS * tb1,
                                                       conv2d_tile_bytes(RC, 1, dl, RS), st>>>(
                     L(kk), 3 + lv, RC / RG, cur, cur, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst,
@@ -1198,9 +1322,9 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
             cur = dst;
         }
         count_launch();
-        k_b_conv2d_tiled<RC, 1, 1, 2, 4><<<B(kf), tb4, conv2d_tile_bytes(RC, 1, 1, 4), st>>>(
-            L(kf), 3 + lv, 1, cur, cur, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
-            outs[lv], s.f.rin);
+        k_b_conv2d_wide<RC, 1, 2, 4><<<B(kf), (CTB_TW / 2) * CTB_TH, conv2d_wide_bytes(RC, 1),
+                                        st>>>(L(kf), lv, cur, 1, n.rw[lv][n.ndil],
+                                              n.rb[lv][n.ndil], outs[lv], s.f.rin);
         SV_LAUNCH_CHECK();
     }
     return SV_OK;

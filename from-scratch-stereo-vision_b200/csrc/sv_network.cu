@@ -402,37 +402,40 @@ __global__ void __launch_bounds__(CT2_TW *CT2_TH *CS)
                                             net_slab(resid, L, p));
 }
 
-// Batched stride-1 convolutions with every output channel in one thread
-// (OC <= 8), two pixels 16 columns apart per thread: the throughput form of
-// k_conv2d_tiled<IC, OC, *, ACT, CS> for the batch.  It keeps that kernel's
-// arithmetic exactly -- each of the CS channel groups' partial sums is its
-// own fmaf chain over (channel, ky, kx) in the same order, combined as the
-// butterfly combines them ((s0 + s1) + (s2 + s3) for CS = 4, s0 + s1 for
-// CS = 2), then the bias and the activation -- so a pair's result is
-// bit-identical to its single-pair run, with one staged input tile for all
-// output channels and half the shared-memory loads per FMA.
-constexpr int CTB_TW = 32, CTB_TH = 4;          // output tile (threads: 16 x 4)
+// 3x3 convolutions (padding = dilation; stride S = 1, or 2 with dilation 1)
+// with every output channel in one thread and PX pixels per thread, CTB_TW /
+// PX columns apart: the register-blocked form of k_conv2d_tiled<IC, OC, *,
+// ACT, CS>.  It keeps that kernel's arithmetic exactly -- each of the CS
+// channel groups' partial sums is its own fmaf chain over (channel, ky, kx)
+// in the same order, combined as the butterfly combines them ((s0 + s1) +
+// (s2 + s3) for CS = 4, s0 + s1 for CS = 2), then the bias and the activation
+// -- so its results are bit-identical to that kernel's, from one staged
+// input tile for all output channels and one 16-byte weight vector per 4
+// output channels, read by the whole warp at once.
+constexpr int CTB_TW = 32, CTB_TH = 4;          // output tile of a CTA
 
-template <int IC, int OC, int ACT, int CS>
+template <int IC, int OC, int ACT, int CS, int PX, int S>
 __device__ __forceinline__ void conv2d_wide_body(int bx, int by, const float *__restrict__ x,
-                                                 int H, int W, int dil,
+                                                 int H, int W, int OH, int OW, int dil,
                                                  const float *__restrict__ w,
                                                  const float *__restrict__ b, float *y,
                                                  const float *__restrict__ resid) {
-    constexpr int CPS = IC / CS, NT = (CTB_TW / 2) * CTB_TH;
-    static_assert(IC % CS == 0 && (CS == 1 || CS == 2 || CS == 4) && OC <= 8, "shape");
+    constexpr int CPS = IC / CS, TXP = CTB_TW / PX, NT = TXP * CTB_TH;
+    constexpr int OCP = (OC + 3) / 4 * 4;
+    static_assert(IC % CS == 0 && (CS == 1 || CS == 2 || CS == 4) && OC <= 16, "shape");
+    static_assert(CTB_TW % PX == 0 && (S == 1 || S == 2), "tile");
     extern __shared__ __align__(16) float tile[];
-    __shared__ __align__(16) float sw[IC * 9 * 8];
-    __shared__ float sb[8];
+    __shared__ __align__(16) float sw[IC * 9 * OCP];
+    __shared__ float sb[OCP];
     const int tid = threadIdx.x;
-    for (int i = tid; i < IC * 9 * 8; i += NT) {
-        const int o = i & 7, ct = i >> 3;             // ct = c * 9 + tap
+    for (int i = tid; i < IC * 9 * OCP; i += NT) {
+        const int o = i % OCP, ct = i / OCP;          // ct = c * 9 + tap
         sw[i] = o < OC ? w[o * IC * 9 + ct] : 0.f;
     }
-    if (tid < 8) sb[tid] = tid < OC ? b[tid] : 0.f;
+    if (tid < OCP) sb[tid] = tid < OC ? b[tid] : 0.f;
     const int ox0 = bx * CTB_TW, oy0 = by * CTB_TH;
-    const int ix0 = ox0 - dil, iy0 = oy0 - dil;
-    const int tw = CTB_TW + 2 * dil, th = CTB_TH + 2 * dil;
+    const int ix0 = ox0 * S - dil, iy0 = oy0 * S - dil;
+    const int tw = (CTB_TW - 1) * S + 2 * dil + 1, th = (CTB_TH - 1) * S + 2 * dil + 1;
     const long HW = (long)H * W;
     for (int i = tid; i < IC * th * tw; i += NT) {
         const int c = i / (th * tw);
@@ -443,12 +446,12 @@ __device__ __forceinline__ void conv2d_wide_body(int bx, int by, const float *__
                                                            : 0.0f;
     }
     __syncthreads();
-    const int lx = tid % (CTB_TW / 2), ly = tid / (CTB_TW / 2);
-    float acc[CS][2][OC];
+    const int lx = tid % TXP, ly = tid / TXP;
+    float acc[CS][PX][OC];
 #pragma unroll
     for (int g = 0; g < CS; ++g)
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
+        for (int q = 0; q < PX; ++q)
 #pragma unroll
             for (int o = 0; o < OC; ++o) acc[g][q][o] = 0.f;
 #pragma unroll
@@ -459,27 +462,33 @@ __device__ __forceinline__ void conv2d_wide_body(int bx, int by, const float *__
             const float *tc = tile + c * th * tw;
 #pragma unroll
             for (int ky = 0; ky < 3; ++ky) {
-                const float *row = tc + (ly + ky * dil) * tw + lx;
+                const float *row = tc + (ly * S + ky * dil) * tw + lx * S;
 #pragma unroll
                 for (int kx = 0; kx < 3; ++kx) {
-                    const float v0 = row[kx * dil], v1 = row[kx * dil + CTB_TW / 2];
-                    const float *wt = sw + (c * 9 + ky * 3 + kx) * 8;
-                    const float4 wa = *reinterpret_cast<const float4 *>(wt);
-                    const float4 wb = *reinterpret_cast<const float4 *>(wt + 4);
-                    const float wv[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+                    float v[PX];
 #pragma unroll
-                    for (int o = 0; o < OC; ++o) {
-                        acc[g][0][o] = fmaf(v0, wv[o], acc[g][0][o]);
-                        acc[g][1][o] = fmaf(v1, wv[o], acc[g][1][o]);
+                    for (int q = 0; q < PX; ++q) v[q] = row[kx * dil + q * TXP * S];
+                    const float *wt = sw + (c * 9 + ky * 3 + kx) * OCP;
+#pragma unroll
+                    for (int o4 = 0; o4 < OCP; o4 += 4) {
+                        const float4 w4 = *reinterpret_cast<const float4 *>(wt + o4);
+                        const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (o4 + k < OC)
+#pragma unroll
+                                for (int q = 0; q < PX; ++q)
+                                    acc[g][q][o4 + k] = fmaf(v[q], wv[k], acc[g][q][o4 + k]);
                     }
                 }
             }
         }
+    const long OHW = (long)OH * OW;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-        const int ox = ox0 + lx + q * (CTB_TW / 2), oy = oy0 + ly;
-        if (ox >= W || oy >= H) continue;
-        const long oi = (long)oy * W + ox;
+    for (int q = 0; q < PX; ++q) {
+        const int ox = ox0 + lx + q * TXP, oy = oy0 + ly;
+        if (ox >= OW || oy >= OH) continue;
+        const long oi = (long)oy * OW + ox;
 #pragma unroll
         for (int o = 0; o < OC; ++o) {
             float s;
@@ -492,30 +501,48 @@ __device__ __forceinline__ void conv2d_wide_body(int bx, int by, const float *__
                 v = resid[oi] + v;
                 v = v > 0.f ? v : v * 0.f;
             }
-            y[o * HW + oi] = v;
+            y[o * OHW + oi] = v;
         }
     }
 }
 
-// Batched Refinement convolution at level lv (0: work / 2, 1: work size).
-template <int IC, int OC, int ACT, int CS>
-__global__ void __launch_bounds__((CTB_TW / 2) * CTB_TH)
-    k_b_conv2d_wide(NetLaunch L, int lv, const float *x, int dil, const float *__restrict__ w,
-                    const float *__restrict__ b, float *y, const float *resid) {
+// The batched form: level lv of conv_level, Z images (1 or 2) per pair.
+template <int IC, int OC, int ACT, int CS, int PX, int S>
+__global__ void __launch_bounds__(CTB_TW / PX * CTB_TH)
+    k_b_conv2d_wide(NetLaunch L, int lv, int Z, const float *x0, const float *x1, int dil,
+                    const float *__restrict__ w, const float *__restrict__ b, float *y0,
+                    float *y1, const float *resid) {
     long long c;
     const int p = net_pair(L, c);
     const NetPair &P = L.pairs[p];
     if (!P.active) return;
-    const int H = lv ? P.Hw : P.Hw / 2, W = lv ? P.Ww : P.Ww / 2;
-    const int tx = (W + CTB_TW - 1) / CTB_TW, ty = (H + CTB_TH - 1) / CTB_TH;
-    const int bx = (int)(c % tx), by = (int)(c / tx);
+    int H, W, OH, OW;
+    conv_level(lv, P.Hw, P.Ww, H, W, OH, OW);
+    const int tx = (OW + CTB_TW - 1) / CTB_TW, ty = (OH + CTB_TH - 1) / CTB_TH;
+    const int img = (int)(c % Z);
+    const long long t = c / Z;
+    const int bx = (int)(t % tx), by = (int)(t / tx);
     if (by >= ty) return;
-    conv2d_wide_body<IC, OC, ACT, CS>(bx, by, net_slab(x, L, p), H, W, dil, w, b,
-                                      net_slab(y, L, p), net_slab(resid, L, p));
+    conv2d_wide_body<IC, OC, ACT, CS, PX, S>(bx, by, net_slab(img ? x1 : x0, L, p), H, W, OH,
+                                             OW, dil, w, b, net_slab(img ? y1 : y0, L, p),
+                                             net_slab(resid, L, p));
 }
 
-static size_t conv2d_wide_bytes(int IC, int dil) {
-    return (size_t)IC * (CTB_TW + 2 * dil) * (CTB_TH + 2 * dil) * sizeof(float);
+static size_t conv2d_wide_bytes(int IC, int S, int dil) {
+    return (size_t)IC * ((CTB_TW - 1) * S + 2 * dil + 1) * ((CTB_TH - 1) * S + 2 * dil + 1) *
+           sizeof(float);
+}
+
+template <int IC, int OC, int ACT, int CS, int PX, int S>
+static void b_conv2d_wide(const NetLaunch &L, unsigned ctas, int lv, int Z, const float *x0,
+                          const float *x1, int dil, const float *w, const float *b, float *y0,
+                          float *y1, const float *resid, cudaStream_t st) {
+    const size_t smem = conv2d_wide_bytes(IC, S, dil);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_b_conv2d_wide<IC, OC, ACT, CS, PX, S>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_b_conv2d_wide<IC, OC, ACT, CS, PX, S><<<ctas, CTB_TW / PX * CTB_TH, smem, st>>>(
+        L, lv, Z, x0, x1, dil, w, b, y0, y1, resid);
 }
 
 // A Refinement level's first convolution (2 -> RC, stride 1, dilation dil,
@@ -664,34 +691,101 @@ __host__ __device__ constexpr int c3_layout(int CS, int CPS, int TD, int which) 
 // Stages rows d0-1 .. d0+TD, y-1 .. y+1, x0-1 .. x0+8 of every channel.
 // CV: the cost volume of CostVolume.forward (stereonet.py:771-799) built on
 // the fly -- |fl(x) - fr(x - d)|, 2.0 where x - d < 0; else x is a C x D x h
-// x w volume.
-template <int C, int TD, int DS, int P, int NT, bool CV>
+// x w volume.  The global loads of C3_SB elements per thread are issued
+// before any of them is used, so a CTA waits for about one memory latency
+// per C3_SB elements instead of one per element (these small launches are
+// bound by that latency).
+constexpr int C3_SB = 8;
+
+template <int C, int TD, int DS, int P, int NT, bool CV, int RS = C3_RS>
 __device__ __forceinline__ void c3_stage(float *tile, const float *__restrict__ a,
                                          const float *__restrict__ bsrc, int D, int h, int w,
                                          int x0, int oy, int d0) {
-    constexpr int PER_C = (TD + 2) * 3 * C3_RS;
     const long hw = (long)h * w;
-    for (int i = threadIdx.x; i < C * PER_C; i += NT) {
-        const int c = i / PER_C;
-        int r = i - c * PER_C;
-        const int dz = r / (3 * C3_RS);
-        r -= dz * 3 * C3_RS;
-        const int ry = r / C3_RS, rx = r - ry * C3_RS;
-        const int dd = d0 - 1 + dz, yy = oy - 1 + ry, xx = x0 - 1 + rx;
-        float v = 0.f;
-        if (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w) {
-            if (CV) {
-                if (xx - dd < 0) {
-                    v = 2.0f;
-                } else {
-                    const long row = c * hw + (long)yy * w;
-                    v = fabsf(__ldg(a + row + xx) - __ldg(bsrc + row + xx - dd));
+    if constexpr (CV) {
+        // The cost volume reads each left-feature value of the tile's rows
+        // once per disparity and each right-feature value once per (x, d)
+        // with the same x - d: stage the distinct ones (3 rows x RS left,
+        // 3 rows x (RS + TD + 1) right per channel), then build the tile
+        // from shared memory, lane l < 30 of a warp owning tile row l / 10,
+        // column l % 10 and the warps taking the (channel, disparity)
+        // slices in turn.
+        constexpr int RW = RS + TD + 1, NL = C * 3 * RS, NR = C * 3 * RW;
+        constexpr int NW = NT / 32, G = C * (TD + 2);
+        __shared__ float sl[NL], sr[NR];
+        const int xr0 = x0 - 1 - (d0 + TD);
+        for (int i0 = threadIdx.x; i0 < NL + NR; i0 += NT * C3_SB) {
+            float v[C3_SB];
+#pragma unroll
+            for (int u = 0; u < C3_SB; ++u) {
+                const int i = i0 + u * NT;
+                v[u] = 0.f;
+                if (i < NL) {
+                    const int c = i / (3 * RS), r = i - c * 3 * RS;
+                    const int ry = r / RS, rx = r - ry * RS;
+                    const int yy = oy - 1 + ry, xx = x0 - 1 + rx;
+                    if (yy >= 0 && yy < h && xx >= 0 && xx < w)
+                        v[u] = __ldg(a + c * hw + (long)yy * w + xx);
+                } else if (i < NL + NR) {
+                    const int j = i - NL;
+                    const int c = j / (3 * RW), r = j - c * 3 * RW;
+                    const int ry = r / RW, k = r - ry * RW;
+                    const int yy = oy - 1 + ry, xx = xr0 + k;
+                    if (yy >= 0 && yy < h && xx >= 0 && xx < w)
+                        v[u] = __ldg(bsrc + c * hw + (long)yy * w + xx);
                 }
-            } else {
-                v = __ldg(a + (c * (long)D + dd) * hw + (long)yy * w + xx);
+            }
+#pragma unroll
+            for (int u = 0; u < C3_SB; ++u) {
+                const int i = i0 + u * NT;
+                if (i < NL) sl[i] = v[u];
+                else if (i < NL + NR) sr[i - NL] = v[u];
             }
         }
-        tile[c * P + dz * DS + ry * C3_RS + rx] = v;
+        __syncthreads();
+        const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+        for (int e = lane; e < 3 * RS; e += 32) {
+            const int ry = e / RS, rx = e - ry * RS;
+            const int yy = oy - 1 + ry, xx = x0 - 1 + rx;
+            const bool pix = yy >= 0 && yy < h && xx >= 0 && xx < w;
+            const float *slp = sl + e, *srp = sr + ry * RW + rx + TD + 1;
+            float *tl = tile + ry * RS + rx;
+#pragma unroll 4
+            for (int g = wp; g < G; g += NW) {
+                const int c = g / (TD + 2), dz = g - c * (TD + 2);
+                const int dd = d0 - 1 + dz;
+                float v = 0.f;
+                if (pix && dd >= 0 && dd < D)
+                    v = xx - dd < 0 ? 2.0f : fabsf(slp[c * 3 * RS] - srp[c * 3 * RW - dz]);
+                tl[c * P + dz * DS] = v;
+            }
+        }
+    } else {
+        constexpr int PER_C = (TD + 2) * 3 * RS, TOTAL = C * PER_C;
+        for (int i0 = threadIdx.x; i0 < TOTAL; i0 += NT * C3_SB) {
+            float va[C3_SB];
+            int slot[C3_SB];
+#pragma unroll
+            for (int u = 0; u < C3_SB; ++u) {
+                const int i = i0 + u * NT;
+                slot[u] = -1;
+                va[u] = 0.f;
+                if (i < TOTAL) {
+                    const int c = i / PER_C;
+                    int r = i - c * PER_C;
+                    const int dz = r / (3 * RS);
+                    r -= dz * 3 * RS;
+                    const int ry = r / RS, rx = r - ry * RS;
+                    const int dd = d0 - 1 + dz, yy = oy - 1 + ry, xx = x0 - 1 + rx;
+                    slot[u] = c * P + dz * DS + ry * RS + rx;
+                    if (dd >= 0 && dd < D && yy >= 0 && yy < h && xx >= 0 && xx < w)
+                        va[u] = __ldg(a + (c * (long)D + dd) * hw + (long)yy * w + xx);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < C3_SB; ++u)
+                if (slot[u] >= 0) tile[slot[u]] = va[u];
+        }
     }
 }
 
@@ -747,9 +841,16 @@ __device__ __forceinline__ void conv3d_split_body(int bx, int by, int bz, const 
     const int og = bz, nd = (D + TD - 1) / TD;
     const int x0 = bx * C3_TX, oy = by / nd, d0 = (by - oy * nd) * TD;
     const int tid = threadIdx.x;
-    for (int i = tid; i < C * 27 * OCG; i += 128) {
-        const int o = i % OCG, ct = i / OCG;       // ct = c * 27 + tap
-        sw[i] = __ldg(wt + (og * OCG + o) * C * 27 + ct);
+    for (int i0 = tid; i0 < C * 27 * OCG; i0 += 128 * C3_SB) {
+        float v[C3_SB];
+#pragma unroll
+        for (int u = 0; u < C3_SB; ++u) {
+            const int i = i0 + u * 128, o = i % OCG, ct = i / OCG;   // ct = c * 27 + tap
+            v[u] = i < C * 27 * OCG ? __ldg(wt + (og * OCG + o) * C * 27 + ct) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < C3_SB; ++u)
+            if (i0 + u * 128 < C * 27 * OCG) sw[i0 + u * 128] = v[u];
     }
     if (tid < OCG) sb[tid] = __ldg(bias + og * OCG + tid);
     c3_stage<C, TD, DS, P, 128, CV>(tile, a, bsrc, D, h, w, x0, oy, d0);
@@ -1098,7 +1199,7 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         const int rc = forward_bf16_front(n, left, right, H, W, h1, w1, h, w, b, st);
         if (rc) return rc;
     } else {
-        // FeatureNet, both images: c1 s2, c2 s2, c3, c4 (4 output channels per thread)
+        // FeatureNet, both images: c1 s2, c2 s2, c3, c4
         constexpr int FG = C % 4 == 0 ? 4 : C;
         const dim3 fg1 = tgrid(w1, h1, 2 * (C / FG)), fg = tgrid(w, h, 2 * (C / FG));
         count_launch();
@@ -1106,13 +1207,16 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
             left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
         count_launch();
         k_conv2d_tiled<C, C, FG, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 2, 1, 2), st>>>(
-            b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1], nullptr);
+            b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1],
+            nullptr);
         count_launch();
         k_conv2d_tiled<C, C, FG, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
-            b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1], nullptr);
+            b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1],
+            nullptr);
         count_launch();
         k_conv2d_tiled<C, C, FG, 0, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
-            b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1], nullptr);
+            b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1],
+            nullptr);
         SV_LAUNCH_CHECK();
         // cost volume + CostFilter c1, c2 (every output channel in each CTA,
         // so the tile is staged once)
@@ -1295,6 +1399,7 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
     const float *guides[2] = {s.gh, s.lw};
     const float *prevs[2] = {s.d0, s.d1};
     float *outs[2] = {s.d1, s.d2};
+    const bool tiled = RC > 8;     // the register-blocked form holds at most 8 channels
     for (int lv = 0; lv < 2; ++lv) {
         const int kk = lv ? NK_R1 : NK_R0, kf = lv ? NK_R1F : NK_R0F;
         float *bufs[2] = {s.f.ra, s.f.rb};
@@ -1306,15 +1411,11 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
             if (i == 0)
                 k_b_conv2d_up<RC, RG><<<B(kk), tb, conv2d_tile_bytes(2, 1, dl), st>>>(
                     L(kk), lv, prevs[lv], guides[lv], dl, n.rw[lv][i], n.rb[lv][i], dst, s.f.rin);
-            else if (RC <= 8) {     // every output channel per thread (same arithmetic)
-                if (conv2d_wide_bytes(RC, dl) > 48 * 1024)
-                    cudaFuncSetAttribute(k_b_conv2d_wide<RC, RC, 1, RS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)conv2d_wide_bytes(RC, dl));
-                k_b_conv2d_wide<RC, RC, 1, RS><<<B(kf), (CTB_TW / 2) * CTB_TH,
-                                                 conv2d_wide_bytes(RC, dl), st>>>(
-                    L(kf), lv, cur, dl, n.rw[lv][i], n.rb[lv][i], dst, nullptr);
-            } else
+            else if (!tiled)
+                b_conv2d_wide<RC, RC, 1, RS, 2, 1>(L(kf), B(kf), lv + 3, 1, cur, cur, dl,
+                                                   n.rw[lv][i], n.rb[lv][i], dst, dst, nullptr,
+                                                   st);
+            else
                 k_b_conv2d_tiled<RC, RC, RG, 1, RS><<<B(kk), RS * tb1,
                                                       conv2d_tile_bytes(RC, 1, dl, RS), st>>>(
                     L(kk), 3 + lv, RC / RG, cur, cur, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst,
@@ -1322,9 +1423,15 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
             cur = dst;
         }
         count_launch();
-        k_b_conv2d_wide<RC, 1, 2, 4><<<B(kf), (CTB_TW / 2) * CTB_TH, conv2d_wide_bytes(RC, 1),
-                                        st>>>(L(kf), lv, cur, 1, n.rw[lv][n.ndil],
-                                              n.rb[lv][n.ndil], outs[lv], s.f.rin);
+        if (!tiled)
+            b_conv2d_wide<RC, 1, 2, 4, 2, 1>(L(kf), B(kf), lv + 3, 1, cur, cur, 1,
+                                             n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
+                                             outs[lv], s.f.rin, st);
+        else
+            k_b_conv2d_tiled<RC, 1, 1, 2, 4><<<B(kf), 4 * tb1, conv2d_tile_bytes(RC, 1, 1, 4),
+                                               st>>>(L(kf), 3 + lv, 1, cur, cur, 1, 1, 1,
+                                                     n.rw[lv][n.ndil], n.rb[lv][n.ndil],
+                                                     outs[lv], outs[lv], s.f.rin);
         SV_LAUNCH_CHECK();
     }
     return SV_OK;

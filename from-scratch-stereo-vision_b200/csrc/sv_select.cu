@@ -273,11 +273,13 @@ __global__ void __launch_bounds__(1024)
 
 // The probe's FP32 map: 32-bit order keys (the order of the floats is the
 // order of the FP64 values they convert to exactly; signed zeros share a
-// key), four 8-bit passes in one CTA of 256 threads -- one bin per thread,
-// so each pass's scan is one shuffle scan and an 8-term prefix -- with the
-// keys in shared memory.  Same result as the FP64 passes, a tenth of the
-// instructions at probe sizes.
-constexpr int SEL32_T = 256;
+// key), four 8-bit passes in one CTA of 1024 threads.  Up to SEL32_K keys a
+// thread stay in registers across the passes (loaded together, so the CTA
+// waits for one memory latency); larger maps (a tall pair's probe in a
+// batch) are read again each pass.  Threads 0..255 own one bin each, so a
+// pass's scan is one shuffle scan and an 8-term prefix.  Same result as the
+// FP64 passes, a small fraction of the instructions at probe sizes.
+constexpr int SEL32_T = 1024, SEL32_K = 16;
 
 __device__ __forceinline__ unsigned sel_key32(float f) {
     const unsigned b = __float_as_uint(f == 0.0f ? 0.0f : f);
@@ -288,127 +290,110 @@ __device__ __forceinline__ float sel_unkey32(unsigned k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
 }
 
-__global__ void __launch_bounds__(SEL32_T)
-    k_sel_small_f32(const float *__restrict__ x, int n, unsigned rank0,
-                    SelState *__restrict__ s, double *mirror) {
-    extern __shared__ unsigned keys32[];
-    __shared__ unsigned hist[SEL32_T];
-    __shared__ unsigned wsum[SEL32_T / 32];
+__device__ __forceinline__ void sel32_count(unsigned *hist, unsigned k, bool valid, unsigned pre,
+                                            int pass) {
+    const int shift = 24 - 8 * pass;
+    unsigned digit = 0xffffffffu;
+    if (valid && (pass == 0 || (k >> (shift + 8)) == (pre >> (shift + 8))))
+        digit = (k >> shift) & 255u;
+    const unsigned same = __match_any_sync(kFull, digit);
+    if (digit != 0xffffffffu && (threadIdx.x & 31) == __ffs(same) - 1)
+        atomicAdd(&hist[digit], __popc(same));
+}
+
+// The key of rank rank0 among the n values x[0..n) (whole CTA, 1024 threads).
+__device__ unsigned sel32_cta(const float *__restrict__ x, int n, unsigned rank0) {
+    __shared__ unsigned hist[256];
+    __shared__ unsigned wsum[8];
     __shared__ unsigned s_prefix, s_rank;
     const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    for (int i = t; i < n; i += SEL32_T) keys32[i] = sel_key32(__ldg(x + i));
+    const bool inreg = n <= SEL32_T * SEL32_K;          // the same for the whole CTA
+    const int nj = (n + SEL32_T - 1) / SEL32_T;
+    unsigned key[SEL32_K];
+    if (inreg) {
+#pragma unroll
+        for (int j = 0; j < SEL32_K; ++j) {
+            const int i = t + j * SEL32_T;
+            key[j] = i < n ? sel_key32(__ldg(x + i)) : 0u;
+        }
+    }
     if (t == 0) {
         s_prefix = 0u;
         s_rank = rank0;
     }
     for (int pass = 0; pass < 4; ++pass) {
         const int shift = 24 - 8 * pass;
-        hist[t] = 0u;
-        __syncthreads();                    // keys, bins and the prefix are ready
+        if (t < 256) hist[t] = 0u;
+        __syncthreads();                    // bins cleared, the prefix published
         const unsigned pre = s_prefix;
-        for (int i0 = 0; i0 < n; i0 += SEL32_T) {
-            const int i = i0 + t;
-            unsigned digit = 0xffffffffu;
-            if (i < n) {
-                const unsigned k = keys32[i];
-                if (pass == 0 || (k >> (shift + 8)) == (pre >> (shift + 8)))
-                    digit = (k >> shift) & 255u;
-            }
-            const unsigned same = __match_any_sync(kFull, digit);
-            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
-                atomicAdd(&hist[digit], __popc(same));
-        }
-        __syncthreads();
-        const unsigned c = hist[t];
-        unsigned incl = c;
+        if (inreg) {
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += y;
+            for (int j = 0; j < SEL32_K; ++j)
+                if (j < nj) sel32_count(hist, key[j], t + j * SEL32_T < n, pre, pass);
+        } else {
+            for (int j = 0; j < nj; ++j) {
+                const int i = t + j * SEL32_T;
+                sel32_count(hist, i < n ? sel_key32(__ldg(x + i)) : 0u, i < n, pre, pass);
+            }
         }
-        if (lane == 31) wsum[wid] = incl;
         __syncthreads();
-        unsigned excl = incl - c;
-        for (int w = 0; w < wid; ++w) excl += wsum[w];
-        const unsigned r = s_rank;
-        __syncthreads();                    // every thread has read the rank
-        if (r >= excl && r < excl + c) {    // exactly one bin holds the rank
+        unsigned c = 0u, incl = 0u;
+        if (t < 256) {
+            c = hist[t];
+            incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(kFull, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane == 31) wsum[wid] = incl;
+        }
+        __syncthreads();
+        unsigned excl = 0u, r = 0u;
+        if (t < 256) {
+            excl = incl - c;
+            for (int w = 0; w < wid; ++w) excl += wsum[w];
+            r = s_rank;
+        }
+        __syncthreads();                    // every bin owner has read the rank
+        if (t < 256 && r >= excl && r < excl + c) {   // exactly one bin holds it
             s_prefix = pre | ((unsigned)t << shift);
             s_rank = r - excl;
         }
     }
     __syncthreads();
-    if (t == 0) {
-        const double v = (double)sel_unkey32(s_prefix);
+    return s_prefix;
+}
+
+__global__ void __launch_bounds__(SEL32_T)
+    k_sel_small_f32(const float *__restrict__ x, int n, unsigned rank0,
+                    SelState *__restrict__ s, double *mirror) {
+    const unsigned k = sel32_cta(x, n, rank0);
+    if (threadIdx.x == 0) {
+        const double v = (double)sel_unkey32(k);
         s->prefix = sel_key(v);
-        s->rank = s_rank;
+        s->rank = 0;
         s->value = v;
         if (mirror) *reinterpret_cast<volatile double *>(mirror) = v;
     }
 }
 
 // Batched probe select: one CTA per pair over the probe's FP32 map (the
-// pass's Ww x Hw values), the same four 8-bit passes over 32-bit keys as
-// k_sel_small_f32 but with the keys read from global memory each pass, so a
-// tall pair's probe (more than SEL_SMALL_CAP values) needs no other path.
+// pass's Ww x Hw values), rank int(0.95 n) as _peak takes it.
 __global__ void __launch_bounds__(SEL32_T)
     k_b_sel_probe(NetLaunch L, const float *x0, SelState *s0) {
-    __shared__ unsigned hist[SEL32_T];
-    __shared__ unsigned wsum[SEL32_T / 32];
-    __shared__ unsigned s_prefix, s_rank;
     long long c;
     const int p = net_pair(L, c);
     const NetPair &P = L.pairs[p];
     if (!P.active) return;
-    const float *__restrict__ x = net_slab(x0, L, p);
-    SelState *s = net_slab(s0, L, p);
     const int n = P.Ww * P.Hw;
-    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-    if (t == 0) {
-        s_prefix = 0u;
-        s_rank = (unsigned)(long long)__dmul_rn((double)n, 0.95);
-    }
-    for (int pass = 0; pass < 4; ++pass) {
-        const int shift = 24 - 8 * pass;
-        hist[t] = 0u;
-        __syncthreads();
-        const unsigned pre = s_prefix;
-        for (int i0 = 0; i0 < n; i0 += SEL32_T) {
-            const int i = i0 + t;
-            unsigned digit = 0xffffffffu;
-            if (i < n) {
-                const unsigned k = sel_key32(__ldg(x + i));
-                if (pass == 0 || (k >> (shift + 8)) == (pre >> (shift + 8)))
-                    digit = (k >> shift) & 255u;
-            }
-            const unsigned same = __match_any_sync(kFull, digit);
-            if (digit != 0xffffffffu && lane == __ffs(same) - 1)
-                atomicAdd(&hist[digit], __popc(same));
-        }
-        __syncthreads();
-        const unsigned cnt = hist[t];
-        unsigned incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += y;
-        }
-        if (lane == 31) wsum[wid] = incl;
-        __syncthreads();
-        unsigned excl = incl - cnt;
-        for (int w = 0; w < wid; ++w) excl += wsum[w];
-        const unsigned r = s_rank;
-        __syncthreads();
-        if (r >= excl && r < excl + cnt) {
-            s_prefix = pre | ((unsigned)t << shift);
-            s_rank = r - excl;
-        }
-    }
-    __syncthreads();
-    if (t == 0) {
-        const double v = (double)sel_unkey32(s_prefix);
+    const unsigned k = sel32_cta(net_slab(x0, L, p), n,
+                                 (unsigned)(long long)__dmul_rn((double)n, 0.95));
+    if (threadIdx.x == 0) {
+        SelState *s = net_slab(s0, L, p);
+        const double v = (double)sel_unkey32(k);
         s->prefix = sel_key(v);
-        s->rank = s_rank;
+        s->rank = 0;
         s->value = v;
     }
 }
@@ -422,9 +407,6 @@ static int select_setup() {
         SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small<double>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(SEL_SMALL_CAP * sizeof(unsigned long long))));
-        SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_small_f32,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(SEL_SMALL_CAP * sizeof(unsigned))));
         SV_CUDA_TRY(cudaFuncSetAttribute(k_sel_compact,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(SEL_CAND_CAP * sizeof(unsigned long long))));
@@ -526,8 +508,7 @@ int launch_select_small_f32(const float *x, long n, long long rank, SelState *st
     const int rc = select_setup();
     if (rc) return rc;
     count_launch();
-    k_sel_small_f32<<<1, SEL32_T, (size_t)n * sizeof(unsigned), st>>>(x, (int)n, (unsigned)rank,
-                                                                       state, mirror);
+    k_sel_small_f32<<<1, SEL32_T, 0, st>>>(x, (int)n, (unsigned)rank, state, mirror);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

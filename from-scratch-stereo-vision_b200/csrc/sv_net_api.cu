@@ -12,6 +12,7 @@
 
 #include "sv_common.cuh"
 #include "sv_network.cuh"
+#include "sv_select.cuh"
 #include "sv_tc.cuh"
 
 // One captured predict_auto stage (a network pass, optionally with the peak
@@ -135,7 +136,8 @@ static int check_net_shape(const NetView &n, int H, int W) {
 
 static int width_for(int W, double target_peak, int max_width, double pk) {
     double m = pk > 1.0e-6 ? pk : 1.0e-6;
-    int w = (int)(W * target_peak / m + 0.5);
+    const double q = W * target_peak / m + 0.5;
+    int w = q < 2147483647.0 ? (q > -2147483648.0 ? (int)q : -2147483647 - 1) : 2147483647;
     if (w > W) w = W;
     if (w > max_width) w = max_width;
     if (w < 48) w = 48;
@@ -261,7 +263,8 @@ static int wait_slot(double *slot, cudaStream_t st, double *out);
 
 // The peak of the stage just queued on st (floored like _peak): from its
 // mapped slot when it published one, else copied out of the workspace.
-static int fetch_peak(const PredictWs &w, cudaStream_t st, double *slot, double *peak) {
+static int fetch_peak(const PredictWs &w, cudaStream_t st, double *slot, double *peak,
+                      bool floor = true) {
     double v = 0.0;
     if (slot) {
         SV_TRY(wait_slot(slot, st, &v));
@@ -286,7 +289,7 @@ static int fetch_peak(const PredictWs &w, cudaStream_t st, double *slot, double 
         SV_CUDA_TRY(cudaStreamSynchronize(st));
         v = *dst;
     }
-    *peak = v > 0.5 ? v : 0.5;                      // _peak's floor
+    *peak = !floor || v > 0.5 ? v : 0.5;            // _peak's floor
     return SV_OK;
 }
 
@@ -665,24 +668,46 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     // requested precision.
     sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, SV_FP32, left, right, disp_full,
                      disp_work, workspace};
+    // The width decisions: from the map's histogram over the width rule's
+    // thresholds (no value select) whenever the rule has at most kWidthBins
+    // of them, which is every max_width up to 560.  The probe stage computes
+    // both rules' thresholds (the probe's, then the full-size maps', which
+    // the passes read from the same workspace).
+    const WidthRule probe_rule{W, max_width, target_peak, W / (double)pw};
+    const WidthRule full_rule{W, max_width, target_peak, 1.0};
+    const int kmax = width_rule_kmax(full_rule), nth = kmax - 48;
+    const bool by_rule = nth <= kWidthBins;
+    unsigned long long *wkeys = reinterpret_cast<unsigned long long *>(w.hist + 2 * SEL_NB);
     double *slot = nullptr;
     SV_TRY(run_stage(mnet, key, st, true, &slot, [&](double *mirror) -> int {
         int rc = check_net_shape(net->view, ph, pw);
+        if (!rc && by_rule) rc = launch_width_rules(probe_rule, full_rule, wkeys, st);
         if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh);
         if (!rc) rc = predict_f32(net, w, pw, ph, SV_FP32, st, true);
         const long np = (long)pw * ph;
         const long long rank = (long long)(np * 0.95);
-        if (!rc && np <= 16384) rc = launch_select_small_f32(w.d2, np, rank, w.sel, st, mirror);
-        else if (!rc) {
+        if (!rc && by_rule) {
+            const WidthFuse f{wkeys, nth, kmax, rank};
+            rc = launch_width_map<float>(w.d2, np, f, w.sel, w.hist, st, mirror);
+        } else if (!rc && np <= 16384) {
+            rc = launch_select_small_f32(w.d2, np, rank, w.sel, st, mirror);
+        } else if (!rc) {
             rc = launch_promote(w.d2, np, w.probe64, st);
             if (!rc) rc = launch_select(w.probe64, np, rank, w.sel, w.hist, st, mirror);
         }
         return rc;
     }));
-    double pk;
-    SV_TRY(fetch_peak(w, st, slot, &pk));
-    const double peak = pk * (W / (double)pw);
-    int work = width_for(W, target_peak, max_width, peak);
+    int work;
+    if (by_rule) {
+        double wv;
+        SV_TRY(fetch_peak(w, st, slot, &wv, false));
+        work = (int)wv;
+    } else {
+        double pk;
+        SV_TRY(fetch_peak(w, st, slot, &pk));
+        const double peak = pk * (W / (double)pw);
+        work = width_for(W, target_peak, max_width, peak);
+    }
     int nt = 0;
     if (work_trace) work_trace[nt++] = work;
     // passes (stereonet.py:3908-3929): the peak after pass i is needed only
@@ -694,9 +719,21 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
                        disp_work, workspace};
         int Ww, Hw;
         SV_TRY(run_stage(mnet, k, st, with_sel, &slot, [&](double *mirror) -> int {
-            // the select's pass 0 runs inside the pass when it resamples
             const long nf = (long)W * H;
             const long long rank = (long long)((long)W * H * 0.95);
+            if (by_rule) {
+                // the whole decision runs inside the pass when it resamples
+                const bool fuse = with_sel && work < W;
+                const WidthFuse f{wkeys + kWidthBins, nth, kmax, rank};
+                const SelFuse sf{w.sel, w.hist, rank, &f, mirror};
+                int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, prec,
+                                               disp_full, disp_work, &Ww, &Hw, st,
+                                               fuse ? &sf : nullptr);
+                if (!rc && with_sel && !fuse)
+                    rc = launch_width_map<double>(disp_full, nf, f, w.sel, w.hist, st, mirror);
+                return rc;
+            }
+            // the select's pass 0 runs inside the pass when it resamples
             const bool fuse = with_sel && work < W && nf > select_small_cap();
             const SelFuse sf{w.sel, w.hist, rank};
             int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, prec,
@@ -712,9 +749,16 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
         *pWw = Ww;
         *pHw = Hw;
         if (!with_sel) break;
-        double np_;
-        SV_TRY(fetch_peak(w, st, slot, &np_));
-        const int nw = width_for(W, target_peak, max_width, np_);
+        int nw;
+        if (by_rule) {
+            double wv;
+            SV_TRY(fetch_peak(w, st, slot, &wv, false));
+            nw = (int)wv;
+        } else {
+            double np_;
+            SV_TRY(fetch_peak(w, st, slot, &np_));
+            nw = width_for(W, target_peak, max_width, np_);
+        }
         if (std::abs(nw - work) <= 0.08 * work) break;
         work = nw;
         if (work_trace) work_trace[nt++] = work;

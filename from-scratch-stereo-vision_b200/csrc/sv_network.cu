@@ -152,12 +152,20 @@ __global__ void k_resize_scale(const T *__restrict__ x, int W, int H, int W2, in
 // (stereonet.py:3957-3959), and the work map itself promoted to FP64 by the
 // threads that fall inside it (the work map is never larger).
 // With sel, also pass 0 of the stage's full-resolution select over the
-// values it writes (the select's first histogram: ghist).
+// values it writes (the select's first histogram: ghist) -- or, with
+// wf.keys, the whole width decision over them (its last CTA writes the
+// width into sel->value and *mirror).
 __device__ __forceinline__ void work_outputs_body(int bx, int by, unsigned nblk, bool copy,
                                                   const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
                    double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
-                   unsigned *ghist) {
+                   unsigned *ghist, const WidthFuse &wf = WidthFuse{nullptr, 0, 0, 0},
+                   double *mirror = nullptr) {
     __shared__ unsigned hist[SEL_NB];
+    __shared__ unsigned long long sk[kWidthBins];
+    if (sel && wf.keys) {                         // the same for every CTA
+        for (int i = sel_tid(); i < wf.m; i += sel_nt()) sk[i] = wf.keys[i];
+        for (int i = sel_tid(); i <= wf.m; i += sel_nt()) hist[i] = 0u;
+    }
     const int ox = bx * blockDim.x + threadIdx.x;
     const int oy = by * blockDim.y + threadIdx.y;
     const bool in = ox < W && oy < H;
@@ -173,6 +181,13 @@ __device__ __forceinline__ void work_outputs_body(int bx, int by, unsigned nblk,
         if (work64 && ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
     }
     if (!sel) return;                              // the same for every CTA
+    if (wf.keys) {
+        __syncthreads();
+        width_count(hist, in ? width_bin(sk, wf.m, sel_key(v)) : -1);
+        __syncthreads();
+        width_finish(wf, sel, ghist, hist, nblk, mirror);
+        return;
+    }
     for (int i = sel_tid(); i < SEL_NB; i += sel_nt()) hist[i] = 0u;
     __syncthreads();
     sel_count(hist, sel_key(v), in, 0ull, 0);
@@ -184,9 +199,9 @@ __device__ __forceinline__ void work_outputs_body(int bx, int by, unsigned nblk,
 __global__ void __launch_bounds__(256)
     k_work_outputs(const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
                    double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
-                   unsigned *ghist) {
+                   unsigned *ghist, WidthFuse wf, double *mirror) {
     work_outputs_body(blockIdx.x, blockIdx.y, gridDim.x * gridDim.y * gridDim.z, false, d, Ww,
-                      Hw, W, H, inv, work64, full64, sel, ghist);
+                      Hw, W, H, inv, work64, full64, sel, ghist, wf, mirror);
 }
 
 // Batched: every active pair's full-resolution map from its work map (the
@@ -1072,9 +1087,11 @@ int launch_work_outputs(const float *d, int Ww, int Hw, int W, int H, double inv
     }
     dim3 blk(32, 8);
     count_launch();
+    const WidthFuse wf = fuse && fuse->width ? *fuse->width : WidthFuse{nullptr, 0, 0, 0};
     k_work_outputs<<<grid2d(W, H, blk), blk, 0, st>>>(d, Ww, Hw, W, H, inv, work64, full64,
                                                        fuse ? fuse->state : nullptr,
-                                                       fuse ? fuse->hist : nullptr);
+                                                       fuse ? fuse->hist : nullptr, wf,
+                                                       fuse ? fuse->mirror : nullptr);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

@@ -68,6 +68,8 @@ struct FwdBufs {
 };
 
 struct SelState;
+struct WidthRule;
+struct WidthFuse;
 
 // A full-resolution select whose pass 0 runs inside a network stage: the
 // stage's resize starts the selection of `rank` (state and histograms
@@ -77,6 +79,8 @@ struct SelFuse {
     SelState *state;
     unsigned *hist;         // the select's histogram words (select_hist_words)
     long long rank;
+    const WidthFuse *width = nullptr;   // a width decision instead of the value
+    double *mirror = nullptr;           // the decision's host-visible copy
 };
 
 // gh (optional): also avgpool2 of the resized left view, [H2/2][W2/2]
@@ -153,6 +157,15 @@ long select_small_cap();
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st, double *mirror = nullptr);
 // the same over FP32 values (exactly their FP64 promotions), n <= 16384
+// predict_auto's width rules: the thresholds of a and b (the same widths)
+// into keys[0..] and keys[kWidthBins..],
+// and a decision over a whole map (clears the state and histogram first).
+int launch_width_rules(const WidthRule &a, const WidthRule &b, unsigned long long *keys,
+                       cudaStream_t st);
+template <typename T>
+int launch_width_map(const T *x, long n, const WidthFuse &f, SelState *state, unsigned *hist,
+                     cudaStream_t st, double *mirror);
+
 int launch_select_small_f32(const float *x, long n, long long rank, SelState *state,
                             cudaStream_t st, double *mirror = nullptr);
 size_t select_state_bytes();

@@ -137,4 +137,141 @@ __device__ __forceinline__ void sel_pass_finish(int pass, SelState *s, unsigned 
     }
 }
 
+// ------------------------------------------------------------------
+// predict_auto's next work width straight from a map, without the value.
+//
+// predict_auto only needs the width that its rule (width_for,
+// stereonet.py:3915-3919) gives for the map's 95% quantile v*:
+//   width(v) = clamp(int(W * target / max(g(v), 1e-6) + 0.5), 48, min(W, max_width)),
+//   g(v) = max(v, 0.5) * scale   (scale = W / probe width for the probe, else 1).
+// width() is monotone non-increasing in the order of the values, so for
+// each width k < kmax there is a smallest order key T_k with width <= k,
+// and width(v*) <= k exactly when fewer than rank + 1 values lie below T_k.
+// A histogram of the map over the m = kmax - 48 thresholds (one pass, fused
+// into the kernel that writes the map) therefore gives the width: with
+// C_j the number of values below the j-th threshold (ascending), the
+// width is kmax minus the number of j with C_j <= rank.  It is the width
+// the exact selection followed by width_for gives, for every map.
+constexpr int kWidthBins = 512;          // thresholds a decision can hold (widths 48 .. 560)
+
+struct WidthRule {
+    int W, max_width;
+    double target, scale;
+};
+
+__host__ __device__ inline int width_rule_kmax(const WidthRule &r) {
+    const int k = r.W < r.max_width ? r.W : r.max_width;
+    return k > 48 ? k : 48;
+}
+
+// width_for of the floored (and scaled) value, in FP64 with every operation
+// rounded as the host rounds it.
+__device__ __forceinline__ int width_rule_of(const WidthRule &r, double v) {
+    const double pk = v > 0.5 ? v : 0.5;
+    const double peak = __dmul_rn(pk, r.scale);
+    const double m = peak > 1.0e-6 ? peak : 1.0e-6;
+    const double q = __dadd_rn(__ddiv_rn(__dmul_rn((double)r.W, r.target), m), 0.5);
+    int w = q < 2147483647.0 ? (q > -2147483648.0 ? (int)q : -2147483647 - 1) : 2147483647;
+    if (w > r.W) w = r.W;
+    if (w > r.max_width) w = r.max_width;
+    if (w < 48) w = 48;
+    return w;
+}
+
+// What a fused or standalone width decision needs: the thresholds (in
+// device memory), their count, the widest width and the quantile's rank.
+struct WidthFuse {
+    const unsigned long long *keys;
+    int m, kmax;
+    long long rank;
+};
+
+// Number of thresholds <= k (the bin of key k), over m ascending keys.
+__device__ __forceinline__ int width_bin(const unsigned long long *keys, int m,
+                                         unsigned long long k) {
+    int lo = 0, hi = m;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] <= k) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Adds bin b (b < 0: nothing) to the shared histogram, warp-aggregated; all
+// 32 lanes call it.
+__device__ __forceinline__ void width_count(unsigned *hist, int b) {
+    const unsigned same = __match_any_sync(kFull, (unsigned)b);
+    if (b >= 0 && (sel_tid() & 31) == __ffs(same) - 1) atomicAdd(&hist[b], __popc(same));
+}
+
+// The width from the decision's totals h[0..m] (whole CTA): the number of
+// j < m whose prefix h[0] + .. + h[j] is <= rank, subtracted from kmax.
+// G: h in global memory, written by other CTAs (read around L1).
+template <bool G>
+__device__ __forceinline__ int width_from_bins(const WidthFuse &f, const unsigned *h) {
+    __shared__ unsigned long long wsum[32];
+    __shared__ unsigned wcnt[32];
+    const int t = sel_tid(), nt = sel_nt(), lane = t & 31, wid = t >> 5, nw = nt >> 5;
+    const int per = (f.m + nt - 1) / nt, j0 = t * per;
+    const int j1 = j0 + per < f.m ? j0 + per : f.m;
+    unsigned long long loc = 0;
+    for (int j = j0; j < j1; ++j) loc += G ? __ldcg(h + j) : h[j];
+    unsigned long long incl = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const unsigned long long v0 = lane < nw ? wsum[lane] : 0ull;
+        unsigned long long v = v0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane < nw) wsum[lane] = v - v0;
+    }
+    __syncthreads();
+    unsigned long long run = wsum[wid] + incl - loc;
+    unsigned cnt = 0;
+    for (int j = j0; j < j1; ++j) {
+        run += G ? __ldcg(h + j) : h[j];
+        if ((long long)run <= f.rank) ++cnt;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(kFull, cnt, o);
+    if (lane == 0) wcnt[wid] = cnt;
+    __syncthreads();
+    unsigned total = 0;
+    for (int w = 0; w < nw; ++w) total += wcnt[w];
+    return f.kmax - (int)total;
+}
+
+// The end of a CTA's share of a decision: its bins (hist, m + 1 of them) go
+// into ghist, and the last of the nblk CTAs turns the totals into the width
+// (into s->value, and *mirror when given).  ghist and s->done[0] start at 0.
+__device__ __forceinline__ void width_finish(const WidthFuse &f, SelState *s, unsigned *ghist,
+                                             const unsigned *hist, unsigned nblk,
+                                             double *mirror) {
+    __shared__ bool last;
+    const int t = sel_tid(), nt = sel_nt();
+    for (int i = t; i <= f.m; i += nt)
+        if (hist[i]) atomicAdd(&ghist[i], hist[i]);
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(&s->done[0], 1u) == nblk - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int width = width_from_bins<true>(f, ghist);
+    if (t == 0) {
+        s->value = (double)width;
+        if (mirror) *reinterpret_cast<volatile double *>(mirror) = (double)width;
+    }
+}
+
 }  // namespace sv

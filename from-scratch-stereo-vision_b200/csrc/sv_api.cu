@@ -260,12 +260,18 @@ int sv_refine_fullres(const void *left, const void *right, int dtype, const doub
     return SV_OK;
 }
 
+// part: LR_ALL, LR_CENSUS (the census of both views only: it needs the
+// images alone, so a caller may run it while the disparity is still being
+// computed) or LR_AFTER_CENSUS (the rest, over the census already in the
+// workspace).
+enum { LR_ALL = 0, LR_CENSUS = 1, LR_AFTER_CENSUS = 2 };
+
 static int lr_refine_impl(const void *left, const void *right, int dtype, const double *disp0,
                           int W, int H, double tol, const sv_refine_params *p, double *out,
                           uint8_t *status, void *workspace, size_t workspace_bytes,
                           void *stream, void *const *events, int n_events,
-                          const uint8_t *rad = nullptr) {
-    if (!left || !right || !disp0 || !out || !status) {
+                          const uint8_t *rad = nullptr, int part = LR_ALL) {
+    if (!left || !right || (part != LR_CENSUS && (!disp0 || !out || !status))) {
         set_error("NULL argument");
         return SV_ERR_NULL;
     }
@@ -286,12 +292,15 @@ static int lr_refine_impl(const void *left, const void *right, int dtype, const 
         if (events) SV_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[ev++], st));
         return SV_OK;
     };
+    if (part == LR_CENSUS)
+        return launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st);
     SV_TRY(mark());
     SV_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(DevFlags), st));
     SV_TRY(launch_base(disp0, N, w.base0, &w.flags->status, st));
     SV_TRY(launch_left_to_right(disp0, W, H, w.d0r, w.base1, st));
     SV_TRY(mark());
-    SV_TRY(launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st));
+    if (part != LR_AFTER_CENSUS)
+        SV_TRY(launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st));
     SV_TRY(mark());
     SV_TRY(launch_band_costs_slot(w.cen0, w.cen1, w.base0, w.base1, W, H, c.R, c.invalid, w.C0,
                              w.C1, 2, st, rad));
@@ -306,6 +315,26 @@ static int lr_refine_impl(const void *left, const void *right, int dtype, const 
     SV_TRY(mark());
     return SV_OK;
 }
+
+}  // extern "C"
+
+namespace sv {
+int lr_refine_census(const void *left, const void *right, int dtype, int W, int H,
+                     const sv_refine_params *p, void *workspace, size_t workspace_bytes,
+                     cudaStream_t st) {
+    return lr_refine_impl(left, right, dtype, nullptr, W, H, 0.0, p, nullptr, nullptr, workspace,
+                          workspace_bytes, st, nullptr, 0, nullptr, LR_CENSUS);
+}
+int lr_refine_after_census(const void *left, const void *right, int dtype, const double *disp0,
+                           int W, int H, double tol, const sv_refine_params *p, double *out,
+                           uint8_t *status, void *workspace, size_t workspace_bytes,
+                           cudaStream_t st) {
+    return lr_refine_impl(left, right, dtype, disp0, W, H, tol, p, out, status, workspace,
+                          workspace_bytes, st, nullptr, 0, nullptr, LR_AFTER_CENSUS);
+}
+}  // namespace sv
+
+extern "C" {
 
 int sv_lr_refine(const void *left, const void *right, int dtype, const double *disp0, int W,
                  int H, double tol, const sv_refine_params *p, double *out, uint8_t *status,

@@ -49,6 +49,44 @@ struct sv_net {
 
 namespace sv {
 
+int lr_refine_census(const void *left, const void *right, int dtype, int W, int H,
+                     const sv_refine_params *p, void *workspace, size_t workspace_bytes,
+                     cudaStream_t st);
+int lr_refine_after_census(const void *left, const void *right, int dtype, const double *disp0,
+                           int W, int H, double tol, const sv_refine_params *p, double *out,
+                           uint8_t *status, void *workspace, size_t workspace_bytes,
+                           cudaStream_t st);
+
+// A second stream of the calling thread on the current device (with a fork
+// and a join event), for work that overlaps the caller's stream.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+static int side_stream(SideStream **out) {
+    constexpr int kDevs = 16;
+    static thread_local SideStream per[kDevs];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevs) return SV_ERR_CUDA;
+    SideStream &x = per[dev];
+    if (!x.s) {
+        SideStream y;
+        if (cudaStreamCreateWithFlags(&y.s, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&y.fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&y.join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            if (y.join) cudaEventDestroy(y.join);
+            if (y.fork) cudaEventDestroy(y.fork);
+            if (y.s) cudaStreamDestroy(y.s);
+            return SV_ERR_CUDA;
+        }
+        x = y;
+    }
+    *out = &x;
+    return SV_OK;
+}
+
 static long param_count(const int *a) {
     long C = a[0], Cm = a[1], Rc = a[3], nd = a[4];
     long n = C * 9 + C + 3 * (C * C * 9 + C);
@@ -629,10 +667,38 @@ int sv_predict_refine(const sv_net *net, const void *left, const void *right, in
                       int *work_trace, void *pworkspace, size_t pworkspace_bytes, double tol,
                       const sv_refine_params *p, double *out, uint8_t *status,
                       void *rworkspace, size_t rworkspace_bytes, void *stream) {
+    cudaStream_t st = (cudaStream_t)stream;
+    SideStream *ss = nullptr;
+    if (st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread) {
+        // lr_refine's census needs the images alone: it runs on a second
+        // stream beside predict_auto's small network launches, and the rest
+        // of lr_refine waits for it
+        if (side_stream(&ss) == SV_OK) {
+            int rc = SV_OK;
+            if (cudaEventRecord(ss->fork, st) != cudaSuccess ||
+                cudaStreamWaitEvent(ss->s, ss->fork, 0) != cudaSuccess) {
+                set_error("stream fork failed");
+                return SV_ERR_CUDA;
+            }
+            rc = lr_refine_census(left, right, dtype, W, H, p, rworkspace, rworkspace_bytes,
+                                  ss->s);
+            if (cudaEventRecord(ss->join, ss->s) != cudaSuccess ||
+                cudaStreamWaitEvent(st, ss->join, 0) != cudaSuccess) {
+                set_error("stream join failed");
+                return SV_ERR_CUDA;
+            }
+            if (rc) return rc;
+        } else {
+            ss = nullptr;
+        }
+    }
     const int rc = sv_predict_auto(net, left, right, dtype, W, H, target_peak, probe_width,
                                    max_width, passes, precision, disp_full, disp_work, pWw, pHw,
                                    work_trace, pworkspace, pworkspace_bytes, stream);
     if (rc) return rc;
+    if (ss)
+        return lr_refine_after_census(left, right, dtype, disp_full, W, H, tol, p, out, status,
+                                      rworkspace, rworkspace_bytes, st);
     return sv_lr_refine(left, right, dtype, disp_full, W, H, tol, p, out, status, rworkspace,
                         rworkspace_bytes, stream);
 }
@@ -668,26 +734,22 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     // requested precision.
     sv_graph_key key{0, W, H, dtype, pw * 65536 + ph, 1, SV_FP32, left, right, disp_full,
                      disp_work, workspace};
-    // The width decisions: from the map's histogram over the width rule's
-    // thresholds (no value select) whenever the rule has at most kWidthBins
-    // of them, which is every max_width up to 560.  The probe stage computes
-    // both rules' thresholds (the probe's, then the full-size maps', which
-    // the passes read from the same workspace).
+    // The width decisions: from a histogram of the widths the rule gives the
+    // map's values (no value select) whenever the rule has at most
+    // kWidthBins + 1 widths (every max_width up to 2095).
     const WidthRule probe_rule{W, max_width, target_peak, W / (double)pw};
     const WidthRule full_rule{W, max_width, target_peak, 1.0};
     const int kmax = width_rule_kmax(full_rule), nth = kmax - 48;
     const bool by_rule = nth <= kWidthBins;
-    unsigned long long *wkeys = reinterpret_cast<unsigned long long *>(w.hist + 2 * SEL_NB);
     double *slot = nullptr;
     SV_TRY(run_stage(mnet, key, st, true, &slot, [&](double *mirror) -> int {
         int rc = check_net_shape(net->view, ph, pw);
-        if (!rc && by_rule) rc = launch_width_rules(probe_rule, full_rule, wkeys, st);
         if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh);
         if (!rc) rc = predict_f32(net, w, pw, ph, SV_FP32, st, true);
         const long np = (long)pw * ph;
         const long long rank = (long long)(np * 0.95);
         if (!rc && by_rule) {
-            const WidthFuse f{wkeys, nth, kmax, rank};
+            const WidthFuse f{probe_rule, nth, kmax, rank};
             rc = launch_width_map<float>(w.d2, np, f, w.sel, w.hist, st, mirror);
         } else if (!rc && np <= 16384) {
             rc = launch_select_small_f32(w.d2, np, rank, w.sel, st, mirror);
@@ -724,7 +786,7 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
             if (by_rule) {
                 // the whole decision runs inside the pass when it resamples
                 const bool fuse = with_sel && work < W;
-                const WidthFuse f{wkeys + kWidthBins, nth, kmax, rank};
+                const WidthFuse f{full_rule, nth, kmax, rank};
                 const SelFuse sf{w.sel, w.hist, rank, &f, mirror};
                 int rc = predict_at_scale_impl(net, w, left, right, dtype, W, H, work, prec,
                                                disp_full, disp_work, &Ww, &Hw, st,

@@ -158,14 +158,10 @@ __global__ void k_resize_scale(const T *__restrict__ x, int W, int H, int W2, in
 __device__ __forceinline__ void work_outputs_body(int bx, int by, unsigned nblk, bool copy,
                                                   const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
                    double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
-                   unsigned *ghist, const WidthFuse &wf = WidthFuse{nullptr, 0, 0, 0},
-                   double *mirror = nullptr) {
-    __shared__ unsigned hist[SEL_NB];
-    __shared__ unsigned long long sk[kWidthBins];
-    if (sel && wf.keys) {                         // the same for every CTA
-        for (int i = sel_tid(); i < wf.m; i += sel_nt()) sk[i] = wf.keys[i];
-        for (int i = sel_tid(); i <= wf.m; i += sel_nt()) hist[i] = 0u;
-    }
+                   unsigned *ghist, const WidthFuse *wf = nullptr, double *mirror = nullptr) {
+    __shared__ unsigned hist[SEL_NB + 1];
+    if (sel && wf)                                // the same for every CTA
+        for (int i = sel_tid(); i <= wf->m; i += sel_nt()) hist[i] = 0u;
     const int ox = bx * blockDim.x + threadIdx.x;
     const int oy = by * blockDim.y + threadIdx.y;
     const bool in = ox < W && oy < H;
@@ -181,11 +177,11 @@ __device__ __forceinline__ void work_outputs_body(int bx, int by, unsigned nblk,
         if (work64 && ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
     }
     if (!sel) return;                              // the same for every CTA
-    if (wf.keys) {
+    if (wf) {
         __syncthreads();
-        width_count(hist, in ? width_bin(sk, wf.m, sel_key(v)) : -1);
+        width_count(hist, in ? width_bin_of(*wf, v) : -1);
         __syncthreads();
-        width_finish(wf, sel, ghist, hist, nblk, mirror);
+        width_finish(*wf, sel, ghist, hist, nblk, mirror);
         return;
     }
     for (int i = sel_tid(); i < SEL_NB; i += sel_nt()) hist[i] = 0u;
@@ -201,7 +197,8 @@ __global__ void __launch_bounds__(256)
                    double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
                    unsigned *ghist, WidthFuse wf, double *mirror) {
     work_outputs_body(blockIdx.x, blockIdx.y, gridDim.x * gridDim.y * gridDim.z, false, d, Ww,
-                      Hw, W, H, inv, work64, full64, sel, ghist, wf, mirror);
+                      Hw, W, H, inv, work64, full64, sel, ghist, wf.m >= 0 ? &wf : nullptr,
+                      mirror);
 }
 
 // Batched: every active pair's full-resolution map from its work map (the
@@ -1087,7 +1084,7 @@ int launch_work_outputs(const float *d, int Ww, int Hw, int W, int H, double inv
     }
     dim3 blk(32, 8);
     count_launch();
-    const WidthFuse wf = fuse && fuse->width ? *fuse->width : WidthFuse{nullptr, 0, 0, 0};
+    const WidthFuse wf = fuse && fuse->width ? *fuse->width : WidthFuse{{0, 0, 0.0, 0.0}, -1, 0, 0};
     k_work_outputs<<<grid2d(W, H, blk), blk, 0, st>>>(d, Ww, Hw, W, H, inv, work64, full64,
                                                        fuse ? fuse->state : nullptr,
                                                        fuse ? fuse->hist : nullptr, wf,

@@ -157,11 +157,8 @@ long select_small_cap();
 int launch_select(const double *x, long n, long long rank, SelState *state, unsigned *hist,
                   cudaStream_t st, double *mirror = nullptr);
 // the same over FP32 values (exactly their FP64 promotions), n <= 16384
-// predict_auto's width rules: the thresholds of a and b (the same widths)
-// into keys[0..] and keys[kWidthBins..],
-// and a decision over a whole map (clears the state and histogram first).
-int launch_width_rules(const WidthRule &a, const WidthRule &b, unsigned long long *keys,
-                       cudaStream_t st);
+// predict_auto's width decision over a whole map (clears the state and
+// histogram first when it needs them).
 template <typename T>
 int launch_width_map(const T *x, long n, const WidthFuse &f, SelState *state, unsigned *hist,
                      cudaStream_t st, double *mirror);

@@ -398,80 +398,19 @@ __global__ void __launch_bounds__(SEL32_T)
     }
 }
 
-// The thresholds of a width decision: key j (ascending in j) is the
-// smallest order key whose value the rule maps to a width <= k = kmax - 1 -
-// j.  In real arithmetic that boundary is v = W * target / ((k + 0.5) *
-// scale); the search starts at the key of that estimate and gallops, then
-// bisects, to the exact key under the rule's FP64 rounding (the rule is
-// monotone in key order and gives 48 <= k at +inf).  Block row y computes
-// table y: rules[y] into keys + y * kWidthBins.
-struct WidthRules {
-    WidthRule r[2];
-};
-
-__global__ void k_width_rule(WidthRules rules, int m, unsigned long long *keys) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= m) return;
-    const WidthRule &r = rules.r[blockIdx.y];
-    const int k = width_rule_kmax(r) - 1 - j;
-    const unsigned long long kmin = sel_key(-INFINITY), kinf = sel_key(INFINITY);
-    auto ok = [&](unsigned long long key) { return width_rule_of(r, sel_unkey(key)) <= k; };
-    unsigned long long lo, hi;                 // !ok(lo) (or lo == kmin), ok(hi)
-    if (ok(kmin)) {
-        keys[blockIdx.y * kWidthBins + j] = kmin;
-        return;
-    }
-    const double est = (double)r.W * r.target / (((double)k + 0.5) * r.scale);
-    unsigned long long g = est >= -INFINITY && est <= INFINITY ? sel_key(est) : kinf;
-    if (g <= kmin) g = kmin + 1;
-    if (g > kinf) g = kinf;
-    if (ok(g)) {
-        hi = g;
-        unsigned long long step = 1;
-        for (;;) {
-            const unsigned long long c = hi - kmin > step ? hi - step : kmin;
-            if (!ok(c)) {
-                lo = c;
-                break;
-            }
-            hi = c;
-            step <<= 1;
-        }
-    } else {
-        lo = g;
-        unsigned long long step = 1;
-        for (;;) {
-            const unsigned long long c = kinf - lo > step ? lo + step : kinf;
-            if (ok(c)) {
-                hi = c;
-                break;
-            }
-            lo = c;
-            step <<= 1;
-        }
-    }
-    while (hi - lo > 1) {                      // smallest ok key in (lo, hi]
-        const unsigned long long mid = lo + (hi - lo) / 2;
-        if (ok(mid)) hi = mid;
-        else lo = mid;
-    }
-    keys[blockIdx.y * kWidthBins + j] = hi;
-}
-
 // A width decision over a whole map (a full-size map no network kernel
 // wrote): CTAs of 256 values, the last one finishing.
 template <typename T>
 __global__ void __launch_bounds__(256)
     k_width_map(const T *__restrict__ x, long n, WidthFuse f, SelState *s, unsigned *ghist,
                 double *mirror) {
-    __shared__ unsigned long long sk[kWidthBins];
     __shared__ unsigned hist[kWidthBins + 1];
     const int t = threadIdx.x;
-    for (int i = t; i < f.m; i += 256) sk[i] = f.keys[i];
-    for (int i = t; i <= f.m; i += 256) hist[i] = 0u;
-    __syncthreads();
     const long i = blockIdx.x * 256L + t;
-    width_count(hist, i < n ? width_bin(sk, f.m, sel_key((double)x[i])) : -1);
+    const double v = i < n ? (double)__ldg(x + i) : 0.0;
+    for (int j = t; j <= f.m; j += 256) hist[j] = 0u;
+    __syncthreads();
+    width_count(hist, i < n ? width_bin_of(f, v) : -1);
     __syncthreads();
     width_finish(f, s, ghist, hist, gridDim.x, mirror);
 }
@@ -484,7 +423,6 @@ constexpr long WIDTH_SMALL_CAP = (long)WIDTH_SMALL_T * WIDTH_SMALL_K;
 template <typename T>
 __global__ void __launch_bounds__(WIDTH_SMALL_T)
     k_width_small(const T *__restrict__ x, int n, WidthFuse f, SelState *s, double *mirror) {
-    __shared__ unsigned long long sk[kWidthBins];
     __shared__ unsigned hist[kWidthBins + 1];
     const int t = threadIdx.x;
     T v[WIDTH_SMALL_K];
@@ -493,7 +431,6 @@ __global__ void __launch_bounds__(WIDTH_SMALL_T)
         const int i = t + u * WIDTH_SMALL_T;
         v[u] = i < n ? __ldg(x + i) : T(0);
     }
-    for (int i = t; i < f.m; i += WIDTH_SMALL_T) sk[i] = f.keys[i];
     for (int i = t; i <= f.m; i += WIDTH_SMALL_T) hist[i] = 0u;
     __syncthreads();
     const int nu = (n + WIDTH_SMALL_T - 1) / WIDTH_SMALL_T;   // the same for the whole CTA
@@ -501,7 +438,7 @@ __global__ void __launch_bounds__(WIDTH_SMALL_T)
     for (int u = 0; u < WIDTH_SMALL_K; ++u)
         if (u < nu) {
             const int i = t + u * WIDTH_SMALL_T;
-            width_count(hist, i < n ? width_bin(sk, f.m, sel_key((double)v[u])) : -1);
+            width_count(hist, i < n ? width_bin_of(f, (double)v[u]) : -1);
         }
     __syncthreads();
     const int width = width_from_bins<false>(f, hist);
@@ -509,21 +446,6 @@ __global__ void __launch_bounds__(WIDTH_SMALL_T)
         s->value = (double)width;
         if (mirror) *reinterpret_cast<volatile double *>(mirror) = (double)width;
     }
-}
-
-int launch_width_rules(const WidthRule &a, const WidthRule &b, unsigned long long *keys,
-                       cudaStream_t st) {
-    const int m = width_rule_kmax(a) - 48;
-    if (m > kWidthBins || width_rule_kmax(b) != width_rule_kmax(a)) {
-        set_error("width rules with %d thresholds (at most %d)", m, kWidthBins);
-        return SV_ERR_PARAM;
-    }
-    if (m > 0) {
-        count_launch();
-        k_width_rule<<<dim3((m + 127) / 128, 2), 128, 0, st>>>(WidthRules{{a, b}}, m, keys);
-        SV_LAUNCH_CHECK();
-    }
-    return SV_OK;
 }
 
 template <typename T>

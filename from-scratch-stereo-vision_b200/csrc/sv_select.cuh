@@ -144,16 +144,13 @@ __device__ __forceinline__ void sel_pass_finish(int pass, SelState *s, unsigned 
 // stereonet.py:3915-3919) gives for the map's 95% quantile v*:
 //   width(v) = clamp(int(W * target / max(g(v), 1e-6) + 0.5), 48, min(W, max_width)),
 //   g(v) = max(v, 0.5) * scale   (scale = W / probe width for the probe, else 1).
-// width() is monotone non-increasing in the order of the values, so for
-// each width k < kmax there is a smallest order key T_k with width <= k,
-// and width(v*) <= k exactly when fewer than rank + 1 values lie below T_k.
-// A histogram of the map over the m = kmax - 48 thresholds (one pass, fused
-// into the kernel that writes the map) therefore gives the width: with
-// C_j the number of values below the j-th threshold (ascending), the
-// width is kmax minus the number of j with C_j <= rank.  It is the width
-// the exact selection followed by width_for gives, for every map.
-constexpr int kWidthBins = 512;          // thresholds a decision can hold (widths 48 .. 560)
-
+// width() is monotone non-increasing in the values' order, so listing the
+// map's widths in the order of its values lists them from the widest down,
+// and width(v*) is the width at position rank of that list: a histogram of
+// the map's widths (one pass, fused into the kernel that writes the map)
+// gives it exactly, for every map.  Bin b holds width kmax - b.  NaN values
+// count as the largest values, as the order keys of positive NaNs sort
+// (bin m, width 48).
 struct WidthRule {
     int W, max_width;
     double target, scale;
@@ -178,24 +175,17 @@ __device__ __forceinline__ int width_rule_of(const WidthRule &r, double v) {
     return w;
 }
 
-// What a fused or standalone width decision needs: the thresholds (in
-// device memory), their count, the widest width and the quantile's rank.
+// What a fused or standalone width decision needs.
 struct WidthFuse {
-    const unsigned long long *keys;
-    int m, kmax;
-    long long rank;
+    WidthRule rule;
+    int m, kmax;            // m + 1 bins: widths kmax .. kmax - m (= 48)
+    long long rank;         // position of the quantile in the map
 };
 
-// Number of thresholds <= k (the bin of key k), over m ascending keys.
-__device__ __forceinline__ int width_bin(const unsigned long long *keys, int m,
-                                         unsigned long long k) {
-    int lo = 0, hi = m;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (keys[mid] <= k) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
+constexpr int kWidthBins = 2048;         // bins a decision can hold (widths up to 2095)
+
+__device__ __forceinline__ int width_bin_of(const WidthFuse &f, double v) {
+    return v != v ? f.m : f.kmax - width_rule_of(f.rule, v);
 }
 
 // Adds bin b (b < 0: nothing) to the shared histogram, warp-aggregated; all

@@ -91,6 +91,7 @@ SIGNATURES = {
     "sv_fill_invalid": (_I, [_VP, _VP, _I, _I, _VP, _VP, _SZ, _VP]),
     "sv_peak_workspace_size": (_SZ, []),
     "sv_peak": (_I, [_VP, ctypes.c_long, _D, _VP, _VP, _SZ, _VP]),
+    "sv_work_width": (_I, [_VP, ctypes.c_long, _I, _D, _I, _D, _VP, _VP, _SZ, _VP]),
     "sv_image_info": (_I, [ctypes.c_char_p, _SZ, ctypes.POINTER(RawImage)]),
     "sv_image_decode_raw": (_I, [ctypes.c_char_p, _SZ, _VP, _SZ, ctypes.POINTER(RawImage)]),
     "sv_image_decode_batch": (_I, [_I, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_SZ),

@@ -632,4 +632,39 @@ int sv_peak(const double *disp, long n, double q, double *out, void *workspace,
     return SV_OK;
 }
 
+int sv_work_width(const double *map, long n, int W, double target_peak, int max_width,
+                  double scale, int *width, void *workspace, size_t workspace_bytes,
+                  void *stream) {
+    if (!map || !width) { sv::set_error("NULL argument"); return SV_ERR_NULL; }
+    if (n < 1 || n >= (1l << 32) || W < 1 || max_width < 1 || !std::isfinite(target_peak) ||
+        !std::isfinite(scale) || !(scale > 0.0)) {
+        sv::set_error("bad arguments");
+        return SV_ERR_PARAM;
+    }
+    const sv::WidthRule r{W, max_width, target_peak, scale};
+    const int kmax = sv::width_rule_kmax(r), m = kmax - 48;
+    if (m > sv::kWidthBins) {
+        sv::set_error("%d possible widths (at most %d)", m + 1, sv::kWidthBins + 1);
+        return SV_ERR_PARAM;
+    }
+    if (!workspace || ((uintptr_t)workspace & 255) ||
+        workspace_bytes < sv_peak_workspace_size()) {
+        sv::set_error("workspace needs %zu bytes, 256-aligned", sv_peak_workspace_size());
+        return SV_ERR_WORKSPACE;
+    }
+    auto *s = static_cast<sv::SelState *>(workspace);
+    auto *hist = reinterpret_cast<unsigned *>(static_cast<char *>(workspace) +
+                                              sv::align256(sizeof(sv::SelState)));
+    cudaStream_t st = (cudaStream_t)stream;
+    const sv::WidthFuse f{r, m, kmax, (long long)(n * 0.95)};
+    const int rc = sv::launch_width_map<double>(map, n, f, s, hist, st, nullptr);
+    if (rc) return rc;
+    double v = 0.0;
+    SV_CUDA_TRY(cudaMemcpyAsync(&v, reinterpret_cast<const char *>(s) + offsetof(sv::SelState, value),
+                                sizeof(double), cudaMemcpyDeviceToHost, st));
+    SV_CUDA_TRY(cudaStreamSynchronize(st));
+    *width = (int)v;
+    return SV_OK;
+}
+
 }  // extern "C"

@@ -206,6 +206,25 @@ def _peak(disp, q=0.95):
     return float(out.item())
 
 
+def work_width(disp, W, target_peak, max_width=320, scale=1.0):
+    """The work width predict_auto takes from a map (stereonet.py:3866-3869
+    and 3915-3919): int(W * target_peak / max(p, 1e-6) + 0.5) clamped to
+    [48, min(W, max_width)], p = max(sorted(disp)[int(n * 0.95)], 0.5) *
+    scale -- decided on the GPU from a histogram of the rule's per-value
+    widths, as predict_auto decides it."""
+    lib = _lib.load()
+    d = disp if isinstance(disp, torch.Tensor) else np.asarray(disp, dtype=np.float64)
+    n = int(d.numel() if isinstance(d, torch.Tensor) else d.size)
+    t = _to_dev(d, n, torch.float64, name="disp")
+    need = lib.sv_peak_workspace_size()
+    ws = torch.empty(need, dtype=torch.uint8, device=t.device)
+    w = ctypes.c_int()
+    _lib.check(lib.sv_work_width(_ptr(t), n, int(W), float(target_peak), int(max_width),
+                                 float(scale), ctypes.byref(w), _ptr(ws), need, _stream()),
+               "work_width")
+    return w.value
+
+
 def predict_auto(net, left, right, W, H, target_peak=None, probe_width=64, max_width=320,
                  passes=3, verbose=True, return_trace=False, *, precision="fp32"):
     """stereonet.py:3872-3929 -> (disp_full, disp_work, W_work, H_work).

@@ -467,6 +467,20 @@ size_t sv_peak_workspace_size(void);
 int sv_peak(const double *disp, long n, double q, double *out, void *workspace,
             size_t workspace_bytes, void *stream);
 
+/* predict_auto's work-width decision over a map (stereonet.py:3866-3869
+ * _peak, then predict_auto's width rule, stereonet.py:3915-3919): the width
+ * int(W * target_peak / max(p, 1e-6) + 0.5) clamped to [48, min(W,
+ * max_width)], p = max(sorted(map)[int(n * 0.95)], 0.5) * scale (scale = W
+ * / probe width for the probe's map, 1 for a full-size one).  Exact for
+ * every map, from a histogram of the widths the rule gives each value (the
+ * rule is monotone in the value), without selecting the quantile itself --
+ * the way predict_auto decides.  map: device FP64 [n], n < 2^32; at most
+ * 2049 possible widths (min(W, max_width) <= 2096).  Synchronises the
+ * stream to return *width.  Same workspace as sv_peak. */
+int sv_work_width(const double *map, long n, int W, double target_peak, int max_width,
+                  double scale, int *width, void *workspace, size_t workspace_bytes,
+                  void *stream);
+
 /* ------------------------------------------------------------------------
  * Input images: PNG (stereonet.py:3499-3601 read_png, with zlib_decompress
  * 3421, inflate 3335 and _unfilter 3456) and PGM/PPM (stereonet.py:265-324

@@ -521,9 +521,15 @@ struct SgmGroupGeom {
     static constexpr int Kp = SL * GL;
     static constexpr int NR = SL / 2;                            // u16x2 registers per lane
     static constexpr int PADL = ((Kp + 4 + 7) / 8) * 8;          // INF slots before slot 0
-    // last word a window can touch (s <= Kp + 2), rounded to 16-byte rows
+    // last word a window can touch (s <= Kp + 2); rows are 8-byte aligned
+    // and 2 mod 4 words long, so the window loads of a warp's groups spread
+    // over twice the banks of 16-byte rows (at most 2-way conflicts at
+    // shift 0 instead of 4-way for 10 groups of 3 lanes)
     static constexpr int LASTW = ((PADL + SL * (GL - 1) + Kp + 1) >> 1) + NR + 1;
-    static constexpr int ROWW = ((LASTW + 1 + 3) / 4) * 4;       // words per row
+    static constexpr int ROWW = (LASTW + 1) % 4 == 2   ? LASTW + 1
+                                : (LASTW + 1) % 4 == 1 ? LASTW + 2
+                                : (LASTW + 1) % 4 == 0 ? LASTW + 3
+                                                       : LASTW + 4;   // words per row
     static constexpr int GPW = 32 / GL;                          // groups per warp
 };
 constexpr int SGMG_WARPS = 4;    // warps per CTA of k_sgm_group
@@ -666,10 +672,12 @@ __device__ __forceinline__ void sgm_line_group(const uint8_t *__restrict__ Cimg,
             bprev = bcur;
             {   // this pixel's path costs for the successor
                 unsigned *__restrict__ ww = ((u & 1) ? row1 : row0) + (G::PADL >> 1) + NR * gl;
-                if constexpr (NR == 4)
-                    *reinterpret_cast<uint4 *>(ww) = make_uint4(L[0], L[1], L[2], L[3]);
-                else
+                if constexpr (NR == 4) {
                     *reinterpret_cast<uint2 *>(ww) = make_uint2(L[0], L[1]);
+                    *reinterpret_cast<uint2 *>(ww + 2) = make_uint2(L[2], L[3]);
+                } else {
+                    *reinterpret_cast<uint2 *>(ww) = make_uint2(L[0], L[1]);
+                }
             }
             // path minimum over the group
             unsigned m2 = L[0];

@@ -81,8 +81,10 @@ __global__ void k_nb_probe_init(NetPair *pairs, int n) {
 // After a stage's select: the next pass's width.  stage 0 is the probe
 // (its peak scaled by W / pw); stage k > 0 the k-th pass, which stops the
 // pair when the width moved by at most 8%.
+// by_rule: the stage's decision already holds the width (a width
+// decision, not a value select).
 __global__ void k_nb_decide(NetPair *pairs, int n, const char *slab0, long long slab,
-                            long long sel_off, double tp, int max_width, int stage) {
+                            long long sel_off, double tp, int max_width, int stage, int by_rule) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     NetPair &p = pairs[i];
@@ -90,15 +92,15 @@ __global__ void k_nb_decide(NetPair *pairs, int n, const char *slab0, long long 
     const SelState *s = reinterpret_cast<const SelState *>(slab0 + (long long)i * slab + sel_off);
     const double v = s->value;
     const double pk = v > 0.5 ? v : 0.5;                 // _peak's floor
-    p.peak = pk;
+    p.peak = by_rule ? 0.0 : pk;
     if (stage == 0) {
         const double peak = __dmul_rn(pk, __ddiv_rn((double)p.W, (double)p.pw));
-        const int work = nb_width_for(p.W, tp, max_width, peak);
+        const int work = by_rule ? (int)v : nb_width_for(p.W, tp, max_width, peak);
         nb_set_work(p, work);
         if (p.ntrace < kNetTrace) p.trace[p.ntrace++] = work;
         return;
     }
-    const int nw = nb_width_for(p.W, tp, max_width, pk);
+    const int nw = by_rule ? (int)v : nb_width_for(p.W, tp, max_width, pk);
     if ((double)abs(nw - p.work) <= __dmul_rn(0.08, (double)p.work)) {
         p.active = 0;                                    // this pass's disparity is final
         return;
@@ -243,22 +245,34 @@ int nb_enqueue(sv_netbatch *nb, cudaStream_t st, bool refine) {
     SV_LAUNCH_CHECK();
     if ((rc = launch_b_resize(g[0], lt, rt, nb->dtype, s, false, st))) return rc;
     if ((rc = launch_b_forward(nb->view, g[0], s, st))) return rc;
-    if ((rc = launch_b_sel_probe(Lone, s, st))) return rc;
+    // the width decisions from histograms of the rule's widths when every
+    // pair's rule has at most kWidthBins + 1 widths (as the single-pair path)
+    int kmax_all = 48;
+    for (const NetPair &q : nb->init) {
+        const int k = width_rule_kmax(WidthRule{q.W, nb->max_width, nb->target_peak, 1.0});
+        kmax_all = k > kmax_all ? k : kmax_all;
+    }
+    const int by_rule = kmax_all - 48 <= kWidthBins;
+    if (by_rule) rc = launch_b_width_probe(Lone, s, nb->target_peak, nb->max_width, st);
+    else rc = launch_b_sel_probe(Lone, s, st);
+    if (rc) return rc;
     count_launch();
     k_nb_decide<<<nbk, tb, 0, st>>>(pairs, n, s0, slab, sel_off, nb->target_peak, nb->max_width,
-                                    0);
+                                    0, by_rule);
     SV_LAUNCH_CHECK();
     // passes (stereonet.py:3918-3929)
     for (int pass = 1; pass <= nb->passes; ++pass) {
         const bool with_sel = pass < nb->passes;
         if ((rc = launch_b_resize(g[1], lt, rt, nb->dtype, s, with_sel, st))) return rc;
         if ((rc = launch_b_forward(nb->view, g[1], s, st))) return rc;
-        if ((rc = launch_b_work_outputs(Lwo, twow, s, with_sel, st))) return rc;
+        if ((rc = launch_b_work_outputs(Lwo, twow, s, with_sel, nb->target_peak,
+                                        by_rule ? nb->max_width : 0, st)))
+            return rc;
         if (!with_sel) break;
-        if ((rc = launch_b_sel_rest(Lsel, tsel, s, st))) return rc;
+        if (!by_rule && (rc = launch_b_sel_rest(Lsel, tsel, s, st))) return rc;
         count_launch();
         k_nb_decide<<<nbk, tb, 0, st>>>(pairs, n, s0, slab, sel_off, nb->target_peak,
-                                        nb->max_width, pass);
+                                        nb->max_width, pass, by_rule);
         SV_LAUNCH_CHECK();
     }
     if (!refine) return SV_OK;

@@ -203,19 +203,25 @@ __global__ void __launch_bounds__(256)
 
 // Batched: every active pair's full-resolution map from its work map (the
 // grid covers each pair's full size exactly), with pass 0 of its select.
+// With a width rule (max_width > 0), the pair's whole width decision runs
+// here (sel->value: the width); else pass 0 of its value select.
 __global__ void __launch_bounds__(256)
     k_b_work_outputs(NetLaunch L, const float *d, double *work64, double *full64, SelState *sel,
-                     unsigned *ghist) {
+                     unsigned *ghist, double target, int max_width) {
     long long c;
     const int p = net_pair(L, c);
     const NetPair &P = L.pairs[p];
     if (!P.active) return;
     const int tx = (P.W + 31) / 32;
     const unsigned nblk = (unsigned)(L.pre[p + 1] - L.pre[p]);
+    WidthFuse wf{{P.W, max_width, target, 1.0}, 0, 0, (long long)((long)P.W * P.H * 0.95)};
+    wf.kmax = width_rule_kmax(wf.rule);
+    wf.m = wf.kmax - 48;
     work_outputs_body((int)(c % tx), (int)(c / tx), nblk, P.native != 0, net_slab(d, L, p), P.Ww,
                       P.Hw, P.W,
                       P.H, P.inv, net_slab(work64, L, p), net_slab(full64, L, p),
-                      net_slab(sel, L, p), net_slab(ghist, L, p));
+                      net_slab(sel, L, p), net_slab(ghist, L, p),
+                      max_width > 0 ? &wf : nullptr);
 }
 
 template <typename T>
@@ -1484,10 +1490,11 @@ int launch_b_resize(const NetStageLaunch &g, const void *const *lt, const void *
 }
 
 int launch_b_work_outputs(const NetLaunch &L, long long total, const NetSlab &s, bool with_sel,
-                          cudaStream_t st) {
+                          double target, int rule_width, cudaStream_t st) {
     count_launch();
     k_b_work_outputs<<<ctas_of(total), dim3(32, 8), 0, st>>>(
-        L, s.d2, nullptr, s.full, with_sel ? s.sel : nullptr, with_sel ? s.hist : nullptr);
+        L, s.d2, nullptr, s.full, with_sel ? s.sel : nullptr, with_sel ? s.hist : nullptr,
+        target, rule_width);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

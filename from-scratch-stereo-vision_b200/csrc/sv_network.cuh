@@ -138,11 +138,16 @@ int launch_b_resize(const NetStageLaunch &g, const void *const *lt, const void *
                     int dtype, const NetSlab &s, bool with_sel, cudaStream_t st);
 int launch_b_forward(const NetView &n, const NetStageLaunch &g, const NetSlab &s,
                      cudaStream_t st);
+// rule_width > 0: each pair's width decision (predict_auto's rule with
+// target and max_width = rule_width) instead of pass 0 of its value select.
 int launch_b_work_outputs(const NetLaunch &L, long long total, const NetSlab &s, bool with_sel,
-                          cudaStream_t st);
+                          double target, int rule_width, cudaStream_t st);
 // The probe's select (one CTA per pair) and passes 1..5 of the
 // full-resolution select after the pass's work outputs ran pass 0.
 int launch_b_sel_probe(const NetLaunch &L, const NetSlab &s, cudaStream_t st);
+// The probe's width decision of every pair (one CTA each, rule with scale W / pw).
+int launch_b_width_probe(const NetLaunch &L, const NetSlab &s, double target, int max_width,
+                         cudaStream_t st);
 int launch_b_sel_rest(const NetLaunch &L, long long total, const NetSlab &s, cudaStream_t st);
 long long select_ctas(long n);
 

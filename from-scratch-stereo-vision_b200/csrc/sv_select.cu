@@ -448,6 +448,40 @@ __global__ void __launch_bounds__(WIDTH_SMALL_T)
     }
 }
 
+// Batched probe decision: one CTA per pair over its probe map (the pass's
+// Ww x Hw FP32 values, read from global memory), rule scale W / pw.
+__global__ void __launch_bounds__(WIDTH_SMALL_T)
+    k_b_width_probe(NetLaunch L, const float *x0, SelState *s0, double target, int max_width) {
+    __shared__ unsigned hist[kWidthBins + 1];
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    const float *__restrict__ x = net_slab(x0, L, p);
+    const int n = P.Ww * P.Hw, t = threadIdx.x;
+    WidthFuse f{{P.W, max_width, target, (double)P.W / (double)P.pw}, 0, 0,
+                (long long)__dmul_rn((double)n, 0.95)};
+    f.kmax = width_rule_kmax(f.rule);
+    f.m = f.kmax - 48;
+    for (int i = t; i <= f.m; i += WIDTH_SMALL_T) hist[i] = 0u;
+    __syncthreads();
+    for (int i0 = 0; i0 < n; i0 += WIDTH_SMALL_T) {     // the same trip count for every thread
+        const int i = i0 + t;
+        width_count(hist, i < n ? width_bin_of(f, (double)__ldg(x + i)) : -1);
+    }
+    __syncthreads();
+    const int width = width_from_bins<false>(f, hist);
+    if (t == 0) net_slab(s0, L, p)->value = (double)width;
+}
+
+int launch_b_width_probe(const NetLaunch &L, const NetSlab &s, double target, int max_width,
+                         cudaStream_t st) {
+    count_launch();
+    k_b_width_probe<<<(unsigned)L.n, WIDTH_SMALL_T, 0, st>>>(L, s.d2, s.sel, target, max_width);
+    SV_LAUNCH_CHECK();
+    return SV_OK;
+}
+
 template <typename T>
 int launch_width_map(const T *x, long n, const WidthFuse &f, SelState *state, unsigned *hist,
                      cudaStream_t st, double *mirror) {

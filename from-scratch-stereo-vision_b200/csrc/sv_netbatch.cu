@@ -389,7 +389,9 @@ int sv_netbatch_create(const sv_net *net, const int *W, const int *H, int n, int
                 nb->pre[k * NK_COUNT + j][i + 1] = nb->pre[k * NK_COUNT + j][i] + ctas[j];
         }
         const int xo = kStages * NK_COUNT;
-        nb->pre[xo][i + 1] = nb->pre[xo][i] + (long long)((w + 31) / 32) * ((h + 7) / 8);
+        nb->pre[xo][i + 1] = nb->pre[xo][i] + (long long)((w + 31) / 32) *
+                                                  ((h + 8 * kWorkRowsBatched - 1) /
+                                                   (8 * kWorkRowsBatched));
         nb->pre[xo + 1][i + 1] = nb->pre[xo + 1][i] + select_ctas((long)w * h);
         nb->pre[xo + 2][i + 1] = i + 1;
     }

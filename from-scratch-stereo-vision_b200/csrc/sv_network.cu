@@ -152,43 +152,46 @@ __global__ void k_resize_scale(const T *__restrict__ x, int W, int H, int W2, in
 // (stereonet.py:3957-3959), and the work map itself promoted to FP64 by the
 // threads that fall inside it (the work map is never larger).
 // With sel, also pass 0 of the stage's full-resolution select over the
-// values it writes (the select's first histogram: ghist) -- or, with
-// wf.keys, the whole width decision over them (its last CTA writes the
-// width into sel->value and *mirror).
+// values it writes (the select's first histogram: ghist) -- or, with wf,
+// the whole width decision over them (its last CTA writes the width into
+// sel->value and *mirror).  A CTA of 32 x 8 threads covers `rows` slabs of
+// 8 rows (one histogram and one hand-off per CTA: fewer, larger CTAs when
+// the map is large).
 __device__ __forceinline__ void work_outputs_body(int bx, int by, unsigned nblk, bool copy,
                                                   const float *__restrict__ d, int Ww, int Hw, int W, int H, double inv,
                    double *__restrict__ work64, double *__restrict__ full64, SelState *sel,
-                   unsigned *ghist, const WidthFuse *wf = nullptr, double *mirror = nullptr) {
+                   unsigned *ghist, const WidthFuse *wf = nullptr, double *mirror = nullptr,
+                   int rows = 1) {
     __shared__ unsigned hist[SEL_NB + 1];
-    if (sel && wf)                                // the same for every CTA
-        for (int i = sel_tid(); i <= wf->m; i += sel_nt()) hist[i] = 0u;
+    if (sel) {                                     // the same for every CTA
+        const int nb = wf ? wf->m + 1 : SEL_NB;
+        for (int i = sel_tid(); i < nb; i += sel_nt()) hist[i] = 0u;
+        __syncthreads();
+    }
     const int ox = bx * blockDim.x + threadIdx.x;
-    const int oy = by * blockDim.y + threadIdx.y;
-    const bool in = ox < W && oy < H;
-    double v = 0.0;
-    if (in) {
-        if (copy) {                  // native resolution: the network output itself
-            v = (double)d[(long)oy * W + ox];
-        } else {
-            const Taps t = bilinear_taps(oy, ox, Hw, Ww, H, W);
-            v = __dmul_rn(blend64<float>(d, t), inv);
+    for (int r = 0; r < rows; ++r) {
+        const int oy = (by * rows + r) * blockDim.y + threadIdx.y;
+        const bool in = ox < W && oy < H;
+        double v = 0.0;
+        if (in) {
+            if (copy) {                  // native resolution: the network output itself
+                v = (double)d[(long)oy * W + ox];
+            } else {
+                const Taps t = bilinear_taps(oy, ox, Hw, Ww, H, W);
+                v = __dmul_rn(blend64<float>(d, t), inv);
+            }
+            full64[(long)oy * W + ox] = v;
+            if (work64 && ox < Ww && oy < Hw)
+                work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
         }
-        full64[(long)oy * W + ox] = v;
-        if (work64 && ox < Ww && oy < Hw) work64[(long)oy * Ww + ox] = (double)d[(long)oy * Ww + ox];
+        if (!sel) continue;
+        if (wf) width_count(hist, in ? width_bin_of(*wf, v) : -1);
+        else sel_count(hist, sel_key(v), in, 0ull, 0);
     }
-    if (!sel) return;                              // the same for every CTA
-    if (wf) {
-        __syncthreads();
-        width_count(hist, in ? width_bin_of(*wf, v) : -1);
-        __syncthreads();
-        width_finish(*wf, sel, ghist, hist, nblk, mirror);
-        return;
-    }
-    for (int i = sel_tid(); i < SEL_NB; i += sel_nt()) hist[i] = 0u;
+    if (!sel) return;
     __syncthreads();
-    sel_count(hist, sel_key(v), in, 0ull, 0);
-    __syncthreads();
-    sel_pass_finish(0, sel, ghist, hist, nblk);
+    if (wf) width_finish(*wf, sel, ghist, hist, nblk, mirror);
+    else sel_pass_finish(0, sel, ghist, hist, nblk);
 }
 
 
@@ -221,7 +224,7 @@ __global__ void __launch_bounds__(256)
                       P.Hw, P.W,
                       P.H, P.inv, net_slab(work64, L, p), net_slab(full64, L, p),
                       net_slab(sel, L, p), net_slab(ghist, L, p),
-                      max_width > 0 ? &wf : nullptr);
+                      max_width > 0 ? &wf : nullptr, nullptr, kWorkRowsBatched);
 }
 
 template <typename T>

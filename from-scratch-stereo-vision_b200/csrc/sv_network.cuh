@@ -138,6 +138,9 @@ int launch_b_resize(const NetStageLaunch &g, const void *const *lt, const void *
                     int dtype, const NetSlab &s, bool with_sel, cudaStream_t st);
 int launch_b_forward(const NetView &n, const NetStageLaunch &g, const NetSlab &s,
                      cudaStream_t st);
+// A CTA of the batched map kernel covers 32 columns x 8 * kWorkRowsBatched
+// rows of its pair's full-resolution map.
+constexpr int kWorkRowsBatched = 8;
 // rule_width > 0: each pair's width decision (predict_auto's rule with
 // target and max_width = rule_width) instead of pass 0 of its value select.
 int launch_b_work_outputs(const NetLaunch &L, long long total, const NetSlab &s, bool with_sel,

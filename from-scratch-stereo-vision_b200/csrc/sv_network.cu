@@ -926,6 +926,162 @@ __global__ void __launch_bounds__(128)
                                       w, wt, bias, net_slab(y, L, p));
 }
 
+// Register-blocked CostFilter convolutions for the batch, where the launch
+// is bound by throughput rather than one CTA's latency: the arithmetic of
+// k_conv3d_split<C, OC, CS, CV> (each of the CS channel groups' partial
+// sums an fmaf chain over (channel, kd, ky, kx) in that order, combined by
+// the same xor butterfly, then bias and leaky ReLU) with every thread
+// computing C3W_V neighbouring columns: the C3W_V + 2 tile values of a
+// (channel, kd, ky) row are read once and feed 3 * C3W_V taps, and one
+// 16-byte weight vector feeds C3W_V voxels.  A CTA covers 8 * C3W_V columns
+// x TD disparities of one row (128 threads: 8 column groups x TD x CS).
+// Bit-identical to k_conv3d_split.
+constexpr int C3W_XP = 8, C3W_V = 2;
+
+// Largest number of lanes of a warp that share a bank for plane stride P
+// and disparity stride DS (lane = position * CS + split).
+__host__ __device__ constexpr int c3w_conflicts(int CS, int CPS, int DS, int P) {
+    int cnt[32] = {};
+    int worst = 0;
+    for (int lane = 0; lane < 32; ++lane) {
+        const int cs = lane % CS, pl = lane / CS;
+        const int bank = (cs * CPS * P + (pl / C3W_XP) * DS + (pl % C3W_XP) * C3W_V) % 32;
+        cnt[bank] += 1;
+        if (cnt[bank] > worst) worst = cnt[bank];
+    }
+    return worst;
+}
+
+// Disparity and plane strides (words) with the fewest bank conflicts.
+__host__ __device__ constexpr int c3w_layout(int CS, int CPS, int TD, int RS, int which) {
+    int best = 33, bds = 0, bp = 0;
+    for (int ds = 3 * RS; ds < 3 * RS + 32; ++ds)
+        for (int pl = (TD + 2) * ds; pl < (TD + 2) * ds + 32; ++pl) {
+            const int c = c3w_conflicts(CS, CPS, ds, pl);
+            if (c < best) {
+                best = c;
+                bds = ds;
+                bp = pl;
+            }
+        }
+    return which == 0 ? bds : bp;
+}
+
+template <int C, int CS>
+struct C3W {
+    static constexpr int CPS = C / CS, TD = 128 / (C3W_XP * CS), TX = C3W_XP * C3W_V;
+    static constexpr int RS = TX + 2;
+    static constexpr int DS = c3w_layout(CS, CPS, TD, RS, 0);
+    static constexpr int P = c3w_layout(CS, CPS, TD, RS, 1);
+};
+
+template <int C, int OC, int CS, bool CV>
+__device__ __forceinline__ void conv3d_wide_body(int bx, int by, const float *__restrict__ a,
+                                                 const float *__restrict__ bsrc, int D, int h,
+                                                 int w, const float *__restrict__ wt,
+                                                 const float *__restrict__ bias,
+                                                 float *__restrict__ y) {
+    using G = C3W<C, CS>;
+    constexpr int CPS = G::CPS, TD = G::TD, TX = G::TX, RS = G::RS, DS = G::DS, P = G::P;
+    constexpr int OCP = (OC + 3) / 4 * 4, V = C3W_V;
+    static_assert(C % CS == 0 && (CS == 2 || CS == 4) && OC <= 8, "shape");
+    __shared__ float tile[C * P];
+    __shared__ __align__(16) float sw[C * 27 * OCP];
+    __shared__ float sb[OCP];
+    const int tid = threadIdx.x;
+    for (int i0 = tid; i0 < C * 27 * OCP; i0 += 128 * C3_SB) {
+        float v[C3_SB];
+#pragma unroll
+        for (int u = 0; u < C3_SB; ++u) {
+            const int i = i0 + u * 128, o = i % OCP, ct = i / OCP;   // ct = c * 27 + tap
+            v[u] = (i < C * 27 * OCP && o < OC) ? __ldg(wt + o * C * 27 + ct) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < C3_SB; ++u)
+            if (i0 + u * 128 < C * 27 * OCP) sw[i0 + u * 128] = v[u];
+    }
+    if (tid < OCP) sb[tid] = tid < OC ? __ldg(bias + tid) : 0.f;
+    const int nd = (D + TD - 1) / TD;
+    const int x0 = bx * TX, oy = by / nd, d0 = (by - oy * nd) * TD;
+    c3_stage<C, TD, DS, P, 128, CV, RS>(tile, a, bsrc, D, h, w, x0, oy, d0);
+    __syncthreads();
+    const int lane = tid & 31, cs = lane % CS, pos = (tid >> 5) * (32 / CS) + lane / CS;
+    const int px = pos % C3W_XP, pd = pos / C3W_XP;
+    float acc[V][OC];
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+#pragma unroll
+        for (int o = 0; o < OC; ++o) acc[q][o] = 0.f;
+    const float *tb = tile + cs * CPS * P + pd * DS + px * V;
+    const float *wb = sw + cs * CPS * 27 * OCP;
+#pragma unroll
+    for (int j = 0; j < CPS; ++j)
+#pragma unroll
+        for (int kd = 0; kd < 3; ++kd)
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+                float r[V + 2];
+#pragma unroll
+                for (int i = 0; i < V + 2; ++i) r[i] = tb[j * P + kd * DS + ky * RS + i];
+#pragma unroll
+                for (int kx = 0; kx < 3; ++kx) {
+                    const float *wp = wb + (j * 27 + kd * 9 + ky * 3 + kx) * OCP;
+#pragma unroll
+                    for (int o4 = 0; o4 < OCP; o4 += 4) {
+                        const float4 w4 = *reinterpret_cast<const float4 *>(wp + o4);
+                        const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (o4 + k < OC)
+#pragma unroll
+                                for (int q = 0; q < V; ++q)
+                                    acc[q][o4 + k] = fmaf(r[q + kx], wv[k], acc[q][o4 + k]);
+                    }
+                }
+            }
+#pragma unroll
+    for (int q = 0; q < V; ++q)
+#pragma unroll
+        for (int o = 0; o < OC; ++o)
+#pragma unroll
+            for (int m = 1; m < CS; m <<= 1) acc[q][o] += __shfl_xor_sync(kFull, acc[q][o], m);
+    const int od = d0 + pd;
+    if (cs != 0 || od >= D) return;
+    const long hw = (long)h * w, total = (long)D * hw;
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+        const int ox = x0 + px * V + q;
+        if (ox >= w) continue;
+        const long idx = (long)od * hw + (long)oy * w + ox;
+#pragma unroll
+        for (int o = 0; o < OC; ++o) {
+            const float u = acc[q][o] + sb[o];
+            y[o * total + idx] = u > 0.f ? u : u * 0.2f;
+        }
+    }
+}
+
+// Batched CostFilter c1 (cost volume built on the fly) or c2 at the pass's
+// quarter size, register-blocked.
+template <int C, int OC, int CS, bool CV>
+__global__ void __launch_bounds__(128)
+    k_b_conv3d_wide(NetLaunch L, const float *a, const float *bsrc, int D,
+                    const float *__restrict__ wt, const float *__restrict__ bias, float *y) {
+    using G = C3W<C, CS>;
+    long long c;
+    const int p = net_pair(L, c);
+    const NetPair &P = L.pairs[p];
+    if (!P.active) return;
+    int h1, w1, h, w;
+    net_quarter(P.Hw, P.Ww, h1, w1, h, w);
+    const int nd = (D + G::TD - 1) / G::TD;
+    const int tx = (w + G::TX - 1) / G::TX, ty = h * nd;
+    const int bx = (int)(c % tx), by = (int)(c / tx);
+    if (by >= ty) return;
+    conv3d_wide_body<C, OC, CS, CV>(bx, by, net_slab(a, L, p), net_slab(bsrc, L, p), D, h, w,
+                                    wt, bias, net_slab(y, L, p));
+}
+
 // ----------------------------------- conv3d #3 + invalid mask + soft-argmin
 // Conv3d #3 (Cm -> 1), CostVolume.invalid_mask (+8 where x < d, d >= 1,
 // stereonet.py:827-840) and SoftArgmin.forward (858-885) in FP32 with
@@ -1353,8 +1509,10 @@ static void stage_ctas_impl(const NetView &n, int Hm, int Wm, long long *o) {
     o[NK_RESIZE] = 2LL * ((Wm + 31) / 32) * ((Hm + 7) / 8);
     o[NK_C1] = 2LL * (C / FG) * t2(w1, h1);
     o[NK_C2] = 2LL * (C / FG) * t2(w, h);
-    o[NK_V1] = (long long)cx * h * ((D + 16 / S1 - 1) / (16 / S1));
-    o[NK_V2] = (long long)cx * h * ((D + 16 / S2 - 1) / (16 / S2));
+    using G1 = C3W<C, S1>;
+    using G2 = C3W<CM, S2>;
+    o[NK_V1] = (long long)((w + G1::TX - 1) / G1::TX) * h * ((D + G1::TD - 1) / G1::TD);
+    o[NK_V2] = (long long)((w + G2::TX - 1) / G2::TX) * h * ((D + G2::TD - 1) / G2::TD);
     o[NK_SA] = (long long)cx * h;
     o[NK_R0] = (long long)(RC / RG) * t2(Wm / 2, Hm / 2);
     o[NK_R0F] = t2(Wm / 2, Hm / 2);
@@ -1407,11 +1565,11 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
     SV_LAUNCH_CHECK();
     constexpr int S1 = C % 4 == 0 ? 4 : 2, S2 = CM % 4 == 0 && CM > 4 ? 4 : 2;
     count_launch();
-    k_b_conv3d_split<C, CM, S1, true><<<B(NK_V1), 128, 0, st>>>(
-        L(NK_V1), 1, s.f.fb[0], s.f.fb[1], D, n.cw[0], n.cb[0], s.f.v0);
+    k_b_conv3d_wide<C, CM, S1, true><<<B(NK_V1), 128, 0, st>>>(
+        L(NK_V1), s.f.fb[0], s.f.fb[1], D, n.cw[0], n.cb[0], s.f.v0);
     count_launch();
-    k_b_conv3d_split<CM, CM, S2, false><<<B(NK_V2), 128, 0, st>>>(
-        L(NK_V2), 1, s.f.v0, nullptr, D, n.cw[1], n.cb[1], s.f.v1);
+    k_b_conv3d_wide<CM, CM, S2, false><<<B(NK_V2), 128, 0, st>>>(
+        L(NK_V2), s.f.v0, nullptr, D, n.cw[1], n.cb[1], s.f.v1);
     constexpr int S3 = CM % 2 == 0 ? 2 : 1;
     count_launch();
     k_b_conv3d_softargmin<CM, S3><<<B(NK_SA), 128 * S3, 0, st>>>(L(NK_SA), s.f.v1, D, n.cw[2],

@@ -559,7 +559,8 @@ static void b_conv2d_wide(const NetLaunch &L, unsigned ctas, int lv, int Z, cons
                           const float *x1, int dil, const float *w, const float *b, float *y0,
                           float *y1, const float *resid, cudaStream_t st) {
     const size_t smem = conv2d_wide_bytes(IC, S, dil);
-    if (smem > 48 * 1024)
+    constexpr size_t kStatic = (size_t)(IC * 9 + 1) * ((OC + 3) / 4 * 4) * sizeof(float);
+    if (smem + kStatic > 48 * 1024)
         cudaFuncSetAttribute(k_b_conv2d_wide<IC, OC, ACT, CS, PX, S>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_b_conv2d_wide<IC, OC, ACT, CS, PX, S><<<ctas, CTB_TW / PX * CTB_TH, smem, st>>>(
@@ -1518,6 +1519,8 @@ static void stage_ctas_impl(const NetView &n, int Hm, int Wm, long long *o) {
     o[NK_R0F] = t2(Wm / 2, Hm / 2);
     o[NK_R1] = (long long)(RC / RG) * t2(Wm, Hm);
     o[NK_R1F] = t2(Wm, Hm);
+    o[NK_C1W] = 2LL * t2(w1, h1);            // k_b_conv2d_wide: both images, all channels
+    o[NK_C2W] = 2LL * t2(w, h);
 }
 
 int net_stage_ctas(const NetView &n, int Hm, int Wm, long long *o) {
@@ -1543,25 +1546,22 @@ static int b_forward_impl(const NetView &n, const NetStageLaunch &g, const NetSl
     const int D = n.D;
     auto L = [&](int k) { return NetLaunch{g.pre[k], g.pairs, g.n, g.slab}; };
     auto B = [&](int k) { return ctas_of(g.total[k]); };
-    const int tb1 = CT2_TW * CT2_TH, tb2 = 2 * tb1;
+    const int tb1 = CT2_TW * CT2_TH;
     const dim3 tb(CT2_TW, CT2_TH);
-    constexpr int FG = C % 4 == 0 ? 4 : C;
-    constexpr int ZF = 2 * (C / FG);
+    // FeatureNet, both images: every output channel and 2 pixels per thread
+    // (the arithmetic of k_conv2d_tiled<.., FG, .., 1 or 2>)
     count_launch();
-    k_b_conv2d_tiled<1, C, FG, 1, 1><<<B(NK_C1), tb1, conv2d_tile_bytes(1, 2, 1), st>>>(
-        L(NK_C1), 0, ZF, s.lw, s.rw, 2, 1, 1, n.fw[0], n.fb[0], s.f.fa[0], s.f.fa[1], nullptr);
+    b_conv2d_wide<1, C, 1, 1, 2, 2>(L(NK_C1W), B(NK_C1W), 0, 2, s.lw, s.rw, 1, n.fw[0], n.fb[0],
+                                    s.f.fa[0], s.f.fa[1], nullptr, st);
     count_launch();
-    k_b_conv2d_tiled<C, C, FG, 1, 2><<<B(NK_C2), tb2, conv2d_tile_bytes(C, 2, 1, 2), st>>>(
-        L(NK_C2), 1, ZF, s.f.fa[0], s.f.fa[1], 2, 1, 1, n.fw[1], n.fb[1], s.f.fb[0], s.f.fb[1],
-        nullptr);
+    b_conv2d_wide<C, C, 1, 2, 2, 2>(L(NK_C2W), B(NK_C2W), 1, 2, s.f.fa[0], s.f.fa[1], 1,
+                                    n.fw[1], n.fb[1], s.f.fb[0], s.f.fb[1], nullptr, st);
     count_launch();
-    k_b_conv2d_tiled<C, C, FG, 1, 2><<<B(NK_C2), tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
-        L(NK_C2), 2, ZF, s.f.fb[0], s.f.fb[1], 1, 1, 1, n.fw[2], n.fb[2], s.f.fa[0], s.f.fa[1],
-        nullptr);
+    b_conv2d_wide<C, C, 1, 2, 2, 1>(L(NK_C2W), B(NK_C2W), 2, 2, s.f.fb[0], s.f.fb[1], 1,
+                                    n.fw[2], n.fb[2], s.f.fa[0], s.f.fa[1], nullptr, st);
     count_launch();
-    k_b_conv2d_tiled<C, C, FG, 0, 2><<<B(NK_C2), tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
-        L(NK_C2), 2, ZF, s.f.fa[0], s.f.fa[1], 1, 1, 1, n.fw[3], n.fb[3], s.f.fb[0], s.f.fb[1],
-        nullptr);
+    b_conv2d_wide<C, C, 0, 2, 2, 1>(L(NK_C2W), B(NK_C2W), 2, 2, s.f.fa[0], s.f.fa[1], 1,
+                                    n.fw[3], n.fb[3], s.f.fb[0], s.f.fb[1], nullptr, st);
     SV_LAUNCH_CHECK();
     constexpr int S1 = C % 4 == 0 ? 4 : 2, S2 = CM % 4 == 0 && CM > 4 ? 4 : 2;
     count_launch();

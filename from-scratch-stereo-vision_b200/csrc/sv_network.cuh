@@ -110,7 +110,7 @@ int launch_forward(const NetView &n, const float *left, const float *right, int 
 // (sv_netbatch.cuh describes the scheme.)  Kernels of one stage, in launch
 // order; a stage's CTA prefix tables are indexed by these.
 enum NetKind { NK_RESIZE, NK_C1, NK_C2, NK_V1, NK_V2, NK_SA, NK_R0, NK_R0F, NK_R1, NK_R1F,
-               NK_COUNT };
+               NK_C1W, NK_C2W, NK_COUNT };
 struct NetPair;
 struct NetLaunch;
 

@@ -666,7 +666,10 @@ __device__ __forceinline__ void sgm_line_group(const uint8_t *__restrict__ Cimg,
                     const unsigned tr = __vimin3_u16x2(__byte_perm(B[r], B[r + 1], 0x5432),
                                                        B[r] + P1P1, B[r + 1] + P1P1);
                     const unsigned v = c[r] + __vminu2(tr, cap) - mm;
-                    L[r] = (v & vm[r]) | ninf[r];
+                    // with K fixed, a register whose two slots lie inside 1..K
+                    // for every lane of the group needs no band mask
+                    if (KC > 0 && r >= 1 && SL * (GL - 1) + 2 * r + 1 <= KC) L[r] = v;
+                    else L[r] = (v & vm[r]) | ninf[r];
                 }
             }
             bprev = bcur;

@@ -1379,22 +1379,24 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
         const int rc = forward_bf16_front(n, left, right, H, W, h1, w1, h, w, b, st);
         if (rc) return rc;
     } else {
-        // FeatureNet, both images: c1 s2, c2 s2, c3, c4
-        constexpr int FG = C % 4 == 0 ? 4 : C;
-        const dim3 fg1 = tgrid(w1, h1, 2 * (C / FG)), fg = tgrid(w, h, 2 * (C / FG));
+        // FeatureNet, both images: c1 s2 (4 output channels per thread), c2 s2,
+        // c3, c4 (2 per thread: shorter chains, more CTAs -- measured faster at
+        // these sizes; the arithmetic per output is the same)
+        constexpr int FG = C % 4 == 0 ? 4 : C, FG2 = C % 2 == 0 ? 2 : C;
+        const dim3 fg1 = tgrid(w1, h1, 2 * (C / FG)), fg = tgrid(w, h, 2 * (C / FG2));
         count_launch();
         k_conv2d_tiled<1, C, FG, 1, 1><<<fg1, tb1, conv2d_tile_bytes(1, 2, 1), st>>>(
             left, right, H, W, h1, w1, 2, 1, 1, n.fw[0], n.fb[0], b.fa[0], b.fa[1], nullptr);
         count_launch();
-        k_conv2d_tiled<C, C, FG, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 2, 1, 2), st>>>(
+        k_conv2d_tiled<C, C, FG2, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 2, 1, 2), st>>>(
             b.fa[0], b.fa[1], h1, w1, h, w, 2, 1, 1, n.fw[1], n.fb[1], b.fb[0], b.fb[1],
             nullptr);
         count_launch();
-        k_conv2d_tiled<C, C, FG, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
+        k_conv2d_tiled<C, C, FG2, 1, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
             b.fb[0], b.fb[1], h, w, h, w, 1, 1, 1, n.fw[2], n.fb[2], b.fa[0], b.fa[1],
             nullptr);
         count_launch();
-        k_conv2d_tiled<C, C, FG, 0, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
+        k_conv2d_tiled<C, C, FG2, 0, 2><<<fg, tb2, conv2d_tile_bytes(C, 1, 1, 2), st>>>(
             b.fa[0], b.fa[1], h, w, h, w, 1, 1, 1, n.fw[3], n.fb[3], b.fb[0], b.fb[1],
             nullptr);
         SV_LAUNCH_CHECK();
@@ -1436,8 +1438,8 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
                 k_conv2d_up<RC, RG><<<tgrid(Wl, Hl, RC / RG), tb, conv2d_tile_bytes(2, 1, dl),
                                       st>>>(prev, ph, pw, guides[lv], Hl, Wl, dl, n.rw[lv][i],
                                             n.rb[lv][i], dst, b.rin);
-            else
-                k_conv2d_tiled<RC, RC, RG, 1, RS><<<tgrid(Wl, Hl, RC / RG), RS * tb1,
+            else            // every output channel per thread (measured faster)
+                k_conv2d_tiled<RC, RC, RC, 1, RS><<<tgrid(Wl, Hl, 1), RS * tb1,
                                                     conv2d_tile_bytes(RC, 1, dl, RS), st>>>(
                     cur, cur, Hl, Wl, Hl, Wl, 1, dl, dl, n.rw[lv][i], n.rb[lv][i], dst, dst,
                     nullptr);

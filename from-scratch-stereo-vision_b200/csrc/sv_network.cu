@@ -1505,6 +1505,8 @@ static void stage_ctas_impl(const NetView &n, int Hm, int Wm, long long *o) {
     constexpr int FG = C % 4 == 0 ? 4 : C;
     constexpr int S1 = C % 4 == 0 ? 4 : 2, S2 = CM % 4 == 0 && CM > 4 ? 4 : 2;
     constexpr int RG = RC % 4 == 0 ? 4 : RC;
+    // one table serves k_b_conv2d_tiled and k_b_conv2d_wide launches alike
+    static_assert(CTB_TW == CT2_TW && CTB_TH == CT2_TH, "the two 2-D tile shapes must agree");
     auto t2 = [](int OW, int OH) {
         return (long long)((OW + CT2_TW - 1) / CT2_TW) * ((OH + CT2_TH - 1) / CT2_TH);
     };

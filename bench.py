@@ -388,14 +388,18 @@ def run_ours(args, rank, world, local):
           for _ in range(args.steps)]
     t0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     t1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    pe = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
 
     def step(i=None):
-        """One pair through predict_auto + lr_refine; with i, lr_refine also
-        records its stage events (used outside the timed region only)."""
+        """One pair through predict_auto + lr_refine; with i, predict_auto's
+        end and lr_refine's stages record events (outside the timed region
+        only; predict_auto returns once its last pass is done, so pe[i]
+        marks the end of its GPU work, not the host's next call)."""
         if i is None:
             pipe.run_device()
         else:
             pipe.predict()
+            pe[i].record()
             pipe.refiner.run_timed(pipe.left, pipe.right, pipe.disp0, pipe.out, pipe.status, ev[i])
 
     # everything runs on the pipeline's own stream (captured passes replay as
@@ -435,7 +439,7 @@ def run_ours(args, rank, world, local):
         torch.cuda.synchronize()
     stage_ms = [sum(ev[i][s].elapsed_time(ev[i][s + 1]) for i in range(args.steps)) / args.steps
                 for s in range(len(stages))]
-    pred_ms = sum(t0[i].elapsed_time(ev[i][0]) for i in range(args.steps)) / args.steps
+    pred_ms = sum(t0[i].elapsed_time(pe[i]) for i in range(args.steps)) / args.steps
     ms = pkg.shard.max_over_ranks(ms, device="cuda")
     value = world * N * args.steps / (ms / 1e3) / 1e6
 

@@ -296,8 +296,7 @@ static int lr_refine_impl(const void *left, const void *right, int dtype, const 
         return launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st);
     SV_TRY(mark());
     SV_CUDA_TRY(cudaMemsetAsync(w.flags, 0, sizeof(DevFlags), st));
-    SV_TRY(launch_base(disp0, N, w.base0, &w.flags->status, st));
-    SV_TRY(launch_left_to_right(disp0, W, H, w.d0r, w.base1, st));
+    SV_TRY(launch_left_to_right(disp0, W, H, w.d0r, w.base1, st, w.base0, &w.flags->status));
     SV_TRY(mark());
     if (part != LR_AFTER_CENSUS)
         SV_TRY(launch_census(left, right, dtype, W, H, c.rx, c.ry, w.cen0, w.cen1, st));

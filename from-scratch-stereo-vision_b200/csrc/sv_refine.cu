@@ -330,7 +330,9 @@ __global__ void __launch_bounds__(256)
 __device__ __forceinline__ void l2r_row(const double *__restrict__ row, int W,
                                         double *__restrict__ dr_row,
                                         int32_t *__restrict__ base_row,
-                                        unsigned char *smem_raw, int *sbuf) {
+                                        unsigned char *smem_raw, int *sbuf,
+                                        int32_t *__restrict__ base_l = nullptr,
+                                        int *flag = nullptr) {
     unsigned long long *key = reinterpret_cast<unsigned long long *>(smem_raw);
     int *win = reinterpret_cast<int *>(key + W);
     unsigned char *hole = reinterpret_cast<unsigned char *>(win + W);
@@ -343,6 +345,16 @@ __device__ __forceinline__ void l2r_row(const double *__restrict__ row, int W,
         double d = row[x];
         int xr = __double2int_rz(__dadd_rn(__dsub_rn((double)x, d), 0.5));
         if (xr >= 0 && xr < W && d > -1.0) atomicMax(&key[xr], ordkey(d == 0.0 ? 0.0 : d));
+        if (base_l) {                             // k_base's value for this pixel
+            int b = 0;
+            if (!(fabs(d) < 1073741824.0)) {
+                flag_error(flag, SV_ERR_DISP);
+            } else {
+                const int v = __double2int_rz(__dadd_rn(d, 0.5));
+                b = v > 0 ? v : 0;
+            }
+            base_l[x] = b;
+        }
     }
     __syncthreads();
     for (int x = threadIdx.x; x < W; x += blockDim.x) {
@@ -393,13 +405,15 @@ __device__ __forceinline__ void l2r_row(const double *__restrict__ row, int W,
     }
 }
 
+// With base_l, also k_base over the left disparity (the rows it reads).
 __global__ void __launch_bounds__(256)
     k_left_to_right(const double *__restrict__ dl, int W, double *__restrict__ dr,
-                    int32_t *__restrict__ base_r) {
+                    int32_t *__restrict__ base_r, int32_t *__restrict__ base_l, int *flag) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int sbuf[32];
     const long r = (long)blockIdx.x * W;
-    l2r_row(dl + r, W, dr + r, base_r ? base_r + r : nullptr, smem_raw, sbuf);
+    l2r_row(dl + r, W, dr + r, base_r ? base_r + r : nullptr, smem_raw, sbuf,
+            base_l ? base_l + r : nullptr, flag);
 }
 
 // ------------------------------------------------------------- LR check
@@ -553,13 +567,13 @@ int launch_sgm_add_path(const uint8_t *C, const int32_t *base, int W, int H, int
 }
 
 int launch_left_to_right(const double *dl, int W, int H, double *dr, int32_t *base_r,
-                         cudaStream_t st) {
+                         cudaStream_t st, int32_t *base_l, int *flag) {
     size_t smem = (size_t)W * (8 + 4 + 1) + 16;
     if (smem > 48 * 1024)
         SV_CUDA_TRY(cudaFuncSetAttribute(k_left_to_right,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem));
-    count_launch(); k_left_to_right<<<H, 256, smem, st>>>(dl, W, dr, base_r);
+    count_launch(); k_left_to_right<<<H, 256, smem, st>>>(dl, W, dr, base_r, base_l, flag);
     SV_LAUNCH_CHECK();
     return SV_OK;
 }

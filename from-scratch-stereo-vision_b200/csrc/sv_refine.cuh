@@ -149,8 +149,9 @@ int launch_sgm_packed(const uint8_t *C0, const uint8_t *C1, const int32_t *b0,
 int launch_wta_slot(const void *L, bool l16, int npaths, int nviews, int W, int H, int R,
                     const int32_t *b0, const int32_t *b1, const double *d00, const double *d01,
                     double uniq, double *out0, double *out1, double *conf0, cudaStream_t st);
+// base_l (optional): also k_base's band centres of dl, errors into flag.
 int launch_left_to_right(const double *dl, int W, int H, double *dr, int32_t *base_r,
-                         cudaStream_t st);
+                         cudaStream_t st, int32_t *base_l = nullptr, int *flag = nullptr);
 int launch_lr_check(const double *dl, const double *dr, const double *disp0, int W, int H,
                     double tol, double *out, uint8_t *status, cudaStream_t st);
 

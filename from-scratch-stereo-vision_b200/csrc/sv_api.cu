@@ -286,7 +286,6 @@ static int lr_refine_impl(const void *left, const void *right, int dtype, const 
     RefineWs w;
     carve_refine(workspace, W, H, c, 2, &w);
     cudaStream_t st = (cudaStream_t)stream;
-    const long N = (long)W * H;
     int ev = 0;
     auto mark = [&]() -> int {
         if (events) SV_CUDA_TRY(cudaEventRecord((cudaEvent_t)events[ev++], st));

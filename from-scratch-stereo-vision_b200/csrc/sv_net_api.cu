@@ -227,15 +227,20 @@ static size_t carve_predict(void *ws, const NetView &n, int Wm, int Hm, PredictW
 
 // predict (stereonet.py:5891-5897) on FP32 images already in lw/rw.
 // gh_ready: the resize already wrote the half-resolution guide
+// decide (optional): the width decision the network's output convolution
+// runs over the map it writes (its state cleared by the stage's resize).
 static int predict_f32(const sv_net *net, const PredictWs &w, int W, int H, int precision,
-                       cudaStream_t st, bool gh_ready = false) {
+                       cudaStream_t st, bool gh_ready = false,
+                       const SelFuse *decide = nullptr) {
     int rc = check_net_shape(net->view, H, W);
     if (rc) return rc;
     if (!gh_ready) {
         rc = launch_avgpool2(w.lw, H, W, w.gh, st);
         if (rc) return rc;
     }
-    return launch_forward(net->view, w.lw, w.rw, H, W, w.gh, w.lw, w.d0, w.d1, w.d2, w.fwd,
+    FwdBufs fb = w.fwd;
+    fb.decide = decide;
+    return launch_forward(net->view, w.lw, w.rw, H, W, w.gh, w.lw, w.d0, w.d1, w.d2, fb,
                           precision, st);
 }
 
@@ -744,14 +749,22 @@ int sv_predict_auto(const sv_net *net, const void *left, const void *right, int 
     double *slot = nullptr;
     SV_TRY(run_stage(mnet, key, st, true, &slot, [&](double *mirror) -> int {
         int rc = check_net_shape(net->view, ph, pw);
-        if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh);
-        if (!rc) rc = predict_f32(net, w, pw, ph, SV_FP32, st, true);
         const long np = (long)pw * ph;
         const long long rank = (long long)(np * 0.95);
-        if (!rc && by_rule) {
+        if (by_rule) {
+            // the probe's decision runs in the network's output convolution;
+            // the stage's resize clears its state
             const WidthFuse f{probe_rule, nth, kmax, rank};
-            rc = launch_width_map<float>(w.d2, np, f, w.sel, w.hist, st, mirror);
-        } else if (!rc && np <= 16384) {
+            const SelFuse sf{w.sel, w.hist, rank, &f, mirror};
+            if (!rc)
+                rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh,
+                                        &sf);
+            if (!rc) rc = predict_f32(net, w, pw, ph, SV_FP32, st, true, &sf);
+            return rc;
+        }
+        if (!rc) rc = launch_resize_pair(left, right, dtype, W, H, pw, ph, w.lw, w.rw, st, w.gh);
+        if (!rc) rc = predict_f32(net, w, pw, ph, SV_FP32, st, true);
+        if (!rc && np <= 16384) {
             rc = launch_select_small_f32(w.d2, np, rank, w.sel, st, mirror);
         } else if (!rc) {
             rc = launch_promote(w.d2, np, w.probe64, st);

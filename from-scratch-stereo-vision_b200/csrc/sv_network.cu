@@ -527,6 +527,32 @@ __device__ __forceinline__ void conv2d_wide_body(int bx, int by, const float *__
     }
 }
 
+// The network's output convolution (Refinement level 1: RC -> 1, residual
+// + ReLU, k_conv2d_tiled<RC, 1, 1, 2, 4>'s arithmetic) followed by a width
+// decision over the values it wrote: each CTA histograms the widths of its
+// tile's outputs and the last CTA turns the totals into the width
+// (predict_auto's probe: no separate decision launch).
+template <int RC>
+__global__ void __launch_bounds__(CT2_TW *CT2_TH * 4)
+    k_conv2d_out_decide(const float *__restrict__ x, int H, int W, const float *__restrict__ w,
+                        const float *__restrict__ b, float *y, const float *__restrict__ resid,
+                        WidthFuse f, SelState *s, unsigned *ghist, double *mirror) {
+    __shared__ unsigned hist[kWidthBins + 1];
+    const int t = threadIdx.x;
+    for (int i = t; i <= f.m; i += CT2_TW * CT2_TH * 4) hist[i] = 0u;
+    conv2d_tiled_body<RC, 1, 1, 2, 4>(blockIdx.x, blockIdx.y, 0, x, x, H, W, H, W, 1, 1, 1, w, b,
+                                      y, y, resid);
+    __syncthreads();                              // the tile's outputs are written
+    int bin = -1;
+    if (t < CT2_TW * CT2_TH) {
+        const int ox = blockIdx.x * CT2_TW + t % CT2_TW, oy = blockIdx.y * CT2_TH + t / CT2_TW;
+        if (ox < W && oy < H) bin = width_bin_of(f, (double)y[(long)oy * W + ox]);
+    }
+    width_count(hist, bin);
+    __syncthreads();
+    width_finish(f, s, ghist, hist, gridDim.x * gridDim.y, mirror);
+}
+
 // The batched form: level lv of conv_level, Z images (1 or 2) per pair.
 template <int IC, int OC, int ACT, int CS, int PX, int S>
 __global__ void __launch_bounds__(CTB_TW / PX * CTB_TH)
@@ -1446,10 +1472,17 @@ static int forward_impl(const NetView &n, const float *left, const float *right,
             cur = dst;
         }
         count_launch();
-        k_conv2d_tiled<RC, 1, 1, 2, 4><<<tgrid(Wl, Hl, 1), tb4, conv2d_tile_bytes(RC, 1, 1, 4),
-                                         st>>>(
-            cur, cur, Hl, Wl, Hl, Wl, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
-            outs[lv], b.rin);
+        if (lv == 1 && b.decide && b.decide->width)
+            k_conv2d_out_decide<RC><<<tgrid(Wl, Hl, 1), tb4, conv2d_tile_bytes(RC, 1, 1, 4),
+                                      st>>>(cur, Hl, Wl, n.rw[lv][n.ndil], n.rb[lv][n.ndil],
+                                            outs[lv], b.rin, *b.decide->width,
+                                            b.decide->state, b.decide->hist,
+                                            b.decide->mirror);
+        else
+            k_conv2d_tiled<RC, 1, 1, 2, 4><<<tgrid(Wl, Hl, 1), tb4,
+                                             conv2d_tile_bytes(RC, 1, 1, 4), st>>>(
+                cur, cur, Hl, Wl, Hl, Wl, 1, 1, 1, n.rw[lv][n.ndil], n.rb[lv][n.ndil], outs[lv],
+                outs[lv], b.rin);
         SV_LAUNCH_CHECK();
         prev = outs[lv];
         ph = Hl;

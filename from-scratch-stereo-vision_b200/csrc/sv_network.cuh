@@ -65,6 +65,9 @@ struct FwdBufs {
     // optional, [h][w]: the soft-argmin distribution's spread (std, quarter
     // px) and peak probability (both or neither)
     float *qspread, *qpmax;
+    // optional: the network's output convolution also runs this width
+    // decision over the values it writes (its state cleared beforehand)
+    const struct SelFuse *decide;
 };
 
 struct SelState;

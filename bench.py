@@ -494,8 +494,9 @@ def run_ours(args, rank, world, local):
                           **{s: round(v, 4) for s, v in zip(stages, stage_ms)}},
             # lr_refine alone (its stage events), both views + LR check per pair
             "refine_only_mpix_s": round(N / (sum(stage_ms) / 1e3) / 1e6, 3),
-            # achieved = the survey's algorithmic SGM bytes (48*K per pixel per
-            # view) / the SGM stage time; a pair's working set is L2-resident,
+            # achieved = the algorithmic SGM bytes (48*K per pixel per view:
+            # u16 costs read, path costs read and written per path) / the SGM
+            # stage time; a pair's working set is L2-resident,
             # so the DRAM bytes ncu measures are far fewer (dram_frac)
             "roofline": {"kernel": "%s (8 paths x 2 views)" % pkg.refine.sgm_kernel_name(),
                          "bound": "hbm",
